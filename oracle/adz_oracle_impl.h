@@ -1,0 +1,363 @@
+/*
+ * ORACLE — test infrastructure only.  Precision template of the driver
+ * restatement, included by adz_oracle.c with REAL = float (the reference's
+ * ``real`` storage) and REAL = double (this project's FP64 extension).
+ * Where Fortran adds two ``real`` values before promoting (e.g.
+ * adz_prepareWinds.F90:42-43, adz_interp_traj.F90:112), the sum is formed in
+ * REAL, as the reference does.
+ */
+
+#define EXT(i, j, k) ((long)((i) - s->lminx) + (long)((j) - s->lminy) * s->nit + (long)((k) - 1) * s->nij)
+#define ARR(i, j, k) ((long)((i) - 1) + (long)((j) - 1) * ni + (long)((k) - 1) * (long)ni * nj)
+#define WP(i, j, k, c)                                                                     \
+  ((long)((i) + 1) + (long)((j) + 1) * (ni + 4) + (long)((k) - 1) * (long)(ni + 4) * (nj + 4) + \
+   (long)((c) - 1) * (long)(ni + 4) * (nj + 4) * nk)
+
+static inline REAL SFX(rmin)(REAL a, REAL b) { return a < b ? a : b; }
+static inline REAL SFX(rmax)(REAL a, REAL b) { return a > b ? a : b; }
+
+/* adz_prepareWinds.F90:16-107 */
+void SFX(orc_prepare_winds)(const orc_set *s, const REAL *uu_ext, const REAL *vv_ext, const REAL *ww_ext,
+                            const REAL *ut0, const REAL *vt0, const REAL *zdt0, REAL *uvw_d, REAL *uu_arr,
+                            REAL *vv_arr, REAL *ww_arr) {
+  const int ni = s->g.ni, nj = s->g.nj, nk = s->g.nk;
+  const double alpha1 = -1.0 / 16.0, alpha2 = 9.0 / 16.0, inv_rayt = s->g.inv_rayt;
+  double *wx = (double *)calloc(nk + 1, sizeof(double));
+  int *km2 = (int *)calloc(nk + 1, sizeof(int));
+  for (int k = 3; k <= nk; k++) wx[k] = s->vw1m[k];
+  for (int k = 2; k <= nk - 1; k++) km2[k] = imax(1, k - 2);
+#pragma omp parallel for num_threads(nthr()) schedule(static)
+  for (int k = 1; k <= nk; k++) {
+    for (int j = s->lminy; j <= s->lmaxy; j++) {
+      double cyj = s->cy[j - s->lminy];
+      for (int i = s->lminx; i <= s->lmaxx; i++) {
+        long e = EXT(i, j, k);
+        uvw_d[3 * e + 0] = (REAL)(inv_rayt * uu_ext[e] * cyj);
+        uvw_d[3 * e + 1] = (REAL)(inv_rayt * vv_ext[e]);
+        double w;
+        if (k == 1) w = s->vw5 * ww_ext[EXT(i, j, 1)];
+        else if (k == nk) w = s->vw6 * ww_ext[EXT(i, j, nk - 1)];
+        else
+          w = wx[k] * ww_ext[EXT(i, j, km2[k])] + s->vw2m[k] * ww_ext[EXT(i, j, k - 1)] +
+              s->vw3m[k] * ww_ext[EXT(i, j, k)] + s->vw4m[k] * ww_ext[EXT(i, j, k + 1)];
+        uvw_d[3 * e + 2] = (REAL)w;
+      }
+    }
+    for (int j = 1; j <= nj; j++) {
+      double cyj = s->cy[j - s->lminy];
+      for (int i = 1; i <= ni; i++) {
+        long a = ARR(i, j, k);
+        REAL u1 = ut0[EXT(i - 2, j, k)] + ut0[EXT(i + 1, j, k)];
+        REAL u2 = ut0[EXT(i, j, k)] + ut0[EXT(i - 1, j, k)];
+        uu_arr[a] = (REAL)((u1 * alpha1 + u2 * alpha2) * inv_rayt * cyj);
+        REAL v1 = vt0[EXT(i, j - 2, k)] + vt0[EXT(i, j + 1, k)];
+        REAL v2 = vt0[EXT(i, j, k)] + vt0[EXT(i, j - 1, k)];
+        vv_arr[a] = (REAL)((v1 * alpha1 + v2 * alpha2) * inv_rayt);
+        double w;
+        if (k == 1) w = s->vw5 * zdt0[EXT(i, j, 1)];
+        else if (k == nk) w = s->vw6 * zdt0[EXT(i, j, nk - 1)];
+        else
+          w = wx[k] * zdt0[EXT(i, j, km2[k])] + s->vw2m[k] * zdt0[EXT(i, j, k - 1)] +
+              s->vw3m[k] * zdt0[EXT(i, j, k)] + s->vw4m[k] * zdt0[EXT(i, j, k + 1)];
+        ww_arr[a] = (REAL)w;
+      }
+    }
+  }
+  free(wx);
+  free(km2);
+}
+
+/* adz_inittraj.F90:25-37 (the caller also sets niter = max(6, itraj)) */
+void SFX(orc_inittraj)(const orc_set *s, REAL *pxyzm, double *wpxyz) {
+  const int ni = s->g.ni, nj = s->g.nj, nk = s->g.nk;
+  for (int k = s->k0m; k <= nk; k++)
+    for (int j = 1; j <= nj; j++)
+      for (int i = 1; i <= ni; i++) {
+        long a = ARR(i, j, k);
+        pxyzm[3 * a + 0] = (REAL)(i + s->g.i0g - 1);
+        wpxyz[WP(i, j, k, 1)] = pxyzm[3 * a + 0];
+        pxyzm[3 * a + 1] = (REAL)(j + s->g.j0g - 1);
+        wpxyz[WP(i, j, k, 2)] = pxyzm[3 * a + 1];
+        pxyzm[3 * a + 2] = (REAL)k;
+        wpxyz[WP(i, j, k, 3)] = pxyzm[3 * a + 2];
+      }
+}
+
+static void SFX(dt_split)(const orc_set *s, double dt, double *dtA, double *dtzA, double *dtD, double *dtzD) {
+  /* adz_traject.F90:38-59 */
+  double a = 0.0, za = 0.0;
+  int adv = s->g.schm_advec;
+  if (adv == 1) { a = dt * 0.5; za = dt * 0.5; }
+  if (adv == 2) { a = dt * s->g.bA_m; za = dt * s->g.bA; }
+  if (adv == 3) { a = (1.0 - s->g.bA_m) * dt; za = (1.0 - s->g.bA) * dt; }
+  *dtD = dt - a; *dtzD = dt - za; *dtA = a; *dtzA = za;
+  if (adv == 0) { *dtA = 0.0; *dtD = 0.0; *dtzA = 0.0; *dtzD = 0.0; }
+}
+
+/* adz_traject.F90:63-108 (iterations) */
+void SFX(orc_traject)(const orc_set *s, double dt, int niter, const REAL *uvw_d, const REAL *uu_arr,
+                      const REAL *vv_arr, const REAL *ww_arr, REAL *uvw_dep, REAL *pxyzm, double *wpxyz) {
+  const int ni = s->g.ni, nj = s->g.nj, nk = s->g.nk;
+  double dtA, dtzA, dtD, dtzD;
+  SFX(dt_split)(s, dt, &dtA, &dtzA, &dtD, &dtzD);
+  int k00 = s->k0m;
+  if (s->k0 > 1) k00 = 1;
+  const double *zm = s->g.zm;
+  const double sig = s->sig;
+  const REAL *f3 = uvw_d + 3 * EXT(1, 1, 1);
+  for (int iter = 1; iter <= niter; iter++) {
+#pragma omp parallel for num_threads(nthr()) schedule(static)
+    for (int k = k00; k <= nk; k++) {
+      long a0 = ARR(1, 1, k);
+#if IS_F32
+#ifdef ORC_USE_REF
+      Tricublin_zyx3_n(uvw_dep + 3 * a0, (float *)f3, (pxpypz *)(pxyzm + 3 * a0), ref_ztab_m_of(s), ni * nj);
+#else
+      orc_zyx3_n_f32(uvw_dep + 3 * a0, f3, pxyzm + 3 * a0, s->ztab_m, ni * nj);
+#endif
+#else
+      orc_zyx3_n_f64(uvw_dep + 3 * a0, f3, pxyzm + 3 * a0, s->ztab_m, ni * nj);
+#endif
+      for (int j = 1; j <= nj; j++)
+        for (int i = 1; i <= ni; i++) {
+          long a = ARR(i, j, k);
+          double xm = (double)(i + s->g.i0g - 1) - (dtD * uvw_dep[3 * a] + dtA * uu_arr[a]) * s->g.inv_hx;
+          double ym = (double)(j + s->g.j0g - 1) - (dtD * uvw_dep[3 * a + 1] + dtA * vv_arr[a]) * s->g.inv_hy;
+          double pos = zm[k] - dtzD * uvw_dep[3 * a + 2] - dtzA * ww_arr[a];
+          double zmv = dmin(dmax(pos, s->g.zmin), s->g.zmax);
+          int kk1 = (int)((zmv - zm[0]) * s->ovdzm + 1.0);
+          kk1 = imin(imax(1, kk1), s->pnz_m);
+          kk1 = s->search_m[kk1 - 1];
+          if (sig * zmv > sig * zm[imin(kk1 + 1, nk + 1)]) kk1 = kk1 + 1;
+          if (sig * zmv < sig * zm[kk1]) kk1 = kk1 - 1;
+          wpxyz[WP(i, j, k, 1)] = xm;
+          pxyzm[3 * a + 0] = (REAL)dmin(dmax(xm, s->iminposx), s->imaxposx);
+          wpxyz[WP(i, j, k, 2)] = ym;
+          pxyzm[3 * a + 1] = (REAL)dmin(dmax(ym, s->iminposy), s->imaxposy);
+          kk1 = imin(nk + 1, imax(0, kk1));
+          int nb = imax(imin(kk1, nk - 1), 1);
+          double w3 = (zmv - zm[nb]) * s->odelz_m[nb] + (double)nb;
+          wpxyz[WP(i, j, k, 3)] = w3;
+          pxyzm[3 * a + 2] = (REAL)w3;
+        }
+    }
+  }
+}
+
+/* zindx, adz_interp_traj.F90:189-204 */
+static inline double SFX(zindx)(const orc_set *s, double posz) {
+  const int nk = s->g.nk;
+  const double *zt = s->g.zt;
+  posz = dmin(dmax(posz, s->g.zmin), s->g.zmax);
+  int kk1 = (int)((posz - zt[0]) * s->ovdzt + 1.0);
+  kk1 = imin(imax(1, kk1), s->pnz_t);
+  kk1 = s->search_t[kk1 - 1];
+  if (s->sig * posz > s->sig * zt[imin(kk1 + 1, nk + 1)]) kk1 = kk1 + 1;
+  if (s->sig * posz < s->sig * zt[kk1]) kk1 = kk1 - 1;
+  kk1 = imin(nk + 1, imax(0, kk1));
+  int nb = imax(imin(kk1, nk - 1), 1);
+  return (posz - zt[nb]) * s->odelz_t[nb] + (double)nb;
+}
+
+/* adz_traject.F90:113-116 (Adz_pm) and adz_interp_traj.F90:16-187 */
+void SFX(orc_interp_traj)(const orc_set *s, double dt, const double *wpxyz, const REAL *uvw_dep, const REAL *zdt0,
+                          const REAL *pxyzm, const REAL *uslt, const REAL *vslt, REAL *pm, REAL *pmu, REAL *pmv,
+                          REAL *pt) {
+  const int ni = s->g.ni, nj = s->g.nj, nk = s->g.nk;
+  double dtA, dtzA, dtD, dtzD;
+  SFX(dt_split)(s, dt, &dtA, &dtzA, &dtD, &dtzD);
+  const double half = 0.5, aa = -0.0625, bb = 0.5625;
+  const double zmin_b = 0.0, zmax_b = (double)(nk + 1);
+  const double *zt = s->g.zt;
+  int k00 = imax(s->k0t - 1, 1);
+  if (s->g.bc_lam_flux != 0 && s->k0 > 1) k00 = 1;
+  const double imnx = s->iminposx, imxx = s->imaxposx, imny = s->iminposy, imxy = s->imaxposy;
+#define W(i, j, k, c) wpxyz[WP(i, j, k, c)]
+#define UD3(i, j, k) uvw_dep[3 * ARR(i, j, k) + 2]
+#define ZD(i, j, k) zdt0[EXT(i, j, k)]
+  if (pm) {
+    long nx = s->in - s->i0 + 1, ny = s->jn - s->j0 + 1;
+    for (int k = s->k0; k <= nk; k++)
+      for (int j = s->j0; j <= s->jn; j++)
+        for (int i = s->i0; i <= s->in; i++) {
+          long o = (i - s->i0) + (j - s->j0) * nx + (long)(k - s->k0) * nx * ny;
+          for (int c = 0; c < 3; c++) pm[3 * o + c] = pxyzm[3 * ARR(i, j, k) + c];
+        }
+  }
+  if (pmu) {
+    long nx = s->inu - s->i0u + 1, ny = s->jn - s->j0 + 1;
+#pragma omp parallel for num_threads(nthr()) schedule(static)
+    for (int k = s->k0; k <= nk; k++)
+      for (int j = s->j0; j <= s->jn; j++)
+        for (int i = s->i0u; i <= s->inu; i++) {
+          double xt = aa * (W(i - 1, j, k, 1) + W(i + 2, j, k, 1)) + bb * (W(i, j, k, 1) + W(i + 1, j, k, 1)) - 0.5;
+          double yt = aa * (W(i - 1, j, k, 2) + W(i + 2, j, k, 2)) + bb * (W(i, j, k, 2) + W(i + 1, j, k, 2));
+          double ztv = aa * (W(i - 1, j, k, 3) + W(i + 2, j, k, 3)) + bb * (W(i, j, k, 3) + W(i + 1, j, k, 3));
+          long o = (i - s->i0u) + (j - s->j0) * nx + (long)(k - s->k0) * nx * ny;
+          pmu[3 * o + 0] = (REAL)dmin(dmax(xt, imnx), imxx);
+          pmu[3 * o + 1] = (REAL)dmin(dmax(yt, imny), imxy);
+          pmu[3 * o + 2] = (REAL)dmin(dmax(ztv, zmin_b), zmax_b);
+        }
+  }
+  if (pmv) {
+    long nx = s->in - s->i0 + 1, ny = s->jnv - s->j0v + 1;
+#pragma omp parallel for num_threads(nthr()) schedule(static)
+    for (int k = s->k0; k <= nk; k++)
+      for (int j = s->j0v; j <= s->jnv; j++)
+        for (int i = s->i0; i <= s->in; i++) {
+          double xt = aa * (W(i, j - 1, k, 1) + W(i, j + 2, k, 1)) + bb * (W(i, j, k, 1) + W(i, j + 1, k, 1));
+          double yt = aa * (W(i, j - 1, k, 2) + W(i, j + 2, k, 2)) + bb * (W(i, j, k, 2) + W(i, j + 1, k, 2)) - 0.5;
+          double ztv = aa * (W(i, j - 1, k, 3) + W(i, j + 2, k, 3)) + bb * (W(i, j, k, 3) + W(i, j + 1, k, 3));
+          long o = (i - s->i0) + (j - s->j0v) * nx + (long)(k - s->k0) * nx * ny;
+          pmv[3 * o + 0] = (REAL)dmin(dmax(xt, imnx), imxx);
+          pmv[3 * o + 1] = (REAL)dmin(dmax(yt, imny), imxy);
+          pmv[3 * o + 2] = (REAL)dmin(dmax(ztv, zmin_b), zmax_b);
+        }
+  }
+  if (pt) {
+    /* pb over (i0b:inb, j0b:jnb, 1:nk) then pt = pb on the t range */
+    long bx = s->inb - s->i0b + 1, by = s->jnb - s->j0b + 1;
+    REAL *pb = (REAL *)malloc(sizeof(REAL) * 3 * bx * by * nk);
+#define PB(i, j, k) (pb + 3 * ((i - s->i0b) + (j - s->j0b) * bx + (long)((k) - 1) * bx * by))
+#pragma omp parallel for num_threads(nthr()) schedule(static)
+    for (int k = imax(k00, 2); k <= nk - 2; k++)
+      for (int j = s->j0b; j <= s->jnb; j++)
+        for (int i = s->i0b; i <= s->inb; i++) {
+          double xt = s->vw1t[k] * W(i, j, k - 1, 1) + s->vw2t[k] * W(i, j, k, 1) + s->vw3t[k] * W(i, j, k + 1, 1) +
+                      s->vw4t[k] * W(i, j, k + 2, 1);
+          double yt = s->vw1t[k] * W(i, j, k - 1, 2) + s->vw2t[k] * W(i, j, k, 2) + s->vw3t[k] * W(i, j, k + 1, 2) +
+                      s->vw4t[k] * W(i, j, k + 2, 2);
+          double wdt = s->vw1t[k] * UD3(i, j, k - 1) + s->vw2t[k] * UD3(i, j, k) + s->vw3t[k] * UD3(i, j, k + 1) +
+                       s->vw4t[k] * UD3(i, j, k + 2);
+          double ztv = zt[k] - dtzD * wdt - dtzA * ZD(i, j, k);
+          REAL *p = PB(i, j, k);
+          p[0] = (REAL)dmin(dmax(xt, imnx), imxx);
+          p[1] = (REAL)dmin(dmax(yt, imny), imxy);
+          p[2] = (REAL)SFX(zindx)(s, ztv);
+        }
+    {
+      int k = nk - 1;
+      for (int j = s->j0b; j <= s->jnb; j++)
+        for (int i = s->i0b; i <= s->inb; i++) {
+          double xt = (W(i, j, k, 1) + W(i, j, k + 1, 1)) * half;
+          double yt = (W(i, j, k, 2) + W(i, j, k + 1, 2)) * half;
+          REAL ws = UD3(i, j, k) + UD3(i, j, k + 1);
+          double wdt = ws * half;
+          double ztv = zt[k] - dtzD * wdt - dtzA * ZD(i, j, k);
+          REAL *p = PB(i, j, k);
+          p[0] = (REAL)dmin(dmax(xt, imnx), imxx);
+          p[1] = (REAL)dmin(dmax(yt, imny), imxy);
+          p[2] = (REAL)SFX(zindx)(s, ztv);
+        }
+    }
+    {
+      int k = nk;
+      for (int j = s->j0b; j <= s->jnb; j++)
+        for (int i = s->i0b; i <= s->inb; i++) {
+          double xt, yt;
+          if (s->g.slt_winds && uslt && vslt) {
+            long a2 = (i - 1) + (long)(j - 1) * ni;
+            xt = (double)(i + s->g.i0g - 1) -
+                 s->g.inv_rayt * dt * uslt[a2] * s->cy[j - s->lminy] * s->g.inv_hx;
+            yt = (double)(j + s->g.j0g - 1) - s->g.inv_rayt * dt * vslt[a2] * s->g.inv_hy;
+          } else {
+            xt = s->wp * W(i, j, k, 1) + s->wm * W(i, j, k - 1, 1);
+            yt = s->wp * W(i, j, k, 2) + s->wm * W(i, j, k - 1, 2);
+          }
+          REAL ws = UD3(i, j, k - 1) + UD3(i, j, k);
+          double wdt = ws * half;
+          double ztv = zt[k] - s->ww * (dtzD * wdt + dtzA * ZD(i, j, k - 1));
+          REAL *p = PB(i, j, k);
+          p[0] = (REAL)dmin(dmax(xt, imnx), imxx);
+          p[1] = (REAL)dmin(dmax(yt, imny), imxy);
+          p[2] = (REAL)SFX(zindx)(s, ztv);
+        }
+    }
+    if (k00 == 1) {
+      for (int j = s->j0b; j <= s->jnb; j++)
+        for (int i = s->i0b; i <= s->inb; i++) {
+          double xt = (W(i, j, 1, 1) + W(i, j, 2, 1)) * half;
+          double yt = (W(i, j, 1, 2) + W(i, j, 2, 2)) * half;
+          REAL ws = UD3(i, j, 1) + UD3(i, j, 2);
+          double wdt = ws * half;
+          double ztv = zt[1] - dtzD * wdt - dtzA * ZD(i, j, 1);
+          REAL *p = PB(i, j, 1);
+          p[0] = (REAL)dmin(dmax(xt, imnx), imxx);
+          p[1] = (REAL)dmin(dmax(yt, imny), imxy);
+          p[2] = (REAL)SFX(zindx)(s, ztv);
+        }
+    }
+    long nx = s->in - s->i0 + 1, ny = s->jn - s->j0 + 1;
+    for (int k = s->k0t; k <= nk; k++)
+      for (int j = s->j0; j <= s->jn; j++)
+        for (int i = s->i0; i <= s->in; i++) {
+          long o = (i - s->i0) + (j - s->j0) * nx + (long)(k - s->k0t) * nx * ny;
+          REAL *p = PB(i, j, k);
+          pt[3 * o + 0] = p[0]; pt[3 * o + 1] = p[1]; pt[3 * o + 2] = p[2];
+        }
+    free(pb);
+#undef PB
+  }
+#undef W
+#undef UD3
+#undef ZD
+}
+
+/* adz_tricub_hlt (adz_interp_hlt.F90:98-182) plus the clip of
+ * adz_post_tr.F90:81-94: one kernel call per k-plane of the set's range. */
+void SFX(orc_tricub)(const orc_set *s, int set, const REAL *pos, int m, const REAL *const *srcs, REAL *const *dsts,
+                     int mono, int clip, REAL *const *lin, REAL *const *mn, REAL *const *mx) {
+  int r[5];
+  set_range(s, set, r);
+  const int nk = s->g.nk;
+  const long nx = r[1] - r[0] + 1, ny = r[3] - r[2] + 1, np = nx * ny;
+  if (np <= 0 || m <= 0) return;
+  const long o111 = EXT(1, 1, 1);
+#pragma omp parallel num_threads(nthr())
+  {
+    REAL **fs = (REAL **)malloc(sizeof(REAL *) * m);
+    REAL *wrk = (REAL *)malloc(sizeof(REAL) * 4 * m * np);
+    REAL *wl = wrk + m * np, *wmi = wrk + 2 * m * np, *wma = wrk + 3 * m * np;
+    for (int q = 0; q < m; q++) fs[q] = (REAL *)srcs[q] + o111;
+#pragma omp for schedule(static)
+    for (int k = r[4]; k <= nk; k++) {
+      const REAL *p = pos + 3 * (long)(k - r[4]) * np;
+#if IS_F32
+#ifdef ORC_USE_REF
+      void *zt = (set == 3) ? ref_ztab_t_of(s) : ref_ztab_m_of(s);
+      if (mono) Tricublin_mono_zyx_m_n(wrk, wl, wmi, wma, fs, (pxpypz *)p, zt, (int)np, m);
+      else Tricublin_zyx1_m_n(wrk, fs, (pxpypz *)p, zt, (int)np, m);
+#else
+      const orc_ztab *zt = (set == 3) ? s->ztab_t : s->ztab_m;
+      if (mono) orc_mono_m_n_f32(wrk, wl, wmi, wma, (const float *const *)fs, p, zt, (int)np, m, 0);
+      else orc_zyx1_m_n_f32(wrk, (const float *const *)fs, p, zt, (int)np, m);
+#endif
+#else
+      const orc_ztab *zt = (set == 3) ? s->ztab_t : s->ztab_m;
+      if (mono) orc_mono_m_n_f64(wrk, wl, wmi, wma, (const double *const *)fs, p, zt, (int)np, m);
+      else orc_zyx1_m_n_f64(wrk, (const double *const *)fs, p, zt, (int)np, m);
+#endif
+      for (int q = 0; q < m; q++)
+        for (int j = r[2]; j <= r[3]; j++)
+          for (int i = r[0]; i <= r[1]; i++) {
+            long w = q * np + (i - r[0]) + (j - r[2]) * nx;
+            long e = EXT(i, j, k);
+            REAL d = wrk[w];
+            if (mono) {
+              REAL lo = wmi[w], hi = wma[w];
+              if (lin && lin[q]) lin[q][e] = SFX(rmax)(lo, SFX(rmin)(hi, wl[w]));
+              if (mn && mn[q]) mn[q][e] = lo;
+              if (mx && mx[q]) mx[q][e] = hi;
+              if (clip) d = SFX(rmax)(lo, SFX(rmin)(hi, d));
+            }
+            dsts[q][e] = d;
+          }
+    }
+    free(fs);
+    free(wrk);
+  }
+}
+
+#undef EXT
+#undef ARR
+#undef WP

@@ -1,0 +1,368 @@
+"""ORACLE — test infrastructure only.
+
+ctypes front end of the CPU restatement (``liboracle.so``) and of the
+reference interpolator compiled unchanged (``_ref/libtricublin_ref.so``,
+``_ref/libadz_ref.so``).  Only the tests, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` import this module; the product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+class OrcZtab(C.Structure):
+    _fields_ = [("z", C.POINTER(C.c_double)), ("ocz", C.POINTER(C.c_double)),
+                ("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int), ("nij", C.c_int),
+                ("offi", C.c_int), ("offj", C.c_int)]
+
+
+class OrcGrid(C.Structure):
+    """Inputs of adz_set (src/gemdyn/src/base/adz_set.F90:16-538)."""
+    _fields_ = [("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int), ("maxcfl", C.c_int),
+                ("i0g", C.c_int), ("j0g", C.c_int),
+                ("west", C.c_int), ("east", C.c_int), ("south", C.c_int), ("north", C.c_int),
+                ("pil_w", C.c_int), ("pil_e", C.c_int), ("pil_s", C.c_int), ("pil_n", C.c_int),
+                ("lam_gbpil_t", C.c_int), ("bc_lam_flux", C.c_int), ("schm_advec", C.c_int),
+                ("itraj", C.c_int), ("slt_winds", C.c_int),
+                ("bA_m", C.c_double), ("bA", C.c_double), ("inv_rayt", C.c_double),
+                ("inv_hx", C.c_double), ("inv_hy", C.c_double),
+                ("cy", C.POINTER(C.c_double)), ("zm", C.POINTER(C.c_double)),
+                ("zt", C.POINTER(C.c_double)), ("zx", C.POINTER(C.c_double)),
+                ("zmin", C.c_double), ("zmax", C.c_double),
+                ("wmstar_nk", C.c_double), ("idz_t_nkm1", C.c_double)]
+
+
+class OrcSet(C.Structure):
+    _fields_ = [("g", OrcGrid)] + [(n, C.c_int) for n in (
+        "halox", "haloy", "lminx", "lmaxx", "lminy", "lmaxy", "nit", "njt", "nij",
+        "i0", "in_", "j0", "jn", "i0u", "inu", "j0v", "jnv", "i0b", "inb", "j0b", "jnb",
+        "k0", "k0t", "k0m", "niu", "njv")] + [
+        ("iminposx", C.c_double), ("imaxposx", C.c_double), ("iminposy", C.c_double),
+        ("imaxposy", C.c_double), ("sig", C.c_double), ("ovdzm", C.c_double), ("ovdzt", C.c_double),
+        ("pnz_m", C.c_int), ("pnz_t", C.c_int),
+        ("search_m", C.POINTER(C.c_int)), ("search_t", C.POINTER(C.c_int))] + [
+        (n, C.POINTER(C.c_double)) for n in (
+            "delz_m", "delz_t", "odelz_m", "odelz_t",
+            "vw1m", "vw2m", "vw3m", "vw4m", "vw1t", "vw2t", "vw3t", "vw4t")] + [
+        ("vw5", C.c_double), ("vw6", C.c_double), ("ww", C.c_double), ("wp", C.c_double),
+        ("wm", C.c_double), ("cy", C.POINTER(C.c_double)),
+        ("ztab_m", C.POINTER(OrcZtab)), ("ztab_t", C.POINTER(OrcZtab))]
+
+
+def build(ref: bool | None = None) -> None:
+    """Compile the restatement (and the reference objects when the reference
+    tree is present)."""
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+    refsrc = "/root/reference/src/gemdyn/src/base/turbo_tricublin.c"
+    if ref or (ref is None and os.path.exists(refsrc)):
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+def _ptrs(arrs, ctype):
+    arr = (C.POINTER(ctype) * len(arrs))()
+    for i, a in enumerate(arrs):
+        arr[i] = a.ctypes.data_as(C.POINTER(ctype))
+    return arr
+
+
+class _Lib:
+    def __init__(self, path: str):
+        self.path = path
+        self.lib = C.CDLL(path)
+        L = self.lib
+        L.orc_vsearch_setup_plus.restype = C.POINTER(OrcZtab)
+        L.orc_vsearch_setup_plus.argtypes = [_f64p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.orc_ztab_free.argtypes = [C.POINTER(OrcZtab)]
+        vp = C.c_void_p
+        for name in ("orc_zyx1_m_n_f32", "orc_zyx1_m_n_f64"):
+            getattr(L, name).argtypes = [vp, vp, vp, C.POINTER(OrcZtab), C.c_int, C.c_int]
+        L.orc_mono_m_n_f32.argtypes = [vp, vp, vp, vp, vp, vp, C.POINTER(OrcZtab), C.c_int, C.c_int, C.c_int]
+        L.orc_mono_m_n_f64.argtypes = [vp, vp, vp, vp, vp, vp, C.POINTER(OrcZtab), C.c_int, C.c_int]
+        for name in ("orc_zyx3_n_f32", "orc_zyx3_n_f64"):
+            getattr(L, name).argtypes = [vp, vp, vp, C.POINTER(OrcZtab), C.c_int]
+        for name in ("orc_cells_f32", "orc_cells_f64"):
+            getattr(L, name).argtypes = [vp, vp, vp, C.POINTER(OrcZtab), C.c_int]
+        L.orc_adz_set.argtypes = [C.POINTER(OrcGrid), C.POINTER(OrcSet)]
+        L.orc_adz_free.argtypes = [C.POINTER(OrcSet)]
+        L.orc_set_npoints.restype = C.c_long
+        L.orc_set_npoints.argtypes = [C.POINTER(OrcSet), C.c_int]
+        L.orc_set_threads.argtypes = [C.c_int]
+        for sfx in ("f32", "f64"):
+            getattr(L, f"orc_prepare_winds_{sfx}").argtypes = [C.POINTER(OrcSet)] + [vp] * 10
+            getattr(L, f"orc_inittraj_{sfx}").argtypes = [C.POINTER(OrcSet), vp, vp]
+            getattr(L, f"orc_traject_{sfx}").argtypes = [C.POINTER(OrcSet), C.c_double, C.c_int] + [vp] * 7
+            getattr(L, f"orc_interp_traj_{sfx}").argtypes = [C.POINTER(OrcSet), C.c_double] + [vp] * 10
+            getattr(L, f"orc_tricub_{sfx}").argtypes = [C.POINTER(OrcSet), C.c_int, vp, C.c_int, vp, vp,
+                                                        C.c_int, C.c_int, vp, vp, vp]
+
+
+_LIBS: dict[str, _Lib] = {}
+
+
+def lib(kind: str = "oracle") -> _Lib:
+    """kind: 'oracle' (restatement) or 'ref' (driver restatement linked with
+    the reference's own interpolator)."""
+    if kind not in _LIBS:
+        path = os.path.join(HERE, "liboracle.so") if kind == "oracle" else os.path.join(REF_DIR, "libadz_ref.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (run oracle.build())")
+        _LIBS[kind] = _Lib(path)
+    return _LIBS[kind]
+
+
+def have_ref() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libadz_ref.so")) and \
+        os.path.exists(os.path.join(REF_DIR, "libtricublin_ref.so"))
+
+
+# --------------------------------------------------------------------------
+# interpolator-level API (reference call shapes, numpy in/out)
+# --------------------------------------------------------------------------
+class Ztab:
+    """Level descriptor of the restatement (Vsearch_setup_plus)."""
+
+    def __init__(self, levels, ni, nj, offi=0, offj=0, kind="oracle"):
+        self.L = lib(kind)
+        self.levels = np.ascontiguousarray(levels, dtype=np.float64)
+        self.ptr = self.L.lib.orc_vsearch_setup_plus(self.levels, len(self.levels), ni, nj, offi, offj)
+        self.ni, self.nj, self.nk = ni, nj, len(self.levels)
+
+    def __del__(self):
+        try:
+            self.L.lib.orc_ztab_free(self.ptr)
+        except Exception:
+            pass
+
+
+def zyx1_m_n(fields, pos, zt: Ztab):
+    """Tricublin_zyx1_m_n; fields: list of flat arrays addressed at f(1,1,1)
+    through ``base`` offsets handled by the caller (pass views)."""
+    f64 = fields[0].dtype == np.float64
+    n, m = pos.shape[0], len(fields)
+    d = np.empty((m, n), dtype=fields[0].dtype)
+    ct = C.c_double if f64 else C.c_float
+    fs = _ptrs(fields, ct)
+    fn = zt.L.lib.orc_zyx1_m_n_f64 if f64 else zt.L.lib.orc_zyx1_m_n_f32
+    fn(d.ctypes.data, C.cast(fs, C.c_void_p), np.ascontiguousarray(pos).ctypes.data, zt.ptr, n, m)
+    return d
+
+
+def mono_m_n(fields, pos, zt: Ztab, box=0):
+    f64 = fields[0].dtype == np.float64
+    n, m = pos.shape[0], len(fields)
+    out = [np.empty((m, n), dtype=fields[0].dtype) for _ in range(4)]
+    ct = C.c_double if f64 else C.c_float
+    fs = _ptrs(fields, ct)
+    p = np.ascontiguousarray(pos)
+    if f64:
+        zt.L.lib.orc_mono_m_n_f64(*(o.ctypes.data for o in out), C.cast(fs, C.c_void_p), p.ctypes.data, zt.ptr, n, m)
+    else:
+        zt.L.lib.orc_mono_m_n_f32(*(o.ctypes.data for o in out), C.cast(fs, C.c_void_p), p.ctypes.data, zt.ptr, n, m,
+                                  box)
+    return out  # d, lin, min, max
+
+
+def zyx3_n(f3, pos, zt: Ztab):
+    f64 = f3.dtype == np.float64
+    n = pos.shape[0]
+    d = np.empty((n, 3), dtype=f3.dtype)
+    fn = zt.L.lib.orc_zyx3_n_f64 if f64 else zt.L.lib.orc_zyx3_n_f32
+    fn(d.ctypes.data, f3.ctypes.data, np.ascontiguousarray(pos).ctypes.data, zt.ptr, n)
+    return d
+
+
+def cells(pos, zt: Ztab):
+    """(corner offset, zlinear) chosen for each position."""
+    n = pos.shape[0]
+    off = np.empty(n, np.int32)
+    zl = np.empty(n, np.int32)
+    fn = zt.L.lib.orc_cells_f64 if pos.dtype == np.float64 else zt.L.lib.orc_cells_f32
+    fn(off.ctypes.data, zl.ctypes.data, np.ascontiguousarray(pos).ctypes.data, zt.ptr, n)
+    return off, zl
+
+
+# --------------------------------------------------------------------------
+# the reference interpolator compiled unchanged (reference symbol names)
+# --------------------------------------------------------------------------
+class RefKernels:
+    """Direct ctypes access to the reference's Tricublin_* (FP32 only)."""
+
+    def __init__(self, scalar: bool = False):
+        name = "libtricublin_ref_scalar.so" if scalar else "libtricublin_ref.so"
+        self.lib = C.CDLL(os.path.join(REF_DIR, name))
+        L = self.lib
+        L.Vsearch_setup_plus.restype = C.c_void_p
+        L.Vsearch_setup_plus.argtypes = [_f64p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        vp = C.c_void_p
+        L.Tricublin_zyx1_n.argtypes = [vp, vp, vp, vp, C.c_int]
+        L.Tricublin_zyx1_n_m.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int]
+        L.Tricublin_zyx1_m_n.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int]
+        L.Tricublin_zyx1_p.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int]
+        L.Tricublin_mono_zyx_n.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int]
+        L.Tricublin_mono_zyx_n_m.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int, C.c_int]
+        L.Tricublin_mono_zyx_m_n.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int, C.c_int]
+        L.Tricublin_zyx3_n.argtypes = [vp, vp, vp, vp, C.c_int]
+        self._keep = []
+
+    def setup(self, levels, ni, nj, offi=0, offj=0):
+        lv = np.ascontiguousarray(levels, dtype=np.float64)
+        self._keep.append(lv)
+        return self.lib.Vsearch_setup_plus(lv, len(lv), ni, nj, offi, offj)
+
+    def zyx1_m_n(self, fields, pos, zt):
+        n, m = pos.shape[0], len(fields)
+        d = np.empty((m, n), np.float32)
+        fs = _ptrs(fields, C.c_float)
+        self.lib.Tricublin_zyx1_m_n(d.ctypes.data, C.cast(fs, C.c_void_p), np.ascontiguousarray(pos).ctypes.data,
+                                    zt, n, m)
+        return d
+
+    def mono_m_n(self, fields, pos, zt):
+        n, m = pos.shape[0], len(fields)
+        out = [np.empty((m, n), np.float32) for _ in range(4)]
+        fs = _ptrs(fields, C.c_float)
+        self.lib.Tricublin_mono_zyx_m_n(*(o.ctypes.data for o in out), C.cast(fs, C.c_void_p),
+                                        np.ascontiguousarray(pos).ctypes.data, zt, n, m)
+        return out
+
+    def zyx3_n(self, f3, pos, zt):
+        n = pos.shape[0]
+        d = np.empty((n, 3), np.float32)
+        self.lib.Tricublin_zyx3_n(d.ctypes.data, f3.ctypes.data, np.ascontiguousarray(pos).ctypes.data, zt, n)
+        return d
+
+
+# --------------------------------------------------------------------------
+# driver restatement: one advection step (adz_main + adz_tracers subset)
+# --------------------------------------------------------------------------
+def make_grid(cfg, i0g=1, j0g=1, lam=True, slt_winds=False, schm_advec=1):
+    """orc_grid for a synth.Config tile (LAM tile touching all four edges)."""
+    from gem_b200 import synth
+    ga = synth.grid_arrays(cfg)
+    keep = {k: np.ascontiguousarray(ga[k], dtype=np.float64) for k in ("cy", "zm", "zt", "zx")}
+    e = 1 if lam else 0
+    p = cfg.pil if lam else 0
+    g = OrcGrid(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk, maxcfl=cfg.maxcfl, i0g=i0g, j0g=j0g,
+                west=e, east=e, south=e, north=e, pil_w=p, pil_e=p, pil_s=p, pil_n=p,
+                lam_gbpil_t=0, bc_lam_flux=1, schm_advec=schm_advec, itraj=cfg.niter,
+                slt_winds=1 if slt_winds else 0, bA_m=0.6, bA=0.6, inv_rayt=ga["inv_rayt"],
+                inv_hx=ga["inv_hx"], inv_hy=ga["inv_hy"],
+                cy=keep["cy"].ctypes.data_as(C.POINTER(C.c_double)),
+                zm=keep["zm"].ctypes.data_as(C.POINTER(C.c_double)),
+                zt=keep["zt"].ctypes.data_as(C.POINTER(C.c_double)),
+                zx=keep["zx"].ctypes.data_as(C.POINTER(C.c_double)),
+                zmin=ga["zmin"], zmax=ga["zmax"], wmstar_nk=ga["wmstar_nk"], idz_t_nkm1=ga["idz_t_nkm1"])
+    return g, keep
+
+
+class Step:
+    """adz_set + one advection step on the CPU (the reference's structure:
+    prepareWinds, Adz_niter trajectory iterations, interp_traj, then
+    adz_tricub_hlt per position set and the monotone clip).
+
+    kind: 'oracle' (restated interpolator) or 'ref' (reference interpolator).
+    prec: 'f32' (the reference's own precision) or 'f64' (FP64 extension).
+    """
+
+    def __init__(self, cfg, kind="oracle", prec="f32", threads=0, **gridkw):
+        self.cfg, self.kind, self.prec = cfg, kind, prec
+        self.L = lib(kind).lib
+        self.L.orc_set_threads(threads)
+        self.grid, self._keep = make_grid(cfg, **gridkw)
+        self.s = OrcSet()
+        self.L.orc_adz_set(C.byref(self.grid), C.byref(self.s))
+        self.dt = np.float32 if prec == "f32" else np.float64
+        s, c = self.s, cfg
+        self.ext_shape = (c.nk, s.njt, s.nit)
+        self.arr_shape = (c.nk, c.nj, c.ni)
+        self.uvw_d = np.zeros(self.ext_shape + (3,), self.dt)
+        self.uu_arr = np.zeros(self.arr_shape, self.dt)
+        self.vv_arr = np.zeros(self.arr_shape, self.dt)
+        self.ww_arr = np.zeros(self.arr_shape, self.dt)
+        self.uvw_dep = np.zeros(self.arr_shape + (3,), self.dt)
+        self.pxyzm = np.zeros(self.arr_shape + (3,), self.dt)
+        self.wpxyz = np.zeros((3, c.nk, c.nj + 4, c.ni + 4), np.float64)
+        self.sets = {q: np.zeros((self.L.orc_set_npoints(C.byref(s), q), 3), self.dt) for q in range(4)}
+        self.cold = True
+
+    def __del__(self):
+        try:
+            self.L.orc_adz_free(C.byref(self.s))
+        except Exception:
+            pass
+
+    def ranges(self):
+        s = self.s
+        return dict(q=(s.i0, s.in_, s.j0, s.jn, s.k0), u=(s.i0u, s.inu, s.j0, s.jn, s.k0),
+                    v=(s.i0, s.in_, s.j0v, s.jnv, s.k0), t=(s.i0, s.in_, s.j0, s.jn, s.k0t))
+
+    def inittraj(self):
+        fn = getattr(self.L, f"orc_inittraj_{self.prec}")
+        fn(C.byref(self.s), self.pxyzm.ctypes.data, self.wpxyz.ctypes.data)
+        self.cold = True
+
+    def traject(self, inp, niter=None):
+        """adz_prepareWinds + iterations + interp_traj. inp: dict of ext arrays."""
+        P = self.prec
+        a = {k: np.ascontiguousarray(inp[k], dtype=self.dt) for k in
+             ("uu_ext", "vv_ext", "ww_ext", "ut0", "vt0", "zdt0")}
+        self._zdt0 = a["zdt0"]
+        getattr(self.L, f"orc_prepare_winds_{P}")(
+            C.byref(self.s), *(a[k].ctypes.data for k in ("uu_ext", "vv_ext", "ww_ext", "ut0", "vt0", "zdt0")),
+            self.uvw_d.ctypes.data, self.uu_arr.ctypes.data, self.vv_arr.ctypes.data, self.ww_arr.ctypes.data)
+        if niter is None:
+            niter = max(6, self.cfg.niter) if self.cold else self.cfg.niter
+        getattr(self.L, f"orc_traject_{P}")(
+            C.byref(self.s), self.cfg.dt, niter, self.uvw_d.ctypes.data, self.uu_arr.ctypes.data,
+            self.vv_arr.ctypes.data, self.ww_arr.ctypes.data, self.uvw_dep.ctypes.data,
+            self.pxyzm.ctypes.data, self.wpxyz.ctypes.data)
+        self.cold = False
+        getattr(self.L, f"orc_interp_traj_{P}")(
+            C.byref(self.s), self.cfg.dt, self.wpxyz.ctypes.data, self.uvw_dep.ctypes.data,
+            a["zdt0"].ctypes.data, self.pxyzm.ctypes.data, None, None,
+            *(self.sets[q].ctypes.data for q in range(4)))
+
+    def tricub(self, set_id, srcs, mono=False, clip=False, post=False):
+        """adz_tricub_hlt on position set set_id (0=q,1=u,2=v,3=t); returns the
+        destination arrays (ext layout, range written, NaN elsewhere) and, if
+        post, (lin, min, max)."""
+        m = len(srcs)
+        srcs = [np.ascontiguousarray(x, dtype=self.dt) for x in srcs]
+        dsts = [np.full(self.ext_shape, np.nan, self.dt) for _ in range(m)]
+        ct = C.c_float if self.prec == "f32" else C.c_double
+        sp, dp = _ptrs(srcs, ct), _ptrs(dsts, ct)
+        lin = mn = mx = None
+        lp = mnp = mxp = None
+        if mono and post:
+            lin = [np.full(self.ext_shape, np.nan, self.dt) for _ in range(m)]
+            mn = [np.full(self.ext_shape, np.nan, self.dt) for _ in range(m)]
+            mx = [np.full(self.ext_shape, np.nan, self.dt) for _ in range(m)]
+            lp, mnp, mxp = (C.cast(_ptrs(z, ct), C.c_void_p) for z in (lin, mn, mx))
+        getattr(self.L, f"orc_tricub_{self.prec}")(
+            C.byref(self.s), set_id, self.sets[set_id].ctypes.data, m, C.cast(sp, C.c_void_p),
+            C.cast(dp, C.c_void_p), int(mono), int(clip), lp, mnp, mxp)
+        if post:
+            return dsts, (lin, mn, mx)
+        return dsts
+
+    def step(self, inp, niter=None):
+        """Trajectory, then u@pmu, v@pmv, w@pt, tracers@pt (clip if cfg.mono)."""
+        self.traject(inp, niter)
+        out = {}
+        out["u"] = self.tricub(1, [inp["src_u"]])[0]
+        out["v"] = self.tricub(2, [inp["src_v"]])[0]
+        out["w"] = self.tricub(3, [inp["src_w"]])[0]
+        if inp.get("tracers"):
+            out["tracers"] = self.tricub(3, inp["tracers"], mono=self.cfg.mono, clip=self.cfg.mono)
+        return out
