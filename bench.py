@@ -1,0 +1,357 @@
+"""Benchmark of the semi-Lagrangian advection step on B200.
+
+Workload (one "step"): one full GEM advection step of a 1024x1024x80 limited-area
+tile (dx = 2.5 km, 80 levels stretched 20 m -> 1 km up to 25 km, dt = 60 s,
+2 trajectory iterations): departure winds prepared, trajectories iterated,
+then u@pmu, v@pmv, w + 4 cosine-bell tracers @pt interpolated (momentum plus 4
+tracers).  Inputs are seeded synthetic fields of that shape (no dataset).
+
+Metric: grid points advanced per second (ni*nj*nk per step / step time).
+``value`` is the mixed-precision product path with inputs resident in HBM;
+``fp64_value`` is the plain FP64 drop-in on the same GPU; ``e2e`` goes
+through the same public API with inputs copied from pinned host memory and
+results copied back every step.  Inputs (>10 GB) exceed the 126 MB L2, so no
+flush is needed between steps.
+
+usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl product|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d.get("hbm_gbs", HBM_FALLBACK_GBS)), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi clock sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index, self.samples, self.proc = index, [], None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[1]) for s in self.samples if len(s) > 8 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 8 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            if len(s) > 8:
+                for nm, v in zip(names, s[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference(size, steps, warmup, threads=0, ntracers=4):
+    """The reference's CPU path: its interpolator compiled unchanged plus the
+    C restatement of the Fortran drivers (OpenMP over k-planes), FP32 fields,
+    on a bounded sample of the workload.  Returns points/s and details."""
+    from oracle import oracle as O
+    from gem_b200 import synth
+    kind = "ref" if O.have_ref() else "oracle"
+    cfg = synth.config_large(*size, ntracers=ntracers)
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    inp = synth.make_inputs(cfg, device=dev, dtype=torch.float32)
+    np_in = {k: (v.cpu().numpy() if torch.is_tensor(v) else [t.cpu().numpy() for t in v]) for k, v in inp.items()}
+    del inp
+    ncores = threads or os.cpu_count()
+    st = O.Step(cfg, kind=kind, prec="f32", threads=ncores)
+    st.inittraj()
+    st.traject(np_in)  # cold start (6 iterations) outside the timing
+    times = []
+    for s in range(warmup + steps):
+        t0 = time.perf_counter()
+        st.step(np_in)
+        dt = time.perf_counter() - t0
+        if s >= warmup:
+            times.append(dt)
+    med = statistics.median(times)
+    cpu = ""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                cpu = line.split(":", 1)[1].strip()
+                break
+    except Exception:
+        pass
+    return {"value": cfg.npoints / med, "unit": "grid-points/s", "cores": ncores,
+            "kind": "reference" if kind == "ref" else "port",
+            "sample": f"{size[0]}x{size[1]}x{size[2]} tile, u,v,w+{ntracers} tracers, FP32 (reference precision), "
+                      f"median of {steps} steps after {warmup} warm-up, {cpu}",
+            "ms_per_step": med * 1e3}
+
+
+# ---------------------------------------------------------------------------
+def run_product(args):
+    from gem_b200 import adz, synth
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    ni, nj, nk = args.size
+    cfg = synth.config_large(ni, nj, nk, seed=4321 + rank, ntracers=args.ntr)
+    npts = cfg.npoints
+    inp64 = synth.make_inputs(cfg, device="cuda", dtype=torch.float64)
+    keys = ["uu_ext", "vv_ext", "ww_ext", "ut0", "vt0", "zdt0", "src_u", "src_v", "src_w"]
+
+    def conv(d, dt):
+        o = {k: d[k].to(dt) for k in keys}
+        o["tracers"] = [t.to(dt) for t in d["tracers"]]
+        return o
+
+    ad = adz.Adz.from_config(cfg)
+    results = {}
+
+    def make_step(prec, data):
+        px, wp = ad.new_state(prec)
+        ad.adz_inittraj(prec, px, wp)
+        dt = adz._field_dtype(prec)
+        outs = {k: torch.zeros(ad.ext_shape, dtype=dt, device="cuda") for k in ("u", "v", "w")}
+        tro = [torch.zeros(ad.ext_shape, dtype=dt, device="cuda") for _ in data["tracers"]]
+
+        def step():
+            adz.step_fused(ad, prec, cfg.dt, data, data, data["tracers"], px, wp, outs, tro, cfg.mono)
+        step()  # cold start: 6 iterations, untimed
+        return step, outs, tro
+
+    def timed(step, K, W, clocks=False):
+        for _ in range(W):
+            step()
+        barrier(ws)
+        clk = Clocks(local) if clocks else None
+        if clk:
+            clk.__enter__()
+            time.sleep(0.3)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier(ws)
+        e0.record()
+        for _ in range(K):
+            step()
+        e1.record()
+        barrier(ws)
+        if clk:
+            clk.__exit__()
+        ms = e0.elapsed_time(e1) / K
+        return max_over_ranks(ms, ws), (clk.summary() if clk else None)
+
+    # plain FP64 drop-in
+    d64 = conv(inp64, torch.float64)
+    step64, _, _ = make_step(adz.FP64, d64)
+    ms64, _ = timed(step64, args.steps, args.warmup)
+    results["fp64"] = ms64
+    del step64
+    torch.cuda.empty_cache()
+    # mixed precision (product)
+    d32 = conv(inp64, torch.float32)
+    del d64, inp64
+    torch.cuda.empty_cache()
+    step32, outs32, tro32 = make_step(adz.MIXED, d32)
+    ms32, clk = timed(step32, args.steps, args.warmup, clocks=True)
+    if ad.status() != 0:
+        raise RuntimeError("device status set during the timed steps")
+
+    # per-launch durations of one step (events between the API calls)
+    s = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    px, wp = ad.new_state(adz.MIXED)
+    ad.adz_inittraj(adz.MIXED, px, wp)
+    ad.adz_traject(adz.MIXED, cfg.dt, d32, px, wp)
+    torch.cuda.synchronize()
+    per = {"traject": [], "set_u": [], "set_v": [], "set_t": []}
+    for _ in range(max(3, min(args.steps, 10))):
+        ev[0].record(s)
+        ad.adz_traject(adz.MIXED, cfg.dt, d32, px, wp)
+        ev[1].record(s)
+        ad.adz_tricub_hlt(adz.MIXED, adz.SET_U, [d32["src_u"]], [outs32["u"]])
+        ev[2].record(s)
+        ad.adz_tricub_hlt(adz.MIXED, adz.SET_V, [d32["src_v"]], [outs32["v"]])
+        ev[3].record(s)
+        ad.adz_tricub_hlt(adz.MIXED, adz.SET_T, [d32["src_w"]] + d32["tracers"], [outs32["w"]] + tro32,
+                          mono=[0] + [1 if cfg.mono else 0] * len(tro32))
+        ev[4].record(s)
+        torch.cuda.synchronize()
+        for q, k in enumerate(per):
+            per[k].append(ev[q].elapsed_time(ev[q + 1]))
+    per = {k: statistics.median(v) for k, v in per.items()}
+    I = ad.info
+    n_t = int(I.npts[3])
+    nf_t = 1 + len(tro32)
+    # algorithmic bytes of the t-set launch per arrival point: FP64 position
+    # (24 B) + departure w and zdot (8 B) + nf fields read and written (8 B each)
+    bytes_t = n_t * (24 + 8 + nf_t * 8)
+    # trajectory launch (prepare + iterations) per grid point: winds in
+    # (3 departure + 3 arrival, FP32) 24 B, departure winds written and read
+    # once (24 B), FP64 positions in and out 48 B, departure w out 4 B
+    bytes_traj = npts * (24 + 24 + 48 + 4)
+    dom = max(per, key=per.get)
+    hbm, hbm_kind = peaks()
+    if dom == "traject":
+        achieved = bytes_traj / (per[dom] * 1e-3) / 1e9
+        traffic = None
+    else:
+        b = bytes_t if dom == "set_t" else npts * (24 + 8)
+        achieved = b / (per[dom] * 1e-3) / 1e9
+        traffic = None
+    step_bytes = npts * (24 + 12 + 12 + 24 + (3 + args.ntr) * 8)
+
+    # end to end: inputs from pinned host memory, results back, every step
+    e2e = None
+    if not args.no_e2e:
+        host_in = {k: d32[k].cpu().pin_memory() for k in keys}
+        host_tr = [t.cpu().pin_memory() for t in d32["tracers"]]
+        host_out = [torch.empty(ad.ext_shape, dtype=torch.float32).pin_memory() for _ in range(3 + len(tro32))]
+        h2d = sum(v.numel() * 4 for v in host_in.values()) + sum(t.numel() * 4 for t in host_tr)
+        d2h = sum(t.numel() * 4 for t in host_out)
+
+        def e2e_step():
+            for k in keys:
+                d32[k].copy_(host_in[k], non_blocking=True)
+            for t, h in zip(d32["tracers"], host_tr):
+                t.copy_(h, non_blocking=True)
+            step32()
+            for h, dsrc in zip(host_out, [outs32["u"], outs32["v"], outs32["w"]] + tro32):
+                h.copy_(dsrc, non_blocking=True)
+        K2 = max(3, min(args.steps, 5))
+        ms_e2e, _ = timed(e2e_step, K2, 1)
+        e2e = {"value": npts * ws / (ms_e2e * 1e-3), "unit": "grid-points/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_reference(args.cpu_size, 2, 1, ntracers=args.ntr)
+    value = npts * ws / (ms32 * 1e-3)
+    line = {
+        "metric": "SL advection grid-points/s at 1024^2x80 (mixed-precision step; plain FP64 GPU drop-in alongside)",
+        "value": value, "unit": "grid-points/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 sums / f64 positions", "data": "synthetic (seeded analytic deformational flow + noise)",
+        "config": {"workload": f"adz step {ni}x{nj}x{nk} LAM tile, u,v,w+{args.ntr} cosine-bell tracers, "
+                               "2 trajectory iterations, dt=60 s, dx=2.5 km, 80 stretched levels",
+                   "points_per_step": npts, "l2": "inputs larger than L2 (no flush)", "parallelism":
+                   f"{ws} independent tiles (one per GPU)" if ws > 1 else "1 tile"},
+        "fp64_value": npts * ws / (ms64 * 1e-3), "fp64_ms_per_step": ms64, "speedup_vs_fp64": ms64 / ms32,
+        "per_launch_ms": per,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind},
+        "step_roofline": {"algorithmic_bytes_per_point": step_bytes / npts,
+                          "achieved_gbs": step_bytes / (ms32 * 1e-3) / 1e9,
+                          "frac": step_bytes / (ms32 * 1e-3) / 1e9 / hbm},
+        "e2e": e2e, "gpu_launches": 5 * args.steps, "clocks": clk, "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def run_reference(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    r = cpu_reference(args.cpu_size, args.steps, args.warmup, ntracers=args.ntr)
+    line = {"impl": "reference",
+            "metric": "SL advection grid-points/s at 1024^2x80 (mixed-precision step; plain FP64 GPU drop-in alongside)",
+            "value": r["value"], "unit": "grid-points/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 fields / f64 coefficients (reference precision)", "data": "synthetic",
+            "config": {"workload": f"adz step, bounded sample {r['sample']}"},
+            "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": r["value"], "unit": "grid-points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="product", choices=["product", "reference"])
+    ap.add_argument("--size", type=lambda s: tuple(int(x) for x in s.split(",")), default=(1024, 1024, 80))
+    ap.add_argument("--cpu-size", type=lambda s: tuple(int(x) for x in s.split(",")), default=(512, 512, 80))
+    ap.add_argument("--ntr", type=int, default=4)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_product(args)
+
+
+if __name__ == "__main__":
+    main()

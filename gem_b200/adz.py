@@ -1,0 +1,288 @@
+"""Python mirror of GEM's adz interface over the B200 C ABI (include/adz_b200.h).
+
+The names follow the reference's Fortran drivers (src/gemdyn/src/base/):
+``adz_set`` (adz_set.F90), ``adz_inittraj`` (adz_inittraj.F90),
+``adz_traject`` (adz_traject.F90 + adz_prepareWinds.F90 + adz_interp_traj.F90),
+``adz_tricub_hlt`` (adz_interp_hlt.F90), ``adz_main`` (adz_main.F90) and
+``adz_tracers`` (adz_tracers.F90 with the clip of adz_post_tr.F90:81-94).
+
+torch supplies device memory and the CUDA stream; all arithmetic runs in the
+library's kernels.  There is no CPU path: without the built library or a CUDA
+device every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libadz_b200.so")
+
+REF32, FP64, MIXED = 0, 1, 2
+SET_Q, SET_U, SET_V, SET_T = 0, 1, 2, 3
+PREC_NAMES = {"ref32": REF32, "fp64": FP64, "mixed": MIXED}
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA runtime error", 3: "fewer than 4 levels",
+          4: "stencil outside the extended array", 5: "non-finite wind or position",
+          6: "bounded device wait expired", 7: "allocation failed", 8: "no CUDA device", 9: "size above capacity"}
+
+
+class AdzError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        super().__init__(f"{what}: adz status {status} ({STATUS.get(status, '?')})")
+
+
+class AdzcGrid(C.Structure):
+    _fields_ = [(n, C.c_int) for n in (
+        "ni", "nj", "nk", "maxcfl", "i0g", "j0g", "west", "east", "south", "north",
+        "pil_w", "pil_e", "pil_s", "pil_n", "lam_gbpil_t", "bc_lam_flux", "schm_advec", "itraj", "slt_winds")] + [
+        ("bA_m", C.c_double), ("bA", C.c_double), ("inv_rayt", C.c_double), ("inv_hx", C.c_double),
+        ("inv_hy", C.c_double), ("cy", C.POINTER(C.c_double)), ("zm", C.POINTER(C.c_double)),
+        ("zt", C.POINTER(C.c_double)), ("zx", C.POINTER(C.c_double)), ("zmin", C.c_double), ("zmax", C.c_double),
+        ("wmstar_nk", C.c_double), ("idz_t_nkm1", C.c_double)]
+
+
+class AdzcInfo(C.Structure):
+    _fields_ = [(n, C.c_int) for n in (
+        "halox", "haloy", "nit", "njt", "i0", "in_", "j0", "jn", "i0u", "inu", "j0v", "jnv",
+        "i0b", "inb", "j0b", "jnb", "k0", "k0t", "k0m")] + [
+        ("npts", C.c_longlong * 4), ("iminposx", C.c_double), ("imaxposx", C.c_double),
+        ("iminposy", C.c_double), ("imaxposy", C.c_double), ("pnz_m", C.c_int), ("pnz_t", C.c_int)]
+
+
+class PxPyPz(C.Structure):
+    _fields_ = [("px", C.c_float), ("py", C.c_float), ("pz", C.c_float)]
+
+
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    """Load the CUDA library; raises when it has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} missing: build it with gem_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        vp, i, d = C.c_void_p, C.c_int, C.c_double
+        L.adzc_setup.argtypes = [C.POINTER(AdzcGrid), C.POINTER(vp)]
+        L.adzc_destroy.argtypes = [vp]
+        L.adzc_query.argtypes = [vp, C.POINTER(AdzcInfo)]
+        L.adzc_inittraj.argtypes = [vp, i, vp, vp, vp]
+        L.adzc_traject.argtypes = [vp, i, d, i] + [vp] * 9
+        L.adzc_tricub.argtypes = [vp, i, i, i, vp, vp, vp, vp, vp, vp, vp]
+        L.adzc_status.argtypes = [vp, i, vp]
+        L.adzc_ztab_create.argtypes = [vp, i, i, i, i, i, C.POINTER(vp)]
+        L.adzc_ztab_destroy.argtypes = [vp]
+        L.adzc_tricublin_m_n.argtypes = [vp, i, vp, vp, vp, i, i, vp]
+        L.adzc_tricublin_mono_m_n.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, i, i, i, vp]
+        L.adzc_tricublin_zyx3_n.argtypes = [vp, i, vp, vp, vp, i, vp]
+        L.adzc_error_string.restype = C.c_char_p
+        L.Vsearch_setup.restype = vp
+        L.Vsearch_setup.argtypes = [vp, i, i, i]
+        L.Vsearch_setup_plus.restype = vp
+        L.Vsearch_setup_plus.argtypes = [vp, i, i, i, i, i]
+        for name in ("Tricublin_zyx1_n", "Tricublin_zyx3_n"):
+            getattr(L, name).argtypes = [vp, vp, vp, vp, i]
+        for name in ("Tricublin_zyx1_n_m", "Tricublin_zyx1_m_n", "Tricublin_zyx1_p"):
+            getattr(L, name).argtypes = [vp, vp, vp, vp, i, i]
+        L.Tricublin_mono_zyx_n.argtypes = [vp, vp, vp, vp, vp, vp, vp, i]
+        for name in ("Tricublin_mono_zyx_n_m", "Tricublin_mono_zyx_m_n"):
+            getattr(L, name).argtypes = [vp, vp, vp, vp, vp, vp, vp, i, i]
+        _LIB = L
+    return _LIB
+
+
+def _check(st: int, what: str):
+    if st != 0:
+        raise AdzError(st, what)
+
+
+def _stream(stream=None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def _ptr_array(tensors):
+    arr = (C.c_void_p * len(tensors))()
+    for q, t in enumerate(tensors):
+        arr[q] = None if t is None else t.data_ptr()
+    return arr
+
+
+def _field_dtype(prec: int):
+    return torch.float64 if prec == FP64 else torch.float32
+
+
+def _pos_dtype(prec: int):
+    return torch.float32 if prec == REF32 else torch.float64
+
+
+# ---------------------------------------------------------------------------
+# level descriptor + interpolators on device data (turbo_tricublin.c ABI)
+# ---------------------------------------------------------------------------
+class Ztab:
+    """Vsearch_setup_plus on the device."""
+
+    def __init__(self, levels, ni, nj, offi=0, offj=0):
+        self.levels = np.ascontiguousarray(levels, dtype=np.float64)
+        self.ptr = C.c_void_p()
+        _check(lib().adzc_ztab_create(self.levels.ctypes.data, len(self.levels), ni, nj, offi, offj,
+                                      C.byref(self.ptr)), "adzc_ztab_create")
+
+    def __del__(self):
+        try:
+            lib().adzc_ztab_destroy(self.ptr)
+        except Exception:
+            pass
+
+
+def tricublin_m_n(zt: Ztab, prec: int, fields, pos, stream=None):
+    """Tricublin_zyx1_m_n on device tensors: returns d[m][n]."""
+    n, m = pos.shape[0], len(fields)
+    d = torch.empty((m, n), dtype=fields[0].dtype, device=pos.device)
+    _check(lib().adzc_tricublin_m_n(zt.ptr, prec, d.data_ptr(), C.cast(_ptr_array(fields), C.c_void_p),
+                                    pos.data_ptr(), n, m, _stream(stream)), "adzc_tricublin_m_n")
+    return d
+
+
+def tricublin_mono_m_n(zt: Ztab, prec: int, fields, pos, box=0, stream=None):
+    n, m = pos.shape[0], len(fields)
+    out = [torch.empty((m, n), dtype=fields[0].dtype, device=pos.device) for _ in range(4)]
+    _check(lib().adzc_tricublin_mono_m_n(zt.ptr, prec, *(o.data_ptr() for o in out),
+                                         C.cast(_ptr_array(fields), C.c_void_p), pos.data_ptr(), n, m, box,
+                                         _stream(stream)), "adzc_tricublin_mono_m_n")
+    return out
+
+
+def tricublin_zyx3_n(zt: Ztab, prec: int, f3, pos, stream=None):
+    n = pos.shape[0]
+    d = torch.empty((n, 3), dtype=f3.dtype, device=pos.device)
+    _check(lib().adzc_tricublin_zyx3_n(zt.ptr, prec, d.data_ptr(), f3.data_ptr(), pos.data_ptr(), n,
+                                       _stream(stream)), "adzc_tricublin_zyx3_n")
+    return d
+
+
+# ---------------------------------------------------------------------------
+# the adz step
+# ---------------------------------------------------------------------------
+class Adz:
+    """adz_set for one tile, then the step entry points.
+
+    Array layouts (torch shapes, C order = Fortran order reversed):
+      ext fields (nk, njt, nit); wpxyz (3, nk, nj+4, ni+4) float64;
+      pxyzm (nk, nj, ni, 3) float32 (REF32 warm start only).
+    """
+
+    def __init__(self, grid: AdzcGrid, keep=None, itraj: int | None = None):
+        self._keep = keep
+        self.grid = grid
+        self.h = C.c_void_p()
+        _check(lib().adzc_setup(C.byref(grid), C.byref(self.h)), "adzc_setup")
+        self.info = AdzcInfo()
+        _check(lib().adzc_query(self.h, C.byref(self.info)), "adzc_query")
+        self.ni, self.nj, self.nk = grid.ni, grid.nj, grid.nk
+
+    @classmethod
+    def from_config(cls, cfg, lam=True, i0g=1, j0g=1, schm_advec=1):
+        """adz_set for a synthetic LAM tile (gem_b200.synth.Config)."""
+        from . import synth
+        ga = synth.grid_arrays(cfg)
+        keep = {k: np.ascontiguousarray(ga[k], dtype=np.float64) for k in ("cy", "zm", "zt", "zx")}
+        e = 1 if lam else 0
+        p = cfg.pil if lam else 0
+        P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+        g = AdzcGrid(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk, maxcfl=cfg.maxcfl, i0g=i0g, j0g=j0g,
+                     west=e, east=e, south=e, north=e, pil_w=p, pil_e=p, pil_s=p, pil_n=p,
+                     lam_gbpil_t=0, bc_lam_flux=1, schm_advec=schm_advec, itraj=cfg.niter, slt_winds=0,
+                     bA_m=0.6, bA=0.6, inv_rayt=ga["inv_rayt"], inv_hx=ga["inv_hx"], inv_hy=ga["inv_hy"],
+                     cy=P(keep["cy"]), zm=P(keep["zm"]), zt=P(keep["zt"]), zx=P(keep["zx"]),
+                     zmin=ga["zmin"], zmax=ga["zmax"], wmstar_nk=ga["wmstar_nk"], idz_t_nkm1=ga["idz_t_nkm1"])
+        return cls(g, keep)
+
+    def __del__(self):
+        try:
+            lib().adzc_destroy(self.h)
+        except Exception:
+            pass
+
+    # shapes ---------------------------------------------------------------
+    @property
+    def ext_shape(self):
+        return (self.nk, self.info.njt, self.info.nit)
+
+    def new_state(self, prec: int, device="cuda"):
+        """Trajectory state arrays: (pxyzm or None, wpxyz)."""
+        wp = torch.zeros((3, self.nk, self.nj + 4, self.ni + 4), dtype=torch.float64, device=device)
+        px = torch.zeros((self.nk, self.nj, self.ni, 3), dtype=torch.float32, device=device) if prec == REF32 else None
+        return px, wp
+
+    def set_range(self, s: int):
+        I = self.info
+        return {SET_Q: (I.i0, I.in_, I.j0, I.jn, I.k0), SET_U: (I.i0u, I.inu, I.j0, I.jn, I.k0),
+                SET_V: (I.i0, I.in_, I.j0v, I.jnv, I.k0), SET_T: (I.i0, I.in_, I.j0, I.jn, I.k0t)}[s]
+
+    def range_mask(self, s: int, device="cpu"):
+        """Boolean mask (ext layout) of the arrival points of set s."""
+        i0, i1, j0, j1, k0 = self.set_range(s)
+        I = self.info
+        m = torch.zeros(self.ext_shape, dtype=torch.bool, device=device)
+        m[k0 - 1:, j0 - 1 + I.haloy:j1 + I.haloy, i0 - 1 + I.halox:i1 + I.halox] = True
+        return m
+
+    # entry points ---------------------------------------------------------
+    def adz_inittraj(self, prec: int, pxyzm, wpxyz, stream=None):
+        _check(lib().adzc_inittraj(self.h, prec, None if pxyzm is None else pxyzm.data_ptr(), wpxyz.data_ptr(),
+                                   _stream(stream)), "adzc_inittraj")
+
+    def adz_traject(self, prec: int, dt: float, winds: dict, pxyzm, wpxyz, niter: int = 0, stream=None):
+        """winds: uu_ext, vv_ext, ww_ext, ut0, vt0, zdt0 (ext layout, field dtype)."""
+        self._zdt0 = winds["zdt0"]
+        _check(lib().adzc_traject(self.h, prec, float(dt), int(niter),
+                                  *(winds[k].data_ptr() for k in ("uu_ext", "vv_ext", "ww_ext", "ut0", "vt0", "zdt0")),
+                                  None if pxyzm is None else pxyzm.data_ptr(), wpxyz.data_ptr(), _stream(stream)),
+               "adzc_traject")
+
+    def adz_tricub_hlt(self, prec: int, set_id: int, srcs, dsts, mono=None, post=None, stream=None):
+        """Interpolate srcs at position set set_id into dsts (ext layout).
+        mono: per-field 0 (none), 1 (bounds + clip), 2 (bounds only);
+        post: optional (lin, min, max) lists of tensors for mono fields."""
+        n = len(srcs)
+        mono_arr = (C.c_int * n)(*mono) if mono is not None else None
+        lin = mn = mx = None
+        if post is not None:
+            lin, mn, mx = (C.cast(_ptr_array(p), C.c_void_p) for p in post)
+        _check(lib().adzc_tricub(self.h, prec, set_id, n, C.cast(_ptr_array(srcs), C.c_void_p),
+                                 C.cast(_ptr_array(dsts), C.c_void_p), mono_arr, lin, mn, mx, _stream(stream)),
+               "adzc_tricub")
+
+    def status(self, reset=True, stream=None) -> int:
+        return lib().adzc_status(self.h, 1 if reset else 0, _stream(stream))
+
+    def adz_main(self, prec, dt, winds, fields, pxyzm, wpxyz, outs, niter=0, stream=None):
+        """Trajectory, then u@pmu, v@pmv, w@pt (adz_main.F90:32-60 with the
+        synthetic momentum set u, v, w)."""
+        self.adz_traject(prec, dt, winds, pxyzm, wpxyz, niter, stream)
+        self.adz_tricub_hlt(prec, SET_U, [fields["src_u"]], [outs["u"]], stream=stream)
+        self.adz_tricub_hlt(prec, SET_V, [fields["src_v"]], [outs["v"]], stream=stream)
+        self.adz_tricub_hlt(prec, SET_T, [fields["src_w"]], [outs["w"]], stream=stream)
+
+    def adz_tracers(self, prec, tracers, outs, mono: bool, stream=None):
+        """All tracers of the t set in one fused launch, clipped when mono
+        (adz_tracers.F90:74-99 + adz_post_tr.F90:81-94)."""
+        if tracers:
+            self.adz_tricub_hlt(prec, SET_T, tracers, outs, mono=[1 if mono else 0] * len(tracers), stream=stream)
+
+
+def step_fused(adz: Adz, prec, dt, winds, fields, tracers, pxyzm, wpxyz, outs, tr_outs, mono, niter=0, stream=None):
+    """One advection step with w and every tracer in the same t-set launch."""
+    adz.adz_traject(prec, dt, winds, pxyzm, wpxyz, niter, stream)
+    adz.adz_tricub_hlt(prec, SET_U, [fields["src_u"]], [outs["u"]], stream=stream)
+    adz.adz_tricub_hlt(prec, SET_V, [fields["src_v"]], [outs["v"]], stream=stream)
+    srcs = [fields["src_w"]] + list(tracers)
+    dsts = [outs["w"]] + list(tr_outs)
+    adz.adz_tricub_hlt(prec, SET_T, srcs, dsts, mono=[0] + [1 if mono else 0] * len(tracers), stream=stream)

@@ -1,0 +1,811 @@
+// Host side of the adz_b200 C ABI (include/adz_b200.h).
+//
+// adzc_setup derives on the host what GEM's adz_set derives
+// (src/gemdyn/src/base/adz_set.F90:71-311, abbreviated B/ below) and uploads
+// it; the step entry points only validate arguments and launch kernels.  Level
+// A keeps the reference interpolator's names and host-pointer calling
+// convention (B/turbo_tricublin.c) on top of the device kernels.
+//
+// Built with -ffp-contract=off: the level tables use the reference's operation
+// order without fused multiply-adds.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "../../include/adz_b200.h"
+#include "adz_types.h"
+
+namespace {
+
+thread_local int g_last_status = ADZC_OK;
+
+int fail(int st) {
+  g_last_status = st;
+  return st;
+}
+
+#define ADZ_CK(x)                                  \
+  do {                                             \
+    if ((x) != cudaSuccess) return fail(ADZC_ERR_CUDA); \
+  } while (0)
+
+template <int P>
+struct Sz;
+
+size_t field_bytes(int prec) { return prec == ADZC_FP64 ? sizeof(double) : sizeof(float); }
+size_t pos_bytes(int prec) { return prec == ADZC_REF32 ? sizeof(float) : sizeof(double); }
+
+cudaError_t dispatch_prepare(int prec, const adz::DGrid& g, const void* uu, const void* vv, const void* ww, void* o,
+                             cudaStream_t s) {
+  switch (prec) {
+    case ADZC_REF32: return adz::launch_prepare<adz::kRef32>(g, uu, vv, ww, o, s);
+    case ADZC_FP64: return adz::launch_prepare<adz::kFp64>(g, uu, vv, ww, o, s);
+    default: return adz::launch_prepare<adz::kMixed>(g, uu, vv, ww, o, s);
+  }
+}
+cudaError_t dispatch_traject(int prec, const adz::DGrid& g, const adz::TrajArgs& a, cudaStream_t s) {
+  switch (prec) {
+    case ADZC_REF32: return adz::launch_traject<adz::kRef32>(g, a, s);
+    case ADZC_FP64: return adz::launch_traject<adz::kFp64>(g, a, s);
+    default: return adz::launch_traject<adz::kMixed>(g, a, s);
+  }
+}
+cudaError_t dispatch_set(int prec, const adz::DGrid& g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
+                         const adz::SetArgs& a, const adz::FieldPtrs& fp, cudaStream_t s) {
+  switch (prec) {
+    case ADZC_REF32: return adz::launch_tricub_set<adz::kRef32>(g, set, i0, nx, j0, ny, k0, nz, a, fp, s);
+    case ADZC_FP64: return adz::launch_tricub_set<adz::kFp64>(g, set, i0, nx, j0, ny, k0, nz, a, fp, s);
+    default: return adz::launch_tricub_set<adz::kMixed>(g, set, i0, nx, j0, ny, k0, nz, a, fp, s);
+  }
+}
+cudaError_t dispatch_pos(int prec, const adz::DZtab& lv, int kind, int n, const void* pos, const adz::FieldPtrs& fp,
+                         cudaStream_t s) {
+  switch (prec) {
+    case ADZC_REF32: return adz::launch_interp_pos<adz::kRef32>(lv, kind, n, pos, fp, s);
+    case ADZC_FP64: return adz::launch_interp_pos<adz::kFp64>(lv, kind, n, pos, fp, s);
+    default: return adz::launch_interp_pos<adz::kMixed>(lv, kind, n, pos, fp, s);
+  }
+}
+cudaError_t dispatch_init(int prec, const adz::DGrid& g, float* pxyzm, double* wpxyz, cudaStream_t s) {
+  switch (prec) {
+    case ADZC_REF32: return adz::launch_inittraj<adz::kRef32>(g, pxyzm, wpxyz, s);
+    case ADZC_FP64: return adz::launch_inittraj<adz::kFp64>(g, pxyzm, wpxyz, s);
+    default: return adz::launch_inittraj<adz::kMixed>(g, pxyzm, wpxyz, s);
+  }
+}
+
+double triprd_inv(double x, double a, double b, double c) { return 1.0 / ((x - a) * (x - b) * (x - c)); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// level descriptor (B/turbo_tricublin.c:164-173, 252-257, 320-380)
+// ---------------------------------------------------------------------------
+struct adzc_ztab {
+  std::vector<double> z, ocz;
+  std::vector<float> zn;
+  int ni = 0, nj = 0, nk = 0, offi = 0, offj = 0;
+  int device = 0;
+  double* d_z = nullptr;
+  double* d_ocz = nullptr;
+  float* d_zn = nullptr;
+  adz::DZtab dev() const {
+    adz::DZtab t;
+    t.z = d_z;
+    t.ocz = d_ocz;
+    t.zn = d_zn;
+    t.ni = ni;
+    t.nj = nj;
+    t.nk = nk;
+    t.nij = ni * nj;
+    t.offi = offi;
+    t.offj = offj;
+    return t;
+  }
+};
+
+static void build_ztab_host(adzc_ztab* lv, const double* levels, int nk, int ni, int nj, int offi, int offj) {
+  const int nkl = std::max(nk, 4);
+  lv->z.assign(levels, levels + nk);
+  lv->ocz.assign(4 * nkl, 1.0);
+  if (nk >= 4) {
+    const double* t = levels;
+    auto den = [&](int e, double a, double b, double c, double d) {
+      lv->ocz[4 * e + 0] = triprd_inv(a, b, c, d);
+      lv->ocz[4 * e + 1] = triprd_inv(b, a, c, d);
+      lv->ocz[4 * e + 2] = triprd_inv(c, a, b, d);
+      lv->ocz[4 * e + 3] = triprd_inv(d, a, b, c);
+    };
+    den(0, t[0], t[1], t[2], t[3]);
+    for (int i = 1; i < nk - 2; i++) den(i, t[i - 1], t[i], t[i + 1], t[i + 2]);
+    den(nk - 2, t[nk - 4], t[nk - 3], t[nk - 2], t[nk - 1]);
+    den(nk - 1, t[nk - 4], t[nk - 3], t[nk - 2], t[nk - 1]);
+  }
+  // FP32 per-interval table of the mixed path (normalised Lagrange nodes)
+  lv->zn.assign(8 * nkl, 0.0f);
+  for (int iz = 1; iz + 2 < nk; iz++) {
+    const double z0 = levels[iz], h = levels[iz + 1] - z0;
+    const double u[4] = {(levels[iz - 1] - z0) / h, 0.0, 1.0, (levels[iz + 2] - z0) / h};
+    lv->zn[8 * iz + 0] = (float)u[0];
+    lv->zn[8 * iz + 1] = (float)u[3];
+    for (int c = 0; c < 4; c++) {
+      double p = 1.0;
+      for (int d = 0; d < 4; d++)
+        if (d != c) p *= (u[c] - u[d]);
+      lv->zn[8 * iz + 2 + c] = (float)(1.0 / p);
+    }
+  }
+  lv->ni = ni;
+  lv->nj = nj;
+  lv->nk = nk;
+  lv->offi = offi;
+  lv->offj = offj;
+}
+
+static int upload_ztab(adzc_ztab* lv) {
+  ADZ_CK(cudaGetDevice(&lv->device));
+  ADZ_CK(cudaMalloc(&lv->d_z, sizeof(double) * lv->z.size()));
+  ADZ_CK(cudaMalloc(&lv->d_ocz, sizeof(double) * lv->ocz.size()));
+  ADZ_CK(cudaMalloc(&lv->d_zn, sizeof(float) * lv->zn.size()));
+  ADZ_CK(cudaMemcpy(lv->d_z, lv->z.data(), sizeof(double) * lv->z.size(), cudaMemcpyHostToDevice));
+  ADZ_CK(cudaMemcpy(lv->d_ocz, lv->ocz.data(), sizeof(double) * lv->ocz.size(), cudaMemcpyHostToDevice));
+  ADZ_CK(cudaMemcpy(lv->d_zn, lv->zn.data(), sizeof(float) * lv->zn.size(), cudaMemcpyHostToDevice));
+  return ADZC_OK;
+}
+
+extern "C" int adzc_ztab_create(const double* levels, int nk, int ni, int nj, int offi, int offj, ztab** out) {
+  if (!levels || !out || nk < 1 || ni < 1 || nj < 1) return fail(ADZC_ERR_ARG);
+  if (nk < 4) return fail(ADZC_ERR_NK);
+  auto* lv = new (std::nothrow) adzc_ztab();
+  if (!lv) return fail(ADZC_ERR_ALLOC);
+  build_ztab_host(lv, levels, nk, ni, nj, offi, offj);
+  int st = upload_ztab(lv);
+  if (st != ADZC_OK) {
+    adzc_ztab_destroy(lv);
+    return st;
+  }
+  *out = lv;
+  return ADZC_OK;
+}
+
+extern "C" int adzc_ztab_destroy(ztab* lv) {
+  if (!lv) return ADZC_OK;
+  cudaFree(lv->d_z);
+  cudaFree(lv->d_ocz);
+  cudaFree(lv->d_zn);
+  delete lv;
+  return ADZC_OK;
+}
+
+extern "C" int adzc_last_error(void) { return g_last_status; }
+
+extern "C" const char* adzc_error_string(int st) {
+  switch (st) {
+    case ADZC_OK: return "ok";
+    case ADZC_ERR_ARG: return "invalid argument";
+    case ADZC_ERR_CUDA: return "CUDA runtime error";
+    case ADZC_ERR_NK: return "fewer than 4 levels";
+    case ADZC_ERR_HALO: return "stencil outside the extended array";
+    case ADZC_ERR_NONFINITE: return "non-finite wind or position";
+    case ADZC_ERR_TIMEOUT: return "bounded device wait expired";
+    case ADZC_ERR_ALLOC: return "allocation failed";
+    case ADZC_ERR_NODEVICE: return "no CUDA device";
+    case ADZC_ERR_SIZE: return "size above capacity";
+    default: return "unknown status";
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Level B interpolators on device data
+// ---------------------------------------------------------------------------
+static int check_prec(int prec) { return (prec == ADZC_REF32 || prec == ADZC_FP64 || prec == ADZC_MIXED); }
+
+static int run_interp(const ztab* lv, int prec, int kind, void* d, void* l, void* mi, void* ma,
+                      const void* const* fs, const void* pxyz, int n, int m, int box, cudaStream_t s) {
+  if (!lv || !check_prec(prec) || n < 0 || m < 0 || (n > 0 && (!d || !pxyz || !fs))) return fail(ADZC_ERR_ARG);
+  if (n == 0) return ADZC_OK;
+  const size_t fb = field_bytes(prec);
+  const adz::DZtab t = lv->dev();
+  if (kind == 2) {
+    adz::FieldPtrs fp{};
+    fp.src[0] = fs[0];
+    fp.dst[0] = d;
+    fp.nf = 1;
+    fp.ostride = 3;
+    ADZ_CK(dispatch_pos(prec, t, 2, n, pxyz, fp, s));
+    return ADZC_OK;
+  }
+  for (int q0 = 0; q0 < m; q0 += adz::kMaxFields) {
+    adz::FieldPtrs fp{};
+    fp.nf = std::min(adz::kMaxFields, m - q0);
+    fp.ostride = 1;
+    fp.box222 = box;
+    for (int q = 0; q < fp.nf; q++) {
+      if (!fs[q0 + q]) return fail(ADZC_ERR_ARG);
+      fp.src[q] = fs[q0 + q];
+      const size_t o = (size_t)(q0 + q) * n * fb;
+      fp.dst[q] = (char*)d + o;
+      if (kind == 1) {
+        if (!l || !mi || !ma) return fail(ADZC_ERR_ARG);
+        fp.lin[q] = (char*)l + o;
+        fp.mn[q] = (char*)mi + o;
+        fp.mx[q] = (char*)ma + o;
+      }
+    }
+    ADZ_CK(dispatch_pos(prec, t, kind, n, pxyz, fp, s));
+  }
+  return ADZC_OK;
+}
+
+extern "C" int adzc_tricublin_m_n(const ztab* lv, int prec, void* d, const void* const* fs, const void* pxyz, int n,
+                                  int m, void* stream) {
+  return run_interp(lv, prec, 0, d, nullptr, nullptr, nullptr, fs, pxyz, n, m, 0, (cudaStream_t)stream);
+}
+
+extern "C" int adzc_tricublin_mono_m_n(const ztab* lv, int prec, void* d, void* l, void* mi, void* ma,
+                                       const void* const* fs, const void* pxyz, int n, int m, int box, void* stream) {
+  return run_interp(lv, prec, 1, d, l, mi, ma, fs, pxyz, n, m, box, (cudaStream_t)stream);
+}
+
+extern "C" int adzc_tricublin_zyx3_n(const ztab* lv, int prec, void* d, const void* f3, const void* pxyz, int n,
+                                     void* stream) {
+  const void* fs[1] = {f3};
+  if (!f3) return fail(ADZC_ERR_ARG);
+  return run_interp(lv, prec, 2, d, nullptr, nullptr, nullptr, fs, pxyz, n, 1, 0, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// adz_set and the step (Level B)
+// ---------------------------------------------------------------------------
+struct adzc_handle {
+  adzc_grid g{};
+  adzc_info info{};
+  adz::DGrid dg{};
+  int device = 0;
+  int niter = 1;
+  int cold = 0;
+  // host copies of the derived tables
+  std::vector<double> zm, zt, odelz_m, odelz_t, vw, cy;
+  std::vector<int> search_m, search_t;
+  double ovdzm = 0, ovdzt = 0, sig = 0;
+  adzc_ztab* tab_m = nullptr;
+  adzc_ztab* tab_t = nullptr;
+  void* d_tables = nullptr;
+  int* d_status = nullptr;
+  // scratch owned by the handle: departure winds (3 x ext) and departure w
+  void* d_uvw = nullptr;
+  size_t uvw_bytes = 0;
+  void* d_wdep = nullptr;
+  size_t wdep_bytes = 0;
+  // last trajectory, read by adzc_tricub
+  int last_prec = -1;
+  const double* wpxyz = nullptr;
+  const float* pxyzm = nullptr;
+  const void* zdt0 = nullptr;
+  adz::DtSplit dt{};
+};
+
+static int build_search(const std::vector<double>& z, int nk, double sig, const std::vector<double>& delz,
+                        double* ovdz, std::vector<int>* tab) {
+  // B/adz_set.F90:193-215; smallest_dz and posz are REAL128 there
+  __float128 smallest = (__float128)(sig * delz[1]);
+  for (int k = 2; k <= nk; k++) {
+    __float128 v = (__float128)(sig * delz[k]);
+    if (v < smallest) smallest = v;
+  }
+  const double ov = (double)((__float128)1.0 / smallest);
+  const double pz = 1.0 + sig * (z[nk + 1] - z[0]) * ov;
+  const int pnz = (int)std::lround(pz);
+  if (pnz < 1 || pnz > (1 << 24)) return ADZC_ERR_ARG;
+  *ovdz = (double)((__float128)sig / smallest);
+  tab->assign(pnz, 0);
+  int k0 = 0;
+  for (int k = 1; k <= pnz; k++) {
+    __float128 posz = (__float128)(sig * z[0]) + (__float128)(double)(k - 1) * smallest;
+    if (posz > (__float128)(sig * z[k0 + 1])) k0 = std::min(nk + 1, k0 + 1);
+    (*tab)[k - 1] = k0;
+  }
+  return ADZC_OK;
+}
+
+static double lag3(double zz, double z1, double z2, double z3, double z4) {  // B/adz_set.F90:530-536
+  return (((zz - z2) * (zz - z3) * (zz - z4)) / ((z1 - z2) * (z1 - z3) * (z1 - z4)));
+}
+
+extern "C" int adzc_setup(const adzc_grid* gin, adzc_handle** out) {
+  if (!gin || !out || !gin->zm || !gin->zt || !gin->zx || !gin->cy) return fail(ADZC_ERR_ARG);
+  const adzc_grid& g = *gin;
+  if (g.ni < 1 || g.nj < 1) return fail(ADZC_ERR_ARG);
+  if (g.nk < 4) return fail(ADZC_ERR_NK);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return fail(ADZC_ERR_NODEVICE);
+  auto* h = new (std::nothrow) adzc_handle();
+  if (!h) return fail(ADZC_ERR_ALLOC);
+  h->g = g;
+  const int ni = g.ni, nj = g.nj, nk = g.nk;
+  const double EPS_8 = 2.e-5;
+  const int BCS_BASE = 4, ext = 1;
+  adzc_info& I = h->info;
+  const int maxcfl = std::max(1, g.maxcfl);  // B/adz_set.F90:71-82
+  I.halox = I.haloy = maxcfl + 1;
+  const int lminx = 1 - I.halox, lmaxx = ni + I.halox, lminy = 1 - I.haloy, lmaxy = nj + I.haloy;
+  I.nit = lmaxx - lminx + 1;
+  I.njt = lmaxy - lminy + 1;
+  const int niu = ni - (g.east ? 1 : 0), njv = nj - (g.north ? 1 : 0);
+  I.i0 = 1 + g.pil_w - (ext + 1) * g.west;  // B/adz_set.F90:94-114
+  I.in = ni - g.pil_e + ext * g.east;
+  I.j0 = 1 + g.pil_s - (ext + 1) * g.south;
+  I.jn = nj - g.pil_n + ext * g.north;
+  I.i0u = 1 + g.pil_w;
+  I.j0v = 1 + g.pil_s;
+  I.inu = niu - g.pil_e;
+  I.jnv = njv - g.pil_n;
+  I.k0 = g.lam_gbpil_t + 1;
+  I.k0t = std::max(1, g.lam_gbpil_t);
+  I.k0m = std::max(I.k0t - 2, 1);
+  if (g.bc_lam_flux != 0) I.k0m = 1;
+  I.iminposx = g.i0g + lminx + EPS_8;  // B/adz_set.F90:132-160
+  I.imaxposx = g.i0g + lmaxx - 2 - EPS_8;
+  I.iminposy = g.j0g + lminy + EPS_8;
+  I.imaxposy = g.j0g + lmaxy - 2 - EPS_8;
+  if (g.west) I.iminposx = g.i0g + BCS_BASE + EPS_8;
+  if (g.east) I.imaxposx = g.i0g + ni - BCS_BASE - 1 - EPS_8;
+  if (g.south) I.iminposy = g.j0g + BCS_BASE + EPS_8;
+  if (g.north) I.imaxposy = g.j0g + nj - BCS_BASE - 1 - EPS_8;
+  I.i0b = 1 + BCS_BASE * g.west;
+  I.inb = ni - BCS_BASE * g.east;
+  I.j0b = 1 + BCS_BASE * g.south;
+  I.jnb = nj - BCS_BASE * g.north;
+  auto np = [&](int a, int b, int c, int d, int k) {
+    return (long long)std::max(0, b - a + 1) * std::max(0, d - c + 1) * std::max(0, nk - k + 1);
+  };
+  I.npts[0] = np(I.i0, I.in, I.j0, I.jn, I.k0);
+  I.npts[1] = np(I.i0u, I.inu, I.j0, I.jn, I.k0);
+  I.npts[2] = np(I.i0, I.in, I.j0v, I.jnv, I.k0);
+  I.npts[3] = np(I.i0, I.in, I.j0, I.jn, I.k0t);
+
+  h->zm.assign(g.zm, g.zm + nk + 2);
+  h->zt.assign(g.zt, g.zt + nk + 2);
+  std::vector<double> zx(g.zx, g.zx + nk + 1);
+  const auto& zm = h->zm;
+  const auto& zt = h->zt;
+  h->sig = (zm[nk] - zm[1]) / std::fabs(zm[nk] - zm[1]);  // B/adz_set.F90:178-179
+  std::vector<double> delz_m(nk + 1), delz_t(nk + 1);
+  h->odelz_m.assign(nk + 1, 0.0);
+  h->odelz_t.assign(nk + 1, 0.0);
+  const float verysmall = 1.17549435e-38f * 1.e5f;  // tiny(real)*1.e5
+  for (int k = 0; k <= nk; k++) {                   // B/adz_set.F90:181-191
+    delz_m[k] = (double)9.e33f;
+    delz_t[k] = (double)9.e33f;
+    if (std::fabs(zm[k + 1] - zm[k]) > verysmall) delz_m[k] = zm[k + 1] - zm[k];
+    if (std::fabs(zt[k + 1] - zt[k]) > verysmall) delz_t[k] = zt[k + 1] - zt[k];
+    h->odelz_m[k] = 1.0 / delz_m[k];
+    h->odelz_t[k] = 1.0 / delz_t[k];
+  }
+  if (build_search(zm, nk, h->sig, delz_m, &h->ovdzm, &h->search_m) != ADZC_OK ||
+      build_search(zt, nk, h->sig, delz_t, &h->ovdzt, &h->search_t) != ADZC_OK) {
+    delete h;
+    return fail(ADZC_ERR_ARG);
+  }
+  I.pnz_m = (int)h->search_m.size();
+  I.pnz_t = (int)h->search_t.size();
+  h->vw.assign(8 * (nk + 1), 0.0);
+  double* vw = h->vw.data();
+  for (int k = 2; k <= nk - 1; k++) {  // B/adz_set.F90:261-271
+    const double rx = zm[k], ra = zx[k - 2], rb = zx[k - 1], rc = zx[k], rd = zx[k + 1];
+    vw[0 * (nk + 1) + k] = lag3(rx, ra, rb, rc, rd);
+    vw[1 * (nk + 1) + k] = lag3(rx, rb, ra, rc, rd);
+    vw[2 * (nk + 1) + k] = lag3(rx, rc, ra, rb, rd);
+    vw[3 * (nk + 1) + k] = lag3(rx, rd, ra, rb, rc);
+  }
+  for (int k = 2; k <= nk - 2; k++) {  // B/adz_set.F90:272-281
+    const double rx = zt[k], ra = zm[k - 1], rb = zm[k], rc = zm[k + 1], rd = zm[k + 2];
+    vw[4 * (nk + 1) + k] = lag3(rx, ra, rb, rc, rd);
+    vw[5 * (nk + 1) + k] = lag3(rx, rb, ra, rc, rd);
+    vw[6 * (nk + 1) + k] = lag3(rx, rc, ra, rb, rd);
+    vw[7 * (nk + 1) + k] = lag3(rx, rd, ra, rb, rc);
+  }
+  h->cy.assign(g.cy, g.cy + I.njt);
+  h->niter = std::max(1, g.itraj);
+
+  int st;
+  if ((st = adzc_ztab_create(zm.data() + 1, nk, I.nit, I.njt, 1 - g.i0g, 1 - g.j0g, &h->tab_m)) != ADZC_OK ||
+      (st = adzc_ztab_create(zt.data() + 1, nk, I.nit, I.njt, 1 - g.i0g, 1 - g.j0g, &h->tab_t)) != ADZC_OK) {
+    adzc_destroy(h);
+    return fail(st);
+  }
+  // one device block for every table
+  const size_t nd = zm.size() + zt.size() + h->odelz_m.size() + h->odelz_t.size() + h->vw.size() + h->cy.size();
+  const size_t ni_ = h->search_m.size() + h->search_t.size() + 1;
+  if (cudaGetDevice(&h->device) != cudaSuccess || cudaMalloc(&h->d_tables, nd * sizeof(double) + ni_ * sizeof(int)) !=
+                                                      cudaSuccess) {
+    adzc_destroy(h);
+    return fail(ADZC_ERR_CUDA);
+  }
+  std::vector<char> blob(nd * sizeof(double) + ni_ * sizeof(int), 0);
+  double* dp = (double*)blob.data();
+  size_t o = 0;
+  auto put = [&](const std::vector<double>& v) {
+    std::memcpy(dp + o, v.data(), v.size() * sizeof(double));
+    const double* dev = (const double*)h->d_tables + o;
+    o += v.size();
+    return dev;
+  };
+  adz::DGrid& D = h->dg;
+  D.zm = put(zm);
+  D.zt = put(zt);
+  D.odelz_m = put(h->odelz_m);
+  D.odelz_t = put(h->odelz_t);
+  D.vw = put(h->vw);
+  D.cy = put(h->cy);
+  int* ip = (int*)(dp + nd);
+  int* dip = (int*)((double*)h->d_tables + nd);
+  std::memcpy(ip, h->search_m.data(), h->search_m.size() * sizeof(int));
+  D.search_m = dip;
+  std::memcpy(ip + h->search_m.size(), h->search_t.data(), h->search_t.size() * sizeof(int));
+  D.search_t = dip + h->search_m.size();
+  h->d_status = dip + h->search_m.size() + h->search_t.size();
+  if (cudaMemcpy(h->d_tables, blob.data(), blob.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    adzc_destroy(h);
+    return fail(ADZC_ERR_CUDA);
+  }
+  D.ni = ni; D.nj = nj; D.nk = nk;
+  D.halox = I.halox; D.haloy = I.haloy;
+  D.lminx = lminx; D.lminy = lminy;
+  D.nit = I.nit; D.njt = I.njt;
+  D.nij = (long long)I.nit * I.njt;
+  D.i0g = g.i0g; D.j0g = g.j0g;
+  D.i0 = I.i0; D.in = I.in; D.j0 = I.j0; D.jn = I.jn;
+  D.i0u = I.i0u; D.inu = I.inu; D.j0v = I.j0v; D.jnv = I.jnv;
+  D.i0b = I.i0b; D.inb = I.inb; D.j0b = I.j0b; D.jnb = I.jnb;
+  D.k0 = I.k0; D.k0t = I.k0t; D.k0m = I.k0m;
+  D.pnz_m = I.pnz_m; D.pnz_t = I.pnz_t;
+  D.slt_winds = g.slt_winds;
+  D.imnx = I.iminposx; D.imxx = I.imaxposx; D.imny = I.iminposy; D.imxy = I.imaxposy;
+  D.sig = h->sig; D.ovdzm = h->ovdzm; D.ovdzt = h->ovdzt;
+  D.zmin = g.zmin; D.zmax = g.zmax;
+  D.inv_rayt = g.inv_rayt; D.inv_hx = g.inv_hx; D.inv_hy = g.inv_hy;
+  D.vw5 = (zx[0] - zm[1]) / (zx[0] - zx[1]);  // B/adz_set.F90:282-284
+  D.vw6 = (zm[nk] - zx[nk]) / (zx[nk - 1] - zx[nk]);
+  D.ww = g.wmstar_nk;  // B/adz_interp_traj.F90:41-43
+  D.wp = (zt[nk] - zm[nk - 1]) * g.idz_t_nkm1;
+  D.wm = 1.0 - D.wp;
+  D.tab_m = h->tab_m->dev();
+  D.tab_t = h->tab_t->dev();
+  D.status = h->d_status;
+  *out = h;
+  return ADZC_OK;
+}
+
+extern "C" int adzc_destroy(adzc_handle* h) {
+  if (!h) return ADZC_OK;
+  adzc_ztab_destroy(h->tab_m);
+  adzc_ztab_destroy(h->tab_t);
+  cudaFree(h->d_tables);
+  cudaFree(h->d_uvw);
+  cudaFree(h->d_wdep);
+  delete h;
+  return ADZC_OK;
+}
+
+extern "C" int adzc_query(const adzc_handle* h, adzc_info* info) {
+  if (!h || !info) return fail(ADZC_ERR_ARG);
+  *info = h->info;
+  return ADZC_OK;
+}
+
+static adz::DtSplit dt_split(const adzc_grid& g, double dt) {  // B/adz_traject.F90:38-59
+  adz::DtSplit s{};
+  double a = 0.0, za = 0.0;
+  if (g.schm_advec == 1) { a = dt * 0.5; za = dt * 0.5; }
+  if (g.schm_advec == 2) { a = dt * g.bA_m; za = dt * g.bA; }
+  if (g.schm_advec == 3) { a = (1.0 - g.bA_m) * dt; za = (1.0 - g.bA) * dt; }
+  s.dtD = dt - a; s.dtzD = dt - za; s.dtA = a; s.dtzA = za;
+  if (g.schm_advec == 0) { s.dtA = s.dtD = s.dtzA = s.dtzD = 0.0; }
+  s.dt = dt;
+  return s;
+}
+
+static int ensure(void** p, size_t* have, size_t need) {
+  if (*have >= need) return ADZC_OK;
+  cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  if (cudaMalloc(p, need) != cudaSuccess) return ADZC_ERR_ALLOC;
+  *have = need;
+  return ADZC_OK;
+}
+
+extern "C" int adzc_inittraj(adzc_handle* h, int prec, void* pxyzm, double* wpxyz, void* stream) {
+  if (!h || !check_prec(prec) || !wpxyz || (prec == ADZC_REF32 && !pxyzm)) return fail(ADZC_ERR_ARG);
+  ADZ_CK(dispatch_init(prec, h->dg, (float*)pxyzm, wpxyz, (cudaStream_t)stream));
+  h->niter = std::max(6, h->g.itraj);  // B/adz_inittraj.F90:25
+  h->cold = 1;
+  return ADZC_OK;
+}
+
+extern "C" int adzc_traject(adzc_handle* h, int prec, double dt, int niter, const void* uu_ext, const void* vv_ext,
+                            const void* ww_ext, const void* ut0, const void* vt0, const void* zdt0, void* pxyzm,
+                            double* wpxyz, void* stream) {
+  if (!h || !check_prec(prec) || !uu_ext || !vv_ext || !ww_ext || !ut0 || !vt0 || !zdt0 || !wpxyz ||
+      (prec == ADZC_REF32 && !pxyzm))
+    return fail(ADZC_ERR_ARG);
+  if (!std::isfinite(dt)) return fail(ADZC_ERR_ARG);
+  const cudaStream_t s = (cudaStream_t)stream;
+  const adz::DGrid& D = h->dg;
+  const size_t fb = field_bytes(prec);
+  if (ensure(&h->d_uvw, &h->uvw_bytes, 3 * fb * (size_t)D.nij * D.nk) != ADZC_OK ||
+      ensure(&h->d_wdep, &h->wdep_bytes, fb * (size_t)D.ni * D.nj * D.nk) != ADZC_OK)
+    return fail(ADZC_ERR_ALLOC);
+  ADZ_CK(dispatch_prepare(prec, D, uu_ext, vv_ext, ww_ext, h->d_uvw, s));
+  adz::TrajArgs a{};
+  a.uvw_d = h->d_uvw;
+  a.ut0 = ut0;
+  a.vt0 = vt0;
+  a.zdt0 = zdt0;
+  a.pxyzm = (float*)pxyzm;
+  a.wpxyz = wpxyz;
+  a.wdep = h->d_wdep;
+  a.niter = niter > 0 ? niter : h->niter;
+  a.cold = h->cold;
+  a.k00 = (D.k0 > 1) ? 1 : D.k0m;  // B/adz_traject.F90:63-64
+  a.dt = dt_split(h->g, dt);
+  ADZ_CK(dispatch_traject(prec, D, a, s));
+  h->niter = std::max(1, h->g.itraj);  // B/adz_traject.F90:120
+  h->cold = 0;
+  h->last_prec = prec;
+  h->wpxyz = wpxyz;
+  h->pxyzm = (const float*)pxyzm;
+  h->zdt0 = zdt0;
+  h->dt = a.dt;
+  return ADZC_OK;
+}
+
+extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const void* const* srcs, void* const* dsts,
+                           const int* mono, void* const* lin, void* const* mn, void* const* mx, void* stream) {
+  if (!h || !check_prec(prec) || set < 0 || set > 3 || nfields < 0 || (nfields > 0 && (!srcs || !dsts)))
+    return fail(ADZC_ERR_ARG);
+  if (h->last_prec != prec || !h->wpxyz) return fail(ADZC_ERR_ARG);
+  const adzc_info& I = h->info;
+  const adz::DGrid& D = h->dg;
+  int i0, i1, j0, j1, k0;
+  switch (set) {
+    case ADZC_SET_Q: i0 = I.i0; i1 = I.in; j0 = I.j0; j1 = I.jn; k0 = I.k0; break;
+    case ADZC_SET_U: i0 = I.i0u; i1 = I.inu; j0 = I.j0; j1 = I.jn; k0 = I.k0; break;
+    case ADZC_SET_V: i0 = I.i0; i1 = I.in; j0 = I.j0v; j1 = I.jnv; k0 = I.k0; break;
+    default: i0 = I.i0; i1 = I.in; j0 = I.j0; j1 = I.jn; k0 = I.k0t; break;
+  }
+  const int nx = i1 - i0 + 1, ny = j1 - j0 + 1, nz = D.nk - k0 + 1;
+  if (nx <= 0 || ny <= 0 || nz <= 0 || nfields == 0) return ADZC_OK;
+  adz::SetArgs a{};
+  a.wpxyz = h->wpxyz;
+  a.pxyzm = h->pxyzm;
+  a.wdep = h->d_wdep;
+  a.zdt0 = h->zdt0;
+  a.dt = h->dt;
+  a.k00 = std::max(I.k0t - 1, 1);  // B/adz_interp_traj.F90:39-40
+  if (h->g.bc_lam_flux != 0 && I.k0 > 1) a.k00 = 1;
+  for (int q0 = 0; q0 < nfields; q0 += adz::kMaxFields) {
+    adz::FieldPtrs fp{};
+    fp.nf = std::min(adz::kMaxFields, nfields - q0);
+    for (int q = 0; q < fp.nf; q++) {
+      const int f = q0 + q;
+      if (!srcs[f] || !dsts[f]) return fail(ADZC_ERR_ARG);
+      fp.src[q] = srcs[f];
+      fp.dst[q] = dsts[f];
+      const int mv = mono ? mono[f] : 0;
+      if (mv != 0) fp.mono_mask |= 1u << q;
+      if (mv == 1) fp.clip_mask |= 1u << q;
+      fp.lin[q] = lin ? lin[f] : nullptr;
+      fp.mn[q] = mn ? mn[f] : nullptr;
+      fp.mx[q] = mx ? mx[f] : nullptr;
+    }
+    ADZ_CK(dispatch_set(prec, D, set, i0, nx, j0, ny, k0, nz, a, fp, (cudaStream_t)stream));
+  }
+  return ADZC_OK;
+}
+
+extern "C" int adzc_status(adzc_handle* h, int reset, void* stream) {
+  if (!h) return fail(ADZC_ERR_ARG);
+  const cudaStream_t s = (cudaStream_t)stream;
+  ADZ_CK(cudaStreamSynchronize(s));
+  int bits = 0;
+  ADZ_CK(cudaMemcpy(&bits, h->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (reset) ADZ_CK(cudaMemset(h->d_status, 0, sizeof(int)));
+  if (bits & adz::kErrHalo) return ADZC_ERR_HALO;
+  if (bits & adz::kErrNonFinite) return ADZC_ERR_NONFINITE;
+  if (bits & adz::kErrTimeout) return ADZC_ERR_TIMEOUT;
+  return ADZC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Level A: the reference ABI with host pointers
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Staging {
+  std::mutex mu;
+  cudaStream_t stream = nullptr;
+  int device = -1;
+  void* buf = nullptr;
+  size_t cap = 0;
+};
+Staging& staging() {
+  static Staging s;
+  return s;
+}
+
+// corner offset the kernel will use for an FP32 position (same arithmetic as
+// the device coef_f32pos) and the stencil extent beyond it
+void corner_f32(const adzc_ztab* lv, const pxpypz& p, long long* lo, long long* hi) {
+  const double px = p.px, py = p.py, pz = p.pz;
+  int ix = (int)px + lv->offi;
+  int iy = (int)py + lv->offj;
+  int iz = (int)pz;
+  if (iz < 1) iz = 1;
+  if (iz > lv->nk - 1) iz = lv->nk - 1;
+  long long ijk = (long long)(ix - 2) + (long long)(iy - 2) * lv->ni + (long long)(iz - 1) * lv->ni * lv->nj;
+  const int iz0 = iz - 1;
+  const bool zl = (iz0 < 1 || iz0 > lv->nk - 3);
+  const long long nij = (long long)lv->ni * lv->nj;
+  if (!zl) ijk -= nij;
+  *lo = ijk;
+  *hi = ijk + 3 + 3LL * lv->ni + (zl ? nij : 3 * nij);
+}
+
+// Stage the touched part of each source (elements [lo, hi] per field, in
+// units of ``comp`` floats) plus positions; returns device base pointers
+// already shifted so that base[off] addresses what f[off] addresses.
+int stage_inputs(const adzc_ztab* lv, int comp, const float* const* fs, int m, const pxpypz* pos, int n,
+                 size_t out_floats, std::vector<const void*>* dbase, void** dpos, float** dout) {
+  Staging& S = staging();
+  int dev = 0;
+  ADZ_CK(cudaGetDevice(&dev));
+  if (S.stream == nullptr || S.device != dev) {
+    if (S.stream) cudaStreamDestroy(S.stream);
+    cudaFree(S.buf);
+    S.buf = nullptr;
+    S.cap = 0;
+    ADZ_CK(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
+    S.device = dev;
+  }
+  long long lo = (1LL << 62), hi = -(1LL << 62);
+  for (int j = 0; j < n; j++) {
+    long long a, b;
+    corner_f32(lv, pos[j], &a, &b);
+    lo = std::min(lo, a);
+    hi = std::max(hi, b);
+  }
+  const size_t span = (size_t)(hi - lo + 1) * comp;
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t need = al(sizeof(pxpypz) * n) + m * al(sizeof(float) * span) + al(sizeof(float) * out_floats);
+  if (S.cap < need) {
+    cudaFree(S.buf);
+    S.buf = nullptr;
+    S.cap = 0;
+    if (cudaMalloc(&S.buf, need) != cudaSuccess) return fail(ADZC_ERR_ALLOC);
+    S.cap = need;
+  }
+  char* p = (char*)S.buf;
+  *dpos = p;
+  ADZ_CK(cudaMemcpyAsync(p, pos, sizeof(pxpypz) * n, cudaMemcpyHostToDevice, S.stream));
+  p += al(sizeof(pxpypz) * n);
+  dbase->clear();
+  for (int q = 0; q < m; q++) {
+    ADZ_CK(cudaMemcpyAsync(p, fs[q] + lo * comp, sizeof(float) * span, cudaMemcpyHostToDevice, S.stream));
+    dbase->push_back((const float*)p - lo * comp);
+    p += al(sizeof(float) * span);
+  }
+  *dout = (float*)p;
+  return ADZC_OK;
+}
+
+void level_a(int kind, float* d, float* l, float* mi, float* ma, float** dp, const float* const* fs, pxpypz* pxyz,
+             ztab* lv, int n, int m, int layout /*0 m_n, 1 n_m, 2 p*/) {
+  if (!lv || n <= 0 || m <= 0 || !fs || !pxyz) {
+    if (n > 0) fail(ADZC_ERR_ARG);
+    return;
+  }
+  Staging& S = staging();
+  std::lock_guard<std::mutex> lock(S.mu);
+  const int comp = (kind == 2) ? 3 : 1;
+  const int nout = (kind == 1) ? 4 : 1;
+  const size_t out_floats = (size_t)nout * m * n * comp;
+  std::vector<const void*> base;
+  void* dpos = nullptr;
+  float* dout = nullptr;
+  if (stage_inputs(lv, comp, fs, (kind == 2) ? 1 : m, pxyz, n, out_floats, &base, &dpos, &dout) != ADZC_OK) return;
+  const adz::DZtab t = lv->dev();
+  int st;
+  if (kind == 2) {
+    adz::FieldPtrs fp{};
+    fp.src[0] = base[0];
+    fp.dst[0] = dout;
+    fp.nf = 1;
+    fp.ostride = 3;
+    st = dispatch_pos(ADZC_REF32, t, 2, n, dpos, fp, S.stream) == cudaSuccess ? ADZC_OK : ADZC_ERR_CUDA;
+  } else {
+    st = run_interp(lv, ADZC_REF32, kind, dout, dout + (size_t)m * n, dout + 2 * (size_t)m * n,
+                    dout + 3 * (size_t)m * n, base.data(), dpos, n, m, 0, S.stream);
+  }
+  if (st != ADZC_OK) {
+    fail(st);
+    return;
+  }
+  std::vector<float> host(out_floats);
+  if (cudaMemcpyAsync(host.data(), dout, sizeof(float) * out_floats, cudaMemcpyDeviceToHost, S.stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(S.stream) != cudaSuccess) {
+    fail(ADZC_ERR_CUDA);
+    return;
+  }
+  if (kind == 2) {
+    std::memcpy(d, host.data(), sizeof(float) * 3 * n);
+    return;
+  }
+  float* outs[4] = {d, l, mi, ma};
+  for (int o = 0; o < nout; o++) {
+    const float* src = host.data() + (size_t)o * m * n;
+    for (int q = 0; q < m; q++) {
+      const float* row = src + (size_t)q * n;
+      if (layout == 0) {
+        std::memcpy(outs[o] + (size_t)q * n, row, sizeof(float) * n);
+      } else if (layout == 1) {
+        float* dst = outs[o];
+        for (int j = 0; j < n; j++) dst[(size_t)j * m + q] = row[j];
+      } else {
+        std::memcpy(dp[q], row, sizeof(float) * n);
+      }
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" ztab* Vsearch_setup_plus(double* levels, int nk, int ni, int nj, int offseti, int offsetj) {
+  ztab* lv = nullptr;
+  if (adzc_ztab_create(levels, nk, ni, nj, offseti, offsetj, &lv) != ADZC_OK) return nullptr;
+  return lv;
+}
+
+extern "C" ztab* Vsearch_setup(double* levels, int nk, int ni, int nj) {
+  return Vsearch_setup_plus(levels, nk, ni, nj, 0, 0);
+}
+
+extern "C" void Tricublin_zyx1_n(float* d, float* f1, pxpypz* pxyz, ztab* lv, int n) {
+  const float* fs[1] = {f1};
+  level_a(0, d, nullptr, nullptr, nullptr, nullptr, fs, pxyz, lv, n, 1, 0);
+}
+extern "C" void Tricublin_zyx1_n_m(float* d, float** fs, pxpypz* pxyz, ztab* lv, int n, int m) {
+  level_a(0, d, nullptr, nullptr, nullptr, nullptr, fs, pxyz, lv, n, m, 1);
+}
+extern "C" void Tricublin_zyx1_m_n(float* dm, float** fs, pxpypz* pxyz, ztab* lv, int n, int m) {
+  level_a(0, dm, nullptr, nullptr, nullptr, nullptr, fs, pxyz, lv, n, m, 0);
+}
+extern "C" void Tricublin_zyx1_p(float** dp, float** fs, pxpypz* pxyz, ztab* lv, int n, int m) {
+  level_a(0, nullptr, nullptr, nullptr, nullptr, dp, fs, pxyz, lv, n, m, 2);
+}
+extern "C" void Tricublin_mono_zyx_n(float* d, float* l, float* mi, float* ma, float* f, pxpypz* pxyz, ztab* lv,
+                                     int n) {
+  const float* fs[1] = {f};
+  level_a(1, d, l, mi, ma, nullptr, fs, pxyz, lv, n, 1, 0);
+}
+extern "C" void Tricublin_mono_zyx_n_m(float* d, float* l, float* mi, float* ma, float** fs, pxpypz* pxyz, ztab* lv,
+                                       int n, int m) {
+  level_a(1, d, l, mi, ma, nullptr, fs, pxyz, lv, n, m, 1);
+}
+extern "C" void Tricublin_mono_zyx_m_n(float* d, float* l, float* mi, float* ma, float** fs, pxpypz* pxyz, ztab* lv,
+                                       int n, int m) {
+  level_a(1, d, l, mi, ma, nullptr, fs, pxyz, lv, n, m, 0);
+}
+extern "C" void Tricublin_zyx3_n(float* d, float* f3, pxpypz* pxyz, ztab* lv, int n) {
+  const float* fs[1] = {f3};
+  level_a(2, d, nullptr, nullptr, nullptr, nullptr, fs, pxyz, lv, n, 1, 0);
+}

@@ -1,0 +1,505 @@
+// Kernels of the advection step, templated on the precision mode.
+//
+//   k_prepare      adz_prepareWinds departure winds (B/adz_prepareWinds.F90:16-107)
+//   k_inittraj     adz_inittraj (B/adz_inittraj.F90:25-37)
+//   k_traject      all Adz_niter fixed-point iterations of one arrival point in
+//                  one thread, arrival winds formed in registers
+//                  (B/adz_traject.F90:63-108, B/adz_prepareWinds.F90:40-97)
+//   k_tricub_set   position of a set derived in registers (B/adz_interp_traj.F90)
+//                  then the multi-field interpolation, mono bounds and clip
+//                  (B/adz_interp_hlt.F90:98-182, B/adz_post_tr.F90:81-94)
+//   k_interp_pos   the reference interpolators on explicit positions
+//                  (B/turbo_tricublin.c:752-1312)
+// B/ = src/gemdyn/src/base/.
+#pragma once
+#include "adz_device.cuh"
+
+namespace adz {
+
+__device__ __forceinline__ long long ext_index(const DGrid& g, int i, int j, int k) {
+  return (long long)(i - g.lminx) + (long long)(j - g.lminy) * g.nit + (long long)(k - 1) * g.nij;
+}
+__device__ __forceinline__ long long arr_index(const DGrid& g, int i, int j, int k) {
+  return (long long)(i - 1) + (long long)(j - 1) * g.ni + (long long)(k - 1) * g.ni * g.nj;
+}
+__device__ __forceinline__ long long wp_index(const DGrid& g, int i, int j, int k, int c) {
+  const long long nx = g.ni + 4, ny = g.nj + 4;
+  return (long long)(i + 1) + (long long)(j + 1) * nx + (long long)(k - 1) * nx * ny +
+         (long long)(c - 1) * nx * ny * g.nk;
+}
+__device__ __forceinline__ double dmin_(double a, double b) { return a < b ? a : b; }
+__device__ __forceinline__ double dmax_(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ int imin_(int a, int b) { return a < b ? a : b; }
+__device__ __forceinline__ int imax_(int a, int b) { return a > b ? a : b; }
+
+// ---------------------------------------------------------------------------
+template <int PREC>
+__global__ void __launch_bounds__(256) k_prepare(DGrid g, const typename Types<PREC>::F* __restrict__ uu,
+                                                 const typename Types<PREC>::F* __restrict__ vv,
+                                                 const typename Types<PREC>::F* __restrict__ ww,
+                                                 typename Types<PREC>::F* __restrict__ uvw_d) {
+  using F = typename Types<PREC>::F;
+  const long long n = g.nij * g.nk;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(e / g.nij) + 1;
+    const long long r = e - (long long)(k - 1) * g.nij;
+    const int jj = (int)(r / g.nit);
+    const double cyj = __ldg(g.cy + jj);
+    const double* vw = g.vw;
+    const int nk = g.nk;
+    uvw_d[3 * e + 0] = (F)(g.inv_rayt * (double)uu[e] * cyj);
+    uvw_d[3 * e + 1] = (F)(g.inv_rayt * (double)vv[e]);
+    double w;
+    if (k == 1) {
+      w = g.vw5 * (double)ww[e];
+    } else if (k == nk) {
+      w = g.vw6 * (double)ww[e - g.nij];
+    } else {
+      const int km2 = imax_(1, k - 2);
+      const double wx = (k >= 3) ? __ldg(vw + 0 * (nk + 1) + k) : 0.0;
+      w = wx * (double)ww[r + (long long)(km2 - 1) * g.nij] + __ldg(vw + 1 * (nk + 1) + k) * (double)ww[e - g.nij] +
+          __ldg(vw + 2 * (nk + 1) + k) * (double)ww[e] + __ldg(vw + 3 * (nk + 1) + k) * (double)ww[e + g.nij];
+    }
+    uvw_d[3 * e + 2] = (F)w;
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <int PREC>
+__global__ void __launch_bounds__(256) k_inittraj(DGrid g, float* __restrict__ pxyzm, double* __restrict__ wpxyz) {
+  const long long n = (long long)g.ni * g.nj * (g.nk - g.k0m + 1);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.ni) + 1;
+    const int j = (int)((t / g.ni) % g.nj) + 1;
+    const int k = (int)(t / ((long long)g.ni * g.nj)) + g.k0m;
+    const float x = (float)(i + g.i0g - 1), y = (float)(j + g.j0g - 1), z = (float)k;
+    if (PREC == kRef32 && pxyzm) {
+      const long long a = arr_index(g, i, j, k);
+      pxyzm[3 * a] = x;
+      pxyzm[3 * a + 1] = y;
+      pxyzm[3 * a + 2] = z;
+    }
+    wpxyz[wp_index(g, i, j, k, 1)] = x;
+    wpxyz[wp_index(g, i, j, k, 2)] = y;
+    wpxyz[wp_index(g, i, j, k, 3)] = z;
+  }
+}
+
+// vertical index search of adz_traject.F90:85-90 / zindx (adz_interp_traj.F90:193-203)
+__device__ __forceinline__ int vsearch(double zv, const double* z, double ovdz, const int* tab, int pnz, double sig,
+                                       int nk) {
+  int kk1 = __double2int_rz((zv - __ldg(z)) * ovdz + 1.0);
+  kk1 = imin_(imax_(1, kk1), pnz);
+  kk1 = __ldg(tab + kk1 - 1);
+  if (sig * zv > sig * __ldg(z + imin_(kk1 + 1, nk + 1))) kk1 = kk1 + 1;
+  if (sig * zv < sig * __ldg(z + kk1)) kk1 = kk1 - 1;
+  return kk1;
+}
+
+__device__ __forceinline__ double zindx_t(const DGrid& g, double posz) {
+  posz = dmin_(dmax_(posz, g.zmin), g.zmax);
+  int kk1 = vsearch(posz, g.zt, g.ovdzt, g.search_t, g.pnz_t, g.sig, g.nk);
+  kk1 = imin_(g.nk + 1, imax_(0, kk1));
+  const int nb = imax_(imin_(kk1, g.nk - 1), 1);
+  return (posz - __ldg(g.zt + nb)) * __ldg(g.odelz_t + nb) + (double)nb;
+}
+
+// stencil of a cell (ix local, x as in the ext array) stays inside the array
+__device__ __forceinline__ bool stencil_ok(const DGrid& g, int off) {
+  // off = corner offset relative to cell (1,1,1): recover corner (i,j) in ext coords
+  const long long e = (long long)off + ext_index(g, 1, 1, 1);
+  const long long plane = g.nij;
+  long long k = e >= 0 ? e / plane : -1;
+  const long long r = e - k * plane;
+  const int j = (int)(r / g.nit), i = (int)(r - (long long)j * g.nit);
+  return e >= 0 && k >= 0 && k <= g.nk - 1 && i >= 0 && i + 3 < g.nit && j >= 0 && j + 3 < g.njt;
+}
+
+// ---------------------------------------------------------------------------
+template <int PREC>
+__global__ void __launch_bounds__(128) k_traject(DGrid g, TrajArgs a) {
+  using F = typename Types<PREC>::F;
+  const long long nplane = (long long)g.ni * g.nj;
+  const long long n = nplane * (g.nk - a.k00 + 1);
+  const F* __restrict__ uvw = (const F*)a.uvw_d;
+  const F* __restrict__ ut0 = (const F*)a.ut0;
+  const F* __restrict__ vt0 = (const F*)a.vt0;
+  const F* __restrict__ zdt0 = (const F*)a.zdt0;
+  const long long e111 = ext_index(g, 1, 1, 1);
+  const F* f3 = uvw + 3 * e111;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.ni) + 1;
+    const int j = (int)((t / g.ni) % g.nj) + 1;
+    const int k = (int)(t / nplane) + a.k00;
+    const int nk = g.nk;
+    const long long e = ext_index(g, i, j, k);
+    const long long ar = arr_index(g, i, j, k);
+    // arrival winds (adz_prepareWinds.F90:40-97); Fortran forms the two sums in ``real``
+    const double alpha1 = -1.0 / 16.0, alpha2 = 9.0 / 16.0;
+    const double cyj = __ldg(g.cy + (j - g.lminy));
+    double ua, va, wa;
+    {
+      const F u1 = ut0[e - 2] + ut0[e + 1], u2 = ut0[e] + ut0[e - 1];
+      const F v1 = vt0[e - 2 * g.nit] + vt0[e + g.nit], v2 = vt0[e] + vt0[e - g.nit];
+      double uad = ((double)u1 * alpha1 + (double)u2 * alpha2) * g.inv_rayt * cyj;
+      double vad = ((double)v1 * alpha1 + (double)v2 * alpha2) * g.inv_rayt;
+      double wad;
+      if (k == 1) {
+        wad = g.vw5 * (double)zdt0[e];
+      } else if (k == nk) {
+        wad = g.vw6 * (double)zdt0[e - g.nij];
+      } else {
+        const int km2 = imax_(1, k - 2);
+        const double wx = (k >= 3) ? __ldg(g.vw + 0 * (nk + 1) + k) : 0.0;
+        wad = wx * (double)zdt0[e - (long long)(k - km2) * g.nij] + __ldg(g.vw + 1 * (nk + 1) + k) * (double)zdt0[e - g.nij] +
+              __ldg(g.vw + 2 * (nk + 1) + k) * (double)zdt0[e] + __ldg(g.vw + 3 * (nk + 1) + k) * (double)zdt0[e + g.nij];
+      }
+      if (PREC == kFp64) {
+        ua = uad; va = vad; wa = wad;
+      } else if (PREC == kRef32) {  // Adz_uu_arr etc. are ``real``
+        ua = (double)(float)uad; va = (double)(float)vad; wa = (double)(float)wad;
+      } else {
+        ua = uad; va = vad; wa = wad;
+      }
+    }
+    // starting position
+    double px, py, pz;
+    if (a.cold) {
+      px = (double)(i + g.i0g - 1); py = (double)(j + g.j0g - 1); pz = (double)k;
+    } else if (PREC == kRef32) {
+      px = a.pxyzm[3 * ar]; py = a.pxyzm[3 * ar + 1]; pz = a.pxyzm[3 * ar + 2];
+    } else {
+      px = dmin_(dmax_(a.wpxyz[wp_index(g, i, j, k, 1)], g.imnx), g.imxx);
+      py = dmin_(dmax_(a.wpxyz[wp_index(g, i, j, k, 2)], g.imny), g.imxy);
+      pz = a.wpxyz[wp_index(g, i, j, k, 3)];
+    }
+    double xm = 0.0, ym = 0.0, w3 = 0.0, wlast = 0.0;
+    bool bad = false, nonfinite = false;
+    for (int it = 0; it < a.niter; it++) {
+      double ud, vd, wd;
+      int off;
+      if (PREC == kMixed) {
+        WF w;
+        coef_mixed(w, px, py, pz, g.tab_m);
+        off = w.off;
+        if (!stencil_ok(g, off)) { bad = true; break; }
+        float o[3];
+        interp3_mixed((const float*)f3 + 3LL * off, w, g.tab_m.ni, g.tab_m.nij, o);
+        ud = o[0]; vd = o[1]; wd = o[2];
+      } else {
+        double c[20];
+        int zl;
+        if (PREC == kRef32) zl = coef_f32pos(c, off, (float)px, (float)py, (float)pz, g.tab_m);
+        else zl = coef_f64pos(c, off, px, py, pz, g.tab_m);
+        if (!stencil_ok(g, off)) { bad = true; break; }
+        double o[3];
+        interp3_exact<F>(f3 + 3LL * off, c, g.tab_m.ni, g.tab_m.nij, zl, o);
+        if (PREC == kRef32) {  // Tricublin_zyx3_n returns ``real``
+          ud = (double)(float)o[0]; vd = (double)(float)o[1]; wd = (double)(float)o[2];
+        } else {
+          ud = o[0]; vd = o[1]; wd = o[2];
+        }
+      }
+      xm = (double)(i + g.i0g - 1) - (a.dt.dtD * ud + a.dt.dtA * ua) * g.inv_hx;
+      ym = (double)(j + g.j0g - 1) - (a.dt.dtD * vd + a.dt.dtA * va) * g.inv_hy;
+      const double pos = __ldg(g.zm + k) - a.dt.dtzD * wd - a.dt.dtzA * wa;
+      const double zmv = dmin_(dmax_(pos, g.zmin), g.zmax);
+      int kk1 = vsearch(zmv, g.zm, g.ovdzm, g.search_m, g.pnz_m, g.sig, nk);
+      kk1 = imin_(nk + 1, imax_(0, kk1));
+      const int nb = imax_(imin_(kk1, nk - 1), 1);
+      w3 = (zmv - __ldg(g.zm + nb)) * __ldg(g.odelz_m + nb) + (double)nb;
+      wlast = wd;
+      const double cx = dmin_(dmax_(xm, g.imnx), g.imxx);
+      const double cyv = dmin_(dmax_(ym, g.imny), g.imxy);
+      if (PREC == kRef32) {
+        px = (float)cx; py = (float)cyv; pz = (float)w3;
+      } else {
+        px = cx; py = cyv; pz = w3;
+      }
+      if (!isfinite(xm) || !isfinite(ym) || !isfinite(w3)) { nonfinite = true; break; }
+    }
+    if (bad || nonfinite) {
+      raise_status(g.status, bad ? kErrHalo : kErrNonFinite);
+      continue;
+    }
+    if (a.niter > 0) {
+      a.wpxyz[wp_index(g, i, j, k, 1)] = xm;
+      a.wpxyz[wp_index(g, i, j, k, 2)] = ym;
+      a.wpxyz[wp_index(g, i, j, k, 3)] = w3;
+      if (PREC == kRef32) {
+        a.pxyzm[3 * ar] = (float)px;
+        a.pxyzm[3 * ar + 1] = (float)py;
+        a.pxyzm[3 * ar + 2] = (float)pz;
+      }
+      ((F*)a.wdep)[ar] = (F)wlast;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// position of arrival point (i,j,k) of a set, adz_interp_traj.F90:45-187
+template <int PREC>
+__device__ __forceinline__ void set_position(const DGrid& g, const SetArgs& a, int set, int i, int j, int k, double& px,
+                                             double& py, double& pz) {
+  using F = typename Types<PREC>::F;
+  const double aa = -0.0625, bb = 0.5625, half = 0.5;
+  const double* W = a.wpxyz;
+#define WPX(ii, jj, kk, cc) W[wp_index(g, ii, jj, kk, cc)]
+  if (set == 0) {
+    if (PREC == kRef32) {
+      const long long ar = arr_index(g, i, j, k);
+      px = a.pxyzm[3 * ar]; py = a.pxyzm[3 * ar + 1]; pz = a.pxyzm[3 * ar + 2];
+    } else {
+      px = dmin_(dmax_(WPX(i, j, k, 1), g.imnx), g.imxx);
+      py = dmin_(dmax_(WPX(i, j, k, 2), g.imny), g.imxy);
+      pz = WPX(i, j, k, 3);
+    }
+    return;
+  }
+  if (set == 1 || set == 2) {
+    const int di = (set == 1), dj = (set == 2);
+    double c[3];
+#pragma unroll
+    for (int q = 1; q <= 3; q++)
+      c[q - 1] = aa * (WPX(i - di, j - dj, k, q) + WPX(i + 2 * di, j + 2 * dj, k, q)) +
+                 bb * (WPX(i, j, k, q) + WPX(i + di, j + dj, k, q));
+    if (set == 1) c[0] = c[0] - 0.5;
+    else c[1] = c[1] - 0.5;
+    px = dmin_(dmax_(c[0], g.imnx), g.imxx);
+    py = dmin_(dmax_(c[1], g.imny), g.imxy);
+    pz = dmin_(dmax_(c[2], 0.0), (double)(g.nk + 1));
+    return;
+  }
+  // set T: Adz_pb
+  const F* wd = (const F*)a.wdep;
+  const F* zd = (const F*)a.zdt0;
+  const int nk = g.nk;
+  const long long e = ext_index(g, i, j, k);
+#define WD(kk) wd[arr_index(g, i, j, kk)]
+  double xt, yt, ztv;
+  if (k >= imax_(a.k00, 2) && k <= nk - 2) {
+    const double* vw = g.vw;
+    const double w1 = __ldg(vw + 4 * (nk + 1) + k), w2 = __ldg(vw + 5 * (nk + 1) + k);
+    const double w3 = __ldg(vw + 6 * (nk + 1) + k), w4 = __ldg(vw + 7 * (nk + 1) + k);
+    xt = w1 * WPX(i, j, k - 1, 1) + w2 * WPX(i, j, k, 1) + w3 * WPX(i, j, k + 1, 1) + w4 * WPX(i, j, k + 2, 1);
+    yt = w1 * WPX(i, j, k - 1, 2) + w2 * WPX(i, j, k, 2) + w3 * WPX(i, j, k + 1, 2) + w4 * WPX(i, j, k + 2, 2);
+    const double wdt = w1 * (double)WD(k - 1) + w2 * (double)WD(k) + w3 * (double)WD(k + 1) + w4 * (double)WD(k + 2);
+    ztv = __ldg(g.zt + k) - a.dt.dtzD * wdt - a.dt.dtzA * (double)zd[e];
+  } else if (k == nk - 1) {
+    xt = (WPX(i, j, k, 1) + WPX(i, j, k + 1, 1)) * half;
+    yt = (WPX(i, j, k, 2) + WPX(i, j, k + 1, 2)) * half;
+    const F ws = WD(k) + WD(k + 1);
+    const double wdt = (double)ws * half;
+    ztv = __ldg(g.zt + k) - a.dt.dtzD * wdt - a.dt.dtzA * (double)zd[e];
+  } else if (k == nk) {
+    if (g.slt_winds && a.uslt && a.vslt) {
+      const long long a2 = (long long)(i - 1) + (long long)(j - 1) * g.ni;
+      xt = (double)(i + g.i0g - 1) -
+           g.inv_rayt * a.dt.dt * (double)((const F*)a.uslt)[a2] * __ldg(g.cy + (j - g.lminy)) * g.inv_hx;
+      yt = (double)(j + g.j0g - 1) - g.inv_rayt * a.dt.dt * (double)((const F*)a.vslt)[a2] * g.inv_hy;
+    } else {
+      xt = g.wp * WPX(i, j, k, 1) + g.wm * WPX(i, j, k - 1, 1);
+      yt = g.wp * WPX(i, j, k, 2) + g.wm * WPX(i, j, k - 1, 2);
+    }
+    const F ws = WD(k - 1) + WD(k);
+    const double wdt = (double)ws * half;
+    ztv = __ldg(g.zt + k) - g.ww * (a.dt.dtzD * wdt + a.dt.dtzA * (double)zd[e - g.nij]);
+  } else {  // k == 1 (k00 == 1)
+    xt = (WPX(i, j, 1, 1) + WPX(i, j, 2, 1)) * half;
+    yt = (WPX(i, j, 1, 2) + WPX(i, j, 2, 2)) * half;
+    const F ws = WD(1) + WD(2);
+    const double wdt = (double)ws * half;
+    ztv = __ldg(g.zt + 1) - a.dt.dtzD * wdt - a.dt.dtzA * (double)zd[e];
+  }
+#undef WD
+#undef WPX
+  px = dmin_(dmax_(xt, g.imnx), g.imxx);
+  py = dmin_(dmax_(yt, g.imny), g.imxy);
+  pz = zindx_t(g, ztv);
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(128) k_tricub_set(DGrid g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
+                                                    SetArgs a, FieldPtrs fp) {
+  using F = typename Types<PREC>::F;
+  const long long nplane = (long long)nx * ny;
+  const long long n = nplane * nz;
+  const DZtab& lv = (set == 3) ? g.tab_t : g.tab_m;
+  const long long e111 = ext_index(g, 1, 1, 1);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nx) + i0;
+    const int j = (int)((t / nx) % ny) + j0;
+    const int k = (int)(t / nplane) + k0;
+    double px, py, pz;
+    set_position<PREC>(g, a, set, i, j, k, px, py, pz);
+    const long long e = ext_index(g, i, j, k);
+    if (PREC == kMixed) {
+      WF w;
+      coef_mixed(w, px, py, pz, lv);
+      if (!stencil_ok(g, w.off)) { raise_status(g.status, kErrHalo); continue; }
+      for (int q = 0; q < fp.nf; q++) {
+        const float* f = (const float*)fp.src[q] + e111 + w.off;
+        if ((fp.mono_mask >> q) & 1u) {
+          float d, lin, mn, mx;
+          interp_mono_mixed(f, w, lv.ni, lv.nij, d, lin, mn, mx);
+          if ((fp.clip_mask >> q) & 1u) d = fmaxf(mn, fminf(mx, d));
+          if (fp.lin[q]) ((float*)fp.lin[q])[e] = fmaxf(mn, fminf(mx, lin));
+          if (fp.mn[q]) ((float*)fp.mn[q])[e] = mn;
+          if (fp.mx[q]) ((float*)fp.mx[q])[e] = mx;
+          ((float*)fp.dst[q])[e] = d;
+        } else {
+          ((float*)fp.dst[q])[e] = interp1_mixed(f, w, lv.ni, lv.nij);
+        }
+      }
+    } else {
+      double c[20];
+      int off, zl;
+      if (PREC == kRef32) zl = coef_f32pos(c, off, (float)px, (float)py, (float)pz, lv);
+      else zl = coef_f64pos(c, off, px, py, pz, lv);
+      if (!stencil_ok(g, off)) { raise_status(g.status, kErrHalo); continue; }
+      for (int q = 0; q < fp.nf; q++) {
+        const F* f = (const F*)fp.src[q] + e111 + off;
+        if ((fp.mono_mask >> q) & 1u) {
+          double d, lin, mn, mx;
+          interp_mono_exact<F>(f, c, lv.ni, lv.nij, zl, fp.box222 != 0, d, lin, mn, mx);
+          F df = (F)d, lf = (F)lin, mnf = (F)mn, mxf = (F)mx;
+          // Adz_post lin/min/max (adz_interp_hlt.F90:156-158), clip of adz_post_tr.F90:86-89
+          if ((fp.clip_mask >> q) & 1u) df = (mnf > ((mxf < df) ? mxf : df)) ? mnf : ((mxf < df) ? mxf : df);
+          if (fp.lin[q]) ((F*)fp.lin[q])[e] = (mnf > ((mxf < lf) ? mxf : lf)) ? mnf : ((mxf < lf) ? mxf : lf);
+          if (fp.mn[q]) ((F*)fp.mn[q])[e] = mnf;
+          if (fp.mx[q]) ((F*)fp.mx[q])[e] = mxf;
+          ((F*)fp.dst[q])[e] = df;
+        } else {
+          ((F*)fp.dst[q])[e] = (F)interp1_exact<F>(f, c, lv.ni, lv.nij, zl);
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// explicit positions; kind 0 = cubic, 1 = mono, 2 = 3-component
+template <int PREC, int KIND>
+__global__ void __launch_bounds__(128) k_interp_pos(DZtab lv, int n, const void* __restrict__ pos, FieldPtrs fp) {
+  using F = typename Types<PREC>::F;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const long long o = (long long)t * fp.ostride;
+    if (PREC == kMixed) {
+      const double* p = (const double*)pos + 3LL * t;
+      WF w;
+      coef_mixed(w, p[0], p[1], p[2], lv);
+      if (KIND == 2) {
+        float r[3];
+        interp3_mixed((const float*)fp.src[0] + 3LL * w.off, w, lv.ni, lv.nij, r);
+        float* d = (float*)fp.dst[0] + 3LL * t;
+        d[0] = r[0]; d[1] = r[1]; d[2] = r[2];
+      } else {
+        for (int q = 0; q < fp.nf; q++) {
+          const float* f = (const float*)fp.src[q] + w.off;
+          if (KIND == 1) {
+            float d, lin, mn, mx;
+            interp_mono_mixed(f, w, lv.ni, lv.nij, d, lin, mn, mx);
+            ((float*)fp.dst[q])[o] = d;
+            ((float*)fp.lin[q])[o] = lin;
+            ((float*)fp.mn[q])[o] = mn;
+            ((float*)fp.mx[q])[o] = mx;
+          } else {
+            ((float*)fp.dst[q])[o] = interp1_mixed(f, w, lv.ni, lv.nij);
+          }
+        }
+      }
+    } else {
+      double c[20];
+      int off, zl;
+      if (PREC == kRef32) {
+        const float* p = (const float*)pos + 3LL * t;
+        zl = coef_f32pos(c, off, p[0], p[1], p[2], lv);
+      } else {
+        const double* p = (const double*)pos + 3LL * t;
+        zl = coef_f64pos(c, off, p[0], p[1], p[2], lv);
+      }
+      if (KIND == 2) {
+        double r[3];
+        interp3_exact<F>((const F*)fp.src[0] + 3LL * off, c, lv.ni, lv.nij, zl, r);
+        F* d = (F*)fp.dst[0] + 3LL * t;
+        d[0] = (F)r[0]; d[1] = (F)r[1]; d[2] = (F)r[2];
+      } else {
+        for (int q = 0; q < fp.nf; q++) {
+          const F* f = (const F*)fp.src[q] + off;
+          if (KIND == 1) {
+            double d, lin, mn, mx;
+            interp_mono_exact<F>(f, c, lv.ni, lv.nij, zl, fp.box222 != 0, d, lin, mn, mx);
+            ((F*)fp.dst[q])[o] = (F)d;
+            ((F*)fp.lin[q])[o] = (F)lin;
+            ((F*)fp.mn[q])[o] = (F)mn;
+            ((F*)fp.mx[q])[o] = (F)mx;
+          } else {
+            ((F*)fp.dst[q])[o] = (F)interp1_exact<F>(f, c, lv.ni, lv.nij, zl);
+          }
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launchers (host)
+inline int grid_for(long long n, int block, int max_blocks = 148 * 64) {
+  long long b = (n + block - 1) / block;
+  if (b > max_blocks) b = max_blocks;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+template <int PREC>
+cudaError_t launch_prepare(const DGrid& g, const void* uu, const void* vv, const void* ww, void* uvw_d,
+                           cudaStream_t s) {
+  using F = typename Types<PREC>::F;
+  const long long n = g.nij * g.nk;
+  k_prepare<PREC><<<grid_for(n, 256), 256, 0, s>>>(g, (const F*)uu, (const F*)vv, (const F*)ww, (F*)uvw_d);
+  return cudaGetLastError();
+}
+
+template <int PREC>
+cudaError_t launch_inittraj(const DGrid& g, float* pxyzm, double* wpxyz, cudaStream_t s) {
+  const long long n = (long long)g.ni * g.nj * (g.nk - g.k0m + 1);
+  k_inittraj<PREC><<<grid_for(n, 256), 256, 0, s>>>(g, pxyzm, wpxyz);
+  return cudaGetLastError();
+}
+
+template <int PREC>
+cudaError_t launch_traject(const DGrid& g, const TrajArgs& a, cudaStream_t s) {
+  const long long n = (long long)g.ni * g.nj * (g.nk - a.k00 + 1);
+  k_traject<PREC><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, a);
+  return cudaGetLastError();
+}
+
+template <int PREC>
+cudaError_t launch_tricub_set(const DGrid& g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
+                              const SetArgs& a, const FieldPtrs& fp, cudaStream_t s) {
+  const long long n = (long long)nx * ny * nz;
+  if (n <= 0) return cudaSuccess;
+  k_tricub_set<PREC><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, set, i0, nx, j0, ny, k0, nz, a, fp);
+  return cudaGetLastError();
+}
+
+template <int PREC>
+cudaError_t launch_interp_pos(const DZtab& lv, int kind, int n, const void* pos, const FieldPtrs& fp,
+                              cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int b = grid_for(n, 128, 1 << 30);
+  if (kind == 0) k_interp_pos<PREC, 0><<<b, 128, 0, s>>>(lv, n, pos, fp);
+  else if (kind == 1) k_interp_pos<PREC, 1><<<b, 128, 0, s>>>(lv, n, pos, fp);
+  else k_interp_pos<PREC, 2><<<b, 128, 0, s>>>(lv, n, pos, fp);
+  return cudaGetLastError();
+}
+
+#define ADZ_INSTANTIATE(P)                                                                                         \
+  template cudaError_t launch_prepare<P>(const DGrid&, const void*, const void*, const void*, void*, cudaStream_t); \
+  template cudaError_t launch_inittraj<P>(const DGrid&, float*, double*, cudaStream_t);                            \
+  template cudaError_t launch_traject<P>(const DGrid&, const TrajArgs&, cudaStream_t);                             \
+  template cudaError_t launch_tricub_set<P>(const DGrid&, int, int, int, int, int, int, int, const SetArgs&,       \
+                                            const FieldPtrs&, cudaStream_t);                                       \
+  template cudaError_t launch_interp_pos<P>(const DZtab&, int, int, const void*, const FieldPtrs&, cudaStream_t);
+
+}  // namespace adz

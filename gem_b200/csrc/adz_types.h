@@ -1,0 +1,119 @@
+// Plain data structures shared by the kernels and the host C-ABI code
+// (no device code here, so g++ can compile the host side).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace adz {
+
+constexpr int kMaxFields = 16;  // fields per launch (more are split in chunks)
+
+enum : int { kRef32 = 0, kFp64 = 1, kMixed = 2 };
+enum : int { kErrHalo = 1 << 0, kErrNonFinite = 1 << 1, kErrTimeout = 1 << 2 };
+
+// Level descriptor (turbo_tricublin.c:164-173) plus the per-interval FP32
+// table of the mixed path: for interval iz the normalised nodes
+// u = {(z[iz-1]-z[iz])/h, 0, 1, (z[iz+2]-z[iz])/h}, h = z[iz+1]-z[iz],
+// stored as {u[0], u[3], 1/prod(u0-ud), ..., 1/prod(u3-ud), 0, 0}.
+struct DZtab {
+  const double* z;
+  const double* ocz;
+  const float* zn;
+  int ni, nj, nk, nij, offi, offj;
+};
+
+// Everything adz_set derives, as the kernels read it.
+struct DGrid {
+  int ni, nj, nk, halox, haloy, lminx, lminy, nit, njt;
+  long long nij;
+  int i0g, j0g;
+  int i0, in, j0, jn, i0u, inu, j0v, jnv, i0b, inb, j0b, jnb, k0, k0t, k0m;
+  int pnz_m, pnz_t, slt_winds;
+  double imnx, imxx, imny, imxy, sig, ovdzm, ovdzt, zmin, zmax;
+  double inv_rayt, inv_hx, inv_hy, vw5, vw6, ww, wp, wm;
+  const int* search_m;
+  const int* search_t;
+  const double* zm;       // Ver_z_8%m(0:nk+1)
+  const double* zt;       // Ver_z_8%t(0:nk+1)
+  const double* odelz_m;  // 0..nk
+  const double* odelz_t;
+  const double* vw;       // 8 x (nk+1): vw1m vw2m vw3m vw4m vw1t vw2t vw3t vw4t
+  const double* cy;       // index j - lminy
+  DZtab tab_m, tab_t;
+  int* status;
+};
+
+struct DtSplit {
+  double dtA, dtD, dtzA, dtzD, dt;
+};
+
+template <int PREC>
+struct Types;
+template <>
+struct Types<kRef32> {
+  using F = float;   // fields and winds
+  using P = float;   // stored positions
+};
+template <>
+struct Types<kFp64> {
+  using F = double;
+  using P = double;
+};
+template <>
+struct Types<kMixed> {
+  using F = float;
+  using P = double;
+};
+
+struct FieldPtrs {
+  const void* src[kMaxFields];
+  void* dst[kMaxFields];
+  void* lin[kMaxFields];
+  void* mn[kMaxFields];
+  void* mx[kMaxFields];
+  int nf;
+  unsigned mono_mask;  // bit q: field q gets bounds (and clip if clip_mask)
+  unsigned clip_mask;
+  int box222;
+  long long ostride;   // explicit-position kernels: output element stride per point
+};
+
+struct TrajArgs {
+  const void* uvw_d;  // ext, 3 interleaved
+  const void* ut0;
+  const void* vt0;
+  const void* zdt0;
+  float* pxyzm;       // REF32 state
+  double* wpxyz;
+  void* wdep;         // (ni,nj,nk) departure vertical wind of the last iteration
+  int niter, cold, k00;
+  DtSplit dt;
+};
+
+struct SetArgs {
+  const double* wpxyz;
+  const float* pxyzm;  // REF32 only
+  const void* wdep;
+  const void* zdt0;
+  const void* uslt;    // optional surface-layer winds (ni,nj)
+  const void* vslt;
+  DtSplit dt;
+  int k00;             // interp_traj k00
+};
+
+
+template <int PREC>
+cudaError_t launch_prepare(const DGrid& g, const void* uu, const void* vv, const void* ww, void* uvw_d,
+                           cudaStream_t s);
+template <int PREC>
+cudaError_t launch_inittraj(const DGrid& g, float* pxyzm, double* wpxyz, cudaStream_t s);
+template <int PREC>
+cudaError_t launch_traject(const DGrid& g, const TrajArgs& a, cudaStream_t s);
+template <int PREC>
+cudaError_t launch_tricub_set(const DGrid& g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
+                              const SetArgs& a, const FieldPtrs& fp, cudaStream_t s);
+template <int PREC>
+cudaError_t launch_interp_pos(const DZtab& lv, int kind, int n, const void* pos, const FieldPtrs& fp,
+                              cudaStream_t s);
+
+}  // namespace adz

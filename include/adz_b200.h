@@ -1,0 +1,195 @@
+/*
+ * adz_b200 — B200 (sm_100a) implementation of GEM's semi-Lagrangian advection
+ * hot path: departure-point trajectories, tricubic Lagrange interpolation of
+ * momentum and tracers, and monotone clipping.
+ *
+ * Plain C ABI: pointers, sizes and an opaque handle; no C++ or torch types.
+ * Reference paths below are relative to the GEM source tree
+ * (src/gemdyn/src/base/ is abbreviated B/).
+ *
+ * Two levels:
+ *   Level A  the reference interpolator ABI, same symbol names and argument
+ *            meaning as B/turbo_tricublin.c (bound from Fortran by
+ *            B/tricublin_f90.inc).  HOST pointers; each call stages its inputs
+ *            on the GPU and copies results back.  A Fortran program linked
+ *            against this library instead of turbo_tricublin.o runs unchanged.
+ *   Level B  device-pointer entry points for the whole adz step (the work of
+ *            B/adz_set.F90, B/adz_traject.F90, B/adz_interp_traj.F90,
+ *            B/adz_interp_hlt.F90, B/adz_post_tr.F90:81-94), stream ordered,
+ *            returning an int status.  This is the product path.
+ *
+ * Precisions (argument ``prec``):
+ *   ADZC_REF32  the reference's own arithmetic: FP32 fields, winds and stored
+ *               positions; FP64 coefficients and sums; results bit-identical
+ *               to the reference's AVX2 build.
+ *   ADZC_FP64   FP64 fields, winds and positions throughout (plain FP64 drop-in).
+ *   ADZC_MIXED  FP32 fields and winds, FP64 positions, cell index and cell
+ *               offset; FP32 stencil weights and sums.
+ * In every precision the cell index of a position is the one the reference
+ * selects: the position rounded to FP32 and truncated.
+ */
+#ifndef ADZ_B200_H
+#define ADZ_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* status codes                                                              */
+/* ------------------------------------------------------------------------ */
+#define ADZC_OK             0
+#define ADZC_ERR_ARG        1  /* NULL pointer, bad size, unknown enum          */
+#define ADZC_ERR_CUDA       2  /* a CUDA runtime call failed                    */
+#define ADZC_ERR_NK         3  /* fewer than 4 levels                          */
+#define ADZC_ERR_HALO       4  /* a stencil would leave the extended array      */
+#define ADZC_ERR_NONFINITE  5  /* NaN/Inf wind or position met by a kernel      */
+#define ADZC_ERR_TIMEOUT    6  /* a bounded device wait gave up                 */
+#define ADZC_ERR_ALLOC      7  /* device or host allocation failed              */
+#define ADZC_ERR_NODEVICE   8  /* no usable CUDA device                         */
+#define ADZC_ERR_SIZE       9  /* request larger than a fixed capacity          */
+
+#define ADZC_REF32 0
+#define ADZC_FP64  1
+#define ADZC_MIXED 2
+
+/* position sets of B/adz_mem.F90:87-88 */
+#define ADZC_SET_Q 0  /* Adz_pm : momentum levels, mass points               */
+#define ADZC_SET_U 1  /* Adz_pmu: momentum levels, u points                  */
+#define ADZC_SET_V 2  /* Adz_pmv: momentum levels, v points                  */
+#define ADZC_SET_T 3  /* Adz_pt : thermodynamic levels, mass points          */
+
+/* ------------------------------------------------------------------------ */
+/* Level A — reference interpolator ABI (host pointers)                      */
+/* ------------------------------------------------------------------------ */
+typedef struct { float px, py, pz; } pxpypz;  /* B/turbo_tricublin.c:157-162 */
+typedef struct adzc_ztab ztab;                /* opaque (B/turbo_tricublin.c:164-173) */
+
+/* B/turbo_tricublin.c:320 — levels(nk), row length ni, rows nj of the source */
+ztab *Vsearch_setup(double *levels, int nk, int ni, int nj);
+/* B/turbo_tricublin.c:370 — plus global-to-local offsets added to (int)px, (int)py */
+ztab *Vsearch_setup_plus(double *levels, int nk, int ni, int nj, int offseti, int offsetj);
+/* B/turbo_tricublin.c:752 — d[n] */
+void Tricublin_zyx1_n(float *d, float *f1, pxpypz *pxyz, ztab *lv, int n);
+/* B/turbo_tricublin.c:771 — d[n][m] */
+void Tricublin_zyx1_n_m(float *d, float **fs, pxpypz *pxyz, ztab *lv, int n, int m);
+/* B/turbo_tricublin.c:793 — d[m][n] */
+void Tricublin_zyx1_m_n(float *dm, float **fs, pxpypz *pxyz, ztab *lv, int n, int m);
+/* B/turbo_tricublin.c:821 — dp[m][n] through a pointer list */
+void Tricublin_zyx1_p(float **dp, float **fs, pxpypz *pxyz, ztab *lv, int n, int m);
+/* B/turbo_tricublin.c:1033 — cubic, trilinear, min, max of one field */
+void Tricublin_mono_zyx_n(float *d, float *l, float *mi, float *ma, float *f, pxpypz *pxyz, ztab *lv, int n);
+/* B/turbo_tricublin.c:1055 — outputs [n][m] */
+void Tricublin_mono_zyx_n_m(float *d, float *l, float *mi, float *ma, float **fs, pxpypz *pxyz, ztab *lv, int n,
+                            int m);
+/* B/turbo_tricublin.c:1080 — outputs [m][n] */
+void Tricublin_mono_zyx_m_n(float *d, float *l, float *mi, float *ma, float **fs, pxpypz *pxyz, ztab *lv, int n,
+                            int m);
+/* B/turbo_tricublin.c:1298 — 3-component interleaved source f3(3,ni,nj,nk), d[n][3] */
+void Tricublin_zyx3_n(float *d, float *f3, pxpypz *pxyz, ztab *lv, int n);
+
+/* ------------------------------------------------------------------------ */
+/* Level B — device pointers                                                 */
+/* ------------------------------------------------------------------------ */
+
+/* status of the last failing call on this thread, and its text */
+int adzc_last_error(void);
+const char *adzc_error_string(int status);
+
+/* Interpolators on device data (the Level A kernels with device pointers and
+ * a CUDA stream, passed as void*).  ``fs`` and ``ds`` are HOST arrays holding
+ * m DEVICE pointers.  Positions: pxpypz (REF32) or double[3] per point
+ * (FP64, MIXED).  Fields: float (REF32, MIXED) or double (FP64).  Results
+ * follow the source type.  d is [m][n].  box: 0 = min/max over the
+ * reference's AVX2 box (x 1..2, y 0..3, z 1..2 of the 4x4x4 stencil),
+ * 1 = the scalar-branch 2x2x2 inner box.  (B/turbo_tricublin.c:752-1312) */
+int adzc_ztab_create(const double *levels, int nk, int ni, int nj, int offi, int offj, ztab **out);
+int adzc_ztab_destroy(ztab *lv);
+int adzc_tricublin_m_n(const ztab *lv, int prec, void *d, const void *const *fs, const void *pxyz, int n, int m,
+                       void *stream);
+int adzc_tricublin_mono_m_n(const ztab *lv, int prec, void *d, void *l, void *mi, void *ma, const void *const *fs,
+                            const void *pxyz, int n, int m, int box, void *stream);
+int adzc_tricublin_zyx3_n(const ztab *lv, int prec, void *d, const void *f3, const void *pxyz, int n, void *stream);
+
+/* Per-tile inputs of adz_set (B/adz_set.F90:16-538).  Level arrays are host
+ * pointers read during adzc_setup only. */
+typedef struct {
+  int ni, nj, nk;                 /* l_ni, l_nj, l_nk (= G_nk)                     */
+  int maxcfl;                     /* Grd_maxcfl: halo = max(1,maxcfl)+1            */
+  int i0g, j0g;                   /* l_i0, l_j0: global index of local (1,1)       */
+  int west, east, south, north;   /* 1 when the tile touches that LAM edge         */
+  int pil_w, pil_e, pil_s, pil_n; /* pilot zone widths (0 on interior edges)       */
+  int lam_gbpil_t;                /* Lam_gbpil_t                                   */
+  int bc_lam_flux;                /* adz_BC_LAM_flux                               */
+  int schm_advec;                 /* Schm_advec: 0 none, 1 traditional, 2, 3        */
+  int itraj;                      /* Adz_itraj                                     */
+  int slt_winds;                  /* Adz_slt_winds (surface-layer winds at k=nk)   */
+  double bA_m, bA;                /* Cstv_bA_m_8, Cstv_bA_8                        */
+  double inv_rayt;                /* Dcst_inv_rayt_8                               */
+  double inv_hx, inv_hy;          /* geomh_inv_hx_8, geomh_inv_hy_8                */
+  const double *cy;               /* Adz_cy_8(1-halo : nj+halo)                    */
+  const double *zm;               /* Ver_z_8%m(0:nk+1)                             */
+  const double *zt;               /* Ver_z_8%t(0:nk+1)                             */
+  const double *zx;               /* Ver_z_8%x(0:nk)                               */
+  double zmin, zmax;              /* Ver_zmin_8, Ver_zmax_8                        */
+  double wmstar_nk;               /* Ver_wmstar_8(nk)                              */
+  double idz_t_nkm1;              /* Ver_idz_8%t(nk-1)                             */
+} adzc_grid;
+
+/* What adz_set derived (ranges are Fortran 1-based, inclusive). */
+typedef struct {
+  int halox, haloy, nit, njt;     /* extended extents: nit = ni+2*halox            */
+  int i0, in, j0, jn;             /* Adz_i0.. (mass points)                        */
+  int i0u, inu, j0v, jnv;         /* u and v point ranges                          */
+  int i0b, inb, j0b, jnb;         /* Adz_pb range                                  */
+  int k0, k0t, k0m;
+  long long npts[4];              /* points of sets Q, U, V, T                     */
+  double iminposx, imaxposx, iminposy, imaxposy;
+  int pnz_m, pnz_t;
+} adzc_info;
+
+typedef struct adzc_handle adzc_handle;
+
+/* adz_set: derive tables on the host and upload them to the current device. */
+int adzc_setup(const adzc_grid *g, adzc_handle **h);
+int adzc_destroy(adzc_handle *h);
+int adzc_query(const adzc_handle *h, adzc_info *info);
+
+/* Array layouts (Fortran column-major; all device pointers):
+ *   ext   (1-halox:ni+halox, 1-haloy:nj+haloy, 1:nk)  winds, sources, outputs
+ *   pxyzm (3, ni, nj, nk) float                        REF32 warm start (Adz_pxyzm)
+ *   wpxyz (-1:ni+2, -1:nj+2, nk, 3) double             Adz_wpxyz
+ * Winds and sources are float (REF32, MIXED) or double (FP64).
+ *
+ * adz_inittraj (B/adz_inittraj.F90:25-37): positions := arrival points; the
+ * next adzc_traject then runs max(6, itraj) iterations. */
+int adzc_inittraj(adzc_handle *h, int prec, void *pxyzm, double *wpxyz, void *stream);
+
+/* adz_prepareWinds + Adz_niter trajectory iterations (niter <= 0: the
+ * handle's current count, as Adz_niter) + the per-point state the position
+ * sets need.  pxyzm is used by REF32 only (NULL otherwise: FP64 and MIXED
+ * restart from wpxyz).  The handle keeps wpxyz, pxyzm, zdt0 and its own
+ * departure-wind scratch for the adzc_tricub calls that follow; they must stay
+ * valid until then.  (B/adz_traject.F90:16-125, B/adz_prepareWinds.F90) */
+int adzc_traject(adzc_handle *h, int prec, double dt, int niter, const void *uu_ext, const void *vv_ext,
+                 const void *ww_ext, const void *ut0, const void *vt0, const void *zdt0, void *pxyzm,
+                 double *wpxyz, void *stream);
+
+/* adz_tricub_hlt on a position set of the last trajectory, positions derived
+ * on the fly as adz_interp_traj does (B/adz_interp_traj.F90:45-187).
+ * srcs/dsts: HOST arrays of nfields DEVICE pointers (ext layout; only the
+ * set's arrival range of dsts is written).  mono: NULL or nfields flags,
+ * 1 = clip to the bound box (B/adz_post_tr.F90:81-94).  lin/mn/mx: NULL or
+ * nfields device pointers (entries may be NULL) receiving Adz_post lin
+ * (clipped), min, max for mono fields (B/adz_interp_hlt.F90:152-156). */
+int adzc_tricub(adzc_handle *h, int prec, int set, int nfields, const void *const *srcs, void *const *dsts,
+                const int *mono, void *const *lin, void *const *mn, void *const *mx, void *stream);
+
+/* Sticky device status of the handle's kernels (ADZC_ERR_HALO,
+ * ADZC_ERR_NONFINITE ...); synchronises the stream; clears it when reset. */
+int adzc_status(adzc_handle *h, int reset, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ADZ_B200_H */
