@@ -157,6 +157,11 @@ int orc_adz_set(const orc_grid *g, orc_set *s) {
   /* ztabs, adz_set.F90:128-131: levels m(1:nk) / t(1:nk), offsets 1-l_i0, 1-l_j0 */
   s->ztab_m = orc_vsearch_setup_plus(zm + 1, nk, s->nit, s->njt, 1 - g->i0g, 1 - g->j0g);
   s->ztab_t = orc_vsearch_setup_plus(zt + 1, nk, s->nit, s->njt, 1 - g->i0g, 1 - g->j0g);
+#ifdef ORC_USE_REF
+  /* the reference's own descriptors (never freed: the reference has no destroy) */
+  s->ref_m = Vsearch_setup_plus((double *)zm + 1, nk, s->nit, s->njt, 1 - g->i0g, 1 - g->j0g);
+  s->ref_t = Vsearch_setup_plus((double *)zt + 1, nk, s->nit, s->njt, 1 - g->i0g, 1 - g->j0g);
+#endif
   return 0;
 }
 
@@ -190,23 +195,8 @@ static void set_range(const orc_set *s, int set, int *r) {
 }
 
 #ifdef ORC_USE_REF
-/* the reference ztab objects are created lazily and cached per orc_set */
-typedef struct { const orc_set *s; void *m, *t; } refz;
-static refz g_refz[8];
-static void *ref_ztab(const orc_set *s, int which) {
-  for (int q = 0; q < 8; q++)
-    if (g_refz[q].s == s && g_refz[q].m) return which ? g_refz[q].t : g_refz[q].m;
-  for (int q = 0; q < 8; q++)
-    if (!g_refz[q].m || q == 7) {
-      g_refz[q].s = s;
-      g_refz[q].m = Vsearch_setup_plus((double *)s->g.zm + 1, s->g.nk, s->nit, s->njt, 1 - s->g.i0g, 1 - s->g.j0g);
-      g_refz[q].t = Vsearch_setup_plus((double *)s->g.zt + 1, s->g.nk, s->nit, s->njt, 1 - s->g.i0g, 1 - s->g.j0g);
-      return which ? g_refz[q].t : g_refz[q].m;
-    }
-  return NULL;
-}
-static void *ref_ztab_m_of(const orc_set *s) { return ref_ztab(s, 0); }
-static void *ref_ztab_t_of(const orc_set *s) { return ref_ztab(s, 1); }
+static void *ref_ztab_m_of(const orc_set *s) { return s->ref_m; }
+static void *ref_ztab_t_of(const orc_set *s) { return s->ref_t; }
 #endif
 
 /* ------------- precision templates ------------- */

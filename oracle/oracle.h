@@ -77,6 +77,7 @@ typedef struct {
   double ww, wp, wm;           /* interp_traj end weights */
   double *cy;                  /* index j - lminy */
   orc_ztab *ztab_m, *ztab_t;
+  void *ref_m, *ref_t;         /* reference ztab objects (reference-linked build only) */
 } orc_set;
 
 int orc_adz_set(const orc_grid *g, orc_set *s);
@@ -90,13 +91,8 @@ void orc_adz_free(orc_set *s);
  *   pxyzm      : (3, 1:ni, 1:nj, 1:nk)        FP32 (ref) / FP64 (f64 oracle)
  *   wpxyz      : (-1:ni+2, -1:nj+2, 1:nk, 3)  FP64
  *   pos sets   : (3, npoints) for ranges u, v, q(=m), t
- * Kernel selection for the FP32 driver: 0 = this restatement, 1 = function
- * pointers installed with orc_set_kernels (the reference build). */
-typedef void (*orc_zyx3_fn)(float *d, float *f3, void *pxyz, void *lv, int n);
-typedef void (*orc_m_n_fn)(float *d, float **fs, void *pxyz, void *lv, int n, int m);
-typedef void (*orc_mono_fn)(float *d, float *l, float *mi, float *ma, float **fs, void *pxyz, void *lv, int n, int m);
-typedef void *(*orc_setup_fn)(double *levels, int nk, int ni, int nj, int offi, int offj);
-void orc_set_kernels(orc_zyx3_fn zyx3, orc_m_n_fn zyx1, orc_mono_fn mono, orc_setup_fn setup);
+ * The FP32 driver calls the restated interpolator, or the reference's own one
+ * in the -DORC_USE_REF build. */
 
 /* number of threads used by the OpenMP loops (0 = runtime default) */
 void orc_set_threads(int n);

@@ -57,7 +57,8 @@ class OrcSet(C.Structure):
             "vw1m", "vw2m", "vw3m", "vw4m", "vw1t", "vw2t", "vw3t", "vw4t")] + [
         ("vw5", C.c_double), ("vw6", C.c_double), ("ww", C.c_double), ("wp", C.c_double),
         ("wm", C.c_double), ("cy", C.POINTER(C.c_double)),
-        ("ztab_m", C.POINTER(OrcZtab)), ("ztab_t", C.POINTER(OrcZtab))]
+        ("ztab_m", C.POINTER(OrcZtab)), ("ztab_t", C.POINTER(OrcZtab)),
+        ("ref_m", C.c_void_p), ("ref_t", C.c_void_p)]
 
 
 def build(ref: bool | None = None) -> None:

@@ -126,3 +126,21 @@ def test_search_tables_and_ranges():
     assert abs(s.iminposx - (5 + 2e-5)) < 1e-12 and abs(s.imaxposx - (60 - 2e-5)) < 1e-12
     tab = np.ctypeslib.as_array(s.search_m, shape=(s.pnz_m,))
     assert tab[0] == 0 and tab[-1] <= cfg.nk + 1 and np.all(np.diff(tab) >= 0)
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="reference build absent")
+def test_driver_reference_build_across_grids():
+    """Successive steps on different grids with the reference interpolator
+    match the restated one (each orc_set carries its own descriptors)."""
+    from gem_b200 import synth
+    for shape in ((40, 36, 12), (64, 48, 20), (40, 36, 12)):
+        cfg = synth.config_small(*shape)
+        inp = synth.make_inputs(cfg, dtype=torch.float64)
+        inp = {k: (v.numpy() if torch.is_tensor(v) else [t.numpy() for t in v]) for k, v in inp.items()}
+        res = []
+        for kind in ("ref", "oracle"):
+            st = O.Step(cfg, kind=kind, prec="f32")
+            st.inittraj()
+            st.step(inp)
+            res.append(st.pxyzm.copy())
+        assert np.array_equal(_bits(res[0]), _bits(res[1])), shape
