@@ -209,15 +209,17 @@ def run_product(args):
         return max_over_ranks(ms, ws), (clk.summary() if clk else None)
 
     # plain FP64 drop-in
-    d64 = conv(inp64, torch.float64)
-    step64, _, _ = make_step(adz.FP64, d64)
-    ms64, _ = timed(step64, args.steps, args.warmup)
+    ms64 = float("nan")
+    if args.only is None:
+        d64 = conv(inp64, torch.float64)
+        step64, _, _ = make_step(adz.FP64, d64)
+        ms64, _ = timed(step64, args.steps, args.warmup)
+        del step64, d64
+        torch.cuda.empty_cache()
     results["fp64"] = ms64
-    del step64
-    torch.cuda.empty_cache()
     # mixed precision (product)
     d32 = conv(inp64, torch.float32)
-    del d64, inp64
+    del inp64
     torch.cuda.empty_cache()
     step32, outs32, tro32 = make_step(adz.MIXED, d32)
     ms32, clk = timed(step32, args.steps, args.warmup, clocks=True)
@@ -346,6 +348,8 @@ def main():
     ap.add_argument("--ntr", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--only", choices=["mixed"], default=None,
+                    help="run the mixed-precision path alone (small profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
