@@ -81,6 +81,7 @@ def lib() -> C.CDLL:
         L.adzc_tricublin_m_n.argtypes = [vp, i, vp, vp, vp, i, i, vp]
         L.adzc_tricublin_mono_m_n.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, i, i, i, vp]
         L.adzc_tricublin_zyx3_n.argtypes = [vp, i, vp, vp, vp, i, vp]
+        L.adzc_step_noalloc.argtypes = [vp, i, d, i] + [vp] * 8 + [vp, vp, vp, vp, vp]
         L.adzc_error_string.restype = C.c_char_p
         L.Vsearch_setup.restype = vp
         L.Vsearch_setup.argtypes = [vp, i, i, i]

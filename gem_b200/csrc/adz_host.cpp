@@ -809,3 +809,27 @@ extern "C" void Tricublin_zyx3_n(float* d, float* f3, pxpypz* pxyz, ztab* lv, in
   const float* fs[1] = {f3};
   level_a(2, d, nullptr, nullptr, nullptr, nullptr, fs, pxyz, lv, n, 1, 0);
 }
+
+// ---------------------------------------------------------------------------
+// accessors used by the no-allocation entry point (adz_noalloc.cu)
+// ---------------------------------------------------------------------------
+#include "adz_internal.h"
+
+int adz_internal_view(const adzc_handle* h, adz::DGrid* dg, adzc_info* info, adzc_grid* g, int* niter, int* cold) {
+  if (!h) return ADZC_ERR_ARG;
+  *dg = h->dg;
+  *info = h->info;
+  *g = h->g;
+  *niter = h->niter;
+  *cold = h->cold;
+  return ADZC_OK;
+}
+
+void adz_internal_after_traject(adzc_handle* h) {
+  h->niter = std::max(1, h->g.itraj);
+  h->cold = 0;
+}
+
+adz::DtSplit adz_internal_dt_split(const adzc_grid& g, double dt) { return dt_split(g, dt); }
+
+int adz_internal_fail(int status) { return fail(status); }

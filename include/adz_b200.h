@@ -189,6 +189,32 @@ int adzc_tricub(adzc_handle *h, int prec, int set, int nfields, const void *cons
  * ADZC_ERR_NONFINITE ...); synchronises the stream; clears it when reset. */
 int adzc_status(adzc_handle *h, int reset, void *stream);
 
+/* One whole advection step that allocates no device memory.  No counterpart
+ * in the reference (its Fortran drivers use automatic arrays).
+ *
+ * For callers that cannot call cudaMalloc while stepping: a host model whose
+ * device memory belongs to its own pool (an OpenACC runtime, a caching
+ * allocator that reserved the GPU at start-up), one held to a device-memory
+ * budget fixed at start-up, or one that must not let the step synchronise the
+ * device.  adzc_traject allocates its scratch on first use; this entry point
+ * keeps the same scratch (departure winds, departure vertical wind) in one
+ * static device array of ADZC_NOALLOC_SCRATCH_BYTES that every GPU loading the
+ * library holds until exit.  Tiles whose scratch does not fit
+ * (3*nit*njt*nk + ni*nj*nk values of the field type, each part rounded up to
+ * 256 bytes) are rejected with ADZC_ERR_SIZE before anything runs.
+ *
+ * Does what adzc_traject followed by adzc_tricub on sets Q, U, V, T does:
+ * nfields[4] fields per set; srcs/dsts/mono hold all sets' entries in that
+ * order (HOST arrays of DEVICE pointers; mono may be NULL).  The first call
+ * on a device resolves the array's device address, so make it before any
+ * stream capture.  All calls share the array and it keeps the last call's
+ * contents: calls that overlap on the GPU race. */
+#define ADZC_NOALLOC_SCRATCH_BYTES (64u << 20)
+int adzc_step_noalloc(adzc_handle *h, int prec, double dt, int niter, const void *uu_ext, const void *vv_ext,
+                      const void *ww_ext, const void *ut0, const void *vt0, const void *zdt0, void *pxyzm,
+                      double *wpxyz, const int *nfields, const void *const *srcs, void *const *dsts,
+                      const int *mono, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
