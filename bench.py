@@ -228,46 +228,38 @@ def run_product(args):
 
     # per-launch durations of one step (events between the API calls)
     s = torch.cuda.current_stream()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     px, wp = ad.new_state(adz.MIXED)
     ad.adz_inittraj(adz.MIXED, px, wp)
     ad.adz_traject(adz.MIXED, cfg.dt, d32, px, wp)
     torch.cuda.synchronize()
-    per = {"traject": [], "set_u": [], "set_v": [], "set_t": []}
+    per = {"traject": [], "sets": []}
+    srcs = [d32["src_u"], d32["src_v"], d32["src_w"]] + d32["tracers"]
+    dsts = [outs32["u"], outs32["v"], outs32["w"]] + tro32
+    monos = [0, 0, 0] + [1 if cfg.mono else 0] * len(tro32)
     for _ in range(max(3, min(args.steps, 10))):
         ev[0].record(s)
         ad.adz_traject(adz.MIXED, cfg.dt, d32, px, wp)
         ev[1].record(s)
-        ad.adz_tricub_hlt(adz.MIXED, adz.SET_U, [d32["src_u"]], [outs32["u"]])
+        ad.adz_tricub_sets(adz.MIXED, [0, 1, 1, 1 + len(tro32)], srcs, dsts, monos)
         ev[2].record(s)
-        ad.adz_tricub_hlt(adz.MIXED, adz.SET_V, [d32["src_v"]], [outs32["v"]])
-        ev[3].record(s)
-        ad.adz_tricub_hlt(adz.MIXED, adz.SET_T, [d32["src_w"]] + d32["tracers"], [outs32["w"]] + tro32,
-                          mono=[0] + [1 if cfg.mono else 0] * len(tro32))
-        ev[4].record(s)
         torch.cuda.synchronize()
-        for q, k in enumerate(per):
-            per[k].append(ev[q].elapsed_time(ev[q + 1]))
+        per["traject"].append(ev[0].elapsed_time(ev[1]))
+        per["sets"].append(ev[1].elapsed_time(ev[2]))
     per = {k: statistics.median(v) for k, v in per.items()}
     I = ad.info
     n_t = int(I.npts[3])
-    nf_t = 1 + len(tro32)
-    # algorithmic bytes of the t-set launch per arrival point: FP64 position
-    # (24 B) + departure w and zdot (8 B) + nf fields read and written (8 B each)
-    bytes_t = n_t * (24 + 8 + nf_t * 8)
-    # trajectory launch (prepare + iterations) per grid point: winds in
-    # (3 departure + 3 arrival, FP32) 24 B, departure winds written and read
-    # once (24 B), FP64 positions in and out 48 B, departure w out 4 B
-    bytes_traj = npts * (24 + 24 + 48 + 4)
+    nf = 3 + len(tro32)
+    # algorithmic bytes (each array read or written once):
+    #   trajectory call, per grid point: departure winds 12 B + arrival winds
+    #   12 B (FP32) + FP64 position in 24 B and out 24 B + departure w out 4 B
+    #   sets launch, per arrival point: FP64 position 24 B + departure w and
+    #   zdot 8 B + every field read and written 8 B
+    bytes_launch = {"traject": npts * 76, "sets": n_t * (24 + 8 + nf * 8)}
     dom = max(per, key=per.get)
     hbm, hbm_kind = peaks()
-    if dom == "traject":
-        achieved = bytes_traj / (per[dom] * 1e-3) / 1e9
-        traffic = None
-    else:
-        b = bytes_t if dom == "set_t" else npts * (24 + 8)
-        achieved = b / (per[dom] * 1e-3) / 1e9
-        traffic = None
+    achieved = bytes_launch[dom] / (per[dom] * 1e-3) / 1e9
+    traffic = None
     step_bytes = npts * (24 + 12 + 12 + 24 + (3 + args.ntr) * 8)
 
     # end to end: inputs from pinned host memory, results back, every step
@@ -312,7 +304,7 @@ def run_product(args):
         "step_roofline": {"algorithmic_bytes_per_point": step_bytes / npts,
                           "achieved_gbs": step_bytes / (ms32 * 1e-3) / 1e9,
                           "frac": step_bytes / (ms32 * 1e-3) / 1e9 / hbm},
-        "e2e": e2e, "gpu_launches": 5 * args.steps, "clocks": clk, "cpu_baseline": cpu,
+        "e2e": e2e, "gpu_launches": 3 * args.steps, "clocks": clk, "cpu_baseline": cpu,
     }
     if rank == 0:
         print(json.dumps(line))

@@ -81,6 +81,7 @@ def lib() -> C.CDLL:
         L.adzc_tricublin_m_n.argtypes = [vp, i, vp, vp, vp, i, i, vp]
         L.adzc_tricublin_mono_m_n.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, i, i, i, vp]
         L.adzc_tricublin_zyx3_n.argtypes = [vp, i, vp, vp, vp, i, vp]
+        L.adzc_tricub_sets.argtypes = [vp, i, vp, vp, vp, vp, vp]
         L.adzc_step_noalloc.argtypes = [vp, i, d, i] + [vp] * 8 + [vp, vp, vp, vp, vp]
         L.adzc_error_string.restype = C.c_char_p
         L.Vsearch_setup.restype = vp
@@ -261,6 +262,14 @@ class Adz:
                                  C.cast(_ptr_array(dsts), C.c_void_p), mono_arr, lin, mn, mx, _stream(stream)),
                "adzc_tricub")
 
+    def adz_tricub_sets(self, prec: int, nfields, srcs, dsts, mono=None, stream=None):
+        """All position sets in one call: nfields = [nQ, nU, nV, nT]."""
+        nf = (C.c_int * 4)(*nfields)
+        mono_arr = (C.c_int * len(srcs))(*mono) if mono is not None else None
+        _check(lib().adzc_tricub_sets(self.h, prec, nf, C.cast(_ptr_array(srcs), C.c_void_p),
+                                      C.cast(_ptr_array(dsts), C.c_void_p), mono_arr, _stream(stream)),
+               "adzc_tricub_sets")
+
     def status(self, reset=True, stream=None) -> int:
         return lib().adzc_status(self.h, 1 if reset else 0, _stream(stream))
 
@@ -280,10 +289,10 @@ class Adz:
 
 
 def step_fused(adz: Adz, prec, dt, winds, fields, tracers, pxyzm, wpxyz, outs, tr_outs, mono, niter=0, stream=None):
-    """One advection step with w and every tracer in the same t-set launch."""
+    """One advection step: trajectory, then u@pmu, v@pmv and w + every tracer
+    @pt through adzc_tricub_sets (one launch for MIXED)."""
     adz.adz_traject(prec, dt, winds, pxyzm, wpxyz, niter, stream)
-    adz.adz_tricub_hlt(prec, SET_U, [fields["src_u"]], [outs["u"]], stream=stream)
-    adz.adz_tricub_hlt(prec, SET_V, [fields["src_v"]], [outs["v"]], stream=stream)
-    srcs = [fields["src_w"]] + list(tracers)
-    dsts = [outs["w"]] + list(tr_outs)
-    adz.adz_tricub_hlt(prec, SET_T, srcs, dsts, mono=[0] + [1 if mono else 0] * len(tracers), stream=stream)
+    srcs = [fields["src_u"], fields["src_v"], fields["src_w"]] + list(tracers)
+    dsts = [outs["u"], outs["v"], outs["w"]] + list(tr_outs)
+    monos = [0, 0, 0] + [1 if mono else 0] * len(tracers)
+    adz.adz_tricub_sets(prec, [0, 1, 1, 1 + len(tracers)], srcs, dsts, monos, stream)

@@ -237,8 +237,10 @@ __device__ __forceinline__ void interp3_exact(const T* __restrict__ f, const dou
 struct WF {
   float cx[4], cy[4], cz[4];
   float lx0, lx1, ly0, ly1, lz0, lz1;
-  int off;
+  int off;  // corner offset relative to cell (1,1,1): xy + zb*nij
   int zl;
+  int xy;   // corner offset within a plane, relative to cell (1,1)
+  int zb;   // 0-based plane of the corner (iz0-1 cubic, iz0 linear)
 };
 
 __device__ __forceinline__ void cubic_w(float t, float* w) {
@@ -262,11 +264,12 @@ __device__ __forceinline__ void coef_mixed(WF& w, double px8, double py8, double
   if (iz > lv.nk - 1) iz = lv.nk - 1;
   const double dz8 = pz8 - iz;
   const float dz = (float)dz8;
-  int ijk = (ix - 2) + (iy - 2) * lv.ni + (iz - 1) * lv.nij;
+  const int xy = (ix - 2) + (iy - 2) * lv.ni;
   const int iz0 = iz - 1;
   const int zl = (iz0 < 1 || iz0 > lv.nk - 3);
-  if (!zl) ijk -= lv.nij;
-  w.off = ijk;
+  w.zb = zl ? iz0 : iz0 - 1;
+  w.xy = xy;
+  w.off = xy + w.zb * lv.nij;
   w.zl = zl;
   cubic_w(fx, w.cx);
   cubic_w(fy, w.cy);

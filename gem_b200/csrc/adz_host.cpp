@@ -541,7 +541,7 @@ extern "C" int adzc_traject(adzc_handle* h, int prec, double dt, int niter, cons
   const cudaStream_t s = (cudaStream_t)stream;
   const adz::DGrid& D = h->dg;
   const size_t fb = field_bytes(prec);
-  if (ensure(&h->d_uvw, &h->uvw_bytes, 3 * fb * (size_t)D.nij * D.nk) != ADZC_OK ||
+  if (ensure(&h->d_uvw, &h->uvw_bytes, adz::uvw_values(prec) * fb * (size_t)D.nij * D.nk) != ADZC_OK ||
       ensure(&h->d_wdep, &h->wdep_bytes, fb * (size_t)D.ni * D.nj * D.nk) != ADZC_OK)
     return fail(ADZC_ERR_ALLOC);
   ADZ_CK(dispatch_prepare(prec, D, uu_ext, vv_ext, ww_ext, h->d_uvw, s));
@@ -608,6 +608,32 @@ extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const
       fp.mx[q] = mx ? mx[f] : nullptr;
     }
     ADZ_CK(dispatch_set(prec, D, set, i0, nx, j0, ny, k0, nz, a, fp, (cudaStream_t)stream));
+  }
+  return ADZC_OK;
+}
+
+extern "C" int adzc_tricub_sets(adzc_handle* h, int prec, const int* nfields, const void* const* srcs,
+                                void* const* dsts, const int* mono, void* stream) {
+  if (!h || !check_prec(prec) || !nfields) return fail(ADZC_ERR_ARG);
+  if (h->last_prec != prec || !h->wpxyz) return fail(ADZC_ERR_ARG);
+  int ntot = 0;
+  for (int q = 0; q < 4; q++) {
+    if (nfields[q] < 0) return fail(ADZC_ERR_ARG);
+    ntot += nfields[q];
+  }
+  if (ntot == 0) return ADZC_OK;
+  if (!srcs || !dsts) return fail(ADZC_ERR_ARG);
+  for (int f = 0; f < ntot; f++)
+    if (!srcs[f] || !dsts[f]) return fail(ADZC_ERR_ARG);
+  // one launch per set (and per chunk of fields)
+  int f0 = 0;
+  for (int q = 0; q < 4; q++) {
+    if (nfields[q] > 0) {
+      const int st = adzc_tricub(h, prec, q, nfields[q], srcs + f0, dsts + f0, mono ? mono + f0 : nullptr, nullptr,
+                                 nullptr, nullptr, stream);
+      if (st != ADZC_OK) return st;
+    }
+    f0 += nfields[q];
   }
   return ADZC_OK;
 }

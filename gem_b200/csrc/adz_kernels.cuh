@@ -14,6 +14,26 @@
 #pragma once
 #include "adz_device.cuh"
 
+// launch bounds of the gather kernels (minimum resident blocks of 128 threads
+// per SM; 0 lets ptxas choose).  A translation unit may set them before
+// including this header.
+#ifndef ADZ_TRAJ_MINB
+#define ADZ_TRAJ_MINB 0
+#endif
+#ifndef ADZ_SET_MINB
+#define ADZ_SET_MINB 0
+#endif
+#if ADZ_TRAJ_MINB > 0
+#define ADZ_TRAJ_BOUNDS __launch_bounds__(128, ADZ_TRAJ_MINB)
+#else
+#define ADZ_TRAJ_BOUNDS __launch_bounds__(128)
+#endif
+#if ADZ_SET_MINB > 0
+#define ADZ_SET_BOUNDS __launch_bounds__(128, ADZ_SET_MINB)
+#else
+#define ADZ_SET_BOUNDS __launch_bounds__(128)
+#endif
+
 namespace adz {
 
 __device__ __forceinline__ long long ext_index(const DGrid& g, int i, int j, int k) {
@@ -117,7 +137,7 @@ __device__ __forceinline__ bool stencil_ok(const DGrid& g, int off) {
 
 // ---------------------------------------------------------------------------
 template <int PREC>
-__global__ void __launch_bounds__(128) k_traject(DGrid g, TrajArgs a) {
+__global__ void ADZ_TRAJ_BOUNDS k_traject(DGrid g, TrajArgs a) {
   using F = typename Types<PREC>::F;
   const long long nplane = (long long)g.ni * g.nj;
   const long long n = nplane * (g.nk - a.k00 + 1);
@@ -319,7 +339,7 @@ __device__ __forceinline__ void set_position(const DGrid& g, const SetArgs& a, i
 }
 
 template <int PREC>
-__global__ void __launch_bounds__(128) k_tricub_set(DGrid g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
+__global__ void ADZ_SET_BOUNDS k_tricub_set(DGrid g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
                                                     SetArgs a, FieldPtrs fp) {
   using F = typename Types<PREC>::F;
   const long long nplane = (long long)nx * ny;

@@ -91,9 +91,9 @@ extern "C" int adzc_step_noalloc(adzc_handle* h, int prec, double dt, int niter,
   adzc_grid G;
   int hn = 1, cold = 0;
   if (adz_internal_view(h, &D, &I, &G, &hn, &cold) != ADZC_OK) return adz_internal_fail(ADZC_ERR_ARG);
-  // scratch: departure winds (3 x extended field) then departure w (ni*nj*nk)
+  // scratch: departure winds (3 values per extended cell) then departure w (ni*nj*nk)
   const size_t fb = (prec == ADZC_FP64) ? sizeof(double) : sizeof(float);
-  const size_t uvw_bytes = align256(3 * fb * (size_t)D.nij * D.nk);
+  const size_t uvw_bytes = align256(adz::uvw_values(prec) * fb * (size_t)D.nij * D.nk);
   const size_t wdep_bytes = align256(fb * (size_t)D.ni * D.nj * D.nk);
   if (uvw_bytes + wdep_bytes > (size_t)ADZC_NOALLOC_SCRATCH_BYTES) return adz_internal_fail(ADZC_ERR_SIZE);
   void* base = nullptr;

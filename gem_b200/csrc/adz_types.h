@@ -102,6 +102,12 @@ struct SetArgs {
 };
 
 
+// values per cell of the departure-wind scratch (u, v, w interleaved)
+inline int uvw_values(int prec) {
+  (void)prec;
+  return 3;
+}
+
 template <int PREC>
 cudaError_t launch_prepare(const DGrid& g, const void* uu, const void* vv, const void* ww, void* uvw_d,
                            cudaStream_t s);

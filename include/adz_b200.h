@@ -185,6 +185,13 @@ int adzc_traject(adzc_handle *h, int prec, double dt, int niter, const void *uu_
 int adzc_tricub(adzc_handle *h, int prec, int set, int nfields, const void *const *srcs, void *const *dsts,
                 const int *mono, void *const *lin, void *const *mn, void *const *mx, void *stream);
 
+/* Every position set of the last trajectory in one call: nfields[4] fields
+ * for sets Q, U, V, T, srcs/dsts/mono holding all sets' entries in that order
+ * (HOST arrays of DEVICE pointers; mono may be NULL).  Same results as
+ * adzc_tricub per set.  (B/adz_main.F90:35-60, B/adz_tracers.F90:74-99) */
+int adzc_tricub_sets(adzc_handle *h, int prec, const int *nfields, const void *const *srcs, void *const *dsts,
+                     const int *mono, void *stream);
+
 /* Sticky device status of the handle's kernels (ADZC_ERR_HALO,
  * ADZC_ERR_NONFINITE ...); synchronises the stream; clears it when reset. */
 int adzc_status(adzc_handle *h, int reset, void *stream);

@@ -283,3 +283,44 @@ def test_nonfinite_wind_sets_status(A):
     ad.adz_traject(A.REF32, cfg.dt, dev, px, wp)
     assert ad.status() in (4, 5)
     assert ad.status() == 0  # reset by the previous read
+
+
+def test_step_mixed_wide_plane_unions(A):
+    """Strong vertical wind noise scatters the departure levels of neighbouring
+    points over many thin bottom layers (warps whose lanes span more than 8
+    levels), including linear-z points at the bottom level, with mono bounds
+    and clipping on every field.  One trajectory iteration on both sides keeps
+    the comparison well conditioned (iterating a map whose vertical Lipschitz
+    constant dt*dw/dz is far above 1 would amplify FP32/FP64 differences)."""
+    from gem_b200 import synth
+    cfg = synth.config_mixed(96, 80, 80)
+    cfg.noise = 6.0
+    np_in, dev = _inputs(cfg, torch.float32)
+    np64 = {k: (v.astype(np.float32).astype(np.float64) if not isinstance(v, list)
+                else [t.astype(np.float32).astype(np.float64) for t in v]) for k, v in np_in.items()}
+    st = O.Step(cfg, kind="oracle", prec="f64")
+    st.inittraj()
+    st.traject(np64, niter=1)
+    ref = st.tricub(3, [np64["src_w"]] + np64["tracers"], mono=True, clip=True)
+    ad = A.Adz.from_config(cfg)
+    px, wp = ad.new_state(A.MIXED)
+    ad.adz_inittraj(A.MIXED, px, wp)
+    ad.adz_traject(A.MIXED, cfg.dt, dev, px, wp, niter=1)
+    srcs = [dev["src_w"]] + dev["tracers"]
+    outs = [torch.full(ad.ext_shape, float("nan"), device="cuda") for _ in srcs]
+    ad.adz_tricub_sets(A.MIXED, [0, 0, 0, len(srcs)], srcs, outs, [1] * len(srcs))
+    assert ad.status() == 0
+    # the oracle clips w as well here (mono on every field)
+    m = ad.range_mask(3).numpy()
+    # many warps span more than 8 levels in this case
+    p = st.sets[3]
+    iz = np.clip(np.trunc(p[:, 2].astype(np.float32)).astype(int), 1, cfg.nk - 1) - 1
+    zl = (iz < 1) | (iz > cfg.nk - 3)
+    zb = np.where(zl, iz, iz - 1)
+    zh = np.where(zl, zb + 1, zb + 3)
+    n = len(zb) // 32 * 32
+    U = zh[:n].reshape(-1, 32).max(1) - zb[:n].reshape(-1, 32).min(1) + 1
+    assert (U > 8).sum() > 100
+    for a, b in zip(outs, ref):
+        a, b = a.cpu().numpy()[m].astype(np.float64), b[m]
+        assert np.max(np.abs(a - b)) / np.max(np.abs(b)) < 1e-5
