@@ -34,7 +34,19 @@
 #define ADZ_SET_BOUNDS __launch_bounds__(128)
 #endif
 
+// MIXED stores the departure winds as three component planes (u, v, w) instead
+// of interleaved triplets: each component gather is then a run of consecutive
+// floats across the warp's lanes, like a single field.
+#ifndef ADZ_MIXED_SOA
+#define ADZ_MIXED_SOA 1
+#endif
+
 namespace adz {
+
+template <int PREC>
+struct WindLayout {
+  static constexpr bool soa = (PREC == kMixed) && (ADZ_MIXED_SOA != 0);
+};
 
 __device__ __forceinline__ long long ext_index(const DGrid& g, int i, int j, int k) {
   return (long long)(i - g.lminx) + (long long)(j - g.lminy) * g.nit + (long long)(k - 1) * g.nij;
@@ -67,8 +79,10 @@ __global__ void __launch_bounds__(256) k_prepare(DGrid g, const typename Types<P
     const double cyj = __ldg(g.cy + jj);
     const double* vw = g.vw;
     const int nk = g.nk;
-    uvw_d[3 * e + 0] = (F)(g.inv_rayt * (double)uu[e] * cyj);
-    uvw_d[3 * e + 1] = (F)(g.inv_rayt * (double)vv[e]);
+    const long long cu = WindLayout<PREC>::soa ? e : 3 * e;
+    const long long cs = WindLayout<PREC>::soa ? n : 1;  // component stride
+    uvw_d[cu] = (F)(g.inv_rayt * (double)uu[e] * cyj);
+    uvw_d[cu + cs] = (F)(g.inv_rayt * (double)vv[e]);
     double w;
     if (k == 1) {
       w = g.vw5 * (double)ww[e];
@@ -80,7 +94,7 @@ __global__ void __launch_bounds__(256) k_prepare(DGrid g, const typename Types<P
       w = wx * (double)ww[r + (long long)(km2 - 1) * g.nij] + __ldg(vw + 1 * (nk + 1) + k) * (double)ww[e - g.nij] +
           __ldg(vw + 2 * (nk + 1) + k) * (double)ww[e] + __ldg(vw + 3 * (nk + 1) + k) * (double)ww[e + g.nij];
     }
-    uvw_d[3 * e + 2] = (F)w;
+    uvw_d[cu + 2 * cs] = (F)w;
   }
 }
 
@@ -203,9 +217,17 @@ __global__ void ADZ_TRAJ_BOUNDS k_traject(DGrid g, TrajArgs a) {
         coef_mixed(w, px, py, pz, g.tab_m);
         off = w.off;
         if (!stencil_ok(g, off)) { bad = true; break; }
-        float o[3];
-        interp3_mixed((const float*)f3 + 3LL * off, w, g.tab_m.ni, g.tab_m.nij, o);
-        ud = o[0]; vd = o[1]; wd = o[2];
+        if (WindLayout<PREC>::soa) {
+          const long long ncell = g.nij * g.nk;
+          const float* fu = (const float*)uvw + e111 + off;
+          ud = interp1_mixed(fu, w, g.tab_m.ni, g.tab_m.nij);
+          vd = interp1_mixed(fu + ncell, w, g.tab_m.ni, g.tab_m.nij);
+          wd = interp1_mixed(fu + 2 * ncell, w, g.tab_m.ni, g.tab_m.nij);
+        } else {
+          float o[3];
+          interp3_mixed((const float*)f3 + 3LL * off, w, g.tab_m.ni, g.tab_m.nij, o);
+          ud = o[0]; vd = o[1]; wd = o[2];
+        }
       } else {
         double c[20];
         int zl;

@@ -1,5 +1,9 @@
 // MIXED instantiation: FP64 positions and cell offsets, FP32 weights and
-// packed FP32 sums.
+// packed FP32 sums.  Departure winds are stored as three component planes
+// (ADZ_MIXED_SOA in adz_kernels.cuh).  Resident blocks per SM were picked by
+// timing the 1024x1024x80 step (trajectory 7 blocks of 128 threads, sets 9).
+#define ADZ_TRAJ_MINB 7
+#define ADZ_SET_MINB 9
 #include "adz_kernels.cuh"
 
 namespace adz {
