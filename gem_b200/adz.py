@@ -54,6 +54,14 @@ class AdzcInfo(C.Structure):
         ("iminposy", C.c_double), ("imaxposy", C.c_double), ("pnz_m", C.c_int), ("pnz_t", C.c_int)]
 
 
+class AdzcDomain(C.Structure):
+    """adzc_domain: one domain of a batch (include/adz_b200.h)."""
+    _fields_ = [("h", C.c_void_p), ("dt", C.c_double), ("niter", C.c_int),
+                ("uu_ext", C.c_void_p), ("vv_ext", C.c_void_p), ("ww_ext", C.c_void_p),
+                ("ut0", C.c_void_p), ("vt0", C.c_void_p), ("zdt0", C.c_void_p), ("wpxyz", C.c_void_p),
+                ("nfields", C.c_int * 4), ("srcs", C.c_void_p), ("dsts", C.c_void_p), ("mono", C.c_void_p)]
+
+
 class PxPyPz(C.Structure):
     _fields_ = [("px", C.c_float), ("py", C.c_float), ("pz", C.c_float)]
 
@@ -83,6 +91,12 @@ def lib() -> C.CDLL:
         L.adzc_tricublin_zyx3_n.argtypes = [vp, i, vp, vp, vp, i, vp]
         L.adzc_tricub_sets.argtypes = [vp, i, vp, vp, vp, vp, vp]
         L.adzc_step_noalloc.argtypes = [vp, i, d, i] + [vp] * 8 + [vp, vp, vp, vp, vp]
+        L.adzc_batch_create.argtypes = [i, i, vp, C.POINTER(vp)]
+        L.adzc_batch_tune.argtypes = [vp, vp]
+        L.adzc_batch_step.argtypes = [vp, vp]
+        L.adzc_batch_query.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
+        L.adzc_batch_status.argtypes = [vp, i, vp]
+        L.adzc_batch_destroy.argtypes = [vp]
         L.adzc_error_string.restype = C.c_char_p
         L.Vsearch_setup.restype = vp
         L.Vsearch_setup.argtypes = [vp, i, i, i]
@@ -296,3 +310,50 @@ def step_fused(adz: Adz, prec, dt, winds, fields, tracers, pxyzm, wpxyz, outs, t
     dsts = [outs["u"], outs["v"], outs["w"]] + list(tr_outs)
     monos = [0, 0, 0] + [1 if mono else 0] * len(tracers)
     adz.adz_tricub_sets(prec, [0, 1, 1, 1 + len(tracers)], srcs, dsts, monos, stream)
+
+
+class Batch:
+    """Independent domains advanced by one persistent launch per step
+    (adzc_batch_*).  ``domains``: dicts with adz (Adz, past its cold start),
+    dt, winds (uu_ext, vv_ext, ww_ext, ut0, vt0, zdt0), wpxyz, nfields
+    [nQ, nU, nV, nT], srcs, dsts (tensors in set order) and mono (per field)."""
+
+    def __init__(self, prec: int, domains):
+        self._keep = []
+        arr = (AdzcDomain * len(domains))()
+        for d, dom in enumerate(domains):
+            w = dom["winds"]
+            srcs, dsts = _ptr_array(dom["srcs"]), _ptr_array(dom["dsts"])
+            mono = (C.c_int * len(dom["srcs"]))(*dom.get("mono", [0] * len(dom["srcs"])))
+            self._keep += [dom["adz"], w, dom["wpxyz"], dom["srcs"], dom["dsts"], srcs, dsts, mono]
+            a = arr[d]
+            a.h, a.dt, a.niter = dom["adz"].h, float(dom["dt"]), int(dom.get("niter", 0))
+            a.uu_ext, a.vv_ext, a.ww_ext = (w[k].data_ptr() for k in ("uu_ext", "vv_ext", "ww_ext"))
+            a.ut0, a.vt0, a.zdt0 = (w[k].data_ptr() for k in ("ut0", "vt0", "zdt0"))
+            a.wpxyz = dom["wpxyz"].data_ptr()
+            for q in range(4):
+                a.nfields[q] = int(dom["nfields"][q])
+            a.srcs, a.dsts, a.mono = C.cast(srcs, C.c_void_p), C.cast(dsts, C.c_void_p), C.cast(mono, C.c_void_p)
+        self.h = C.c_void_p()
+        _check(lib().adzc_batch_create(prec, len(domains), C.cast(arr, C.c_void_p), C.byref(self.h)),
+               "adzc_batch_create")
+
+    def tune(self, stream=None):
+        _check(lib().adzc_batch_tune(self.h, _stream(stream)), "adzc_batch_tune")
+
+    def step(self, stream=None):
+        _check(lib().adzc_batch_step(self.h, _stream(stream)), "adzc_batch_step")
+
+    def query(self):
+        r, b, n = C.c_int(), C.c_int(), C.c_longlong()
+        _check(lib().adzc_batch_query(self.h, C.byref(r), C.byref(b), C.byref(n)), "adzc_batch_query")
+        return {"rows_per_item": r.value, "blocks_per_sm": b.value, "items": n.value}
+
+    def status(self, reset=True, stream=None) -> int:
+        return lib().adzc_batch_status(self.h, 1 if reset else 0, _stream(stream))
+
+    def __del__(self):
+        try:
+            lib().adzc_batch_destroy(self.h)
+        except Exception:
+            pass

@@ -1,0 +1,324 @@
+// Batches of independent limited-area domains stepped by ONE persistent launch.
+//
+// Work items (domain, phase, group, first point, count) are laid out phase by
+// phase: every departure-wind item (phase 0) of every domain, then every
+// trajectory item (phase 1), then every interpolation item (phase 2, one
+// field group of one position set).  Blocks take items from an atomic queue.
+// An item of phase p>0 first waits until all items of phase p-1 of its own
+// domain have completed (per-domain counters).  Every such item was taken by
+// a block that is running and never waits on anything later in the queue, so
+// the wait always ends; it is bounded anyway (kErrTimeout, item skipped).
+// Counters are released with a device-scope fence by every writer thread and
+// read with acquire semantics; positions written in the same launch are read
+// around L1.
+//
+// The tile of an item is ``rows`` consecutive rows of one level band
+// (rows * row length points); adzc_batch_tune times candidate row counts and
+// resident block counts and keeps the fastest.  The tuned launch is captured
+// in a CUDA graph (counter reset + persistent kernel) and replayed per step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/adz_b200.h"
+#include "adz_internal.h"
+#include "adz_types.h"
+
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct adzc_batch {
+  int prec = 0, ndom = 0;
+  std::vector<adz::BDom> doms;
+  std::vector<adzc_handle*> handles;
+  adz::BDom* d_doms = nullptr;
+  adz::BItem* d_items = nullptr;
+  size_t items_cap = 0;
+  long long nitems = 0;
+  unsigned* d_need = nullptr;
+  unsigned long long* d_next = nullptr;
+  unsigned* d_done = nullptr;
+  int* d_status = nullptr;
+  int rows = 8, bps = 4, sms = 148;
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+int build_items(adzc_batch* b, int rows) {
+  std::vector<adz::BItem> items;
+  std::vector<unsigned> need(2 * b->ndom, 0);
+  for (int phase = 0; phase < 3; phase++) {
+    for (int d = 0; d < b->ndom; d++) {
+      const adz::BDom& D = b->doms[d];
+      auto push = [&](int group, long long n, long long chunk) {
+        for (long long s = 0; s < n; s += chunk) {
+          adz::BItem it{};
+          it.dom = d;
+          it.phase = phase;
+          it.group = group;
+          it.start = s;
+          it.count = std::min(chunk, n - s);
+          items.push_back(it);
+          if (phase < 2) need[2 * d + phase]++;
+        }
+      };
+      if (phase == 0) push(0, D.g.nij * D.g.nk, (long long)rows * D.g.nit);
+      if (phase == 1) push(0, (long long)D.g.ni * D.g.nj * (D.g.nk - D.ta.k00 + 1), (long long)rows * D.g.ni);
+      if (phase == 2)
+        for (int q = 0; q < D.ngroups; q++) {
+          const int* r = D.grange[q];
+          push(q, (long long)r[1] * r[3] * (D.g.nk - r[4] + 1), (long long)rows * r[1]);
+        }
+    }
+  }
+  if (items.size() > b->items_cap) {
+    cudaFree(b->d_items);
+    b->d_items = nullptr;
+    if (cudaMalloc(&b->d_items, items.size() * sizeof(adz::BItem)) != cudaSuccess) return ADZC_ERR_ALLOC;
+    b->items_cap = items.size();
+  }
+  if (cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(adz::BItem), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->d_need, need.data(), need.size() * sizeof(unsigned), cudaMemcpyHostToDevice) != cudaSuccess)
+    return ADZC_ERR_CUDA;
+  b->nitems = (long long)items.size();
+  b->rows = rows;
+  return ADZC_OK;
+}
+
+cudaError_t enqueue(adzc_batch* b, cudaStream_t s) {
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(b->d_done, 0, 2 * b->ndom * sizeof(unsigned), s)) != cudaSuccess) return e;
+  const int grid = b->bps * b->sms;
+  if (b->prec == ADZC_FP64)
+    return adz::launch_batch<adz::kFp64>(grid, b->d_doms, b->d_items, b->nitems, b->d_need, b->d_next, b->d_done,
+                                         b->d_status, s);
+  return adz::launch_batch<adz::kMixed>(grid, b->d_doms, b->d_items, b->nitems, b->d_need, b->d_next, b->d_done,
+                                        b->d_status, s);
+}
+
+// the handles' positions now live in the domains' wpxyz (adzc_tricub may follow)
+void record(adzc_batch* b) {
+  for (int d = 0; d < b->ndom; d++)
+    adz_internal_record_positions(b->handles[d], b->prec, (double*)b->doms[d].ta.wpxyz, b->doms[d].ta.zdt0,
+                                  b->doms[d].ta.dt);
+}
+
+int capture(adzc_batch* b) {
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  if (b->graph) {
+    cudaGraphDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  if (cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return ADZC_ERR_CUDA;
+  const cudaError_t e = enqueue(b, b->cap);
+  cudaGraph_t g = nullptr;
+  if (cudaStreamEndCapture(b->cap, &g) != cudaSuccess || e != cudaSuccess || !g) return ADZC_ERR_CUDA;
+  b->graph = g;
+  if (cudaGraphInstantiate(&b->exec, g, 0) != cudaSuccess) return ADZC_ERR_CUDA;
+  return ADZC_OK;
+}
+
+}  // namespace
+
+extern "C" int adzc_batch_destroy(adzc_batch* b) {
+  if (!b) return ADZC_OK;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  cudaFree(b->d_doms);
+  cudaFree(b->d_items);
+  cudaFree(b->d_need);
+  cudaFree(b->d_next);
+  cudaFree(b->d_done);
+  cudaFree(b->d_status);
+  delete b;
+  return ADZC_OK;
+}
+
+extern "C" int adzc_batch_create(int prec, int ndom, const adzc_domain* doms, adzc_batch** out) {
+  if (!out || ndom < 1 || !doms || (prec != ADZC_FP64 && prec != ADZC_MIXED)) return adz_internal_fail(ADZC_ERR_ARG);
+  auto* b = new (std::nothrow) adzc_batch();
+  if (!b) return adz_internal_fail(ADZC_ERR_ALLOC);
+  b->prec = prec;
+  b->ndom = ndom;
+  b->doms.resize(ndom);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+  b->bps = std::max(1, prec == ADZC_FP64 ? adz::batch_resident_blocks<adz::kFp64>()
+                                         : adz::batch_resident_blocks<adz::kMixed>());
+  for (int d = 0; d < ndom; d++) {
+    const adzc_domain& in = doms[d];
+    adz::BDom& D = b->doms[d];
+    memset(&D, 0, sizeof(D));
+    adzc_info I;
+    adzc_grid G;
+    int niter = 1, cold = 0;
+    if (!in.h || !in.uu_ext || !in.vv_ext || !in.ww_ext || !in.ut0 || !in.vt0 || !in.zdt0 || !in.wpxyz ||
+        adz_internal_view(in.h, &D.g, &I, &G, &niter, &cold) != ADZC_OK || cold || !adz_internal_warm(in.h)) {
+      adzc_batch_destroy(b);
+      return adz_internal_fail(ADZC_ERR_ARG);
+    }
+    void *uvw = nullptr, *wdep = nullptr;
+    if (adz_internal_scratch(in.h, prec, &uvw, &wdep) != ADZC_OK) {
+      adzc_batch_destroy(b);
+      return adz_internal_fail(ADZC_ERR_ALLOC);
+    }
+    D.uu = in.uu_ext;
+    D.vv = in.vv_ext;
+    D.ww = in.ww_ext;
+    D.ta.uvw_d = uvw;
+    D.ta.ut0 = in.ut0;
+    D.ta.vt0 = in.vt0;
+    D.ta.zdt0 = in.zdt0;
+    D.ta.wpxyz = in.wpxyz;
+    D.ta.wdep = wdep;
+    D.ta.niter = in.niter > 0 ? in.niter : niter;
+    D.ta.cold = 0;
+    D.ta.k00 = (D.g.k0 > 1) ? 1 : D.g.k0m;
+    D.ta.dt = adz_internal_dt_split(G, in.dt);
+    D.sa.wpxyz = in.wpxyz;
+    D.sa.wdep = wdep;
+    D.sa.zdt0 = in.zdt0;
+    D.sa.dt = D.ta.dt;
+    D.sa.k00 = std::max(I.k0t - 1, 1);
+    if (G.bc_lam_flux != 0 && I.k0 > 1) D.sa.k00 = 1;
+    const int r[4][5] = {{I.i0, I.in, I.j0, I.jn, I.k0},
+                         {I.i0u, I.inu, I.j0, I.jn, I.k0},
+                         {I.i0, I.in, I.j0v, I.jnv, I.k0},
+                         {I.i0, I.in, I.j0, I.jn, I.k0t}};
+    int f0 = 0;
+    for (int set = 0; set < 4; set++) {
+      const int nf = in.nfields[set];
+      if (nf < 0) {
+        adzc_batch_destroy(b);
+        return adz_internal_fail(ADZC_ERR_ARG);
+      }
+      for (int q0 = 0; q0 < nf; q0 += adz::kMaxFields) {
+        if (D.ngroups == adz::kMaxGroups) {
+          adzc_batch_destroy(b);
+          return adz_internal_fail(ADZC_ERR_SIZE);
+        }
+        const int gi = D.ngroups++;
+        D.gset[gi] = set;
+        D.grange[gi][0] = r[set][0];
+        D.grange[gi][1] = r[set][1] - r[set][0] + 1;
+        D.grange[gi][2] = r[set][2];
+        D.grange[gi][3] = r[set][3] - r[set][2] + 1;
+        D.grange[gi][4] = r[set][4];
+        adz::FieldPtrs& fp = D.gfp[gi];
+        fp.nf = std::min(adz::kMaxFields, nf - q0);
+        for (int q = 0; q < fp.nf; q++) {
+          const int f = f0 + q0 + q;
+          if (!in.srcs || !in.dsts || !in.srcs[f] || !in.dsts[f]) {
+            adzc_batch_destroy(b);
+            return adz_internal_fail(ADZC_ERR_ARG);
+          }
+          fp.src[q] = in.srcs[f];
+          fp.dst[q] = in.dsts[f];
+          const int mv = in.mono ? in.mono[f] : 0;
+          if (mv != 0) fp.mono_mask |= 1u << q;
+          if (mv == 1) fp.clip_mask |= 1u << q;
+        }
+      }
+      f0 += nf;
+    }
+    b->handles.push_back(in.h);
+  }
+  if (cudaMalloc(&b->d_doms, ndom * sizeof(adz::BDom)) != cudaSuccess ||
+      cudaMalloc(&b->d_need, 2 * ndom * sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc(&b->d_next, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&b->d_done, 2 * ndom * sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc(&b->d_status, sizeof(int)) != cudaSuccess ||
+      cudaMemcpy(b->d_doms, b->doms.data(), ndom * sizeof(adz::BDom), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(b->d_status, 0, sizeof(int)) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess) {
+    adzc_batch_destroy(b);
+    return adz_internal_fail(ADZC_ERR_CUDA);
+  }
+  int st = build_items(b, b->rows);
+  if (st == ADZC_OK) st = capture(b);
+  if (st != ADZC_OK) {
+    adzc_batch_destroy(b);
+    return adz_internal_fail(st);
+  }
+  *out = b;
+  return ADZC_OK;
+}
+
+extern "C" int adzc_batch_step(adzc_batch* b, void* stream) {
+  if (!b || !b->exec) return adz_internal_fail(ADZC_ERR_ARG);
+  if (cudaGraphLaunch(b->exec, (cudaStream_t)stream) != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
+  record(b);
+  return ADZC_OK;
+}
+
+extern "C" int adzc_batch_tune(adzc_batch* b, void* stream) {
+  if (!b) return adz_internal_fail(ADZC_ERR_ARG);
+  const cudaStream_t s = (cudaStream_t)stream;
+  const int rows_c[] = {2, 8, 32};
+  const int res = std::max(1, b->prec == ADZC_FP64 ? adz::batch_resident_blocks<adz::kFp64>()
+                                                   : adz::batch_resident_blocks<adz::kMixed>());
+  const int bps_c[] = {std::max(1, res / 2), res};
+  float best = 1e30f;
+  int br = b->rows, bb = b->bps;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
+  for (int r : rows_c)
+    for (int p : bps_c) {
+      b->bps = p;
+      if (build_items(b, r) != ADZC_OK || enqueue(b, s) != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
+      cudaEventRecord(e0, s);
+      for (int rep = 0; rep < 2; rep++) enqueue(b, s);
+      cudaEventRecord(e1, s);
+      if (cudaEventSynchronize(e1) != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) {
+        best = ms;
+        br = r;
+        bb = p;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->bps = bb;
+  int st = build_items(b, br);
+  if (st == ADZC_OK) st = capture(b);
+  record(b);
+  return st == ADZC_OK ? ADZC_OK : adz_internal_fail(st);
+}
+
+extern "C" int adzc_batch_query(const adzc_batch* b, int* rows, int* blocks_per_sm, long long* nitems) {
+  if (!b) return adz_internal_fail(ADZC_ERR_ARG);
+  if (rows) *rows = b->rows;
+  if (blocks_per_sm) *blocks_per_sm = b->bps;
+  if (nitems) *nitems = b->nitems;
+  return ADZC_OK;
+}
+
+extern "C" int adzc_batch_status(adzc_batch* b, int reset, void* stream) {
+  if (!b) return adz_internal_fail(ADZC_ERR_ARG);
+  if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
+  int bits = 0;
+  if (cudaMemcpy(&bits, b->d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return adz_internal_fail(ADZC_ERR_CUDA);
+  if (reset) cudaMemset(b->d_status, 0, sizeof(int));
+  if (bits & adz::kErrTimeout) return ADZC_ERR_TIMEOUT;
+  for (adzc_handle* h : b->handles) {
+    const int st = adzc_status(h, reset, stream);
+    if (st != ADZC_OK) return st;
+  }
+  return ADZC_OK;
+}

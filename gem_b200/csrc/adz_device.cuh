@@ -103,9 +103,17 @@ __device__ __forceinline__ int coef_f64pos(double* c, int& off, double px8, doub
   return coef_cell(c, off, px, py, dz, ix, iy, iz, lv);
 }
 
-template <typename T>
+// source loads: read-only path, or (COH) the coherent L1 path for data that
+// the same launch wrote before an acquire (persistent batch kernel)
+template <bool COH, typename T>
+__device__ __forceinline__ T ldin(const T* p) {
+  if (COH) return __ldca(p);
+  return __ldg(p);
+}
+
+template <typename T, bool COH = false>
 __device__ __forceinline__ double ldd(const T* p) {
-  return (double)__ldg(p);
+  return (double)ldin<COH>(p);
 }
 
 // single field cubic, turbo_tricublin.c:551-615 (AVX2 order)
@@ -199,7 +207,7 @@ __device__ __forceinline__ void interp_mono_exact(const T* __restrict__ f, const
 }
 
 // 3-component interleaved source, turbo_tricublin.c:1153-1272 (AVX2 order)
-template <typename T>
+template <typename T, bool COH = false>
 __device__ __forceinline__ void interp3_exact(const T* __restrict__ f, const double* c, int ni, int ninj, int zlinear,
                                               double* out) {
   const int n3 = 3 * ni, nn3 = 3 * ninj;
@@ -214,10 +222,10 @@ __device__ __forceinline__ void interp3_exact(const T* __restrict__ f, const dou
       const T* p1 = p0 + ninjl;
       const T* p2 = p1 + nn3;
       const T* p3 = p2 + ninjl;
-      double za = ldd(p0) * c[8];
-      za = fma(ldd(p1), c[9], za);
-      za = fma(ldd(p2), c[10], za);
-      za = fma(ldd(p3), c[11], za);
+      double za = ldd<T, COH>(p0) * c[8];
+      za = fma(ldd<T, COH>(p1), c[9], za);
+      za = fma(ldd<T, COH>(p2), c[10], za);
+      za = fma(ldd<T, COH>(p3), c[11], za);
       ya[e] = (r == 0) ? za * c[4] : fma(za, c[4 + r], ya[e]);
     }
   }
@@ -300,6 +308,7 @@ __device__ __forceinline__ void coef_mixed(WF& w, double px8, double py8, double
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
 // single field, FP32 sums with the two x-column pairs packed
+template <bool COH = false>
 __device__ __forceinline__ float interp1_mixed(const float* __restrict__ f, const WF& w, int ni, int ninj) {
   const int ninjl = w.zl ? 0 : ninj;
   const float2 cz0 = f2(w.cz[0], w.cz[0]), cz1 = f2(w.cz[1], w.cz[1]);
@@ -311,14 +320,14 @@ __device__ __forceinline__ float interp1_mixed(const float* __restrict__ f, cons
     const float* p1 = s + ninjl;
     const float* p2 = p1 + ninj;
     const float* p3 = p2 + ninjl;
-    float2 za = __fmul2_rn(f2(__ldg(s), __ldg(s + 1)), cz0);
-    float2 zb = __fmul2_rn(f2(__ldg(s + 2), __ldg(s + 3)), cz0);
-    za = __ffma2_rn(f2(__ldg(p1), __ldg(p1 + 1)), cz1, za);
-    zb = __ffma2_rn(f2(__ldg(p1 + 2), __ldg(p1 + 3)), cz1, zb);
-    za = __ffma2_rn(f2(__ldg(p2), __ldg(p2 + 1)), cz2, za);
-    zb = __ffma2_rn(f2(__ldg(p2 + 2), __ldg(p2 + 3)), cz2, zb);
-    za = __ffma2_rn(f2(__ldg(p3), __ldg(p3 + 1)), cz3, za);
-    zb = __ffma2_rn(f2(__ldg(p3 + 2), __ldg(p3 + 3)), cz3, zb);
+    float2 za = __fmul2_rn(f2(ldin<COH>(s), ldin<COH>(s + 1)), cz0);
+    float2 zb = __fmul2_rn(f2(ldin<COH>(s + 2), ldin<COH>(s + 3)), cz0);
+    za = __ffma2_rn(f2(ldin<COH>(p1), ldin<COH>(p1 + 1)), cz1, za);
+    zb = __ffma2_rn(f2(ldin<COH>(p1 + 2), ldin<COH>(p1 + 3)), cz1, zb);
+    za = __ffma2_rn(f2(ldin<COH>(p2), ldin<COH>(p2 + 1)), cz2, za);
+    zb = __ffma2_rn(f2(ldin<COH>(p2 + 2), ldin<COH>(p2 + 3)), cz2, zb);
+    za = __ffma2_rn(f2(ldin<COH>(p3), ldin<COH>(p3 + 1)), cz3, za);
+    zb = __ffma2_rn(f2(ldin<COH>(p3 + 2), ldin<COH>(p3 + 3)), cz3, zb);
     const float2 cyr = f2(w.cy[r], w.cy[r]);
     ya = __ffma2_rn(za, cyr, ya);
     yb = __ffma2_rn(zb, cyr, yb);
@@ -375,6 +384,7 @@ __device__ __forceinline__ void interp_mono_mixed(const float* __restrict__ f, c
 }
 
 // 3-component interleaved source (departure winds), FP32 sums
+template <bool COH = false>
 __device__ __forceinline__ void interp3_mixed(const float* __restrict__ f, const WF& w, int ni, int ninj,
                                               float* out) {
   const int n3 = 3 * ni, nn3 = 3 * ninj;
@@ -393,10 +403,10 @@ __device__ __forceinline__ void interp3_mixed(const float* __restrict__ f, const
     const float2 cyr = f2(w.cy[r], w.cy[r]);
 #pragma unroll
     for (int e = 0; e < 6; e++) {
-      float2 z = __fmul2_rn(f2(__ldg(s + 2 * e), __ldg(s + 2 * e + 1)), cz0);
-      z = __ffma2_rn(f2(__ldg(p1 + 2 * e), __ldg(p1 + 2 * e + 1)), cz1, z);
-      z = __ffma2_rn(f2(__ldg(p2 + 2 * e), __ldg(p2 + 2 * e + 1)), cz2, z);
-      z = __ffma2_rn(f2(__ldg(p3 + 2 * e), __ldg(p3 + 2 * e + 1)), cz3, z);
+      float2 z = __fmul2_rn(f2(ldin<COH>(s + 2 * e), ldin<COH>(s + 2 * e + 1)), cz0);
+      z = __ffma2_rn(f2(ldin<COH>(p1 + 2 * e), ldin<COH>(p1 + 2 * e + 1)), cz1, z);
+      z = __ffma2_rn(f2(ldin<COH>(p2 + 2 * e), ldin<COH>(p2 + 2 * e + 1)), cz2, z);
+      z = __ffma2_rn(f2(ldin<COH>(p3 + 2 * e), ldin<COH>(p3 + 2 * e + 1)), cz3, z);
       y[e] = __ffma2_rn(z, cyr, y[e]);
     }
   }

@@ -851,6 +851,8 @@ int adz_internal_view(const adzc_handle* h, adz::DGrid* dg, adzc_info* info, adz
   return ADZC_OK;
 }
 
+int adz_internal_warm(const adzc_handle* h) { return h && !h->cold && h->wpxyz != nullptr; }
+
 void adz_internal_after_traject(adzc_handle* h) {
   h->niter = std::max(1, h->g.itraj);
   h->cold = 0;
@@ -858,4 +860,25 @@ void adz_internal_after_traject(adzc_handle* h) {
 
 adz::DtSplit adz_internal_dt_split(const adzc_grid& g, double dt) { return dt_split(g, dt); }
 
+void adz_internal_record_positions(adzc_handle* h, int prec, double* wpxyz, const void* zdt0, const adz::DtSplit& dt) {
+  adz_internal_after_traject(h);
+  h->last_prec = prec;
+  h->wpxyz = wpxyz;
+  h->pxyzm = nullptr;
+  h->zdt0 = zdt0;
+  h->dt = dt;
+}
+
 int adz_internal_fail(int status) { return fail(status); }
+
+int adz_internal_scratch(adzc_handle* h, int prec, void** uvw, void** wdep) {
+  if (!h || !uvw || !wdep) return ADZC_ERR_ARG;
+  const adz::DGrid& D = h->dg;
+  const size_t fb = field_bytes(prec);
+  if (ensure(&h->d_uvw, &h->uvw_bytes, adz::uvw_values(prec) * fb * (size_t)D.nij * D.nk) != ADZC_OK ||
+      ensure(&h->d_wdep, &h->wdep_bytes, fb * (size_t)D.ni * D.nj * D.nk) != ADZC_OK)
+    return ADZC_ERR_ALLOC;
+  *uvw = h->d_uvw;
+  *wdep = h->d_wdep;
+  return ADZC_OK;
+}

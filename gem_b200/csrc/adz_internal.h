@@ -8,6 +8,12 @@
 int adz_internal_view(const adzc_handle* h, adz::DGrid* dg, adzc_info* info, adzc_grid* g, int* niter, int* cold);
 // the bookkeeping adzc_traject does after its launches (Adz_niter := Adz_itraj)
 void adz_internal_after_traject(adzc_handle* h);
+// 1 when the handle has completed a trajectory and is past its cold start
+int adz_internal_warm(const adzc_handle* h);
 // dt split of adz_traject.F90:38-59
 adz::DtSplit adz_internal_dt_split(const adzc_grid& g, double dt);
+// after a trajectory computed outside adzc_traject: positions now live in wpxyz
+void adz_internal_record_positions(adzc_handle* h, int prec, double* wpxyz, const void* zdt0, const adz::DtSplit& dt);
 int adz_internal_fail(int status);
+// the handle's departure-wind and departure-w scratch for a precision (allocated on first use)
+int adz_internal_scratch(adzc_handle* h, int prec, void** uvw, void** wdep);

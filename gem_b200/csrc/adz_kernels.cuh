@@ -65,37 +65,46 @@ __device__ __forceinline__ int imin_(int a, int b) { return a < b ? a : b; }
 __device__ __forceinline__ int imax_(int a, int b) { return a > b ? a : b; }
 
 // ---------------------------------------------------------------------------
+// departure winds of one extended cell e (adz_prepareWinds.F90:26-97)
+template <int PREC>
+__device__ __forceinline__ void prepare_cell(const DGrid& g, const typename Types<PREC>::F* __restrict__ uu,
+                                             const typename Types<PREC>::F* __restrict__ vv,
+                                             const typename Types<PREC>::F* __restrict__ ww,
+                                             typename Types<PREC>::F* __restrict__ uvw_d, long long e) {
+  using F = typename Types<PREC>::F;
+  const long long n = g.nij * g.nk;
+  const int k = (int)(e / g.nij) + 1;
+  const long long r = e - (long long)(k - 1) * g.nij;
+  const int jj = (int)(r / g.nit);
+  const double cyj = __ldg(g.cy + jj);
+  const double* vw = g.vw;
+  const int nk = g.nk;
+  const long long cu = WindLayout<PREC>::soa ? e : 3 * e;
+  const long long cs = WindLayout<PREC>::soa ? n : 1;  // component stride
+  uvw_d[cu] = (F)(g.inv_rayt * (double)uu[e] * cyj);
+  uvw_d[cu + cs] = (F)(g.inv_rayt * (double)vv[e]);
+  double w;
+  if (k == 1) {
+    w = g.vw5 * (double)ww[e];
+  } else if (k == nk) {
+    w = g.vw6 * (double)ww[e - g.nij];
+  } else {
+    const int km2 = imax_(1, k - 2);
+    const double wx = (k >= 3) ? __ldg(vw + 0 * (nk + 1) + k) : 0.0;
+    w = wx * (double)ww[r + (long long)(km2 - 1) * g.nij] + __ldg(vw + 1 * (nk + 1) + k) * (double)ww[e - g.nij] +
+        __ldg(vw + 2 * (nk + 1) + k) * (double)ww[e] + __ldg(vw + 3 * (nk + 1) + k) * (double)ww[e + g.nij];
+  }
+  uvw_d[cu + 2 * cs] = (F)w;
+}
+
 template <int PREC>
 __global__ void __launch_bounds__(256) k_prepare(DGrid g, const typename Types<PREC>::F* __restrict__ uu,
                                                  const typename Types<PREC>::F* __restrict__ vv,
                                                  const typename Types<PREC>::F* __restrict__ ww,
                                                  typename Types<PREC>::F* __restrict__ uvw_d) {
-  using F = typename Types<PREC>::F;
   const long long n = g.nij * g.nk;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(e / g.nij) + 1;
-    const long long r = e - (long long)(k - 1) * g.nij;
-    const int jj = (int)(r / g.nit);
-    const double cyj = __ldg(g.cy + jj);
-    const double* vw = g.vw;
-    const int nk = g.nk;
-    const long long cu = WindLayout<PREC>::soa ? e : 3 * e;
-    const long long cs = WindLayout<PREC>::soa ? n : 1;  // component stride
-    uvw_d[cu] = (F)(g.inv_rayt * (double)uu[e] * cyj);
-    uvw_d[cu + cs] = (F)(g.inv_rayt * (double)vv[e]);
-    double w;
-    if (k == 1) {
-      w = g.vw5 * (double)ww[e];
-    } else if (k == nk) {
-      w = g.vw6 * (double)ww[e - g.nij];
-    } else {
-      const int km2 = imax_(1, k - 2);
-      const double wx = (k >= 3) ? __ldg(vw + 0 * (nk + 1) + k) : 0.0;
-      w = wx * (double)ww[r + (long long)(km2 - 1) * g.nij] + __ldg(vw + 1 * (nk + 1) + k) * (double)ww[e - g.nij] +
-          __ldg(vw + 2 * (nk + 1) + k) * (double)ww[e] + __ldg(vw + 3 * (nk + 1) + k) * (double)ww[e + g.nij];
-    }
-    uvw_d[cu + 2 * cs] = (F)w;
-  }
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    prepare_cell<PREC>(g, uu, vv, ww, uvw_d, e);
 }
 
 // ---------------------------------------------------------------------------
@@ -150,143 +159,157 @@ __device__ __forceinline__ bool stencil_ok(const DGrid& g, int off) {
 }
 
 // ---------------------------------------------------------------------------
-template <int PREC>
-__global__ void ADZ_TRAJ_BOUNDS k_traject(DGrid g, TrajArgs a) {
+// COH: the departure winds were written earlier in the same launch (batch)
+template <int PREC, bool COH = false>
+__device__ __forceinline__ void traject_point(const DGrid& g, const TrajArgs& a, int i, int j, int k) {
   using F = typename Types<PREC>::F;
-  const long long nplane = (long long)g.ni * g.nj;
-  const long long n = nplane * (g.nk - a.k00 + 1);
   const F* __restrict__ uvw = (const F*)a.uvw_d;
   const F* __restrict__ ut0 = (const F*)a.ut0;
   const F* __restrict__ vt0 = (const F*)a.vt0;
   const F* __restrict__ zdt0 = (const F*)a.zdt0;
   const long long e111 = ext_index(g, 1, 1, 1);
   const F* f3 = uvw + 3 * e111;
+  const int nk = g.nk;
+  const long long e = ext_index(g, i, j, k);
+  const long long ar = arr_index(g, i, j, k);
+  // arrival winds (adz_prepareWinds.F90:40-97); Fortran forms the two sums in ``real``
+  const double alpha1 = -1.0 / 16.0, alpha2 = 9.0 / 16.0;
+  const double cyj = __ldg(g.cy + (j - g.lminy));
+  double ua, va, wa;
+  {
+    const F u1 = ut0[e - 2] + ut0[e + 1], u2 = ut0[e] + ut0[e - 1];
+    const F v1 = vt0[e - 2 * g.nit] + vt0[e + g.nit], v2 = vt0[e] + vt0[e - g.nit];
+    double uad = ((double)u1 * alpha1 + (double)u2 * alpha2) * g.inv_rayt * cyj;
+    double vad = ((double)v1 * alpha1 + (double)v2 * alpha2) * g.inv_rayt;
+    double wad;
+    if (k == 1) {
+      wad = g.vw5 * (double)zdt0[e];
+    } else if (k == nk) {
+      wad = g.vw6 * (double)zdt0[e - g.nij];
+    } else {
+      const int km2 = imax_(1, k - 2);
+      const double wx = (k >= 3) ? __ldg(g.vw + 0 * (nk + 1) + k) : 0.0;
+      wad = wx * (double)zdt0[e - (long long)(k - km2) * g.nij] + __ldg(g.vw + 1 * (nk + 1) + k) * (double)zdt0[e - g.nij] +
+            __ldg(g.vw + 2 * (nk + 1) + k) * (double)zdt0[e] + __ldg(g.vw + 3 * (nk + 1) + k) * (double)zdt0[e + g.nij];
+    }
+    if (PREC == kFp64) {
+      ua = uad; va = vad; wa = wad;
+    } else if (PREC == kRef32) {  // Adz_uu_arr etc. are ``real``
+      ua = (double)(float)uad; va = (double)(float)vad; wa = (double)(float)wad;
+    } else {
+      ua = uad; va = vad; wa = wad;
+    }
+  }
+  // starting position
+  double px, py, pz;
+  if (a.cold) {
+    px = (double)(i + g.i0g - 1); py = (double)(j + g.j0g - 1); pz = (double)k;
+  } else if (PREC == kRef32) {
+    px = a.pxyzm[3 * ar]; py = a.pxyzm[3 * ar + 1]; pz = a.pxyzm[3 * ar + 2];
+  } else {
+    px = dmin_(dmax_(a.wpxyz[wp_index(g, i, j, k, 1)], g.imnx), g.imxx);
+    py = dmin_(dmax_(a.wpxyz[wp_index(g, i, j, k, 2)], g.imny), g.imxy);
+    pz = a.wpxyz[wp_index(g, i, j, k, 3)];
+  }
+  double xm = 0.0, ym = 0.0, w3 = 0.0, wlast = 0.0;
+  bool bad = false, nonfinite = false;
+  for (int it = 0; it < a.niter; it++) {
+    double ud, vd, wd;
+    int off;
+    if (PREC == kMixed) {
+      WF w;
+      coef_mixed(w, px, py, pz, g.tab_m);
+      off = w.off;
+      if (!stencil_ok(g, off)) { bad = true; break; }
+      if (WindLayout<PREC>::soa) {
+        const long long ncell = g.nij * g.nk;
+        const float* fu = (const float*)uvw + e111 + off;
+        ud = interp1_mixed<COH>(fu, w, g.tab_m.ni, g.tab_m.nij);
+        vd = interp1_mixed<COH>(fu + ncell, w, g.tab_m.ni, g.tab_m.nij);
+        wd = interp1_mixed<COH>(fu + 2 * ncell, w, g.tab_m.ni, g.tab_m.nij);
+      } else {
+        float o[3];
+        interp3_mixed<COH>((const float*)f3 + 3LL * off, w, g.tab_m.ni, g.tab_m.nij, o);
+        ud = o[0]; vd = o[1]; wd = o[2];
+      }
+    } else {
+      double c[20];
+      int zl;
+      if (PREC == kRef32) zl = coef_f32pos(c, off, (float)px, (float)py, (float)pz, g.tab_m);
+      else zl = coef_f64pos(c, off, px, py, pz, g.tab_m);
+      if (!stencil_ok(g, off)) { bad = true; break; }
+      double o[3];
+      interp3_exact<F, COH>(f3 + 3LL * off, c, g.tab_m.ni, g.tab_m.nij, zl, o);
+      if (PREC == kRef32) {  // Tricublin_zyx3_n returns ``real``
+        ud = (double)(float)o[0]; vd = (double)(float)o[1]; wd = (double)(float)o[2];
+      } else {
+        ud = o[0]; vd = o[1]; wd = o[2];
+      }
+    }
+    xm = (double)(i + g.i0g - 1) - (a.dt.dtD * ud + a.dt.dtA * ua) * g.inv_hx;
+    ym = (double)(j + g.j0g - 1) - (a.dt.dtD * vd + a.dt.dtA * va) * g.inv_hy;
+    const double pos = __ldg(g.zm + k) - a.dt.dtzD * wd - a.dt.dtzA * wa;
+    const double zmv = dmin_(dmax_(pos, g.zmin), g.zmax);
+    int kk1 = vsearch(zmv, g.zm, g.ovdzm, g.search_m, g.pnz_m, g.sig, nk);
+    kk1 = imin_(nk + 1, imax_(0, kk1));
+    const int nb = imax_(imin_(kk1, nk - 1), 1);
+    w3 = (zmv - __ldg(g.zm + nb)) * __ldg(g.odelz_m + nb) + (double)nb;
+    wlast = wd;
+    const double cx = dmin_(dmax_(xm, g.imnx), g.imxx);
+    const double cyv = dmin_(dmax_(ym, g.imny), g.imxy);
+    if (PREC == kRef32) {
+      px = (float)cx; py = (float)cyv; pz = (float)w3;
+    } else {
+      px = cx; py = cyv; pz = w3;
+    }
+    if (!isfinite(xm) || !isfinite(ym) || !isfinite(w3)) { nonfinite = true; break; }
+  }
+  if (bad || nonfinite) {
+    raise_status(g.status, bad ? kErrHalo : kErrNonFinite);
+    return;
+  }
+  if (a.niter > 0) {
+    a.wpxyz[wp_index(g, i, j, k, 1)] = xm;
+    a.wpxyz[wp_index(g, i, j, k, 2)] = ym;
+    a.wpxyz[wp_index(g, i, j, k, 3)] = w3;
+    if (PREC == kRef32) {
+      a.pxyzm[3 * ar] = (float)px;
+      a.pxyzm[3 * ar + 1] = (float)py;
+      a.pxyzm[3 * ar + 2] = (float)pz;
+    }
+    ((F*)a.wdep)[ar] = (F)wlast;
+  }
+}
+
+template <int PREC>
+__global__ void ADZ_TRAJ_BOUNDS k_traject(DGrid g, TrajArgs a) {
+  const long long nplane = (long long)g.ni * g.nj;
+  const long long n = nplane * (g.nk - a.k00 + 1);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t % g.ni) + 1;
     const int j = (int)((t / g.ni) % g.nj) + 1;
     const int k = (int)(t / nplane) + a.k00;
-    const int nk = g.nk;
-    const long long e = ext_index(g, i, j, k);
-    const long long ar = arr_index(g, i, j, k);
-    // arrival winds (adz_prepareWinds.F90:40-97); Fortran forms the two sums in ``real``
-    const double alpha1 = -1.0 / 16.0, alpha2 = 9.0 / 16.0;
-    const double cyj = __ldg(g.cy + (j - g.lminy));
-    double ua, va, wa;
-    {
-      const F u1 = ut0[e - 2] + ut0[e + 1], u2 = ut0[e] + ut0[e - 1];
-      const F v1 = vt0[e - 2 * g.nit] + vt0[e + g.nit], v2 = vt0[e] + vt0[e - g.nit];
-      double uad = ((double)u1 * alpha1 + (double)u2 * alpha2) * g.inv_rayt * cyj;
-      double vad = ((double)v1 * alpha1 + (double)v2 * alpha2) * g.inv_rayt;
-      double wad;
-      if (k == 1) {
-        wad = g.vw5 * (double)zdt0[e];
-      } else if (k == nk) {
-        wad = g.vw6 * (double)zdt0[e - g.nij];
-      } else {
-        const int km2 = imax_(1, k - 2);
-        const double wx = (k >= 3) ? __ldg(g.vw + 0 * (nk + 1) + k) : 0.0;
-        wad = wx * (double)zdt0[e - (long long)(k - km2) * g.nij] + __ldg(g.vw + 1 * (nk + 1) + k) * (double)zdt0[e - g.nij] +
-              __ldg(g.vw + 2 * (nk + 1) + k) * (double)zdt0[e] + __ldg(g.vw + 3 * (nk + 1) + k) * (double)zdt0[e + g.nij];
-      }
-      if (PREC == kFp64) {
-        ua = uad; va = vad; wa = wad;
-      } else if (PREC == kRef32) {  // Adz_uu_arr etc. are ``real``
-        ua = (double)(float)uad; va = (double)(float)vad; wa = (double)(float)wad;
-      } else {
-        ua = uad; va = vad; wa = wad;
-      }
-    }
-    // starting position
-    double px, py, pz;
-    if (a.cold) {
-      px = (double)(i + g.i0g - 1); py = (double)(j + g.j0g - 1); pz = (double)k;
-    } else if (PREC == kRef32) {
-      px = a.pxyzm[3 * ar]; py = a.pxyzm[3 * ar + 1]; pz = a.pxyzm[3 * ar + 2];
-    } else {
-      px = dmin_(dmax_(a.wpxyz[wp_index(g, i, j, k, 1)], g.imnx), g.imxx);
-      py = dmin_(dmax_(a.wpxyz[wp_index(g, i, j, k, 2)], g.imny), g.imxy);
-      pz = a.wpxyz[wp_index(g, i, j, k, 3)];
-    }
-    double xm = 0.0, ym = 0.0, w3 = 0.0, wlast = 0.0;
-    bool bad = false, nonfinite = false;
-    for (int it = 0; it < a.niter; it++) {
-      double ud, vd, wd;
-      int off;
-      if (PREC == kMixed) {
-        WF w;
-        coef_mixed(w, px, py, pz, g.tab_m);
-        off = w.off;
-        if (!stencil_ok(g, off)) { bad = true; break; }
-        if (WindLayout<PREC>::soa) {
-          const long long ncell = g.nij * g.nk;
-          const float* fu = (const float*)uvw + e111 + off;
-          ud = interp1_mixed(fu, w, g.tab_m.ni, g.tab_m.nij);
-          vd = interp1_mixed(fu + ncell, w, g.tab_m.ni, g.tab_m.nij);
-          wd = interp1_mixed(fu + 2 * ncell, w, g.tab_m.ni, g.tab_m.nij);
-        } else {
-          float o[3];
-          interp3_mixed((const float*)f3 + 3LL * off, w, g.tab_m.ni, g.tab_m.nij, o);
-          ud = o[0]; vd = o[1]; wd = o[2];
-        }
-      } else {
-        double c[20];
-        int zl;
-        if (PREC == kRef32) zl = coef_f32pos(c, off, (float)px, (float)py, (float)pz, g.tab_m);
-        else zl = coef_f64pos(c, off, px, py, pz, g.tab_m);
-        if (!stencil_ok(g, off)) { bad = true; break; }
-        double o[3];
-        interp3_exact<F>(f3 + 3LL * off, c, g.tab_m.ni, g.tab_m.nij, zl, o);
-        if (PREC == kRef32) {  // Tricublin_zyx3_n returns ``real``
-          ud = (double)(float)o[0]; vd = (double)(float)o[1]; wd = (double)(float)o[2];
-        } else {
-          ud = o[0]; vd = o[1]; wd = o[2];
-        }
-      }
-      xm = (double)(i + g.i0g - 1) - (a.dt.dtD * ud + a.dt.dtA * ua) * g.inv_hx;
-      ym = (double)(j + g.j0g - 1) - (a.dt.dtD * vd + a.dt.dtA * va) * g.inv_hy;
-      const double pos = __ldg(g.zm + k) - a.dt.dtzD * wd - a.dt.dtzA * wa;
-      const double zmv = dmin_(dmax_(pos, g.zmin), g.zmax);
-      int kk1 = vsearch(zmv, g.zm, g.ovdzm, g.search_m, g.pnz_m, g.sig, nk);
-      kk1 = imin_(nk + 1, imax_(0, kk1));
-      const int nb = imax_(imin_(kk1, nk - 1), 1);
-      w3 = (zmv - __ldg(g.zm + nb)) * __ldg(g.odelz_m + nb) + (double)nb;
-      wlast = wd;
-      const double cx = dmin_(dmax_(xm, g.imnx), g.imxx);
-      const double cyv = dmin_(dmax_(ym, g.imny), g.imxy);
-      if (PREC == kRef32) {
-        px = (float)cx; py = (float)cyv; pz = (float)w3;
-      } else {
-        px = cx; py = cyv; pz = w3;
-      }
-      if (!isfinite(xm) || !isfinite(ym) || !isfinite(w3)) { nonfinite = true; break; }
-    }
-    if (bad || nonfinite) {
-      raise_status(g.status, bad ? kErrHalo : kErrNonFinite);
-      continue;
-    }
-    if (a.niter > 0) {
-      a.wpxyz[wp_index(g, i, j, k, 1)] = xm;
-      a.wpxyz[wp_index(g, i, j, k, 2)] = ym;
-      a.wpxyz[wp_index(g, i, j, k, 3)] = w3;
-      if (PREC == kRef32) {
-        a.pxyzm[3 * ar] = (float)px;
-        a.pxyzm[3 * ar + 1] = (float)py;
-        a.pxyzm[3 * ar + 2] = (float)pz;
-      }
-      ((F*)a.wdep)[ar] = (F)wlast;
-    }
+    traject_point<PREC>(g, a, i, j, k);
   }
 }
 
 // ---------------------------------------------------------------------------
 // position of arrival point (i,j,k) of a set, adz_interp_traj.F90:45-187
-template <int PREC>
+// CG: read the trajectory arrays around L1 (ld.global.cg), for a kernel that
+// wrote them itself earlier in the same launch
+template <typename T, bool CG>
+__device__ __forceinline__ T ld_traj(const T* p) {
+  if (CG) return __ldcg(p);
+  return *p;
+}
+
+template <int PREC, bool CG = false>
 __device__ __forceinline__ void set_position(const DGrid& g, const SetArgs& a, int set, int i, int j, int k, double& px,
                                              double& py, double& pz) {
   using F = typename Types<PREC>::F;
   const double aa = -0.0625, bb = 0.5625, half = 0.5;
   const double* W = a.wpxyz;
-#define WPX(ii, jj, kk, cc) W[wp_index(g, ii, jj, kk, cc)]
+#define WPX(ii, jj, kk, cc) ld_traj<double, CG>(W + wp_index(g, ii, jj, kk, cc))
   if (set == 0) {
     if (PREC == kRef32) {
       const long long ar = arr_index(g, i, j, k);
@@ -317,7 +340,7 @@ __device__ __forceinline__ void set_position(const DGrid& g, const SetArgs& a, i
   const F* zd = (const F*)a.zdt0;
   const int nk = g.nk;
   const long long e = ext_index(g, i, j, k);
-#define WD(kk) wd[arr_index(g, i, j, kk)]
+#define WD(kk) ld_traj<F, CG>(wd + arr_index(g, i, j, kk))
   double xt, yt, ztv;
   if (k >= imax_(a.k00, 2) && k <= nk - 2) {
     const double* vw = g.vw;
@@ -360,62 +383,68 @@ __device__ __forceinline__ void set_position(const DGrid& g, const SetArgs& a, i
   pz = zindx_t(g, ztv);
 }
 
-template <int PREC>
-__global__ void ADZ_SET_BOUNDS k_tricub_set(DGrid g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
-                                                    SetArgs a, FieldPtrs fp) {
+template <int PREC, bool CG = false>
+__device__ __forceinline__ void set_point(const DGrid& g, int set, const SetArgs& a, const FieldPtrs& fp, int i,
+                                          int j, int k) {
   using F = typename Types<PREC>::F;
-  const long long nplane = (long long)nx * ny;
-  const long long n = nplane * nz;
   const DZtab& lv = (set == 3) ? g.tab_t : g.tab_m;
   const long long e111 = ext_index(g, 1, 1, 1);
+  double px, py, pz;
+  set_position<PREC, CG>(g, a, set, i, j, k, px, py, pz);
+  const long long e = ext_index(g, i, j, k);
+  if (PREC == kMixed) {
+    WF w;
+    coef_mixed(w, px, py, pz, lv);
+    if (!stencil_ok(g, w.off)) { raise_status(g.status, kErrHalo); return; }
+    for (int q = 0; q < fp.nf; q++) {
+      const float* f = (const float*)fp.src[q] + e111 + w.off;
+      if ((fp.mono_mask >> q) & 1u) {
+        float d, lin, mn, mx;
+        interp_mono_mixed(f, w, lv.ni, lv.nij, d, lin, mn, mx);
+        if ((fp.clip_mask >> q) & 1u) d = fmaxf(mn, fminf(mx, d));
+        if (fp.lin[q]) ((float*)fp.lin[q])[e] = fmaxf(mn, fminf(mx, lin));
+        if (fp.mn[q]) ((float*)fp.mn[q])[e] = mn;
+        if (fp.mx[q]) ((float*)fp.mx[q])[e] = mx;
+        ((float*)fp.dst[q])[e] = d;
+      } else {
+        ((float*)fp.dst[q])[e] = interp1_mixed(f, w, lv.ni, lv.nij);
+      }
+    }
+  } else {
+    double c[20];
+    int off, zl;
+    if (PREC == kRef32) zl = coef_f32pos(c, off, (float)px, (float)py, (float)pz, lv);
+    else zl = coef_f64pos(c, off, px, py, pz, lv);
+    if (!stencil_ok(g, off)) { raise_status(g.status, kErrHalo); return; }
+    for (int q = 0; q < fp.nf; q++) {
+      const F* f = (const F*)fp.src[q] + e111 + off;
+      if ((fp.mono_mask >> q) & 1u) {
+        double d, lin, mn, mx;
+        interp_mono_exact<F>(f, c, lv.ni, lv.nij, zl, fp.box222 != 0, d, lin, mn, mx);
+        F df = (F)d, lf = (F)lin, mnf = (F)mn, mxf = (F)mx;
+        // Adz_post lin/min/max (adz_interp_hlt.F90:156-158), clip of adz_post_tr.F90:86-89
+        if ((fp.clip_mask >> q) & 1u) df = (mnf > ((mxf < df) ? mxf : df)) ? mnf : ((mxf < df) ? mxf : df);
+        if (fp.lin[q]) ((F*)fp.lin[q])[e] = (mnf > ((mxf < lf) ? mxf : lf)) ? mnf : ((mxf < lf) ? mxf : lf);
+        if (fp.mn[q]) ((F*)fp.mn[q])[e] = mnf;
+        if (fp.mx[q]) ((F*)fp.mx[q])[e] = mxf;
+        ((F*)fp.dst[q])[e] = df;
+      } else {
+        ((F*)fp.dst[q])[e] = (F)interp1_exact<F>(f, c, lv.ni, lv.nij, zl);
+      }
+    }
+  }
+}
+
+template <int PREC>
+__global__ void ADZ_SET_BOUNDS k_tricub_set(DGrid g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
+                                            SetArgs a, FieldPtrs fp) {
+  const long long nplane = (long long)nx * ny;
+  const long long n = nplane * nz;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t % nx) + i0;
     const int j = (int)((t / nx) % ny) + j0;
     const int k = (int)(t / nplane) + k0;
-    double px, py, pz;
-    set_position<PREC>(g, a, set, i, j, k, px, py, pz);
-    const long long e = ext_index(g, i, j, k);
-    if (PREC == kMixed) {
-      WF w;
-      coef_mixed(w, px, py, pz, lv);
-      if (!stencil_ok(g, w.off)) { raise_status(g.status, kErrHalo); continue; }
-      for (int q = 0; q < fp.nf; q++) {
-        const float* f = (const float*)fp.src[q] + e111 + w.off;
-        if ((fp.mono_mask >> q) & 1u) {
-          float d, lin, mn, mx;
-          interp_mono_mixed(f, w, lv.ni, lv.nij, d, lin, mn, mx);
-          if ((fp.clip_mask >> q) & 1u) d = fmaxf(mn, fminf(mx, d));
-          if (fp.lin[q]) ((float*)fp.lin[q])[e] = fmaxf(mn, fminf(mx, lin));
-          if (fp.mn[q]) ((float*)fp.mn[q])[e] = mn;
-          if (fp.mx[q]) ((float*)fp.mx[q])[e] = mx;
-          ((float*)fp.dst[q])[e] = d;
-        } else {
-          ((float*)fp.dst[q])[e] = interp1_mixed(f, w, lv.ni, lv.nij);
-        }
-      }
-    } else {
-      double c[20];
-      int off, zl;
-      if (PREC == kRef32) zl = coef_f32pos(c, off, (float)px, (float)py, (float)pz, lv);
-      else zl = coef_f64pos(c, off, px, py, pz, lv);
-      if (!stencil_ok(g, off)) { raise_status(g.status, kErrHalo); continue; }
-      for (int q = 0; q < fp.nf; q++) {
-        const F* f = (const F*)fp.src[q] + e111 + off;
-        if ((fp.mono_mask >> q) & 1u) {
-          double d, lin, mn, mx;
-          interp_mono_exact<F>(f, c, lv.ni, lv.nij, zl, fp.box222 != 0, d, lin, mn, mx);
-          F df = (F)d, lf = (F)lin, mnf = (F)mn, mxf = (F)mx;
-          // Adz_post lin/min/max (adz_interp_hlt.F90:156-158), clip of adz_post_tr.F90:86-89
-          if ((fp.clip_mask >> q) & 1u) df = (mnf > ((mxf < df) ? mxf : df)) ? mnf : ((mxf < df) ? mxf : df);
-          if (fp.lin[q]) ((F*)fp.lin[q])[e] = (mnf > ((mxf < lf) ? mxf : lf)) ? mnf : ((mxf < lf) ? mxf : lf);
-          if (fp.mn[q]) ((F*)fp.mn[q])[e] = mnf;
-          if (fp.mx[q]) ((F*)fp.mx[q])[e] = mxf;
-          ((F*)fp.dst[q])[e] = df;
-        } else {
-          ((F*)fp.dst[q])[e] = (F)interp1_exact<F>(f, c, lv.ni, lv.nij, zl);
-        }
-      }
-    }
+    set_point<PREC>(g, set, a, fp, i, j, k);
   }
 }
 
@@ -485,6 +514,96 @@ __global__ void __launch_bounds__(128) k_interp_pos(DZtab lv, int n, const void*
 }
 
 // ---------------------------------------------------------------------------
+// persistent batch kernel: work items (domain, phase, group, first, count) taken
+// from an atomic queue; phase p>0 items wait (bounded) on the per-domain count
+// of completed phase p-1 items.  Item list and host side: adz_batch.cu.
+constexpr unsigned long long kDepSpins = 1ull << 24;  // >= 1 s of 64 ns sleeps
+
+template <int PREC>
+__global__ void __launch_bounds__(128) k_batch(const BDom* __restrict__ doms, const BItem* __restrict__ items,
+                                               long long nitems, const unsigned* __restrict__ need,
+                                               unsigned long long* __restrict__ next, unsigned* __restrict__ done,
+                                               int* __restrict__ status) {
+  __shared__ long long cur;
+  __shared__ int dep_ok;
+  __shared__ DGrid sg;
+  __shared__ TrajArgs sta;
+  __shared__ SetArgs ssa;
+  __shared__ FieldPtrs sfp;
+  __shared__ const void* swind[4];
+  __shared__ int sset, srange[5];
+  for (;;) {
+    if (threadIdx.x == 0) cur = (long long)atomicAdd(next, 1ull);
+    __syncthreads();
+    const long long it = cur;
+    if (it >= nitems) break;
+    const BItem item = items[it];
+    if (threadIdx.x == 0) {
+      dep_ok = 1;
+      if (item.phase > 0) {
+        const unsigned target = need[item.dom * 2 + item.phase - 1];
+        const unsigned* d = done + item.dom * 2 + item.phase - 1;
+        unsigned long long spins = 0;
+        unsigned v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(d) : "memory");
+        while (v < target) {
+          if (++spins > kDepSpins) {
+            dep_ok = 0;
+            atomicOr(status, kErrTimeout);
+            break;
+          }
+          __nanosleep(64);
+          asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(d) : "memory");
+        }
+      }
+      sg = doms[item.dom].g;
+      if (item.phase == 0) {
+        swind[0] = doms[item.dom].uu;
+        swind[1] = doms[item.dom].vv;
+        swind[2] = doms[item.dom].ww;
+        swind[3] = doms[item.dom].ta.uvw_d;
+      }
+      if (item.phase == 1) sta = doms[item.dom].ta;
+      if (item.phase == 2) {
+        ssa = doms[item.dom].sa;
+        sfp = doms[item.dom].gfp[item.group];
+        sset = doms[item.dom].gset[item.group];
+        for (int q = 0; q < 5; q++) srange[q] = doms[item.dom].grange[item.group][q];
+      }
+    }
+    __syncthreads();
+    if (dep_ok) {
+      const long long end = item.start + item.count;
+      if (item.phase == 0) {
+        using F = typename Types<PREC>::F;
+        for (long long e = item.start + threadIdx.x; e < end; e += blockDim.x)
+          prepare_cell<PREC>(sg, (const F*)swind[0], (const F*)swind[1], (const F*)swind[2], (F*)swind[3], e);
+      } else if (item.phase == 1) {
+        const long long plane = (long long)sg.ni * sg.nj;
+        for (long long t = item.start + threadIdx.x; t < end; t += blockDim.x) {
+          const int i = (int)(t % sg.ni) + 1, j = (int)((t / sg.ni) % sg.nj) + 1;
+          const int k = (int)(t / plane) + sta.k00;
+          traject_point<PREC, true>(sg, sta, i, j, k);
+        }
+      } else {
+        const int nx = srange[1], ny = srange[3];
+        const long long plane = (long long)nx * ny;
+        for (long long t = item.start + threadIdx.x; t < end; t += blockDim.x) {
+          const int i = (int)(t % nx) + srange[0], j = (int)((t / nx) % ny) + srange[2];
+          const int k = (int)(t / plane) + srange[4];
+          set_point<PREC, true>(sg, sset, ssa, sfp, i, j, k);
+        }
+      }
+    }
+    __syncthreads();  // the block's writes of this item precede thread 0's fence
+    if (threadIdx.x == 0 && item.phase < 2) {
+      __threadfence();
+      atomicAdd(done + item.dom * 2 + item.phase, 1u);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // launchers (host)
 inline int grid_for(long long n, int block, int max_blocks = 148 * 64) {
   long long b = (n + block - 1) / block;
@@ -536,12 +655,29 @@ cudaError_t launch_interp_pos(const DZtab& lv, int kind, int n, const void* pos,
   return cudaGetLastError();
 }
 
+template <int PREC>
+cudaError_t launch_batch(int grid, const BDom* doms, const BItem* items, long long nitems, const unsigned* need,
+                         unsigned long long* next, unsigned* done, int* status, cudaStream_t s) {
+  k_batch<PREC><<<grid, 128, 0, s>>>(doms, items, nitems, need, next, done, status);
+  return cudaGetLastError();
+}
+
+template <int PREC>
+int batch_resident_blocks() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch<PREC>, 128, 0) != cudaSuccess) return 0;
+  return n;
+}
+
 #define ADZ_INSTANTIATE(P)                                                                                         \
   template cudaError_t launch_prepare<P>(const DGrid&, const void*, const void*, const void*, void*, cudaStream_t); \
   template cudaError_t launch_inittraj<P>(const DGrid&, float*, double*, cudaStream_t);                            \
   template cudaError_t launch_traject<P>(const DGrid&, const TrajArgs&, cudaStream_t);                             \
   template cudaError_t launch_tricub_set<P>(const DGrid&, int, int, int, int, int, int, int, const SetArgs&,       \
                                             const FieldPtrs&, cudaStream_t);                                       \
-  template cudaError_t launch_interp_pos<P>(const DZtab&, int, int, const void*, const FieldPtrs&, cudaStream_t);
+  template cudaError_t launch_interp_pos<P>(const DZtab&, int, int, const void*, const FieldPtrs&, cudaStream_t); \
+  template cudaError_t launch_batch<P>(int, const BDom*, const BItem*, long long, const unsigned*,                \
+                                       unsigned long long*, unsigned*, int*, cudaStream_t);                        \
+  template int batch_resident_blocks<P>();
 
 }  // namespace adz

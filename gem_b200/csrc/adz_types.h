@@ -122,4 +122,31 @@ template <int PREC>
 cudaError_t launch_interp_pos(const DZtab& lv, int kind, int n, const void* pos, const FieldPtrs& fp,
                               cudaStream_t s);
 
+// ---- batches of domains in one persistent launch (adz_batch.cu) ----
+constexpr int kMaxGroups = 8;  // field groups per domain (a set may need several)
+
+struct BDom {
+  DGrid g;
+  const void* uu;  // departure winds (ext layout) read by phase 0
+  const void* vv;
+  const void* ww;
+  TrajArgs ta;
+  SetArgs sa;
+  int ngroups;
+  int gset[kMaxGroups];        // position set of each group
+  int grange[kMaxGroups][5];   // i0, nx, j0, ny, k0 of each group's set
+  FieldPtrs gfp[kMaxGroups];
+};
+
+struct BItem {
+  int dom, phase, group, pad;
+  long long start, count;
+};
+
+template <int PREC>
+cudaError_t launch_batch(int grid, const BDom* doms, const BItem* items, long long nitems, const unsigned* need,
+                         unsigned long long* next, unsigned* done, int* status, cudaStream_t s);
+template <int PREC>
+int batch_resident_blocks();  // k_batch blocks of 128 threads resident per SM
+
 }  // namespace adz

@@ -150,6 +150,31 @@ def config_mixed(ni=1024, nj=1024, nk=80, seed=4321, ntracers=8) -> Config:
     return c
 
 
+def config_batch(n=16, seed=2024, size=(256, 1024), levels=(40, 80), tracers=(1, 20)) -> list:
+    """Independent limited-area domains of uneven size for one batched step:
+    ni, nj seeded integers in ``size``, nk in ``levels``, 1-20 log-normal
+    FP32 tracers (mono on), each domain with its own deformational-flow phase,
+    U0 in 20-60 m/s and dt in 60-300 s.  The grid length keeps the Courant
+    number near 2 (dx = max(2.5 km, U0 dt / 2)); W0 keeps the vertical
+    displacement per step at 30 m."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for d in range(n):
+        ni = int(rng.integers(size[0], size[1] + 1))
+        nj = int(rng.integers(size[0], size[1] + 1))
+        nk = int(rng.integers(levels[0], levels[1] + 1))
+        ntr = int(rng.integers(tracers[0], tracers[1] + 1))
+        u0 = float(rng.uniform(20.0, 60.0))
+        dt = float(rng.uniform(60.0, 300.0))
+        ph = (float(rng.uniform(0, 1)), float(rng.uniform(0, 1)))
+        dx = max(2.5e3, u0 * dt / 2.0)
+        c = Config(f"batch{d}", ni, nj, nk, dx, dt, stretched_levels(nk, 20.0, 1000.0, 25e3), seed=seed + 97 * d,
+                   ntracers=ntr, tracer_kind="lognormal", mono=True, phase=ph, u0=u0, w0=30.0 / dt,
+                   bell_radius=0.2 * ni * dx)
+        out.append(c)
+    return out
+
+
 def _coords(cfg: Config, device, dtype):
     H = cfg.halo
     nit, njt = cfg.ni + 2 * H, cfg.nj + 2 * H

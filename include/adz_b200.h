@@ -196,6 +196,40 @@ int adzc_tricub_sets(adzc_handle *h, int prec, const int *nfields, const void *c
  * ADZC_ERR_NONFINITE ...); synchronises the stream; clears it when reset. */
 int adzc_status(adzc_handle *h, int reset, void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* Batches of independent domains: one persistent launch per step            */
+/* ------------------------------------------------------------------------ */
+/* Each domain is a tile set up with adzc_setup and already past its cold
+ * start (adzc_inittraj + one adzc_traject).  The batch steps every domain as
+ * adzc_traject + adzc_tricub on each set would (B/adz_main.F90 and
+ * B/adz_tracers.F90 for many limited-area domains at once) in ONE persistent
+ * kernel launch, replayed from a CUDA graph.  ADZC_FP64 or ADZC_MIXED. */
+typedef struct {
+  adzc_handle *h;
+  double dt;
+  int niter;                      /* 0: the handle's Adz_itraj                     */
+  const void *uu_ext, *vv_ext, *ww_ext, *ut0, *vt0, *zdt0;
+  double *wpxyz;
+  int nfields[4];                 /* fields of sets Q, U, V, T                     */
+  const void *const *srcs;        /* HOST arrays of DEVICE pointers, all sets      */
+  void *const *dsts;              /* in set order; copied by adzc_batch_create    */
+  const int *mono;                /* NULL or per field 0/1/2 as in adzc_tricub     */
+} adzc_domain;
+
+typedef struct adzc_batch adzc_batch;
+
+int adzc_batch_create(int prec, int ndom, const adzc_domain *doms, adzc_batch **out);
+/* autotuner: times candidate tile heights (rows per work item) and resident
+ * blocks per SM on these domains, keeps the fastest and re-captures the graph.
+ * The timed launches are real steps: they advance the domains' positions. */
+int adzc_batch_tune(adzc_batch *b, void *stream);
+int adzc_batch_step(adzc_batch *b, void *stream);
+int adzc_batch_query(const adzc_batch *b, int *rows_per_item, int *blocks_per_sm, long long *nitems);
+/* synchronises; ADZC_ERR_TIMEOUT when a dependency wait gave up, else the
+ * first non-zero status of the domains' handles */
+int adzc_batch_status(adzc_batch *b, int reset, void *stream);
+int adzc_batch_destroy(adzc_batch *b);
+
 /* One whole advection step that allocates no device memory.  No counterpart
  * in the reference (its Fortran drivers use automatic arrays).
  *
