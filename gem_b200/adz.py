@@ -304,7 +304,7 @@ class Adz:
 
 def step_fused(adz: Adz, prec, dt, winds, fields, tracers, pxyzm, wpxyz, outs, tr_outs, mono, niter=0, stream=None):
     """One advection step: trajectory, then u@pmu, v@pmv and w + every tracer
-    @pt through adzc_tricub_sets (one launch for MIXED)."""
+    @pt through adzc_tricub_sets (one launch per position set)."""
     adz.adz_traject(prec, dt, winds, pxyzm, wpxyz, niter, stream)
     srcs = [fields["src_u"], fields["src_v"], fields["src_w"]] + list(tracers)
     dsts = [outs["u"], outs["v"], outs["w"]] + list(tr_outs)

@@ -43,7 +43,7 @@ struct adzc_batch {
   unsigned long long* d_next = nullptr;
   unsigned* d_done = nullptr;
   int* d_status = nullptr;
-  int rows = 8, bps = 4, sms = 148;
+  int rows = 8, bps = 4, sms = 148, variant = 0;
   cudaStream_t cap = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -98,10 +98,15 @@ cudaError_t enqueue(adzc_batch* b, cudaStream_t s) {
   if ((e = cudaMemsetAsync(b->d_done, 0, 2 * b->ndom * sizeof(unsigned), s)) != cudaSuccess) return e;
   const int grid = b->bps * b->sms;
   if (b->prec == ADZC_FP64)
-    return adz::launch_batch<adz::kFp64>(grid, b->d_doms, b->d_items, b->nitems, b->d_need, b->d_next, b->d_done,
-                                         b->d_status, s);
-  return adz::launch_batch<adz::kMixed>(grid, b->d_doms, b->d_items, b->nitems, b->d_need, b->d_next, b->d_done,
-                                        b->d_status, s);
+    return adz::launch_batch<adz::kFp64>(b->variant, grid, b->d_doms, b->d_items, b->nitems, b->d_need, b->d_next,
+                                         b->d_done, b->d_status, s);
+  return adz::launch_batch<adz::kMixed>(b->variant, grid, b->d_doms, b->d_items, b->nitems, b->d_need, b->d_next,
+                                        b->d_done, b->d_status, s);
+}
+
+int resident(const adzc_batch* b, int variant) {
+  return b->prec == ADZC_FP64 ? adz::batch_resident_blocks<adz::kFp64>(variant)
+                              : adz::batch_resident_blocks<adz::kMixed>(variant);
 }
 
 // the handles' positions now live in the domains' wpxyz (adzc_tricub may follow)
@@ -156,8 +161,7 @@ extern "C" int adzc_batch_create(int prec, int ndom, const adzc_domain* doms, ad
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
-  b->bps = std::max(1, prec == ADZC_FP64 ? adz::batch_resident_blocks<adz::kFp64>()
-                                         : adz::batch_resident_blocks<adz::kMixed>());
+  b->bps = std::max(1, resident(b, 0));
   for (int d = 0; d < ndom; d++) {
     const adzc_domain& in = doms[d];
     adz::BDom& D = b->doms[d];
@@ -268,33 +272,43 @@ extern "C" int adzc_batch_tune(adzc_batch* b, void* stream) {
   if (!b) return adz_internal_fail(ADZC_ERR_ARG);
   const cudaStream_t s = (cudaStream_t)stream;
   const int rows_c[] = {2, 8, 32};
-  const int res = std::max(1, b->prec == ADZC_FP64 ? adz::batch_resident_blocks<adz::kFp64>()
-                                                   : adz::batch_resident_blocks<adz::kMixed>());
-  const int bps_c[] = {std::max(1, res / 2), res};
   float best = 1e30f;
-  int br = b->rows, bb = b->bps;
+  int br = b->rows, bb = b->bps, bv = b->variant;
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
-  for (int r : rows_c)
-    for (int p : bps_c) {
-      b->bps = p;
-      if (build_items(b, r) != ADZC_OK || enqueue(b, s) != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
+  int st = ADZC_OK;
+  for (int v = 0; v < adz::kBatchVariants && st == ADZC_OK; v++) {
+    const int res = resident(b, v);  // persistent: every block resident
+    if (res < 1) continue;
+    for (int r : rows_c) {
+      b->variant = v;
+      b->bps = res;
+      if (build_items(b, r) != ADZC_OK || enqueue(b, s) != cudaSuccess) {
+        st = ADZC_ERR_CUDA;
+        break;
+      }
       cudaEventRecord(e0, s);
       for (int rep = 0; rep < 2; rep++) enqueue(b, s);
       cudaEventRecord(e1, s);
-      if (cudaEventSynchronize(e1) != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        st = ADZC_ERR_CUDA;
+        break;
+      }
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
       if (ms < best) {
         best = ms;
         br = r;
-        bb = p;
+        bb = res;
+        bv = v;
       }
     }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   b->bps = bb;
-  int st = build_items(b, br);
+  b->variant = bv;
+  if (st == ADZC_OK) st = build_items(b, br);
   if (st == ADZC_OK) st = capture(b);
   record(b);
   return st == ADZC_OK ? ADZC_OK : adz_internal_fail(st);

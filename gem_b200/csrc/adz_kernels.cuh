@@ -519,11 +519,22 @@ __global__ void __launch_bounds__(128) k_interp_pos(DZtab lv, int n, const void*
 // of completed phase p-1 items.  Item list and host side: adz_batch.cu.
 constexpr unsigned long long kDepSpins = 1ull << 24;  // >= 1 s of 64 ns sleeps
 
-template <int PREC>
-__global__ void __launch_bounds__(128) k_batch(const BDom* __restrict__ doms, const BItem* __restrict__ items,
-                                               long long nitems, const unsigned* __restrict__ need,
-                                               unsigned long long* __restrict__ next, unsigned* __restrict__ done,
-                                               int* __restrict__ status) {
+// block-wide copy of a descriptor into shared memory (8-byte words)
+template <typename T>
+__device__ __forceinline__ void block_copy(T* dst, const T* src) {
+  static_assert(sizeof(T) % 8 == 0, "descriptor size");
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
+  for (int q = threadIdx.x; q < (int)(sizeof(T) / 8); q += blockDim.x) d[q] = s[q];
+}
+
+// MINB: minimum resident blocks per SM handed to ptxas (register budget);
+// the autotuner picks the variant
+template <int PREC, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_batch(const BDom* __restrict__ doms, const BItem* __restrict__ items,
+                                                     long long nitems, const unsigned* __restrict__ need,
+                                                     unsigned long long* __restrict__ next,
+                                                     unsigned* __restrict__ done, int* __restrict__ status) {
   __shared__ long long cur;
   __shared__ int dep_ok;
   __shared__ DGrid sg;
@@ -556,19 +567,18 @@ __global__ void __launch_bounds__(128) k_batch(const BDom* __restrict__ doms, co
           asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(d) : "memory");
         }
       }
-      sg = doms[item.dom].g;
-      if (item.phase == 0) {
-        swind[0] = doms[item.dom].uu;
-        swind[1] = doms[item.dom].vv;
-        swind[2] = doms[item.dom].ww;
-        swind[3] = doms[item.dom].ta.uvw_d;
-      }
-      if (item.phase == 1) sta = doms[item.dom].ta;
+    }
+    {
+      const BDom& D = doms[item.dom];
+      block_copy(&sg, &D.g);
+      if (item.phase == 0 && threadIdx.x < 4)
+        swind[threadIdx.x] = threadIdx.x == 0 ? D.uu : threadIdx.x == 1 ? D.vv : threadIdx.x == 2 ? D.ww : D.ta.uvw_d;
+      if (item.phase == 1) block_copy(&sta, &D.ta);
       if (item.phase == 2) {
-        ssa = doms[item.dom].sa;
-        sfp = doms[item.dom].gfp[item.group];
-        sset = doms[item.dom].gset[item.group];
-        for (int q = 0; q < 5; q++) srange[q] = doms[item.dom].grange[item.group][q];
+        block_copy(&ssa, &D.sa);
+        block_copy(&sfp, &D.gfp[item.group]);
+        if (threadIdx.x < 5) srange[threadIdx.x] = D.grange[item.group][threadIdx.x];
+        if (threadIdx.x == 5) sset = D.gset[item.group];
       }
     }
     __syncthreads();
@@ -655,18 +665,42 @@ cudaError_t launch_interp_pos(const DZtab& lv, int kind, int n, const void* pos,
   return cudaGetLastError();
 }
 
+// register-budget variants of the batch kernel (minimum resident blocks of
+// 128 threads per SM handed to ptxas); FP64 needs about twice the registers
+template <int PREC, int V>
+struct BatchMinB {
+  static constexpr int value = PREC == kFp64 ? 4 + V : (V == 0 ? 6 : V == 1 ? 7 : 9);
+};
+
 template <int PREC>
-cudaError_t launch_batch(int grid, const BDom* doms, const BItem* items, long long nitems, const unsigned* need,
-                         unsigned long long* next, unsigned* done, int* status, cudaStream_t s) {
-  k_batch<PREC><<<grid, 128, 0, s>>>(doms, items, nitems, need, next, done, status);
-  return cudaGetLastError();
+cudaError_t launch_batch(int variant, int grid, const BDom* doms, const BItem* items, long long nitems,
+                         const unsigned* need, unsigned long long* next, unsigned* done, int* status,
+                         cudaStream_t s) {
+  if constexpr (PREC == kRef32) {
+    return cudaErrorNotSupported;
+  } else {
+    if (variant == 1)
+      k_batch<PREC, BatchMinB<PREC, 1>::value><<<grid, 128, 0, s>>>(doms, items, nitems, need, next, done, status);
+    else if (variant == 2)
+      k_batch<PREC, BatchMinB<PREC, 2>::value><<<grid, 128, 0, s>>>(doms, items, nitems, need, next, done, status);
+    else
+      k_batch<PREC, BatchMinB<PREC, 0>::value><<<grid, 128, 0, s>>>(doms, items, nitems, need, next, done, status);
+    return cudaGetLastError();
+  }
 }
 
 template <int PREC>
-int batch_resident_blocks() {
-  int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch<PREC>, 128, 0) != cudaSuccess) return 0;
-  return n;
+int batch_resident_blocks(int variant) {
+  if constexpr (PREC == kRef32) {
+    return 0;
+  } else {
+    const void* f = variant == 1   ? (const void*)k_batch<PREC, BatchMinB<PREC, 1>::value>
+                    : variant == 2 ? (const void*)k_batch<PREC, BatchMinB<PREC, 2>::value>
+                                   : (const void*)k_batch<PREC, BatchMinB<PREC, 0>::value>;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, 128, 0) != cudaSuccess) return 0;
+    return n;
+  }
 }
 
 #define ADZ_INSTANTIATE(P)                                                                                         \
@@ -676,8 +710,8 @@ int batch_resident_blocks() {
   template cudaError_t launch_tricub_set<P>(const DGrid&, int, int, int, int, int, int, int, const SetArgs&,       \
                                             const FieldPtrs&, cudaStream_t);                                       \
   template cudaError_t launch_interp_pos<P>(const DZtab&, int, int, const void*, const FieldPtrs&, cudaStream_t); \
-  template cudaError_t launch_batch<P>(int, const BDom*, const BItem*, long long, const unsigned*,                \
+  template cudaError_t launch_batch<P>(int, int, const BDom*, const BItem*, long long, const unsigned*,           \
                                        unsigned long long*, unsigned*, int*, cudaStream_t);                        \
-  template int batch_resident_blocks<P>();
+  template int batch_resident_blocks<P>(int);
 
 }  // namespace adz

@@ -143,10 +143,12 @@ struct BItem {
   long long start, count;
 };
 
+constexpr int kBatchVariants = 3;  // register budgets of the batch kernel
 template <int PREC>
-cudaError_t launch_batch(int grid, const BDom* doms, const BItem* items, long long nitems, const unsigned* need,
-                         unsigned long long* next, unsigned* done, int* status, cudaStream_t s);
+cudaError_t launch_batch(int variant, int grid, const BDom* doms, const BItem* items, long long nitems,
+                         const unsigned* need, unsigned long long* next, unsigned* done, int* status,
+                         cudaStream_t s);
 template <int PREC>
-int batch_resident_blocks();  // k_batch blocks of 128 threads resident per SM
+int batch_resident_blocks(int variant);  // blocks of 128 threads resident per SM
 
 }  // namespace adz
