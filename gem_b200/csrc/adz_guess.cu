@@ -1,0 +1,597 @@
+// Learned starting guess for the departure-point iteration, and the
+// iteration run to a convergence tolerance.
+//
+// The reference starts the fixed-point iteration of adz_traject.F90 from the
+// arrival point on a cold start (adz_inittraj.F90) and runs a fixed number of
+// updates.  Here a small network, 82 -> 128 -> 128 -> 3 with GELU, predicts the
+// departure displacement of every arrival point from the departure winds
+// around it; the plain iteration then finishes from that guess to a stated
+// tolerance (k_traject_tol), falling back to the plain start where the guess
+// does not converge.
+//
+// Inference runs on the 5th-generation tensor cores: a persistent kernel keeps
+// the BF16 weights in shared memory, each CTA of 128 threads gathers the
+// features of 128 arrival points into a BF16 tile, and one elected thread
+// issues tcgen05.mma for each layer with the FP32 accumulator in tensor
+// memory; the epilogue (tcgen05.ld, bias, GELU, BF16) writes the next layer's
+// input tile in place.  Operands use the K-major no-swizzle layout of 8x16-byte
+// core matrices (K chunks of a row group adjacent).  Every wait on the MMA barrier is bounded: on expiry the CTA
+// raises kErrTimeout in the handle's status, waits (bounded) for its MMA in
+// flight, frees its tensor memory and stops.
+//
+// Feature definition, network and training: oracle/guess_oracle.py restates
+// them; the training kernels are in adz_train.cu.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/adz_b200.h"
+#include "adz_internal.h"
+#include "adz_types.h"
+
+namespace adz {
+namespace guess {
+
+constexpr int kFeat = ADZC_GUESS_NFEAT;  // 82
+constexpr int kK1 = 96;                  // features padded to the MMA K step
+constexpr int kHid = ADZC_GUESS_HIDDEN;  // 128
+constexpr int kN3 = 16;                  // 3 outputs padded to the smallest N
+constexpr int kRows = 128;               // arrival points per tile (MMA M)
+
+// weight image: core-matrix layouts of W1 (128x96), W2 (128x128), W3 (16x128),
+// then FP32 biases b1 (128), b2 (128), b3 (16); copied verbatim to shared memory
+constexpr int kW1 = 0;
+constexpr int kW2 = kW1 + kHid * kK1 * 2;
+constexpr int kW3 = kW2 + kHid * kHid * 2;
+constexpr int kB1 = kW3 + kN3 * kHid * 2;
+constexpr int kB2 = kB1 + kHid * 4;
+constexpr int kB3 = kB2 + kHid * 4;
+constexpr int kNetBytes = kB3 + kN3 * 4;  // 62528
+// shared memory of one CTA: weight image, activation tile, barrier, TMEM address
+constexpr int kA = (kNetBytes + 1023) / 1024 * 1024;
+constexpr int kBar = kA + kRows * kHid * 2;
+constexpr int kTaddr = kBar + 8;
+constexpr int kSmem = kTaddr + 8 + 1024;  // + alignment slack
+constexpr int kTmemCols = 128;
+constexpr unsigned kWaitPolls = 1u << 20;
+static_assert(kNetBytes % 16 == 0, "weight image copied in 16-byte words");
+
+// byte offset of element (r, k) of a K-major BF16 operand with row length
+// KC stored as 8-row x 16-byte core matrices: the K chunks of a row group
+// adjacent (LBO = 128 B), row groups KC * 16 B apart (SBO).  With this
+// arrangement every byte an MMA addresses stays inside the operand whichever
+// way round the two strides are read.
+__host__ __device__ constexpr int core_off(int r, int k, int KC) {
+  return (r >> 3) * (KC * 16) + ((k >> 3) << 7) + ((r & 7) << 4) + ((k & 7) << 1);
+}
+
+// shared-memory matrix descriptor: start, LBO, SBO (all >> 4), version 1,
+// no swizzle
+__device__ __forceinline__ unsigned long long smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  const unsigned long long lo = ((addr >> 4) & 0x3FFFu) | (((lbo >> 4) & 0x3FFFu) << 16);
+  const unsigned long long hi = ((sbo >> 4) & 0x3FFFu) | (1u << 14);
+  return lo | (hi << 32);
+}
+
+// instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, M x N
+__host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+  for (unsigned n = 0; n < kWaitPolls; n++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, unsigned long long a, unsigned long long b, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+      :
+      : "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// 32 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int q = 0; q < 32; q++) v[q] = __uint_as_float(r[q]);
+}
+
+__device__ __forceinline__ float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// tanh form of GELU (Hendrycks and Gimpel, 2016)
+__device__ __forceinline__ float gelu_fast(float x) {
+  const float u = 0.7978845608028654f * fmaf(0.044715f * x, x * x, x);
+  return 0.5f * x * (1.0f + tanh_approx(u));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+struct Args {
+  DGrid g;
+  const float* uvw;  // prepared departure winds, three component planes (MIXED scratch)
+  double* wpxyz;     // start positions out
+  float* disp;       // optional displacement out (npts x 3)
+  float* feat;       // features out (training data), npts x 82
+  const long long* idx;  // features of these points only (NULL: all)
+  const unsigned char* net;
+  long long npts;
+  int k00;
+  double dt;
+};
+
+__device__ __forceinline__ long long ext_at(const DGrid& g, int i, int j, int k) {
+  return (long long)(i - g.lminx) + (long long)(j - g.lminy) * g.nit + (long long)(k - 1) * g.nij;
+}
+
+__device__ __forceinline__ long long wp_at(const DGrid& g, int i, int j, int k, int c) {
+  const long long nx = g.ni + 4, ny = g.nj + 4;
+  return (long long)(i + 1) + (long long)(j + 1) * nx + (long long)(k - 1) * nx * ny +
+         (long long)(c - 1) * nx * ny * g.nk;
+}
+
+__device__ __forceinline__ void point_of(const DGrid& g, int k00, long long t, int& i, int& j, int& k) {
+  const long long plane = (long long)g.ni * g.nj;
+  i = (int)(t % g.ni) + 1;
+  j = (int)((t / g.ni) % g.nj) + 1;
+  k = (int)(t / plane) + k00;
+}
+
+// feature q (0..81) of arrival point (i,j,k): oracle/guess_oracle.py:features
+template <int Q>
+__device__ __forceinline__ float feature(const DGrid& g, const float* uvw, long long ncell, int i, int j, int k,
+                                         double sx, double sy, double sz, double dt) {
+  if (Q >= kFeat) return 0.0f;
+  if (Q == kFeat - 1) return (float)(dt / ADZC_GUESS_DT_SCALE);
+  constexpr int n = Q / 3, c = Q % 3;
+  constexpr int dk = n / 9 - 1, dj = (n / 3) % 3 - 1, di = n % 3 - 1;
+  int kq = k + dk;
+  kq = kq < 1 ? 1 : (kq > g.nk ? g.nk : kq);
+  const long long e = ext_at(g, i + di, j + dj, kq);
+  const double v = (double)__ldg(uvw + c * ncell + e);
+  return (float)(v * (c == 0 ? sx : c == 1 ? sy : sz));
+}
+
+template <int Q0>
+__device__ __forceinline__ void features8(const DGrid& g, const float* uvw, long long ncell, int i, int j, int k,
+                                          double sx, double sy, double sz, double dt, float* f) {
+  f[0] = feature<Q0 + 0>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
+  f[1] = feature<Q0 + 1>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
+  f[2] = feature<Q0 + 2>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
+  f[3] = feature<Q0 + 3>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
+  f[4] = feature<Q0 + 4>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
+  f[5] = feature<Q0 + 5>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
+  f[6] = feature<Q0 + 6>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
+  f[7] = feature<Q0 + 7>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
+}
+
+__device__ __forceinline__ void scales(const DGrid& g, int k, double dt, double& sx, double& sy, double& sz) {
+  sx = dt * g.inv_hx;
+  sy = dt * g.inv_hy;
+  const int nb = k < 1 ? 1 : (k > g.nk - 1 ? g.nk - 1 : k);
+  sz = dt * __ldg(g.odelz_m + nb);
+}
+
+// features of a chunk of 8 into the tile (row r, K chunk KC)
+template <int KC>
+__device__ __forceinline__ void put_chunk(unsigned char* A, int r, bool valid, const DGrid& g, const float* uvw,
+                                          long long ncell, int i, int j, int k, double sx, double sy, double sz,
+                                          double dt) {
+  float f[8];
+  if (valid) {
+    features8<KC * 8>(g, uvw, ncell, i, j, k, sx, sy, sz, dt, f);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 8; q++) f[q] = 0.0f;
+  }
+  uint4 w;
+  w.x = pack_bf16(f[0], f[1]);
+  w.y = pack_bf16(f[2], f[3]);
+  w.z = pack_bf16(f[4], f[5]);
+  w.w = pack_bf16(f[6], f[7]);
+  *reinterpret_cast<uint4*>(A + core_off(r, KC * 8, kHid)) = w;
+}
+
+// training features: FP32, all 82 per point
+__global__ void __launch_bounds__(128) k_features(Args a, long long n) {
+  const DGrid& g = a.g;
+  const long long ncell = g.nij * g.nk;
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+    const long long t = a.idx ? a.idx[s] : s;
+    if (t < 0 || t >= a.npts) continue;
+    int i, j, k;
+    point_of(g, a.k00, t, i, j, k);
+    double sx, sy, sz;
+    scales(g, k, a.dt, sx, sy, sz);
+    float* o = a.feat + s * kFeat;
+    float f[8];
+#define ADZ_FEAT_CHUNK(KC)                                                        \
+  features8<KC * 8>(g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt, f);               \
+  for (int q = 0; q < 8 && KC * 8 + q < kFeat; q++) o[KC * 8 + q] = f[q];
+    ADZ_FEAT_CHUNK(0) ADZ_FEAT_CHUNK(1) ADZ_FEAT_CHUNK(2) ADZ_FEAT_CHUNK(3) ADZ_FEAT_CHUNK(4)
+    ADZ_FEAT_CHUNK(5) ADZ_FEAT_CHUNK(6) ADZ_FEAT_CHUNK(7) ADZ_FEAT_CHUNK(8) ADZ_FEAT_CHUNK(9)
+    ADZ_FEAT_CHUNK(10)
+#undef ADZ_FEAT_CHUNK
+  }
+}
+
+// epilogue of a hidden layer: 128 accumulator columns of this thread's row,
+// + bias, GELU, BF16, written as the next layer's K-major input row
+__device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, const float* bias, unsigned char* A, int r) {
+#pragma unroll
+  for (int c0 = 0; c0 < kHid; c0 += 32) {
+    float v[32];
+    tmem_ld32(tmem_row + c0, v);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      uint4 w;
+      const int c = c0 + 8 * q;
+      w.x = pack_bf16(gelu_fast(v[8 * q + 0] + bias[c + 0]), gelu_fast(v[8 * q + 1] + bias[c + 1]));
+      w.y = pack_bf16(gelu_fast(v[8 * q + 2] + bias[c + 2]), gelu_fast(v[8 * q + 3] + bias[c + 3]));
+      w.z = pack_bf16(gelu_fast(v[8 * q + 4] + bias[c + 4]), gelu_fast(v[8 * q + 5] + bias[c + 5]));
+      w.w = pack_bf16(gelu_fast(v[8 * q + 6] + bias[c + 6]), gelu_fast(v[8 * q + 7] + bias[c + 7]));
+      *reinterpret_cast<uint4*>(A + core_off(r, c, kHid)) = w;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128, 1) k_guess(Args a) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const DGrid& g = a.g;
+  // weight image -> shared memory
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(a.net);
+    uint4* dst = reinterpret_cast<uint4*>(sm);
+    for (int q = tid; q < kNetBytes / 16; q += blockDim.x) dst[q] = src[q];
+  }
+  const uint32_t s_base = smem_u32(sm);
+  const uint32_t bar = s_base + kBar;
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s_base + kTaddr),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kTaddr);
+  const uint32_t tmem_row = tmem + ((uint32_t)(warp * 32) << 16);
+  unsigned char* A = sm + kA;
+  const float* b1 = reinterpret_cast<const float*>(sm + kB1);
+  const float* b2 = reinterpret_cast<const float*>(sm + kB2);
+  const float* b3 = reinterpret_cast<const float*>(sm + kB3);
+  const uint32_t a_addr = s_base + kA, w1 = s_base + kW1, w2 = s_base + kW2, w3 = s_base + kW3;
+  const uint32_t id_hid = instr_desc(kRows, kHid), id_out = instr_desc(kRows, kN3);
+  const long long ncell = g.nij * g.nk;
+  const long long ntiles = (a.npts + kRows - 1) / kRows;
+  uint32_t parity = 0;
+  bool failed = false, pending = false;
+
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long t = tile * kRows + tid;
+    const bool valid = t < a.npts;
+    int i = 1, j = 1, k = 1;
+    if (valid) point_of(g, a.k00, t, i, j, k);
+    double sx, sy, sz;
+    scales(g, k, a.dt, sx, sy, sz);
+    put_chunk<0>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
+    put_chunk<1>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
+    put_chunk<2>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
+    put_chunk<3>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
+    put_chunk<4>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
+    put_chunk<5>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
+    put_chunk<6>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
+    put_chunk<7>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
+    put_chunk<8>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
+    put_chunk<9>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
+    put_chunk<10>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
+    put_chunk<11>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
+
+    // three layers: tile [128 x K] . W^T -> TMEM, epilogue back into the tile
+    float y[3] = {0.f, 0.f, 0.f};
+#pragma unroll 1
+    for (int layer = 0; layer < 3; layer++) {
+      fence_async_smem();
+      fence_before();
+      __syncthreads();
+      fence_after();
+      if (tid == 0) {
+        const int ksteps = layer == 0 ? kK1 / 16 : kHid / 16;
+        const uint32_t wb = layer == 0 ? w1 : layer == 1 ? w2 : w3;
+        const uint32_t wsbo = (layer == 0 ? kK1 : kHid) * 16;  // row-group stride of the weights
+        const uint32_t idesc = layer == 2 ? id_out : id_hid;
+        for (int s = 0; s < ksteps; s++) {  // K step of 16 = two 16-byte chunks
+          const unsigned long long da = smem_desc(a_addr + s * 256, 128, kHid * 16);
+          const unsigned long long db = smem_desc(wb + s * 256, 128, wsbo);
+          mma_bf16(tmem, da, db, idesc, s > 0 ? 1u : 0u);
+        }
+        mma_commit(bar);
+      }
+      pending = true;
+      const bool ok = mbar_wait_bounded(bar, parity);
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        break;
+      }
+      pending = false;
+      parity ^= 1u;
+      fence_after();
+      if (layer < 2) {
+        hidden_epilogue(tmem_row, layer == 0 ? b1 : b2, A, tid);
+      } else {
+        float v[32];
+        tmem_ld32(tmem_row, v);  // columns 0..31; the first 3 are the outputs
+        y[0] = v[0] + b3[0];
+        y[1] = v[1] + b3[1];
+        y[2] = v[2] + b3[2];
+      }
+    }
+    if (failed) break;
+    if (valid) {
+      if (a.disp) {
+        a.disp[3 * t + 0] = y[0];
+        a.disp[3 * t + 1] = y[1];
+        a.disp[3 * t + 2] = y[2];
+      }
+      if (a.wpxyz) {
+        const double X = (double)(i + g.i0g - 1), Y = (double)(j + g.j0g - 1);
+        double pz = (double)k - (double)y[2];
+        pz = pz < 1.0 ? 1.0 : (pz > (double)g.nk ? (double)g.nk : pz);
+        a.wpxyz[wp_at(g, i, j, k, 1)] = X - (double)y[0];
+        a.wpxyz[wp_at(g, i, j, k, 2)] = Y - (double)y[1];
+        a.wpxyz[wp_at(g, i, j, k, 3)] = pz;
+      }
+    }
+  }
+  if (failed) {
+    if (tid == 0) atomicOr(g.status, kErrTimeout);
+    if (pending) mbar_wait_bounded(bar, parity);  // let the MMA in flight finish before freeing its memory
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+// BF16 round to nearest even on the host
+inline uint16_t bf16_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7F800000u) == 0x7F800000u && (u & 0x7FFFFFu)) return (uint16_t)((u >> 16) | 0x40);
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
+}  // namespace guess
+}  // namespace adz
+
+struct adzc_guess {
+  unsigned char* d_net = nullptr;
+  int device = 0;
+};
+
+namespace {
+
+using adz::guess::Args;
+
+int check_handle(adzc_handle* h, adz::DGrid* dg, adzc_info* info, adzc_grid* gr) {
+  int niter = 0, cold = 0;
+  return adz_internal_view(h, dg, info, gr, &niter, &cold);
+}
+
+// departure winds of the MIXED path into the handle's scratch
+int prepare_mixed(adzc_handle* h, const adz::DGrid& D, const void* uu, const void* vv, const void* ww, void** uvw,
+                  void** wdep, cudaStream_t s) {
+  if (adz_internal_scratch(h, ADZC_MIXED, uvw, wdep) != ADZC_OK) return ADZC_ERR_ALLOC;
+  if (adz::launch_prepare<adz::kMixed>(D, uu, vv, ww, *uvw, s) != cudaSuccess) return ADZC_ERR_CUDA;
+  return ADZC_OK;
+}
+
+int k00_of(const adz::DGrid& D) { return (D.k0 > 1) ? 1 : D.k0m; }  // B/adz_traject.F90:63-64
+
+}  // namespace
+
+extern "C" int adzc_guess_create(const float* const* params, adzc_guess** out) {
+  using namespace adz::guess;
+  if (!params || !out) return adz_internal_fail(ADZC_ERR_ARG);
+  for (int q = 0; q < 6; q++)
+    if (!params[q]) return adz_internal_fail(ADZC_ERR_ARG);
+  std::vector<unsigned char> img(kNetBytes, 0);
+  auto put = [&](int base, int kcap, const float* W, int n, int kdim) {  // rows beyond n and K beyond kdim stay 0
+    for (int r = 0; r < n; r++)
+      for (int k = 0; k < kdim; k++) {
+        const uint16_t b = bf16_bits(W[(size_t)r * kdim + k]);
+        std::memcpy(&img[base + core_off(r, k, kcap)], &b, 2);
+      }
+  };
+  put(kW1, kK1, params[0], kHid, kFeat);
+  put(kW2, kHid, params[2], kHid, kHid);
+  put(kW3, kHid, params[4], ADZC_GUESS_NOUT, kHid);
+  std::memcpy(&img[kB1], params[1], kHid * 4);
+  std::memcpy(&img[kB2], params[3], kHid * 4);
+  std::memcpy(&img[kB3], params[5], ADZC_GUESS_NOUT * 4);
+  auto* net = new (std::nothrow) adzc_guess();
+  if (!net) return adz_internal_fail(ADZC_ERR_ALLOC);
+  cudaGetDevice(&net->device);
+  if (cudaMalloc(&net->d_net, kNetBytes) != cudaSuccess) {
+    delete net;
+    return adz_internal_fail(ADZC_ERR_ALLOC);
+  }
+  if (cudaMemcpy(net->d_net, img.data(), kNetBytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(net->d_net);
+    delete net;
+    return adz_internal_fail(ADZC_ERR_CUDA);
+  }
+  *out = net;
+  return ADZC_OK;
+}
+
+extern "C" int adzc_guess_destroy(adzc_guess* net) {
+  if (!net) return ADZC_OK;
+  cudaFree(net->d_net);
+  delete net;
+  return ADZC_OK;
+}
+
+extern "C" long long adzc_guess_npoints(adzc_handle* h) {
+  adz::DGrid D;
+  adzc_info I;
+  adzc_grid G;
+  if (!h || check_handle(h, &D, &I, &G) != ADZC_OK) return -1;
+  return (long long)D.ni * D.nj * (D.nk - k00_of(D) + 1);
+}
+
+extern "C" int adzc_guess_features(adzc_handle* h, double dt, const void* uu_ext, const void* vv_ext,
+                                   const void* ww_ext, const long long* idx, long long n, float* features,
+                                   void* stream) {
+  adz::DGrid D;
+  adzc_info I;
+  adzc_grid G;
+  if (!h || !uu_ext || !vv_ext || !ww_ext || !features || n < 0 || !std::isfinite(dt) ||
+      check_handle(h, &D, &I, &G) != ADZC_OK)
+    return adz_internal_fail(ADZC_ERR_ARG);
+  const cudaStream_t s = (cudaStream_t)stream;
+  void *uvw = nullptr, *wdep = nullptr;
+  int st = prepare_mixed(h, D, uu_ext, vv_ext, ww_ext, &uvw, &wdep, s);
+  if (st != ADZC_OK) return adz_internal_fail(st);
+  Args a{};
+  a.g = D;
+  a.uvw = (const float*)uvw;
+  a.feat = features;
+  a.idx = idx;
+  a.k00 = k00_of(D);
+  a.npts = (long long)D.ni * D.nj * (D.nk - a.k00 + 1);
+  a.dt = dt;
+  if (!idx) n = a.npts;
+  if (n == 0) return ADZC_OK;
+  const long long blocks = std::min<long long>((n + 127) / 128, 148LL * 64);
+  adz::guess::k_features<<<(int)blocks, 128, 0, s>>>(a, n);
+  return cudaGetLastError() == cudaSuccess ? ADZC_OK : adz_internal_fail(ADZC_ERR_CUDA);
+}
+
+extern "C" int adzc_guess_apply(adzc_handle* h, const adzc_guess* net, double dt, const void* uu_ext,
+                                const void* vv_ext, const void* ww_ext, double* wpxyz, float* disp, void* stream) {
+  using namespace adz::guess;
+  adz::DGrid D;
+  adzc_info I;
+  adzc_grid G;
+  if (!h || !net || !uu_ext || !vv_ext || !ww_ext || (!wpxyz && !disp) || !std::isfinite(dt) ||
+      check_handle(h, &D, &I, &G) != ADZC_OK)
+    return adz_internal_fail(ADZC_ERR_ARG);
+  const cudaStream_t s = (cudaStream_t)stream;
+  void *uvw = nullptr, *wdep = nullptr;
+  int st = prepare_mixed(h, D, uu_ext, vv_ext, ww_ext, &uvw, &wdep, s);
+  if (st != ADZC_OK) return adz_internal_fail(st);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (cudaFuncSetAttribute(k_guess, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem) != cudaSuccess)
+    return adz_internal_fail(ADZC_ERR_CUDA);
+  Args a{};
+  a.g = D;
+  a.uvw = (const float*)uvw;
+  a.wpxyz = wpxyz;
+  a.disp = disp;
+  a.net = net->d_net;
+  a.k00 = k00_of(D);
+  a.npts = (long long)D.ni * D.nj * (D.nk - a.k00 + 1);
+  a.dt = dt;
+  if (a.npts <= 0) return ADZC_OK;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long ntiles = (a.npts + kRows - 1) / kRows;
+  const int grid = (int)std::min<long long>(ntiles, 2LL * sms);
+  k_guess<<<grid, 128, kSmem, s>>>(a);
+  return cudaGetLastError() == cudaSuccess ? ADZC_OK : adz_internal_fail(ADZC_ERR_CUDA);
+}
+
+extern "C" int adzc_traject_tol(adzc_handle* h, int prec, double dt, double tol, int maxit, int start,
+                                const void* uu_ext, const void* vv_ext, const void* ww_ext, const void* ut0,
+                                const void* vt0, const void* zdt0, double* wpxyz, unsigned char* iters,
+                                unsigned long long* stats, void* stream) {
+  adz::DGrid D;
+  adzc_info I;
+  adzc_grid G;
+  if (!h || (prec != ADZC_MIXED && prec != ADZC_FP64) || !uu_ext || !vv_ext || !ww_ext || !ut0 || !vt0 || !zdt0 ||
+      !wpxyz || maxit < 1 || maxit > 127 || !(tol >= 0.0) || (start != 0 && start != 1) || !std::isfinite(dt) ||
+      check_handle(h, &D, &I, &G) != ADZC_OK)
+    return adz_internal_fail(ADZC_ERR_ARG);
+  const cudaStream_t s = (cudaStream_t)stream;
+  void *uvw = nullptr, *wdep = nullptr;
+  if (adz_internal_scratch(h, prec, &uvw, &wdep) != ADZC_OK) return adz_internal_fail(ADZC_ERR_ALLOC);
+  const cudaError_t pe = prec == ADZC_FP64 ? adz::launch_prepare<adz::kFp64>(D, uu_ext, vv_ext, ww_ext, uvw, s)
+                                           : adz::launch_prepare<adz::kMixed>(D, uu_ext, vv_ext, ww_ext, uvw, s);
+  if (pe != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
+  adz::TrajArgs a{};
+  a.uvw_d = uvw;
+  a.ut0 = ut0;
+  a.vt0 = vt0;
+  a.zdt0 = zdt0;
+  a.wpxyz = wpxyz;
+  a.wdep = wdep;
+  a.niter = maxit;
+  a.cold = start == 0 ? 1 : 0;
+  a.k00 = k00_of(D);
+  a.dt = adz_internal_dt_split(G, dt);
+  const cudaError_t te = prec == ADZC_FP64 ? adz::launch_traject_tol<adz::kFp64>(D, a, tol, maxit, iters, stats, s)
+                                           : adz::launch_traject_tol<adz::kMixed>(D, a, tol, maxit, iters, stats, s);
+  if (te != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
+  adz_internal_record_positions(h, prec, wpxyz, zdt0, a.dt);
+  return ADZC_OK;
+}

@@ -159,126 +159,213 @@ __device__ __forceinline__ bool stencil_ok(const DGrid& g, int off) {
 }
 
 // ---------------------------------------------------------------------------
-// COH: the departure winds were written earlier in the same launch (batch)
-template <int PREC, bool COH = false>
-__device__ __forceinline__ void traject_point(const DGrid& g, const TrajArgs& a, int i, int j, int k) {
+// arrival winds (adz_prepareWinds.F90:40-97); Fortran forms the two sums in ``real``
+template <int PREC>
+__device__ __forceinline__ void arrival_winds(const DGrid& g, const TrajArgs& a, int j, int k, long long e, double& ua,
+                                              double& va, double& wa) {
   using F = typename Types<PREC>::F;
-  const F* __restrict__ uvw = (const F*)a.uvw_d;
   const F* __restrict__ ut0 = (const F*)a.ut0;
   const F* __restrict__ vt0 = (const F*)a.vt0;
   const F* __restrict__ zdt0 = (const F*)a.zdt0;
+  const int nk = g.nk;
+  const double alpha1 = -1.0 / 16.0, alpha2 = 9.0 / 16.0;
+  const double cyj = __ldg(g.cy + (j - g.lminy));
+  const F u1 = ut0[e - 2] + ut0[e + 1], u2 = ut0[e] + ut0[e - 1];
+  const F v1 = vt0[e - 2 * g.nit] + vt0[e + g.nit], v2 = vt0[e] + vt0[e - g.nit];
+  double uad = ((double)u1 * alpha1 + (double)u2 * alpha2) * g.inv_rayt * cyj;
+  double vad = ((double)v1 * alpha1 + (double)v2 * alpha2) * g.inv_rayt;
+  double wad;
+  if (k == 1) {
+    wad = g.vw5 * (double)zdt0[e];
+  } else if (k == nk) {
+    wad = g.vw6 * (double)zdt0[e - g.nij];
+  } else {
+    const int km2 = imax_(1, k - 2);
+    const double wx = (k >= 3) ? __ldg(g.vw + 0 * (nk + 1) + k) : 0.0;
+    wad = wx * (double)zdt0[e - (long long)(k - km2) * g.nij] + __ldg(g.vw + 1 * (nk + 1) + k) * (double)zdt0[e - g.nij] +
+          __ldg(g.vw + 2 * (nk + 1) + k) * (double)zdt0[e] + __ldg(g.vw + 3 * (nk + 1) + k) * (double)zdt0[e + g.nij];
+  }
+  if (PREC == kRef32) {  // Adz_uu_arr etc. are ``real``
+    ua = (double)(float)uad; va = (double)(float)vad; wa = (double)(float)wad;
+  } else {
+    ua = uad; va = vad; wa = wad;
+  }
+}
+
+// one fixed-point update (adz_traject.F90:66-110): departure winds at
+// (px,py,pz), new departure point (xm, ym, w3) and the clipped start of the
+// next update in (px,py,pz).  Returns 0, kErrHalo or kErrNonFinite.
+// COH: the departure winds were written earlier in the same launch (batch)
+template <int PREC, bool COH>
+__device__ __forceinline__ int traj_update(const DGrid& g, const TrajArgs& a, int i, int j, int k, double ua,
+                                           double va, double wa, double& px, double& py, double& pz, double& xm,
+                                           double& ym, double& w3, double& wd) {
+  using F = typename Types<PREC>::F;
+  const F* __restrict__ uvw = (const F*)a.uvw_d;
   const long long e111 = ext_index(g, 1, 1, 1);
   const F* f3 = uvw + 3 * e111;
   const int nk = g.nk;
-  const long long e = ext_index(g, i, j, k);
-  const long long ar = arr_index(g, i, j, k);
-  // arrival winds (adz_prepareWinds.F90:40-97); Fortran forms the two sums in ``real``
-  const double alpha1 = -1.0 / 16.0, alpha2 = 9.0 / 16.0;
-  const double cyj = __ldg(g.cy + (j - g.lminy));
-  double ua, va, wa;
-  {
-    const F u1 = ut0[e - 2] + ut0[e + 1], u2 = ut0[e] + ut0[e - 1];
-    const F v1 = vt0[e - 2 * g.nit] + vt0[e + g.nit], v2 = vt0[e] + vt0[e - g.nit];
-    double uad = ((double)u1 * alpha1 + (double)u2 * alpha2) * g.inv_rayt * cyj;
-    double vad = ((double)v1 * alpha1 + (double)v2 * alpha2) * g.inv_rayt;
-    double wad;
-    if (k == 1) {
-      wad = g.vw5 * (double)zdt0[e];
-    } else if (k == nk) {
-      wad = g.vw6 * (double)zdt0[e - g.nij];
+  double ud, vd;
+  int off;
+  if (PREC == kMixed) {
+    WF w;
+    coef_mixed(w, px, py, pz, g.tab_m);
+    off = w.off;
+    if (!stencil_ok(g, off)) return kErrHalo;
+    if (WindLayout<PREC>::soa) {
+      const long long ncell = g.nij * g.nk;
+      const float* fu = (const float*)uvw + e111 + off;
+      ud = interp1_mixed<COH>(fu, w, g.tab_m.ni, g.tab_m.nij);
+      vd = interp1_mixed<COH>(fu + ncell, w, g.tab_m.ni, g.tab_m.nij);
+      wd = interp1_mixed<COH>(fu + 2 * ncell, w, g.tab_m.ni, g.tab_m.nij);
     } else {
-      const int km2 = imax_(1, k - 2);
-      const double wx = (k >= 3) ? __ldg(g.vw + 0 * (nk + 1) + k) : 0.0;
-      wad = wx * (double)zdt0[e - (long long)(k - km2) * g.nij] + __ldg(g.vw + 1 * (nk + 1) + k) * (double)zdt0[e - g.nij] +
-            __ldg(g.vw + 2 * (nk + 1) + k) * (double)zdt0[e] + __ldg(g.vw + 3 * (nk + 1) + k) * (double)zdt0[e + g.nij];
+      float o[3];
+      interp3_mixed<COH>((const float*)f3 + 3LL * off, w, g.tab_m.ni, g.tab_m.nij, o);
+      ud = o[0]; vd = o[1]; wd = o[2];
     }
-    if (PREC == kFp64) {
-      ua = uad; va = vad; wa = wad;
-    } else if (PREC == kRef32) {  // Adz_uu_arr etc. are ``real``
-      ua = (double)(float)uad; va = (double)(float)vad; wa = (double)(float)wad;
+  } else {
+    double c[20];
+    int zl;
+    if (PREC == kRef32) zl = coef_f32pos(c, off, (float)px, (float)py, (float)pz, g.tab_m);
+    else zl = coef_f64pos(c, off, px, py, pz, g.tab_m);
+    if (!stencil_ok(g, off)) return kErrHalo;
+    double o[3];
+    interp3_exact<F, COH>(f3 + 3LL * off, c, g.tab_m.ni, g.tab_m.nij, zl, o);
+    if (PREC == kRef32) {  // Tricublin_zyx3_n returns ``real``
+      ud = (double)(float)o[0]; vd = (double)(float)o[1]; wd = (double)(float)o[2];
     } else {
-      ua = uad; va = vad; wa = wad;
+      ud = o[0]; vd = o[1]; wd = o[2];
     }
   }
-  // starting position
-  double px, py, pz;
-  if (a.cold) {
-    px = (double)(i + g.i0g - 1); py = (double)(j + g.j0g - 1); pz = (double)k;
-  } else if (PREC == kRef32) {
+  xm = (double)(i + g.i0g - 1) - (a.dt.dtD * ud + a.dt.dtA * ua) * g.inv_hx;
+  ym = (double)(j + g.j0g - 1) - (a.dt.dtD * vd + a.dt.dtA * va) * g.inv_hy;
+  const double pos = __ldg(g.zm + k) - a.dt.dtzD * wd - a.dt.dtzA * wa;
+  const double zmv = dmin_(dmax_(pos, g.zmin), g.zmax);
+  int kk1 = vsearch(zmv, g.zm, g.ovdzm, g.search_m, g.pnz_m, g.sig, nk);
+  kk1 = imin_(nk + 1, imax_(0, kk1));
+  const int nb = imax_(imin_(kk1, nk - 1), 1);
+  w3 = (zmv - __ldg(g.zm + nb)) * __ldg(g.odelz_m + nb) + (double)nb;
+  const double cx = dmin_(dmax_(xm, g.imnx), g.imxx);
+  const double cyv = dmin_(dmax_(ym, g.imny), g.imxy);
+  if (PREC == kRef32) {
+    px = (float)cx; py = (float)cyv; pz = (float)w3;
+  } else {
+    px = cx; py = cyv; pz = w3;
+  }
+  if (!isfinite(xm) || !isfinite(ym) || !isfinite(w3)) return kErrNonFinite;
+  return 0;
+}
+
+// starting position of a warm trajectory: the stored departure point, x and y
+// clipped to the interpolation range
+template <int PREC>
+__device__ __forceinline__ void warm_start(const DGrid& g, const TrajArgs& a, int i, int j, int k, double& px,
+                                           double& py, double& pz) {
+  if (PREC == kRef32) {
+    const long long ar = arr_index(g, i, j, k);
     px = a.pxyzm[3 * ar]; py = a.pxyzm[3 * ar + 1]; pz = a.pxyzm[3 * ar + 2];
   } else {
     px = dmin_(dmax_(a.wpxyz[wp_index(g, i, j, k, 1)], g.imnx), g.imxx);
     py = dmin_(dmax_(a.wpxyz[wp_index(g, i, j, k, 2)], g.imny), g.imxy);
     pz = a.wpxyz[wp_index(g, i, j, k, 3)];
   }
-  double xm = 0.0, ym = 0.0, w3 = 0.0, wlast = 0.0;
-  bool bad = false, nonfinite = false;
-  for (int it = 0; it < a.niter; it++) {
-    double ud, vd, wd;
-    int off;
-    if (PREC == kMixed) {
-      WF w;
-      coef_mixed(w, px, py, pz, g.tab_m);
-      off = w.off;
-      if (!stencil_ok(g, off)) { bad = true; break; }
-      if (WindLayout<PREC>::soa) {
-        const long long ncell = g.nij * g.nk;
-        const float* fu = (const float*)uvw + e111 + off;
-        ud = interp1_mixed<COH>(fu, w, g.tab_m.ni, g.tab_m.nij);
-        vd = interp1_mixed<COH>(fu + ncell, w, g.tab_m.ni, g.tab_m.nij);
-        wd = interp1_mixed<COH>(fu + 2 * ncell, w, g.tab_m.ni, g.tab_m.nij);
-      } else {
-        float o[3];
-        interp3_mixed<COH>((const float*)f3 + 3LL * off, w, g.tab_m.ni, g.tab_m.nij, o);
-        ud = o[0]; vd = o[1]; wd = o[2];
-      }
-    } else {
-      double c[20];
-      int zl;
-      if (PREC == kRef32) zl = coef_f32pos(c, off, (float)px, (float)py, (float)pz, g.tab_m);
-      else zl = coef_f64pos(c, off, px, py, pz, g.tab_m);
-      if (!stencil_ok(g, off)) { bad = true; break; }
-      double o[3];
-      interp3_exact<F, COH>(f3 + 3LL * off, c, g.tab_m.ni, g.tab_m.nij, zl, o);
-      if (PREC == kRef32) {  // Tricublin_zyx3_n returns ``real``
-        ud = (double)(float)o[0]; vd = (double)(float)o[1]; wd = (double)(float)o[2];
-      } else {
-        ud = o[0]; vd = o[1]; wd = o[2];
-      }
-    }
-    xm = (double)(i + g.i0g - 1) - (a.dt.dtD * ud + a.dt.dtA * ua) * g.inv_hx;
-    ym = (double)(j + g.j0g - 1) - (a.dt.dtD * vd + a.dt.dtA * va) * g.inv_hy;
-    const double pos = __ldg(g.zm + k) - a.dt.dtzD * wd - a.dt.dtzA * wa;
-    const double zmv = dmin_(dmax_(pos, g.zmin), g.zmax);
-    int kk1 = vsearch(zmv, g.zm, g.ovdzm, g.search_m, g.pnz_m, g.sig, nk);
-    kk1 = imin_(nk + 1, imax_(0, kk1));
-    const int nb = imax_(imin_(kk1, nk - 1), 1);
-    w3 = (zmv - __ldg(g.zm + nb)) * __ldg(g.odelz_m + nb) + (double)nb;
-    wlast = wd;
-    const double cx = dmin_(dmax_(xm, g.imnx), g.imxx);
-    const double cyv = dmin_(dmax_(ym, g.imny), g.imxy);
-    if (PREC == kRef32) {
-      px = (float)cx; py = (float)cyv; pz = (float)w3;
-    } else {
-      px = cx; py = cyv; pz = w3;
-    }
-    if (!isfinite(xm) || !isfinite(ym) || !isfinite(w3)) { nonfinite = true; break; }
+}
+
+// store the departure point of (i,j,k) (adz_traject.F90:112-118)
+template <int PREC>
+__device__ __forceinline__ void traj_store(const DGrid& g, const TrajArgs& a, int i, int j, int k, double xm, double ym,
+                                           double w3, double px, double py, double pz, double wd) {
+  using F = typename Types<PREC>::F;
+  a.wpxyz[wp_index(g, i, j, k, 1)] = xm;
+  a.wpxyz[wp_index(g, i, j, k, 2)] = ym;
+  a.wpxyz[wp_index(g, i, j, k, 3)] = w3;
+  const long long ar = arr_index(g, i, j, k);
+  if (PREC == kRef32) {
+    a.pxyzm[3 * ar] = (float)px;
+    a.pxyzm[3 * ar + 1] = (float)py;
+    a.pxyzm[3 * ar + 2] = (float)pz;
   }
-  if (bad || nonfinite) {
-    raise_status(g.status, bad ? kErrHalo : kErrNonFinite);
+  ((F*)a.wdep)[ar] = (F)wd;
+}
+
+// ---------------------------------------------------------------------------
+// COH: the departure winds were written earlier in the same launch (batch)
+template <int PREC, bool COH = false>
+__device__ __forceinline__ void traject_point(const DGrid& g, const TrajArgs& a, int i, int j, int k) {
+  const long long e = ext_index(g, i, j, k);
+  double ua, va, wa;
+  arrival_winds<PREC>(g, a, j, k, e, ua, va, wa);
+  double px, py, pz;
+  if (a.cold) {
+    px = (double)(i + g.i0g - 1); py = (double)(j + g.j0g - 1); pz = (double)k;
+  } else {
+    warm_start<PREC>(g, a, i, j, k, px, py, pz);
+  }
+  double xm = 0.0, ym = 0.0, w3 = 0.0, wlast = 0.0;
+  int st = 0;
+  for (int it = 0; it < a.niter; it++) {
+    double wd;
+    st = traj_update<PREC, COH>(g, a, i, j, k, ua, va, wa, px, py, pz, xm, ym, w3, wd);
+    if (st) break;
+    wlast = wd;
+  }
+  if (st) {
+    raise_status(g.status, st);
     return;
   }
-  if (a.niter > 0) {
-    a.wpxyz[wp_index(g, i, j, k, 1)] = xm;
-    a.wpxyz[wp_index(g, i, j, k, 2)] = ym;
-    a.wpxyz[wp_index(g, i, j, k, 3)] = w3;
-    if (PREC == kRef32) {
-      a.pxyzm[3 * ar] = (float)px;
-      a.pxyzm[3 * ar + 1] = (float)py;
-      a.pxyzm[3 * ar + 2] = (float)pz;
-    }
-    ((F*)a.wdep)[ar] = (F)wlast;
+  if (a.niter > 0) traj_store<PREC>(g, a, i, j, k, xm, ym, w3, px, py, pz, wlast);
+}
+
+// Iterate to a convergence tolerance instead of a fixed count: stop once no
+// coordinate of the clipped departure point moves by more than ``tol`` grid
+// indices, after at most ``maxit`` updates.  The start is the arrival point
+// (a.cold) or the stored point (a learned guess).  A guessed start that has
+// not converged after ``maxit`` updates falls back to the plain iteration
+// from the arrival point.  Per point: updates used (iters, saturating at 255;
+// +128 when the fallback ran), and block sums into stats[0] updates,
+// stats[1] fallbacks, stats[2] points not converged.
+template <int PREC>
+__device__ __forceinline__ void traject_point_tol(const DGrid& g, const TrajArgs& a, int i, int j, int k, double tol,
+                                                  int maxit, unsigned char* iters, unsigned long long* cnt) {
+  const long long e = ext_index(g, i, j, k);
+  double ua, va, wa;
+  arrival_winds<PREC>(g, a, j, k, e, ua, va, wa);
+  const double X = (double)(i + g.i0g - 1), Y = (double)(j + g.j0g - 1), Z = (double)k;
+  double px, py, pz;
+  if (a.cold) {
+    px = X; py = Y; pz = Z;
+  } else {
+    warm_start<PREC>(g, a, i, j, k, px, py, pz);
   }
+  double xm = 0.0, ym = 0.0, w3 = 0.0, wlast = 0.0;
+  int st = 0, used = 0, pass = a.cold ? 1 : 0;
+  bool conv = false;
+  for (;;) {
+    for (int it = 0; it < maxit; it++) {
+      const double qx = px, qy = py, qz = pz;
+      double wd;
+      st = traj_update<PREC, false>(g, a, i, j, k, ua, va, wa, px, py, pz, xm, ym, w3, wd);
+      if (st) break;
+      wlast = wd;
+      used++;
+      if (fabs(px - qx) <= tol && fabs(py - qy) <= tol && fabs(pz - qz) <= tol) {
+        conv = true;
+        break;
+      }
+    }
+    if (st || conv || pass == 1) break;
+    pass = 1;  // fallback: plain iteration from the arrival point
+    cnt[1]++;
+    px = X; py = Y; pz = Z;
+  }
+  cnt[0] += used;
+  if (!conv) cnt[2]++;
+  if (iters) iters[arr_index(g, i, j, k)] = (unsigned char)(imin_(used, 127) + ((pass == 1 && !a.cold) ? 128 : 0));
+  if (st) {
+    raise_status(g.status, st);
+    return;
+  }
+  if (used > 0) traj_store<PREC>(g, a, i, j, k, xm, ym, w3, px, py, pz, wlast);
 }
 
 template <int PREC>
@@ -290,6 +377,28 @@ __global__ void ADZ_TRAJ_BOUNDS k_traject(DGrid g, TrajArgs a) {
     const int j = (int)((t / g.ni) % g.nj) + 1;
     const int k = (int)(t / nplane) + a.k00;
     traject_point<PREC>(g, a, i, j, k);
+  }
+}
+
+template <int PREC>
+__global__ void ADZ_TRAJ_BOUNDS k_traject_tol(DGrid g, TrajArgs a, double tol, int maxit, unsigned char* iters,
+                                              unsigned long long* stats) {
+  const long long nplane = (long long)g.ni * g.nj;
+  const long long n = nplane * (g.nk - a.k00 + 1);
+  unsigned long long cnt[3] = {0, 0, 0};
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.ni) + 1;
+    const int j = (int)((t / g.ni) % g.nj) + 1;
+    const int k = (int)(t / nplane) + a.k00;
+    traject_point_tol<PREC>(g, a, i, j, k, tol, maxit, iters, cnt);
+  }
+  if (stats) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      unsigned long long v = cnt[q];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if ((threadIdx.x & 31) == 0 && v) atomicAdd(stats + q, v);
+    }
   }
 }
 
@@ -646,6 +755,14 @@ cudaError_t launch_traject(const DGrid& g, const TrajArgs& a, cudaStream_t s) {
 }
 
 template <int PREC>
+cudaError_t launch_traject_tol(const DGrid& g, const TrajArgs& a, double tol, int maxit, unsigned char* iters,
+                               unsigned long long* stats, cudaStream_t s) {
+  const long long n = (long long)g.ni * g.nj * (g.nk - a.k00 + 1);
+  k_traject_tol<PREC><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, a, tol, maxit, iters, stats);
+  return cudaGetLastError();
+}
+
+template <int PREC>
 cudaError_t launch_tricub_set(const DGrid& g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
                               const SetArgs& a, const FieldPtrs& fp, cudaStream_t s) {
   const long long n = (long long)nx * ny * nz;
@@ -707,6 +824,8 @@ int batch_resident_blocks(int variant) {
   template cudaError_t launch_prepare<P>(const DGrid&, const void*, const void*, const void*, void*, cudaStream_t); \
   template cudaError_t launch_inittraj<P>(const DGrid&, float*, double*, cudaStream_t);                            \
   template cudaError_t launch_traject<P>(const DGrid&, const TrajArgs&, cudaStream_t);                             \
+  template cudaError_t launch_traject_tol<P>(const DGrid&, const TrajArgs&, double, int, unsigned char*,           \
+                                             unsigned long long*, cudaStream_t);                                   \
   template cudaError_t launch_tricub_set<P>(const DGrid&, int, int, int, int, int, int, int, const SetArgs&,       \
                                             const FieldPtrs&, cudaStream_t);                                       \
   template cudaError_t launch_interp_pos<P>(const DZtab&, int, int, const void*, const FieldPtrs&, cudaStream_t); \

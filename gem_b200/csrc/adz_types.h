@@ -116,6 +116,9 @@ cudaError_t launch_inittraj(const DGrid& g, float* pxyzm, double* wpxyz, cudaStr
 template <int PREC>
 cudaError_t launch_traject(const DGrid& g, const TrajArgs& a, cudaStream_t s);
 template <int PREC>
+cudaError_t launch_traject_tol(const DGrid& g, const TrajArgs& a, double tol, int maxit, unsigned char* iters,
+                               unsigned long long* stats, cudaStream_t s);
+template <int PREC>
 cudaError_t launch_tricub_set(const DGrid& g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
                               const SetArgs& a, const FieldPtrs& fp, cudaStream_t s);
 template <int PREC>

@@ -230,6 +230,64 @@ int adzc_batch_query(const adzc_batch *b, int *rows_per_item, int *blocks_per_sm
 int adzc_batch_status(adzc_batch *b, int reset, void *stream);
 int adzc_batch_destroy(adzc_batch *b);
 
+/* ------------------------------------------------------------------------ */
+/* Trajectory to a convergence tolerance, and a learned starting guess        */
+/* ------------------------------------------------------------------------ */
+/* The reference iterates the departure point a fixed number of times
+ * (B/adz_traject.F90:66-110; max(6, itraj) on a cold start,
+ * B/adz_inittraj.F90:25).  adzc_traject_tol runs the same update until no
+ * coordinate of the departure point moves by more than tol grid indices
+ * between two updates, at most maxit (1..127) times.
+ *   start 0: from the arrival point (the reference's cold start);
+ *   start 1: from the points in wpxyz, e.g. written by adzc_guess_apply.
+ *            A point that has not converged after maxit updates restarts
+ *            from the arrival point (fallback).
+ * iters (NULL or ni*nj*nk bytes, arr layout): updates used per point, +128
+ * where the fallback ran.  stats (NULL or 3 zeroed device counters, summed
+ * into): updates, fallbacks, points not converged.  ADZC_FP64 or ADZC_MIXED;
+ * adzc_tricub may follow as after adzc_traject. */
+int adzc_traject_tol(adzc_handle *h, int prec, double dt, double tol, int maxit, int start, const void *uu_ext,
+                     const void *vv_ext, const void *ww_ext, const void *ut0, const void *vt0, const void *zdt0,
+                     double *wpxyz, unsigned char *iters, unsigned long long *stats, void *stream);
+
+/* Learned starting guess (no counterpart in the reference): a network
+ * 82 -> 128 -> 128 -> 3 with GELU predicts the departure displacement of
+ * each arrival point (i, j, k >= k00, order k, j, i) from the departure winds
+ * at the 27 surrounding points, as Courant numbers, and dt / 300 s.
+ * params: HOST FP32 arrays W1 (128x82, row = output), b1 (128), W2 (128x128),
+ * b2 (128), W3 (3x128), b3 (3).  Inference: BF16 weights and layer inputs,
+ * FP32 accumulation on the tensor cores.  MIXED winds (FP32 fields). */
+#define ADZC_GUESS_NFEAT 82
+#define ADZC_GUESS_HIDDEN 128
+#define ADZC_GUESS_NOUT 3
+#define ADZC_GUESS_DT_SCALE 300.0
+typedef struct adzc_guess adzc_guess;
+int adzc_guess_create(const float *const *params, adzc_guess **out);
+int adzc_guess_destroy(adzc_guess *net);
+/* arrival points of the trajectory (ni*nj*(nk-k00+1)), -1 on a bad handle */
+long long adzc_guess_npoints(adzc_handle *h);
+/* start points X - d, Y - d, k - d (vertical clipped to 1..nk) into wpxyz,
+ * and/or the raw displacement d into disp (npoints x 3) */
+int adzc_guess_apply(adzc_handle *h, const adzc_guess *net, double dt, const void *uu_ext, const void *vv_ext,
+                     const void *ww_ext, double *wpxyz, float *disp, void *stream);
+/* FP32 features (n x 82) of the points idx[0..n) (device; NULL: all points) */
+int adzc_guess_features(adzc_handle *h, double dt, const void *uu_ext, const void *vv_ext, const void *ww_ext,
+                        const long long *idx, long long n, float *features, void *stream);
+
+/* Training of the guess network in FP32: mean over the batch of the squared
+ * displacement error, Adam (b1 0.9, b2 0.999, eps 1e-8).  x (batch x 82) and
+ * target (batch x 3) are DEVICE arrays. */
+#define ADZC_MLP_NPARAM 27523
+typedef struct adzc_mlp adzc_mlp;
+int adzc_mlp_create(const float *params, int max_batch, adzc_mlp **out); /* HOST flat parameter vector */
+int adzc_mlp_destroy(adzc_mlp *t);
+int adzc_mlp_forward(adzc_mlp *t, const float *x, int batch, float *y, void *stream);
+int adzc_mlp_grad(adzc_mlp *t, const float *x, const float *target, int batch, void *stream);
+int adzc_mlp_adam(adzc_mlp *t, float lr, void *stream);
+/* what 0: parameters, 1: gradients (ADZC_MLP_NPARAM floats), 2: loss of the
+ * last adzc_mlp_grad (1 float); synchronises the stream */
+int adzc_mlp_read(adzc_mlp *t, int what, float *host_out, void *stream);
+
 /* One whole advection step that allocates no device memory.  No counterpart
  * in the reference (its Fortran drivers use automatic arrays).
  *
