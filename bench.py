@@ -34,6 +34,12 @@ import numpy as np  # noqa: E402
 import torch  # noqa: E402
 
 HBM_FALLBACK_GBS = 6650.0
+TENSOR_FALLBACK_TFLOPS = 1590.0
+# DRAM bytes (read + write) per arrival point of each MIXED launch, from the
+# ncu capture of the 384x384x80 case with u, v, w + 4 tracers
+# (profiles/k_tricub_set_k_traject_mixed_384x384x80.md); traffic grows in
+# proportion to the points, so it scales to the benched tile
+MEASURED_TRAFFIC_PER_POINT = {"traject": 74.2, "sets": 122.8}
 
 
 def peaks():
@@ -259,7 +265,7 @@ def run_product(args):
     dom = max(per, key=per.get)
     hbm, hbm_kind = peaks()
     achieved = bytes_launch[dom] / (per[dom] * 1e-3) / 1e9
-    traffic = None
+    traffic = MEASURED_TRAFFIC_PER_POINT[dom] * npts if args.ntr == 4 else None
     step_bytes = npts * (24 + 12 + 12 + 24 + (3 + args.ntr) * 8)
 
     # end to end: inputs from pinned host memory, results back, every step
@@ -290,6 +296,11 @@ def run_product(args):
         torch.cuda.empty_cache()
         batch = measure_batch(args, timed, ws)
 
+    gsum = None
+    if not args.no_guess and os.path.exists(args.guess_weights):
+        torch.cuda.empty_cache()
+        gsum = measure_guess(args, timed, ws, rank)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_reference(args.cpu_size, 2, 1, ntracers=args.ntr)
@@ -311,7 +322,7 @@ def run_product(args):
                           "achieved_gbs": step_bytes / (ms32 * 1e-3) / 1e9,
                           "frac": step_bytes / (ms32 * 1e-3) / 1e9 / hbm},
         "e2e": e2e, "gpu_launches": LAUNCHES_PER_STEP * args.steps, "clocks": clk, "cpu_baseline": cpu,
-        "batch": batch,
+        "batch": batch, "learned_guess": gsum,
     }
     if rank == 0:
         print(json.dumps(line))
@@ -374,6 +385,75 @@ def measure_batch(args, timed, ws):
     return out
 
 
+def measure_guess(args, timed, ws, rank):
+    """Cold start of the 1024x1024x80 tile (no previous departure points):
+    the reference's 6 fixed updates from the arrival point, the plain update
+    run to the project tolerance from the arrival point, and the learned
+    guess (BF16 tensor-core inference) followed by the plain update to the
+    same tolerance.  Reports updates per point, fallbacks, the guess error
+    against the converged departure points (1e-6) and the time of each."""
+    from gem_b200 import adz, guess, synth
+    prec = adz.MIXED
+    ni, nj, nk = args.size
+    cfg = synth.config_cold(ni, nj, nk, seed=4321 + rank)
+    inp = synth.make_inputs(cfg, device="cuda", dtype=torch.float32, with_fields=False)
+    ad = adz.Adz.from_config(cfg)
+    n = guess.npoints(ad)
+    net = guess.GuessNet(guess.load_weights(args.guess_weights))
+    _, wp_ref = ad.new_state(prec)
+    guess.traject_tol(ad, prec, cfg.dt, inp, wp_ref, tol=1e-6, maxit=60, start=0)
+    d_ref = guess.displacement(ad, wp_ref)
+    disp = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+    net.apply(ad, cfg.dt, inp, disp=disp)
+    e = (disp.double() - d_ref).abs()
+    sub = e[torch.randint(0, n, (min(n, 1 << 22),), device="cuda")]
+    gerr = {"rms": [float(v) for v in e.pow(2).mean(0).sqrt()], "max": [float(v) for v in e.max(0).values],
+            "p99": [float(v) for v in torch.quantile(sub, 0.99, dim=0)], "unit": "grid indices (x, y, level)"}
+
+    wps = {k: ad.new_state(prec)[1] for k in ("fixed", "plain", "learned")}
+    stats = {k: torch.zeros(3, dtype=torch.int64, device="cuda") for k in ("plain", "learned")}
+
+    def fixed():
+        ad.adz_inittraj(prec, None, wps["fixed"])
+        ad.adz_traject(prec, cfg.dt, inp, None, wps["fixed"])
+
+    def plain():
+        stats["plain"].zero_()
+        guess.traject_tol(ad, prec, cfg.dt, inp, wps["plain"], start=0, stats=stats["plain"])
+
+    def learned():
+        stats["learned"].zero_()
+        net.apply(ad, cfg.dt, inp, wpxyz=wps["learned"])
+        guess.traject_tol(ad, prec, cfg.dt, inp, wps["learned"], start=1, stats=stats["learned"])
+
+    def infer():
+        net.apply(ad, cfg.dt, inp, disp=disp)
+
+    K, W = max(3, min(args.steps, 10)), args.warmup
+    ms = {"fixed6": timed(fixed, K, W)[0], "plain_tol": timed(plain, K, W)[0], "learned_tol": timed(learned, K, W)[0],
+          "inference": timed(infer, K, W)[0]}
+    if ad.status() != 0:
+        raise RuntimeError("device status set during the cold-start measurement")
+    sp, sl = stats["plain"].cpu().tolist(), stats["learned"].cpu().tolist()
+    acc = {k: [float(v) for v in (guess.displacement(ad, wps[k]) - d_ref).abs().max(0).values] for k in wps}
+    _, hbm_kind = peaks()
+    pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if hbm_kind == "measured" else {}
+    peak_tf = float(pk.get("bf16_tflops", TENSOR_FALLBACK_TFLOPS))
+    flops = n * 2.0 * 128 * (96 + 128 + 16)  # padded MMA work per arrival point
+    tf = flops / (ms["inference"] * 1e-3) / 1e12
+    return {"workload": f"cold start of the {ni}x{nj}x{nk} tile, {n} arrival points, MIXED, "
+                        "vertical-wind noise 0.02 m/s",
+            "tolerance": guess.TOL, "max_updates": guess.MAXIT,
+            "updates_per_point": {"fixed_reference": 6, "plain": sp[0] / n, "learned": sl[0] / n},
+            "updates_saved_per_point": (sp[0] - sl[0]) / n,
+            "fallback_rate": sl[1] / n, "not_converged": {"plain": sp[2], "learned": sl[2]},
+            "guess_error": gerr, "max_error_vs_converged": acc, "ms": ms,
+            "speedup_learned_vs_plain": ms["plain_tol"] / ms["learned_tol"],
+            "inference_roofline": {"bound": "tensor", "achieved": tf, "peak": peak_tf, "unit": "TFLOP/s",
+                                   "frac": tf / peak_tf, "flops_per_point": flops / n,
+                                   "note": "includes the departure-wind preparation launch"}}
+
+
 def run_reference(args):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -404,6 +484,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-domain measurement")
     ap.add_argument("--batch-domains", type=int, default=16)
+    ap.add_argument("--no-guess", action="store_true", help="skip the learned-guess cold-start measurement")
+    ap.add_argument("--guess-weights", default=os.path.join(ROOT, "gem_b200", "data", "guess_mlp.npz"))
     ap.add_argument("--only", choices=["mixed"], default=None,
                     help="run the mixed-precision path alone (small profiling runs)")
     args = ap.parse_args()

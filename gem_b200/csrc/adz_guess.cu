@@ -10,10 +10,12 @@
 // does not converge.
 //
 // Inference runs on the 5th-generation tensor cores: a persistent kernel keeps
-// the BF16 weights in shared memory, each CTA of 128 threads gathers the
+// the BF16 weights in shared memory, each CTA of 256 threads gathers the
 // features of 128 arrival points into a BF16 tile, and one elected thread
 // issues tcgen05.mma for each layer with the FP32 accumulator in tensor
-// memory; the epilogue (tcgen05.ld, bias, GELU, BF16) writes the next layer's
+// memory; two threads per arrival point share the feature gathers and the
+// epilogue (tcgen05.ld, bias, GELU with the hardware tanh on BF16
+// pairs, BF16) writes the next layer's
 // input tile in place.  Operands use the K-major no-swizzle layout of 8x16-byte
 // core matrices (K chunks of a row group adjacent).  Every wait on the MMA barrier is bounded: on expiry the CTA
 // raises kErrTimeout in the handle's status, waits (bounded) for its MMA in
@@ -42,6 +44,7 @@ constexpr int kK1 = 96;                  // features padded to the MMA K step
 constexpr int kHid = ADZC_GUESS_HIDDEN;  // 128
 constexpr int kN3 = 16;                  // 3 outputs padded to the smallest N
 constexpr int kRows = 128;               // arrival points per tile (MMA M)
+constexpr int kThreads = 256;            // two threads per point: each half of the K chunks / columns
 
 // weight image: core-matrix layouts of W1 (128x96), W2 (128x128), W3 (16x128),
 // then FP32 biases b1 (128), b2 (128), b3 (16); copied verbatim to shared memory
@@ -140,21 +143,23 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   for (int q = 0; q < 32; q++) v[q] = __uint_as_float(r[q]);
 }
 
-__device__ __forceinline__ float tanh_approx(float x) {
-  float y;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
-// tanh form of GELU (Hendrycks and Gimpel, 2016)
-__device__ __forceinline__ float gelu_fast(float x) {
-  const float u = 0.7978845608028654f * fmaf(0.044715f * x, x * x, x);
-  return 0.5f * x * (1.0f + tanh_approx(u));
-}
-
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
   return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// tanh form of GELU (Hendrycks and Gimpel, 2016) of a pair, packed to BF16:
+// u = c h (1 + 0.044715 h^2) on an FP32 pair, the tanh by the hardware
+// approximation on a BF16 pair, then h (0.5 + 0.5 tanh u) on BF16 pairs
+__device__ __forceinline__ uint32_t gelu_bf16x2(float2 h) {
+  const float c = 0.7978845608028654f;
+  const float2 p = __ffma2_rn(__fmul2_rn(h, h), make_float2(0.044715f * c, 0.044715f * c), make_float2(c, c));
+  const float2 u = __fmul2_rn(h, p);
+  uint32_t t, sh, g;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(pack_bf16(u.x, u.y)));
+  asm("fma.rn.bf16x2 %0, %1, %2, %2;" : "=r"(sh) : "r"(t), "r"(0x3F003F00u));  // 0.5 t + 0.5
+  asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(g) : "r"(pack_bf16(h.x, h.y)), "r"(sh));
+  return g;
 }
 
 struct Args {
@@ -170,10 +175,6 @@ struct Args {
   double dt;
 };
 
-__device__ __forceinline__ long long ext_at(const DGrid& g, int i, int j, int k) {
-  return (long long)(i - g.lminx) + (long long)(j - g.lminy) * g.nit + (long long)(k - 1) * g.nij;
-}
-
 __device__ __forceinline__ long long wp_at(const DGrid& g, int i, int j, int k, int c) {
   const long long nx = g.ni + 4, ny = g.nj + 4;
   return (long long)(i + 1) + (long long)(j + 1) * nx + (long long)(k - 1) * nx * ny +
@@ -187,49 +188,62 @@ __device__ __forceinline__ void point_of(const DGrid& g, int k00, long long t, i
   k = (int)(t / plane) + k00;
 }
 
+// the 27 neighbourhood rows of an arrival point: row (dk, dj) starts at
+// column i - 1 of plane k + dk (clamped to 1..nk), row j + dj; components are
+// ncell apart.  Scales turn winds into Courant numbers.
+struct Nbr {
+  const float* row[9];
+  long long ncell;
+  float sx, sy, sz, dts;
+};
+
+__device__ __forceinline__ void neighbourhood(const DGrid& g, const float* uvw, int i, int j, int k, double dt,
+                                              Nbr& nb) {
+  nb.ncell = g.nij * g.nk;
+  const long long r0 = (long long)(i - 1 - g.lminx) + (long long)(j - g.lminy) * g.nit;
+#pragma unroll
+  for (int dk = 0; dk < 3; dk++) {
+    int kq = k + dk - 1;
+    kq = kq < 1 ? 1 : (kq > g.nk ? g.nk : kq);
+#pragma unroll
+    for (int dj = 0; dj < 3; dj++) nb.row[dk * 3 + dj] = uvw + (long long)(kq - 1) * g.nij + r0 + (long long)(dj - 1) * g.nit;
+  }
+  const int kb = k < 1 ? 1 : (k > g.nk - 1 ? g.nk - 1 : k);
+  nb.sx = (float)(dt * g.inv_hx);
+  nb.sy = (float)(dt * g.inv_hy);
+  nb.sz = (float)(dt * __ldg(g.odelz_m + kb));
+  nb.dts = (float)(dt / ADZC_GUESS_DT_SCALE);
+}
+
 // feature q (0..81) of arrival point (i,j,k): oracle/guess_oracle.py:features
 template <int Q>
-__device__ __forceinline__ float feature(const DGrid& g, const float* uvw, long long ncell, int i, int j, int k,
-                                         double sx, double sy, double sz, double dt) {
+__device__ __forceinline__ float feature(const Nbr& nb) {
   if (Q >= kFeat) return 0.0f;
-  if (Q == kFeat - 1) return (float)(dt / ADZC_GUESS_DT_SCALE);
+  if (Q == kFeat - 1) return nb.dts;
   constexpr int n = Q / 3, c = Q % 3;
-  constexpr int dk = n / 9 - 1, dj = (n / 3) % 3 - 1, di = n % 3 - 1;
-  int kq = k + dk;
-  kq = kq < 1 ? 1 : (kq > g.nk ? g.nk : kq);
-  const long long e = ext_at(g, i + di, j + dj, kq);
-  const double v = (double)__ldg(uvw + c * ncell + e);
-  return (float)(v * (c == 0 ? sx : c == 1 ? sy : sz));
+  constexpr int dk = n / 9, dj = (n / 3) % 3, di = n % 3;
+  const float v = __ldg(nb.row[dk * 3 + dj] + c * nb.ncell + di);
+  return v * (c == 0 ? nb.sx : c == 1 ? nb.sy : nb.sz);
 }
 
 template <int Q0>
-__device__ __forceinline__ void features8(const DGrid& g, const float* uvw, long long ncell, int i, int j, int k,
-                                          double sx, double sy, double sz, double dt, float* f) {
-  f[0] = feature<Q0 + 0>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
-  f[1] = feature<Q0 + 1>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
-  f[2] = feature<Q0 + 2>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
-  f[3] = feature<Q0 + 3>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
-  f[4] = feature<Q0 + 4>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
-  f[5] = feature<Q0 + 5>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
-  f[6] = feature<Q0 + 6>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
-  f[7] = feature<Q0 + 7>(g, uvw, ncell, i, j, k, sx, sy, sz, dt);
-}
-
-__device__ __forceinline__ void scales(const DGrid& g, int k, double dt, double& sx, double& sy, double& sz) {
-  sx = dt * g.inv_hx;
-  sy = dt * g.inv_hy;
-  const int nb = k < 1 ? 1 : (k > g.nk - 1 ? g.nk - 1 : k);
-  sz = dt * __ldg(g.odelz_m + nb);
+__device__ __forceinline__ void features8(const Nbr& nb, float* f) {
+  f[0] = feature<Q0 + 0>(nb);
+  f[1] = feature<Q0 + 1>(nb);
+  f[2] = feature<Q0 + 2>(nb);
+  f[3] = feature<Q0 + 3>(nb);
+  f[4] = feature<Q0 + 4>(nb);
+  f[5] = feature<Q0 + 5>(nb);
+  f[6] = feature<Q0 + 6>(nb);
+  f[7] = feature<Q0 + 7>(nb);
 }
 
 // features of a chunk of 8 into the tile (row r, K chunk KC)
 template <int KC>
-__device__ __forceinline__ void put_chunk(unsigned char* A, int r, bool valid, const DGrid& g, const float* uvw,
-                                          long long ncell, int i, int j, int k, double sx, double sy, double sz,
-                                          double dt) {
+__device__ __forceinline__ void put_chunk(unsigned char* A, int r, bool valid, const Nbr& nb) {
   float f[8];
   if (valid) {
-    features8<KC * 8>(g, uvw, ncell, i, j, k, sx, sy, sz, dt, f);
+    features8<KC * 8>(nb, f);
   } else {
 #pragma unroll
     for (int q = 0; q < 8; q++) f[q] = 0.0f;
@@ -245,18 +259,17 @@ __device__ __forceinline__ void put_chunk(unsigned char* A, int r, bool valid, c
 // training features: FP32, all 82 per point
 __global__ void __launch_bounds__(128) k_features(Args a, long long n) {
   const DGrid& g = a.g;
-  const long long ncell = g.nij * g.nk;
   for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
     const long long t = a.idx ? a.idx[s] : s;
     if (t < 0 || t >= a.npts) continue;
     int i, j, k;
     point_of(g, a.k00, t, i, j, k);
-    double sx, sy, sz;
-    scales(g, k, a.dt, sx, sy, sz);
+    Nbr nb;
+    neighbourhood(g, a.uvw, i, j, k, a.dt, nb);
     float* o = a.feat + s * kFeat;
     float f[8];
-#define ADZ_FEAT_CHUNK(KC)                                                        \
-  features8<KC * 8>(g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt, f);               \
+#define ADZ_FEAT_CHUNK(KC)                                    \
+  features8<KC * 8>(nb, f);                                   \
   for (int q = 0; q < 8 && KC * 8 + q < kFeat; q++) o[KC * 8 + q] = f[q];
     ADZ_FEAT_CHUNK(0) ADZ_FEAT_CHUNK(1) ADZ_FEAT_CHUNK(2) ADZ_FEAT_CHUNK(3) ADZ_FEAT_CHUNK(4)
     ADZ_FEAT_CHUNK(5) ADZ_FEAT_CHUNK(6) ADZ_FEAT_CHUNK(7) ADZ_FEAT_CHUNK(8) ADZ_FEAT_CHUNK(9)
@@ -265,30 +278,40 @@ __global__ void __launch_bounds__(128) k_features(Args a, long long n) {
   }
 }
 
-// epilogue of a hidden layer: 128 accumulator columns of this thread's row,
+// epilogue of a hidden layer: this thread's half (64) of the accumulator
+// columns of its row,
 // + bias, GELU, BF16, written as the next layer's K-major input row
-__device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, const float* bias, unsigned char* A, int r) {
+__device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, const float* bias, unsigned char* A, int r,
+                                                int half) {
 #pragma unroll
-  for (int c0 = 0; c0 < kHid; c0 += 32) {
+  for (int c0 = half * (kHid / 2); c0 < (half + 1) * (kHid / 2); c0 += 32) {
     float v[32];
     tmem_ld32(tmem_row + c0, v);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       uint4 w;
       const int c = c0 + 8 * q;
-      w.x = pack_bf16(gelu_fast(v[8 * q + 0] + bias[c + 0]), gelu_fast(v[8 * q + 1] + bias[c + 1]));
-      w.y = pack_bf16(gelu_fast(v[8 * q + 2] + bias[c + 2]), gelu_fast(v[8 * q + 3] + bias[c + 3]));
-      w.z = pack_bf16(gelu_fast(v[8 * q + 4] + bias[c + 4]), gelu_fast(v[8 * q + 5] + bias[c + 5]));
-      w.w = pack_bf16(gelu_fast(v[8 * q + 6] + bias[c + 6]), gelu_fast(v[8 * q + 7] + bias[c + 7]));
+      const float2 b01 = *reinterpret_cast<const float2*>(bias + c), b23 = *reinterpret_cast<const float2*>(bias + c + 2);
+      const float2 b45 = *reinterpret_cast<const float2*>(bias + c + 4), b67 = *reinterpret_cast<const float2*>(bias + c + 6);
+      const float2 h01 = __fadd2_rn(make_float2(v[8 * q + 0], v[8 * q + 1]), b01);
+      const float2 h23 = __fadd2_rn(make_float2(v[8 * q + 2], v[8 * q + 3]), b23);
+      const float2 h45 = __fadd2_rn(make_float2(v[8 * q + 4], v[8 * q + 5]), b45);
+      const float2 h67 = __fadd2_rn(make_float2(v[8 * q + 6], v[8 * q + 7]), b67);
+      w.x = gelu_bf16x2(h01);
+      w.y = gelu_bf16x2(h23);
+      w.z = gelu_bf16x2(h45);
+      w.w = gelu_bf16x2(h67);
       *reinterpret_cast<uint4*>(A + core_off(r, c, kHid)) = w;
     }
   }
 }
 
-__global__ void __launch_bounds__(128, 1) k_guess(Args a) {
+__global__ void __launch_bounds__(kThreads, 2) k_guess(Args a) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const int tid = threadIdx.x, warp = tid >> 5;
+  // thread tid: row (arrival point) tid % 128 of the tile, half tid / 128;
+  // warp w reads TMEM lanes 32 (w % 4) .. +31, the lanes of its rows
+  const int tid = threadIdx.x, warp = tid >> 5, row = tid & (kRows - 1), half = tid / kRows;
   const DGrid& g = a.g;
   // weight image -> shared memory
   {
@@ -312,37 +335,39 @@ __global__ void __launch_bounds__(128, 1) k_guess(Args a) {
   __syncthreads();
   fence_after();
   const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kTaddr);
-  const uint32_t tmem_row = tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t tmem_row = tmem + ((uint32_t)((warp & 3) * 32) << 16);
   unsigned char* A = sm + kA;
   const float* b1 = reinterpret_cast<const float*>(sm + kB1);
   const float* b2 = reinterpret_cast<const float*>(sm + kB2);
   const float* b3 = reinterpret_cast<const float*>(sm + kB3);
   const uint32_t a_addr = s_base + kA, w1 = s_base + kW1, w2 = s_base + kW2, w3 = s_base + kW3;
   const uint32_t id_hid = instr_desc(kRows, kHid), id_out = instr_desc(kRows, kN3);
-  const long long ncell = g.nij * g.nk;
   const long long ntiles = (a.npts + kRows - 1) / kRows;
   uint32_t parity = 0;
   bool failed = false, pending = false;
 
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long long t = tile * kRows + tid;
+    const long long t = tile * kRows + row;
     const bool valid = t < a.npts;
     int i = 1, j = 1, k = 1;
     if (valid) point_of(g, a.k00, t, i, j, k);
-    double sx, sy, sz;
-    scales(g, k, a.dt, sx, sy, sz);
-    put_chunk<0>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
-    put_chunk<1>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
-    put_chunk<2>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
-    put_chunk<3>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
-    put_chunk<4>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
-    put_chunk<5>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
-    put_chunk<6>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
-    put_chunk<7>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
-    put_chunk<8>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
-    put_chunk<9>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
-    put_chunk<10>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
-    put_chunk<11>(A, tid, valid, g, a.uvw, ncell, i, j, k, sx, sy, sz, a.dt);
+    Nbr nb;
+    neighbourhood(g, a.uvw, i, j, k, a.dt, nb);
+    if (half == 0) {
+      put_chunk<0>(A, row, valid, nb);
+      put_chunk<1>(A, row, valid, nb);
+      put_chunk<2>(A, row, valid, nb);
+      put_chunk<3>(A, row, valid, nb);
+      put_chunk<4>(A, row, valid, nb);
+      put_chunk<5>(A, row, valid, nb);
+    } else {
+      put_chunk<6>(A, row, valid, nb);
+      put_chunk<7>(A, row, valid, nb);
+      put_chunk<8>(A, row, valid, nb);
+      put_chunk<9>(A, row, valid, nb);
+      put_chunk<10>(A, row, valid, nb);
+      put_chunk<11>(A, row, valid, nb);
+    }
 
     // three layers: tile [128 x K] . W^T -> TMEM, epilogue back into the tile
     float y[3] = {0.f, 0.f, 0.f};
@@ -365,7 +390,8 @@ __global__ void __launch_bounds__(128, 1) k_guess(Args a) {
         mma_commit(bar);
       }
       pending = true;
-      const bool ok = mbar_wait_bounded(bar, parity);
+      // one thread waits for the MMA; the block barrier releases the others
+      const bool ok = tid == 0 ? mbar_wait_bounded(bar, parity) : true;
       if (__syncthreads_or(!ok)) {
         failed = true;
         break;
@@ -374,8 +400,8 @@ __global__ void __launch_bounds__(128, 1) k_guess(Args a) {
       parity ^= 1u;
       fence_after();
       if (layer < 2) {
-        hidden_epilogue(tmem_row, layer == 0 ? b1 : b2, A, tid);
-      } else {
+        hidden_epilogue(tmem_row, layer == 0 ? b1 : b2, A, row, half);
+      } else if (half == 0) {
         float v[32];
         tmem_ld32(tmem_row, v);  // columns 0..31; the first 3 are the outputs
         y[0] = v[0] + b3[0];
@@ -384,7 +410,7 @@ __global__ void __launch_bounds__(128, 1) k_guess(Args a) {
       }
     }
     if (failed) break;
-    if (valid) {
+    if (valid && half == 0) {
       if (a.disp) {
         a.disp[3 * t + 0] = y[0];
         a.disp[3 * t + 1] = y[1];
@@ -402,7 +428,7 @@ __global__ void __launch_bounds__(128, 1) k_guess(Args a) {
   }
   if (failed) {
     if (tid == 0) atomicOr(g.status, kErrTimeout);
-    if (pending) mbar_wait_bounded(bar, parity);  // let the MMA in flight finish before freeing its memory
+    if (pending && tid == 0) mbar_wait_bounded(bar, parity);  // let the MMA in flight finish before freeing its memory
   }
   fence_before();
   __syncthreads();
@@ -557,7 +583,7 @@ extern "C" int adzc_guess_apply(adzc_handle* h, const adzc_guess* net, double dt
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const long long ntiles = (a.npts + kRows - 1) / kRows;
   const int grid = (int)std::min<long long>(ntiles, 2LL * sms);
-  k_guess<<<grid, 128, kSmem, s>>>(a);
+  k_guess<<<grid, kThreads, kSmem, s>>>(a);
   return cudaGetLastError() == cudaSuccess ? ADZC_OK : adz_internal_fail(ADZC_ERR_CUDA);
 }
 

@@ -69,6 +69,18 @@ def unflatten(v) -> dict:
     return out
 
 
+def init_params(seed: int = 0) -> dict:
+    """Initial weights: normal with variance 2 / fan-in, output layer scaled
+    by 0.1, zero biases."""
+    rng = np.random.default_rng(seed)
+    p = {}
+    for name, (n, k) in {"1": (HID, NFEAT), "2": (HID, HID), "3": (NOUT, HID)}.items():
+        p["W" + name] = (rng.standard_normal((n, k)) * np.sqrt(2.0 / k)).astype(np.float32)
+        p["b" + name] = np.zeros(n, np.float32)
+    p["W3"] *= np.float32(0.1)
+    return p
+
+
 def load_weights(path: str = DEFAULT_WEIGHTS) -> dict:
     with np.load(path) as z:
         return {k: z[k].astype(np.float32) for k in ORDER}
