@@ -99,28 +99,41 @@ class Clocks:
 
 
 def dist_init():
+    """One process per GPU under torchrun; NCCL on GPUs, gloo without."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
+    if ws > 1 and not torch.distributed.is_initialized():
         import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        torch.distributed.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return ws, rank, local
+
+
+def _dev():
+    return "cuda" if torch.cuda.is_available() else "cpu"
 
 
 def max_over_ranks(x: float, ws: int) -> float:
     if ws == 1:
         return x
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    t = torch.tensor([x], device=_dev(), dtype=torch.float64)
     torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     return float(t.item())
 
 
 def barrier(ws):
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
     if ws > 1:
         torch.distributed.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
+
+
+def tile_seed(rank: int) -> int:
+    """Each rank advances its own tile (weak scaling, no data-path collective)."""
+    return 4321 + rank
 
 
 # ---------------------------------------------------------------------------
@@ -169,7 +182,7 @@ def run_product(args):
     ws, rank, local = dist_init()
     torch.cuda.set_device(local)
     ni, nj, nk = args.size
-    cfg = synth.config_large(ni, nj, nk, seed=4321 + rank, ntracers=args.ntr)
+    cfg = synth.config_large(ni, nj, nk, seed=tile_seed(rank), ntracers=args.ntr)
     npts = cfg.npoints
     inp64 = synth.make_inputs(cfg, device="cuda", dtype=torch.float64)
     keys = ["uu_ext", "vv_ext", "ww_ext", "ut0", "vt0", "zdt0", "src_u", "src_v", "src_w"]
@@ -296,6 +309,11 @@ def run_product(args):
         torch.cuda.empty_cache()
         batch = measure_batch(args, timed, ws)
 
+    tsum = None
+    if not args.no_tracers:
+        torch.cuda.empty_cache()
+        tsum = measure_tracers(args, timed, ws, rank)
+
     gsum = None
     if not args.no_guess and os.path.exists(args.guess_weights):
         torch.cuda.empty_cache()
@@ -322,7 +340,7 @@ def run_product(args):
                           "achieved_gbs": step_bytes / (ms32 * 1e-3) / 1e9,
                           "frac": step_bytes / (ms32 * 1e-3) / 1e9 / hbm},
         "e2e": e2e, "gpu_launches": LAUNCHES_PER_STEP * args.steps, "clocks": clk, "cpu_baseline": cpu,
-        "batch": batch, "learned_guess": gsum,
+        "tracers8": tsum, "batch": batch, "learned_guess": gsum,
     }
     if rank == 0:
         print(json.dumps(line))
@@ -385,6 +403,42 @@ def measure_batch(args, timed, ws):
     return out
 
 
+def measure_tracers(args, timed, ws, rank):
+    """The multi-tracer workload: the 1024x1024x80 flow with u, v, w and 8
+    log-normal (sigma 1) tracers, mono clipping on; MIXED and the FP64
+    drop-in, one step each as in the headline."""
+    from gem_b200 import adz, synth
+    ni, nj, nk = args.size
+    cfg = synth.config_mixed(ni, nj, nk, seed=tile_seed(rank), ntracers=8)
+    out = {"workload": f"adz step {ni}x{nj}x{nk}, u,v,w + 8 log-normal tracers, mono clipping",
+           "points_per_step": cfg.npoints}
+    for name, prec in (("fp64", adz.FP64), ("mixed", adz.MIXED)):
+        dt = adz._field_dtype(prec)
+        data = synth.make_inputs(cfg, device="cuda", dtype=dt)
+        ad = adz.Adz.from_config(cfg)
+        px, wp = ad.new_state(prec)
+        ad.adz_inittraj(prec, px, wp)
+        outs = {k: torch.zeros(ad.ext_shape, dtype=dt, device="cuda") for k in ("u", "v", "w")}
+        tro = [torch.zeros(ad.ext_shape, dtype=dt, device="cuda") for _ in data["tracers"]]
+
+        def step():
+            adz.step_fused(ad, prec, cfg.dt, data, data, data["tracers"], px, wp, outs, tro, cfg.mono)
+        step()  # cold start, untimed
+        ms, _ = timed(step, max(3, min(args.steps, 10)), args.warmup)
+        if ad.status() != 0:
+            raise RuntimeError("device status set during the multi-tracer steps")
+        out[name + "_ms_per_step"] = ms
+        out[name + "_value"] = cfg.npoints * ws / (ms * 1e-3)
+        del data, outs, tro, step, ad, px, wp
+        torch.cuda.empty_cache()
+    out["speedup_vs_fp64"] = out["fp64_ms_per_step"] / out["mixed_ms_per_step"]
+    hbm, _ = peaks()
+    out["step_roofline"] = {"algorithmic_bytes_per_point": 160.0,
+                            "achieved_gbs": 160.0 * cfg.npoints / (out["mixed_ms_per_step"] * 1e-3) / 1e9}
+    out["step_roofline"]["frac"] = out["step_roofline"]["achieved_gbs"] / hbm
+    return out
+
+
 def measure_guess(args, timed, ws, rank):
     """Cold start of the 1024x1024x80 tile (no previous departure points):
     the reference's 6 fixed updates from the arrival point, the plain update
@@ -395,7 +449,7 @@ def measure_guess(args, timed, ws, rank):
     from gem_b200 import adz, guess, synth
     prec = adz.MIXED
     ni, nj, nk = args.size
-    cfg = synth.config_cold(ni, nj, nk, seed=4321 + rank)
+    cfg = synth.config_cold(ni, nj, nk, seed=tile_seed(rank))
     inp = synth.make_inputs(cfg, device="cuda", dtype=torch.float32, with_fields=False)
     ad = adz.Adz.from_config(cfg)
     n = guess.npoints(ad)
@@ -485,6 +539,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-domain measurement")
     ap.add_argument("--batch-domains", type=int, default=16)
     ap.add_argument("--no-guess", action="store_true", help="skip the learned-guess cold-start measurement")
+    ap.add_argument("--no-tracers", action="store_true", help="skip the 8-tracer mono measurement")
     ap.add_argument("--guess-weights", default=os.path.join(ROOT, "gem_b200", "data", "guess_mlp.npz"))
     ap.add_argument("--only", choices=["mixed"], default=None,
                     help="run the mixed-precision path alone (small profiling runs)")
