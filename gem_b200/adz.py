@@ -23,6 +23,7 @@ LIB_PATH = os.path.join(HERE, "libadz_b200.so")
 
 REF32, FP64, MIXED = 0, 1, 2
 SET_Q, SET_U, SET_V, SET_T = 0, 1, 2, 3
+QV = 4  # mono flag bit: BICUBH_QV interpolation of that field (set T)
 PREC_NAMES = {"ref32": REF32, "fp64": FP64, "mixed": MIXED}
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA runtime error", 3: "fewer than 4 levels",

@@ -232,6 +232,10 @@ extern "C" int adzc_batch_create(int prec, int ndom, const adzc_domain* doms, ad
           fp.src[q] = in.srcs[f];
           fp.dst[q] = in.dsts[f];
           const int mv = in.mono ? in.mono[f] : 0;
+          if (mv < 0 || mv > 2) {  // tricubic fields only
+            adzc_batch_destroy(b);
+            return adz_internal_fail(ADZC_ERR_ARG);
+          }
           if (mv != 0) fp.mono_mask |= 1u << q;
           if (mv == 1) fp.clip_mask |= 1u << q;
         }

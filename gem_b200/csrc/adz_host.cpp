@@ -57,6 +57,14 @@ cudaError_t dispatch_traject(int prec, const adz::DGrid& g, const adz::TrajArgs&
     default: return adz::launch_traject<adz::kMixed>(g, a, s);
   }
 }
+cudaError_t dispatch_qv(int prec, const adz::DGrid& g, int i0, int nx, int j0, int ny, int k0, int nz,
+                        const adz::SetArgs& a, const adz::FieldPtrs& fp, cudaStream_t s) {
+  switch (prec) {
+    case ADZC_REF32: return adz::launch_qv_set<adz::kRef32>(g, i0, nx, j0, ny, k0, nz, a, fp, s);
+    case ADZC_FP64: return adz::launch_qv_set<adz::kFp64>(g, i0, nx, j0, ny, k0, nz, a, fp, s);
+    default: return adz::launch_qv_set<adz::kMixed>(g, i0, nx, j0, ny, k0, nz, a, fp, s);
+  }
+}
 cudaError_t dispatch_set(int prec, const adz::DGrid& g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
                          const adz::SetArgs& a, const adz::FieldPtrs& fp, cudaStream_t s) {
   switch (prec) {
@@ -272,7 +280,7 @@ struct adzc_handle {
   int niter = 1;
   int cold = 0;
   // host copies of the derived tables
-  std::vector<double> zm, zt, odelz_m, odelz_t, vw, cy;
+  std::vector<double> zm, zt, odelz_m, odelz_t, vw, cy, delz_t, qv_t;
   std::vector<int> search_m, search_t;
   double ovdzm = 0, ovdzt = 0, sig = 0;
   adzc_ztab* tab_m = nullptr;
@@ -412,6 +420,31 @@ extern "C" int adzc_setup(const adzc_grid* gin, adzc_handle** out) {
     vw[6 * (nk + 1) + k] = lag3(rx, rc, ra, rb, rd);
     vw[7 * (nk + 1) + k] = lag3(rx, rd, ra, rb, rc);
   }
+  // BICUBH_QV denominators on thermo levels (B/adz_set.F90:286-311), products left to right
+  h->qv_t.assign(10 * (nk + 1), 0.0);
+  for (int k = 2; k <= nk - 2; k++) {
+    const double ra = zt[k - 1], rb = zt[k], rc = zt[k + 1], rd = zt[k + 2];
+    double* q = h->qv_t.data() + 10 * k;
+    q[0] = 1.0 / ((ra - rb) * (ra - rc) * (ra - rd));
+    q[1] = 1.0 / ((rb - ra) * (rb - rc) * (rb - rd));
+    q[2] = 1.0 / ((rc - ra) * (rc - rb) * (rc - rd));
+    q[3] = 1.0 / ((rd - ra) * (rd - rb) * (rd - rc));
+  }
+  for (int k = 3; k <= nk - 3; k++) {
+    const double r[6] = {zt[k - 2], zt[k - 1], zt[k], zt[k + 1], zt[k + 2], zt[k + 3]};
+    double* q = h->qv_t.data() + 10 * k + 4;
+    for (int a = 0; a < 6; a++) {  // product over the other five nodes, in order
+      double prod = 0.0;
+      bool first = true;
+      for (int b = 0; b < 6; b++) {
+        if (b == a) continue;
+        prod = first ? (r[a] - r[b]) : prod * (r[a] - r[b]);
+        first = false;
+      }
+      q[a] = 1.0 / prod;
+    }
+  }
+  h->delz_t = delz_t;
   h->cy.assign(g.cy, g.cy + I.njt);
   h->niter = std::max(1, g.itraj);
 
@@ -422,7 +455,8 @@ extern "C" int adzc_setup(const adzc_grid* gin, adzc_handle** out) {
     return fail(st);
   }
   // one device block for every table
-  const size_t nd = zm.size() + zt.size() + h->odelz_m.size() + h->odelz_t.size() + h->vw.size() + h->cy.size();
+  const size_t nd = zm.size() + zt.size() + h->odelz_m.size() + h->odelz_t.size() + h->vw.size() + h->cy.size() +
+                    h->delz_t.size() + h->qv_t.size();
   const size_t ni_ = h->search_m.size() + h->search_t.size() + 1;
   if (cudaGetDevice(&h->device) != cudaSuccess || cudaMalloc(&h->d_tables, nd * sizeof(double) + ni_ * sizeof(int)) !=
                                                       cudaSuccess) {
@@ -445,6 +479,8 @@ extern "C" int adzc_setup(const adzc_grid* gin, adzc_handle** out) {
   D.odelz_t = put(h->odelz_t);
   D.vw = put(h->vw);
   D.cy = put(h->cy);
+  D.delz_t = put(h->delz_t);
+  D.qv_t = put(h->qv_t);
   int* ip = (int*)(dp + nd);
   int* dip = (int*)((double*)h->d_tables + nd);
   std::memcpy(ip, h->search_m.data(), h->search_m.size() * sizeof(int));
@@ -592,22 +628,37 @@ extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const
   a.dt = h->dt;
   a.k00 = std::max(I.k0t - 1, 1);  // B/adz_interp_traj.F90:39-40
   if (h->g.bc_lam_flux != 0 && I.k0 > 1) a.k00 = 1;
-  for (int q0 = 0; q0 < nfields; q0 += adz::kMaxFields) {
-    adz::FieldPtrs fp{};
-    fp.nf = std::min(adz::kMaxFields, nfields - q0);
-    for (int q = 0; q < fp.nf; q++) {
-      const int f = q0 + q;
-      if (!srcs[f] || !dsts[f]) return fail(ADZC_ERR_ARG);
-      fp.src[q] = srcs[f];
-      fp.dst[q] = dsts[f];
-      const int mv = mono ? mono[f] : 0;
-      if (mv != 0) fp.mono_mask |= 1u << q;
-      if (mv == 1) fp.clip_mask |= 1u << q;
-      fp.lin[q] = lin ? lin[f] : nullptr;
-      fp.mn[q] = mn ? mn[f] : nullptr;
-      fp.mx[q] = mx ? mx[f] : nullptr;
+  // tricubic fields, then BICUBH_QV fields (set t only), in groups of kMaxFields
+  std::vector<int> groups[2];
+  for (int f = 0; f < nfields; f++) {
+    const int mv = mono ? mono[f] : 0;
+    if ((mv & ~(3 | ADZC_QV)) != 0 || (mv & 3) == 3) return fail(ADZC_ERR_ARG);
+    if ((mv & ADZC_QV) && set != ADZC_SET_T) return fail(ADZC_ERR_ARG);
+    if (!srcs[f] || !dsts[f]) return fail(ADZC_ERR_ARG);
+    groups[(mv & ADZC_QV) ? 1 : 0].push_back(f);
+  }
+  for (int kind = 0; kind < 2; kind++) {
+    const std::vector<int>& fl = groups[kind];
+    for (size_t q0 = 0; q0 < fl.size(); q0 += adz::kMaxFields) {
+      adz::FieldPtrs fp{};
+      fp.nf = (int)std::min<size_t>(adz::kMaxFields, fl.size() - q0);
+      for (int q = 0; q < fp.nf; q++) {
+        const int f = fl[q0 + q];
+        fp.src[q] = srcs[f];
+        fp.dst[q] = dsts[f];
+        const int mv = (mono ? mono[f] : 0) & 3;
+        if (mv != 0) fp.mono_mask |= 1u << q;
+        if (mv == 1) fp.clip_mask |= 1u << q;
+        fp.lin[q] = lin ? lin[f] : nullptr;
+        fp.mn[q] = mn ? mn[f] : nullptr;
+        fp.mx[q] = mx ? mx[f] : nullptr;
+      }
+      if (kind == 0) {
+        ADZ_CK(dispatch_set(prec, D, set, i0, nx, j0, ny, k0, nz, a, fp, (cudaStream_t)stream));
+      } else {
+        ADZ_CK(dispatch_qv(prec, D, i0, nx, j0, ny, k0, nz, a, fp, (cudaStream_t)stream));
+      }
     }
-    ADZ_CK(dispatch_set(prec, D, set, i0, nx, j0, ny, k0, nz, a, fp, (cudaStream_t)stream));
   }
   return ADZC_OK;
 }

@@ -13,6 +13,7 @@
 // B/ = src/gemdyn/src/base/.
 #pragma once
 #include "adz_device.cuh"
+#include "adz_qv.cuh"
 
 // launch bounds of the gather kernels (minimum resident blocks of 128 threads
 // per SM; 0 lets ptxas choose).  A translation unit may set them before
@@ -557,6 +558,65 @@ __global__ void ADZ_SET_BOUNDS k_tricub_set(DGrid g, int set, int i0, int nx, in
   }
 }
 
+// BICUBH_QV fields at position set t (adz_interp_hlt.F90:113-116 with
+// F_QV_L): lin/min/max of the inner 2x2x2 box always formed, written where
+// asked; clip as adz_post_tr.F90:81-94
+template <int PREC>
+__device__ __forceinline__ void qv_point(const DGrid& g, const SetArgs& a, const FieldPtrs& fp, int i, int j, int k) {
+  using F = typename Types<PREC>::F;
+  double px, py, pz;
+  set_position<PREC, false>(g, a, 3, i, j, k, px, py, pz);
+  if (PREC == kRef32) {  // Adz_pt is ``real``
+    px = (double)(float)px;
+    py = (double)(float)py;
+    pz = (double)(float)pz;
+  }
+  QvCoef c;
+  qv_coef<PREC>(g, px, py, pz, c);
+  if (!qv_stencil_ok(g, c)) {
+    raise_status(g.status, kErrHalo);
+    return;
+  }
+  const long long e = ext_index(g, i, j, k);
+  const long long base = ext_index(g, 1, 1, 1) + c.off;
+  if (PREC == kMixed) {
+    QvCoefF w;
+    qv_to_float(c, w);
+    for (int q = 0; q < fp.nf; q++) {
+      float d, lin, mn, mx;
+      interp_qv_mixed((const float*)fp.src[q] + base, g.nit, g.nij, c, w, d, lin, mn, mx);
+      if ((fp.clip_mask >> q) & 1u) d = fmaxf(mn, fminf(mx, d));
+      if (fp.lin[q]) ((float*)fp.lin[q])[e] = fmaxf(mn, fminf(mx, lin));
+      if (fp.mn[q]) ((float*)fp.mn[q])[e] = mn;
+      if (fp.mx[q]) ((float*)fp.mx[q])[e] = mx;
+      ((float*)fp.dst[q])[e] = d;
+    }
+  } else {
+    for (int q = 0; q < fp.nf; q++) {
+      F d, lin, mn, mx;
+      interp_qv_exact<F>((const F*)fp.src[q] + base, g.nit, g.nij, c, d, lin, mn, mx);
+      if ((fp.clip_mask >> q) & 1u) d = (mn > ((mx < d) ? mx : d)) ? mn : ((mx < d) ? mx : d);
+      if (fp.lin[q]) ((F*)fp.lin[q])[e] = (mn > ((mx < lin) ? mx : lin)) ? mn : ((mx < lin) ? mx : lin);
+      if (fp.mn[q]) ((F*)fp.mn[q])[e] = mn;
+      if (fp.mx[q]) ((F*)fp.mx[q])[e] = mx;
+      ((F*)fp.dst[q])[e] = d;
+    }
+  }
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(128) k_qv_set(DGrid g, int i0, int nx, int j0, int ny, int k0, int nz, SetArgs a,
+                                                FieldPtrs fp) {
+  const long long nplane = (long long)nx * ny;
+  const long long n = nplane * nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nx) + i0;
+    const int j = (int)((t / nx) % ny) + j0;
+    const int k = (int)(t / nplane) + k0;
+    qv_point<PREC>(g, a, fp, i, j, k);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // explicit positions; kind 0 = cubic, 1 = mono, 2 = 3-component
 template <int PREC, int KIND>
@@ -772,6 +832,15 @@ cudaError_t launch_tricub_set(const DGrid& g, int set, int i0, int nx, int j0, i
 }
 
 template <int PREC>
+cudaError_t launch_qv_set(const DGrid& g, int i0, int nx, int j0, int ny, int k0, int nz, const SetArgs& a,
+                          const FieldPtrs& fp, cudaStream_t s) {
+  const long long n = (long long)nx * ny * nz;
+  if (n <= 0) return cudaSuccess;
+  k_qv_set<PREC><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, i0, nx, j0, ny, k0, nz, a, fp);
+  return cudaGetLastError();
+}
+
+template <int PREC>
 cudaError_t launch_interp_pos(const DZtab& lv, int kind, int n, const void* pos, const FieldPtrs& fp,
                               cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
@@ -829,6 +898,8 @@ int batch_resident_blocks(int variant) {
   template cudaError_t launch_tricub_set<P>(const DGrid&, int, int, int, int, int, int, int, const SetArgs&,       \
                                             const FieldPtrs&, cudaStream_t);                                       \
   template cudaError_t launch_interp_pos<P>(const DZtab&, int, int, const void*, const FieldPtrs&, cudaStream_t); \
+  template cudaError_t launch_qv_set<P>(const DGrid&, int, int, int, int, int, int, const SetArgs&,               \
+                                        const FieldPtrs&, cudaStream_t);                                          \
   template cudaError_t launch_batch<P>(int, int, const BDom*, const BItem*, long long, const unsigned*,           \
                                        unsigned long long*, unsigned*, int*, cudaStream_t);                        \
   template int batch_resident_blocks<P>(int);

@@ -85,6 +85,8 @@ extern "C" int adzc_step_noalloc(adzc_handle* h, int prec, double dt, int niter,
   if (ntot > 0 && (!srcs || !dsts)) return adz_internal_fail(ADZC_ERR_ARG);
   for (int f = 0; f < ntot; f++)
     if (!srcs[f] || !dsts[f]) return adz_internal_fail(ADZC_ERR_ARG);
+  for (int f = 0; mono && f < ntot; f++)  // tricubic fields only: mono 0, 1 or 2
+    if (mono[f] < 0 || mono[f] > 2) return adz_internal_fail(ADZC_ERR_ARG);
 
   adz::DGrid D;
   adzc_info I;

@@ -39,6 +39,8 @@ struct DGrid {
   const double* odelz_t;
   const double* vw;       // 8 x (nk+1): vw1m vw2m vw3m vw4m vw1t vw2t vw3t vw4t
   const double* cy;       // index j - lminy
+  const double* delz_t;   // 0..nk
+  const double* qv_t;     // BICUBH_QV denominators, 10 per level (B/adz_set.F90:286-311)
   DZtab tab_m, tab_t;
   int* status;
 };
@@ -121,6 +123,9 @@ cudaError_t launch_traject_tol(const DGrid& g, const TrajArgs& a, double tol, in
 template <int PREC>
 cudaError_t launch_tricub_set(const DGrid& g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
                               const SetArgs& a, const FieldPtrs& fp, cudaStream_t s);
+template <int PREC>
+cudaError_t launch_qv_set(const DGrid& g, int i0, int nx, int j0, int ny, int k0, int nz, const SetArgs& a,
+                          const FieldPtrs& fp, cudaStream_t s);
 template <int PREC>
 cudaError_t launch_interp_pos(const DZtab& lv, int kind, int n, const void* pos, const FieldPtrs& fp,
                               cudaStream_t s);

@@ -179,9 +179,14 @@ int adzc_traject(adzc_handle *h, int prec, double dt, int niter, const void *uu_
  * on the fly as adz_interp_traj does (B/adz_interp_traj.F90:45-187).
  * srcs/dsts: HOST arrays of nfields DEVICE pointers (ext layout; only the
  * set's arrival range of dsts is written).  mono: NULL or nfields flags,
- * 1 = clip to the bound box (B/adz_post_tr.F90:81-94).  lin/mn/mx: NULL or
- * nfields device pointers (entries may be NULL) receiving Adz_post lin
- * (clipped), min, max for mono fields (B/adz_interp_hlt.F90:152-156). */
+ * 1 = clip to the bound box (B/adz_post_tr.F90:81-94), 2 = bounds only;
+ * | ADZC_QV (set T only) interpolates that field with BICUBH_QV instead:
+ * bicubic horizontal, quintic vertical (B/bicubHQV_lin_mono.F90:20-172, the
+ * F_QV_L branch of B/adz_interp_hlt.F90:113), bounds over the inner 2x2x2
+ * box.  lin/mn/mx: NULL or nfields device pointers (entries may be NULL)
+ * receiving Adz_post lin (clipped), min, max for mono and QV fields
+ * (B/adz_interp_hlt.F90:152-156). */
+#define ADZC_QV 4
 int adzc_tricub(adzc_handle *h, int prec, int set, int nfields, const void *const *srcs, void *const *dsts,
                 const int *mono, void *const *lin, void *const *mn, void *const *mx, void *stream);
 

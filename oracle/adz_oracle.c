@@ -148,6 +148,30 @@ int orc_adz_set(const orc_grid *g, orc_set *s) {
     s->vw3t[k] = lag3(rx, rc, ra, rb, rd);
     s->vw4t[k] = lag3(rx, rd, ra, rb, rc);
   }
+  /* BICUBH_QV denominators, adz_set.F90:286-311 (products left to right) */
+  s->qv_t = (double *)calloc((size_t)(nk + 1) * 10, sizeof(double));
+  for (int k = 2; k <= nk - 2; k++) {
+    const double ra = zt[k - 1], rb = zt[k], rc = zt[k + 1], rd = zt[k + 2];
+    double *q = s->qv_t + (size_t)k * 10;
+    q[0] = 1.0 / ((ra - rb) * (ra - rc) * (ra - rd));
+    q[1] = 1.0 / ((rb - ra) * (rb - rc) * (rb - rd));
+    q[2] = 1.0 / ((rc - ra) * (rc - rb) * (rc - rd));
+    q[3] = 1.0 / ((rd - ra) * (rd - rb) * (rd - rc));
+  }
+  for (int k = 3; k <= nk - 3; k++) {
+    const double r[6] = {zt[k - 2], zt[k - 1], zt[k], zt[k + 1], zt[k + 2], zt[k + 3]};
+    double *q = s->qv_t + (size_t)k * 10 + 4;
+    for (int a = 0; a < 6; a++) { /* quiprod(r_a, the other five in order) */
+      double p = 1.0;
+      int first = 1;
+      for (int b = 0; b < 6; b++) {
+        if (b == a) continue;
+        if (first) { p = r[a] - r[b]; first = 0; }
+        else p = p * (r[a] - r[b]);
+      }
+      q[a] = 1.0 / p;
+    }
+  }
   s->vw5 = (zx[0] - zm[1]) / (zx[0] - zx[1]); /* adz_set.F90:282-284 */
   s->vw6 = (zm[nk] - zx[nk]) / (zx[nk - 1] - zx[nk]);
   /* adz_interp_traj.F90:41-43 */
@@ -170,6 +194,7 @@ void orc_adz_free(orc_set *s) {
   free(s->search_m); free(s->search_t); free(s->cy);
   free(s->vw1m); free(s->vw2m); free(s->vw3m); free(s->vw4m);
   free(s->vw1t); free(s->vw2t); free(s->vw3t); free(s->vw4t);
+  free(s->qv_t);
   orc_ztab_free(s->ztab_m); orc_ztab_free(s->ztab_t);
   memset(s, 0, sizeof(*s));
 }

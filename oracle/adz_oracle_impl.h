@@ -358,6 +358,152 @@ void SFX(orc_tricub)(const orc_set *s, int set, const REAL *pos, int m, const RE
   }
 }
 
+/* BICUBH_QV at one position: bicubHQV_lin_mono.F90:66-147 (coefficients)
+ * and bicubHQV_lin_min_max_zyx.F90:20-83 (sums, lin, min/max), operation
+ * order as written.  The cell index of an FP64 position is that of its FP32
+ * rounding, as for the tricubic interpolator.  Returns the 0-based ext offset
+ * of the stencil origin (column i-1, row j-1, first plane) and the six plane
+ * offsets in po[]. */
+static long SFX(qv_coef)(const orc_set *s, REAL px, REAL py, REAL pz, double cx[4], double cy[4], double qz[6],
+                         double lx[2], double ly[2], double lz[2], long po[6]) {
+  const int nk = s->g.nk;
+  const double ov6 = 1.0 / 6.0, ov2 = 1.0 / 2.0;
+  const double *posz = s->g.zt, *dz = s->delz_t, *odz = s->odelz_t;
+  int ii1 = (int)(float)px;
+  double del = (double)px - (double)ii1;
+  double del12 = (del - 1) * (del - 2), del10 = (del + 1) * del;
+  cx[0] = -(del * del12 * ov6);
+  cx[1] = (del + 1) * del12 * ov2;
+  cx[2] = -(del10 * (del - 2) * ov2);
+  cx[3] = del10 * (del - 1) * ov6;
+  lx[0] = 1.0 - del;
+  lx[1] = del;
+  int jj1 = (int)(float)py;
+  del = (double)py - (double)jj1;
+  del12 = (del - 1) * (del - 2);
+  del10 = (del + 1) * del;
+  cy[0] = -(del * del12 * ov6);
+  cy[1] = (del + 1) * del12 * ov2;
+  cy[2] = -(del10 * (del - 2) * ov2);
+  cy[3] = del10 * (del - 1) * ov6;
+  ly[0] = 1.0 - del;
+  ly[1] = del;
+  int kk1 = (int)(float)pz;
+  const int quintic = (kk1 >= 3) && (kk1 <= nk - 3);
+  const int cubic = (kk1 == 2) || (kk1 == nk - 2);
+  if (!quintic && !cubic) kk1 = kk1 < 1 ? 1 : (kk1 > nk - 1 ? nk - 1 : kk1);
+  const double zt = posz[kk1] + ((double)pz - (double)kk1) * dz[kk1];
+  lz[1] = (zt - posz[kk1]) * odz[kk1];
+  lz[0] = 1.0 - lz[1];
+  const double *q = s->qv_t + (size_t)kk1 * 10;
+  int kb;
+  if (quintic) {
+    kb = kk1 - 2;
+    const double rx = posz[kk1 - 2], ra = posz[kk1 - 1], rb = posz[kk1], rc = posz[kk1 + 1], rd = posz[kk1 + 2],
+                 re = posz[kk1 + 3];
+    qz[0] = (zt - ra) * (zt - rb) * (zt - rc) * (zt - rd) * (zt - re) * q[4];
+    qz[1] = (zt - rx) * (zt - rb) * (zt - rc) * (zt - rd) * (zt - re) * q[5];
+    qz[2] = (zt - rx) * (zt - ra) * (zt - rc) * (zt - rd) * (zt - re) * q[6];
+    qz[3] = (zt - rx) * (zt - ra) * (zt - rb) * (zt - rd) * (zt - re) * q[7];
+    qz[4] = (zt - rx) * (zt - ra) * (zt - rb) * (zt - rc) * (zt - re) * q[8];
+    qz[5] = (zt - rx) * (zt - ra) * (zt - rb) * (zt - rc) * (zt - rd) * q[9];
+  } else if (cubic) {
+    kb = kk1 - 1;
+    const double ra = posz[kk1 - 1], rb = posz[kk1], rc = posz[kk1 + 1], rd = posz[kk1 + 2];
+    qz[0] = 0.0;
+    qz[1] = (zt - rb) * (zt - rc) * (zt - rd) * q[0];
+    qz[2] = (zt - ra) * (zt - rc) * (zt - rd) * q[1];
+    qz[3] = (zt - ra) * (zt - rb) * (zt - rd) * q[2];
+    qz[4] = (zt - ra) * (zt - rb) * (zt - rc) * q[3];
+    qz[5] = 0.0;
+  } else {
+    kb = kk1;
+    qz[0] = 0.0;
+    qz[1] = 0.0;
+    qz[3] = (zt - posz[kk1]) * odz[kk1];
+    qz[2] = 1.0 - qz[3];
+    qz[4] = 0.0;
+    qz[5] = 0.0;
+  }
+  /* plane offsets of the zyx kernel: ninj1..ninj5 */
+  const long nij = s->nij;
+  const long ninjc = quintic ? nij : 0, ninjl = (quintic || cubic) ? nij : 0;
+  po[0] = 0;
+  po[1] = ninjc;
+  po[2] = po[1] + ninjl;
+  po[3] = po[2] + nij;
+  po[4] = po[3] + ninjl;
+  po[5] = po[4] + ninjc;
+  const int il = ii1 - (s->g.i0g - 1), jl = jj1 - (s->g.j0g - 1);
+  return EXT(il - 1, jl - 1, kb);
+}
+
+static void SFX(qv_point)(const REAL *src, long ni, const double cx[4], const double cy[4], const double qz[6],
+                          const double lx[2], const double ly[2], const double lz[2], const long po[6], REAL *xyz,
+                          REAL *li, REAL *mi, REAL *ma) {
+  const long ni2 = ni + ni, ni3 = ni2 + ni;
+  REAL dst[4], dsl[3];
+  for (int i = 0; i < 4; i++) {
+    const double va = src[i] * qz[0] + src[i + po[1]] * qz[1] + src[i + po[2]] * qz[2] + src[i + po[3]] * qz[3] +
+                      src[i + po[4]] * qz[4] + src[i + po[5]] * qz[5];
+    const double vb = src[i + ni] * qz[0] + src[i + ni + po[1]] * qz[1] + src[i + ni + po[2]] * qz[2] +
+                      src[i + ni + po[3]] * qz[3] + src[i + ni + po[4]] * qz[4] + src[i + ni + po[5]] * qz[5];
+    const double vc = src[i + ni2] * qz[0] + src[i + ni2 + po[1]] * qz[1] + src[i + ni2 + po[2]] * qz[2] +
+                      src[i + ni2 + po[3]] * qz[3] + src[i + ni2 + po[4]] * qz[4] + src[i + ni2 + po[5]] * qz[5];
+    const double vd = src[i + ni3] * qz[0] + src[i + ni3 + po[1]] * qz[1] + src[i + ni3 + po[2]] * qz[2] +
+                      src[i + ni3 + po[3]] * qz[3] + src[i + ni3 + po[4]] * qz[4] + src[i + ni3 + po[5]] * qz[5];
+    dst[i] = (REAL)(va * cy[0] + vb * cy[1] + vc * cy[2] + vd * cy[3]);
+  }
+  *xyz = (REAL)(dst[0] * cx[0] + dst[1] * cx[1] + dst[2] * cx[2] + dst[3] * cx[3]);
+  for (int i = 1; i <= 2; i++) {
+    const double vb = src[i + ni + po[2]] * lz[0] + src[i + ni + po[3]] * lz[1];
+    const double vc = src[i + ni2 + po[2]] * lz[0] + src[i + ni2 + po[3]] * lz[1];
+    dsl[i] = (REAL)(vb * ly[0] + vc * ly[1]);
+  }
+  *li = (REAL)(dsl[1] * lx[0] + dsl[2] * lx[1]);
+  REAL hi = src[1 + ni + po[2]], lo = hi;
+  for (int i = 1; i <= 2; i++) {
+    const REAL v[4] = {src[i + ni + po[2]], src[i + ni + po[3]], src[i + ni2 + po[2]], src[i + ni2 + po[3]]};
+    for (int q = 0; q < 4; q++) {
+      hi = SFX(rmax)(hi, v[q]);
+      lo = SFX(rmin)(lo, v[q]);
+    }
+  }
+  *mi = lo;
+  *ma = hi;
+}
+
+/* adz_tricub_hlt with F_QV_L (adz_interp_hlt.F90:113-116 and the scatter of
+ * :119-158) on position set t, plus the clip of adz_post_tr.F90:81-94. */
+void SFX(orc_tricub_qv)(const orc_set *s, const REAL *pos, int m, const REAL *const *srcs, REAL *const *dsts,
+                        int clip, REAL *const *lin, REAL *const *mn, REAL *const *mx) {
+  int r[5];
+  set_range(s, 3, r);
+  const int nk = s->g.nk;
+  const long nx = r[1] - r[0] + 1, ny = r[3] - r[2] + 1, np = nx * ny;
+  if (np <= 0 || m <= 0) return;
+#pragma omp parallel for schedule(static) num_threads(nthr())
+  for (int k = r[4]; k <= nk; k++) {
+    for (int j = r[2]; j <= r[3]; j++)
+      for (int i = r[0]; i <= r[1]; i++) {
+        const REAL *p = pos + 3 * ((long)(k - r[4]) * np + (i - r[0]) + (long)(j - r[2]) * nx);
+        double cx[4], cy[4], qz[6], lx[2], ly[2], lz[2];
+        long po[6];
+        const long o = SFX(qv_coef)(s, p[0], p[1], p[2], cx, cy, qz, lx, ly, lz, po);
+        const long e = EXT(i, j, k);
+        for (int q = 0; q < m; q++) {
+          REAL d, l, lo, hi;
+          SFX(qv_point)(srcs[q] + o, s->nit, cx, cy, qz, lx, ly, lz, po, &d, &l, &lo, &hi);
+          if (lin && lin[q]) lin[q][e] = SFX(rmax)(lo, SFX(rmin)(hi, l));
+          if (mn && mn[q]) mn[q][e] = lo;
+          if (mx && mx[q]) mx[q][e] = hi;
+          if (clip) d = SFX(rmax)(lo, SFX(rmin)(hi, d));
+          dsts[q][e] = d;
+        }
+      }
+  }
+}
+
 #undef EXT
 #undef ARR
 #undef WP

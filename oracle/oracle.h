@@ -78,6 +78,10 @@ typedef struct {
   double *cy;                  /* index j - lminy */
   orc_ztab *ztab_m, *ztab_t;
   void *ref_m, *ref_t;         /* reference ztab objects (reference-linked build only) */
+  /* BICUBH_QV denominators on thermo levels, 10 per level k (slot k*10 + q):
+   * q 0..3 cubic Adz_zabcd/zbacd/zcabd/zdabc_8%t (k = 2..nk-2),
+   * q 4..9 quintic Adz_zxabcde..zexabcd_8%t (k = 3..nk-3), adz_set.F90:286-311 */
+  double *qv_t;
 } orc_set;
 
 int orc_adz_set(const orc_grid *g, orc_set *s);
@@ -129,6 +133,16 @@ void orc_interp_traj_f64(const orc_set *s, double dt, const double *wpxyz, const
 void orc_tricub_f64(const orc_set *s, int set, const double *pos, int m, const double *const *srcs,
                     double *const *dsts, int mono, int clip, double *const *lin, double *const *mn,
                     double *const *mx);
+
+/* BICUBH_QV (bicubHQV_lin_mono.F90:20-172 with bicubHQV_lin_min_max_zyx.F90):
+ * bicubic horizontal, quintic vertical (cubic at levels 2 and nk-2, linear
+ * at the ends) on thermo levels, at position set t; lin/min/max over the
+ * inner 2x2x2 box.  Arguments as orc_tricub_* (always computes lin/min/max;
+ * they may be NULL). */
+void orc_tricub_qv_f32(const orc_set *s, const float *pos, int m, const float *const *srcs, float *const *dsts,
+                       int clip, float *const *lin, float *const *mn, float *const *mx);
+void orc_tricub_qv_f64(const orc_set *s, const double *pos, int m, const double *const *srcs, double *const *dsts,
+                       int clip, double *const *lin, double *const *mn, double *const *mx);
 
 /* number of points of a position set (0=q/pm, 1=u, 2=v, 3=t) */
 long orc_set_npoints(const orc_set *s, int set);

@@ -58,7 +58,7 @@ class OrcSet(C.Structure):
         ("vw5", C.c_double), ("vw6", C.c_double), ("ww", C.c_double), ("wp", C.c_double),
         ("wm", C.c_double), ("cy", C.POINTER(C.c_double)),
         ("ztab_m", C.POINTER(OrcZtab)), ("ztab_t", C.POINTER(OrcZtab)),
-        ("ref_m", C.c_void_p), ("ref_t", C.c_void_p)]
+        ("ref_m", C.c_void_p), ("ref_t", C.c_void_p), ("qv_t", C.c_void_p)]
 
 
 def build(ref: bool | None = None) -> None:
@@ -106,6 +106,8 @@ class _Lib:
             getattr(L, f"orc_interp_traj_{sfx}").argtypes = [C.POINTER(OrcSet), C.c_double] + [vp] * 10
             getattr(L, f"orc_tricub_{sfx}").argtypes = [C.POINTER(OrcSet), C.c_int, vp, C.c_int, vp, vp,
                                                         C.c_int, C.c_int, vp, vp, vp]
+            getattr(L, f"orc_tricub_qv_{sfx}").argtypes = [C.POINTER(OrcSet), vp, C.c_int, vp, vp, C.c_int,
+                                                           vp, vp, vp]
 
 
 _LIBS: dict[str, _Lib] = {}
@@ -355,6 +357,23 @@ class Step:
             C.cast(dp, C.c_void_p), int(mono), int(clip), lp, mnp, mxp)
         if post:
             return dsts, (lin, mn, mx)
+        return dsts
+
+    def tricub_qv(self, srcs, clip=False, post=False):
+        """adz_tricub_hlt with BICUBH_QV at position set t (bicubHQV_lin_mono.F90);
+        returns the destinations (ext layout, range written, NaN elsewhere) and,
+        if post, (lin, min, max)."""
+        m = len(srcs)
+        srcs = [np.ascontiguousarray(x, dtype=self.dt) for x in srcs]
+        dsts = [np.full(self.ext_shape, np.nan, self.dt) for _ in range(m)]
+        ct = C.c_float if self.prec == "f32" else C.c_double
+        extra = [[np.full(self.ext_shape, np.nan, self.dt) for _ in range(m)] for _ in range(3)]
+        ptr = [C.cast(_ptrs(z, ct), C.c_void_p) for z in extra]
+        getattr(self.L, f"orc_tricub_qv_{self.prec}")(
+            C.byref(self.s), self.sets[3].ctypes.data, m, C.cast(_ptrs(srcs, ct), C.c_void_p),
+            C.cast(_ptrs(dsts, ct), C.c_void_p), int(clip), *ptr)
+        if post:
+            return dsts, tuple(extra)
         return dsts
 
     def step(self, inp, niter=None):
