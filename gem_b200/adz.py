@@ -63,6 +63,13 @@ class AdzcDomain(C.Structure):
                 ("nfields", C.c_int * 4), ("srcs", C.c_void_p), ("dsts", C.c_void_p), ("mono", C.c_void_p)]
 
 
+class AdzcBcTracer(C.Structure):
+    """adzc_bc_tracer: one tracer of a Bermejo-Conde call (include/adz_b200.h)."""
+    _fields_ = [("p", C.c_void_p), ("m", C.c_void_p), ("lin", C.c_void_p), ("min", C.c_void_p),
+                ("max", C.c_void_p), ("fo", C.c_void_p), ("fi", C.c_void_p), ("pkps", C.c_void_p),
+                ("weight", C.c_int), ("p_exp", C.c_double)]
+
+
 class PxPyPz(C.Structure):
     _fields_ = [("px", C.c_float), ("py", C.c_float), ("pz", C.c_float)]
 
@@ -98,6 +105,7 @@ def lib() -> C.CDLL:
         L.adzc_batch_query.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
         L.adzc_batch_status.argtypes = [vp, i, vp]
         L.adzc_batch_destroy.argtypes = [vp]
+        L.adzc_bermejo_conde.argtypes = [vp, i, i, vp, vp, vp, vp, i, vp, vp, vp]
         L.adzc_error_string.restype = C.c_char_p
         L.Vsearch_setup.restype = vp
         L.Vsearch_setup.argtypes = [vp, i, i, i]
@@ -358,3 +366,22 @@ class Batch:
             lib().adzc_batch_destroy(self.h)
         except Exception:
             pass
+
+
+def bermejo_conde(adz: Adz, prec: int, tracers, airm_p, airm_m, mask, deficit, min_max=True, diag=None,
+                  stream=None):
+    """Bermejo-Conde mass fixer (adzc_bermejo_conde) on a group of tracers.
+    tracers: dicts with p, m (fixed in place), lin, min, max and optionally fo,
+    fi, pkps, weight (1), p_exp (1.0); deficit: device float64 (ntr,)."""
+    arr = (AdzcBcTracer * len(tracers))()
+    ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+    for q, t in enumerate(tracers):
+        a = arr[q]
+        a.p, a.m, a.lin = ptr(t["p"]), ptr(t["m"]), ptr(t["lin"])
+        a.min, a.max = ptr(t.get("min")), ptr(t.get("max"))
+        a.fo, a.fi, a.pkps = ptr(t.get("fo")), ptr(t.get("fi")), ptr(t.get("pkps"))
+        a.weight, a.p_exp = int(t.get("weight", 1)), float(t.get("p_exp", 1.0))
+    _check(lib().adzc_bermejo_conde(adz.h, prec, len(tracers), C.cast(arr, C.c_void_p), airm_p.data_ptr(),
+                                    airm_m.data_ptr(), mask.data_ptr(), int(min_max), deficit.data_ptr(),
+                                    None if diag is None else diag.data_ptr(), _stream(stream)),
+           "adzc_bermejo_conde")

@@ -291,6 +291,8 @@ struct adzc_handle {
   void* d_uvw = nullptr;
   size_t uvw_bytes = 0;
   void* d_wdep = nullptr;
+  void* d_aux = nullptr;  // mass-fixer scratch
+  size_t aux_bytes = 0;
   size_t wdep_bytes = 0;
   // last trajectory, read by adzc_tricub
   int last_prec = -1;
@@ -527,6 +529,7 @@ extern "C" int adzc_destroy(adzc_handle* h) {
   cudaFree(h->d_tables);
   cudaFree(h->d_uvw);
   cudaFree(h->d_wdep);
+  cudaFree(h->d_aux);
   delete h;
   return ADZC_OK;
 }
@@ -931,5 +934,12 @@ int adz_internal_scratch(adzc_handle* h, int prec, void** uvw, void** wdep) {
     return ADZC_ERR_ALLOC;
   *uvw = h->d_uvw;
   *wdep = h->d_wdep;
+  return ADZC_OK;
+}
+
+int adz_internal_aux(adzc_handle* h, size_t bytes, void** p) {
+  if (!h || !p) return ADZC_ERR_ARG;
+  if (ensure(&h->d_aux, &h->aux_bytes, bytes) != ADZC_OK) return ADZC_ERR_ALLOC;
+  *p = h->d_aux;
   return ADZC_OK;
 }

@@ -1,6 +1,7 @@
 // Internal accessors between the host C-ABI translation units (not part of
 // the public ABI).
 #pragma once
+#include <cstddef>
 #include "../../include/adz_b200.h"
 #include "adz_types.h"
 
@@ -17,3 +18,5 @@ void adz_internal_record_positions(adzc_handle* h, int prec, double* wpxyz, cons
 int adz_internal_fail(int status);
 // the handle's departure-wind and departure-w scratch for a precision (allocated on first use)
 int adz_internal_scratch(adzc_handle* h, int prec, void** uvw, void** wdep);
+// a handle-owned device buffer of at least bytes for auxiliary passes (mass fixers)
+int adz_internal_aux(adzc_handle* h, size_t bytes, void** p);

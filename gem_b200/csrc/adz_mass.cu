@@ -1,0 +1,334 @@
+// Bermejo-Conde mass fixer (B/Bermejo_Conde.F90:16-251, B/mass_tr_PM.F90,
+// B/mass_tr_X.F90, driven as B/adz_post_tr.F90:140-236 does) for a group of
+// tracers, device-resident from start to end: no host synchronisation, the
+// per-tracer scalars (masses, deficit, lambda, proportion) live in device
+// memory between the launches.
+//
+// Every mass is an FP64 sum of (field * air mass) * area mask over the core
+// region, the first product in the field type as the reference forms it.
+// Sums are deterministic: each block reduces a fixed slice in a fixed tree
+// order, then one thread per tracer adds the block partials in index order.
+// The order differs from the reference's sequential loop, so masses agree to
+// rounding (about 1e-15 relative), not bit for bit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/adz_b200.h"
+#include "adz_internal.h"
+#include "adz_types.h"
+
+namespace adz {
+namespace mass {
+
+constexpr int kBlocks = 256;   // blocks per tracer in a reduction
+constexpr int kThreads = 256;
+
+template <typename T>
+struct Tr {
+  const T* p;
+  T* m;
+  const T* lin;
+  const T* mn;
+  const T* mx;
+  const T* fo;
+  const T* fi;
+  const T* pkps;
+  int weight;
+  double p_exp;
+};
+
+struct State {
+  double mass_p, mass_m, fo, fi, tot_p, def, wei, lambda, bc_r, prop, bc;
+  int skip;
+};
+
+struct Region {
+  int i0, nx, j0, ny, k0, nz;
+  __host__ __device__ long long n() const { return (long long)nx * ny * nz; }
+};
+
+struct Geo {
+  int lminx, lminy, nit, ni;
+  long long nij;
+  const double* mask;  // (ni, nj)
+};
+
+__device__ __forceinline__ void point(const Region& r, long long t, int& i, int& j, int& k) {
+  i = r.i0 + (int)(t % r.nx);
+  j = r.j0 + (int)((t / r.nx) % r.ny);
+  k = r.k0 + (int)(t / ((long long)r.nx * r.ny));
+}
+
+__device__ __forceinline__ long long ext(const Geo& g, int i, int j, int k) {
+  return (long long)(i - g.lminx) + (long long)(j - g.lminy) * g.nit + (long long)(k - 1) * g.nij;
+}
+
+__device__ __forceinline__ double sign1(double x) { return signbit(x) ? -1.0 : 1.0; }
+
+// weight of Bermejo_Conde.F90:87-137 (stored as T by the reference)
+template <typename T>
+__device__ __forceinline__ T bc_weight(const Tr<T>& tr, long long e, double sd) {
+  const T hmlt = tr.m[e] - tr.lin[e];
+  const double hml = (double)hmlt;
+  if ((int)sd != (int)sign1(hml)) return (T)0;
+  const double a = fabs(hml);
+  const double pw = (tr.p_exp == 1.0) ? a : pow(a, tr.p_exp);
+  if (tr.weight == 1) return (T)(pw * sd);
+  if (tr.weight == 2) return (T)(pw * sd * (double)(tr.m[e] > (T)0 ? tr.m[e] : (T)0));
+  return (T)(pw * sd * (double)tr.pkps[e]);
+}
+
+enum Mode { kPM = 0, kFlux = 1, kWei = 2, kM = 3 };
+
+// block partial sums of one or two masses; blockIdx.y = tracer
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kThreads) k_reduce(const Tr<T>* __restrict__ trs, const State* __restrict__ st,
+                                                     Region r, Geo g, const T* __restrict__ air_p,
+                                                     const T* __restrict__ air_m, double* __restrict__ part) {
+  const int q = blockIdx.y;
+  const Tr<T> tr = trs[q];
+  const long long n = r.n();
+  const long long chunk = (n + kBlocks - 1) / kBlocks;
+  const long long b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+  double s0 = 0.0, s1 = 0.0;
+  const bool skip = (MODE == kM || MODE == kWei) && st[q].skip;
+  const double sd = MODE == kWei ? sign1(st[q].def) : 1.0;
+  if (!skip && !(MODE == kFlux && (!tr.fo || !tr.fi))) {
+    for (long long t = b0 + threadIdx.x; t < b1; t += kThreads) {
+      int i, j, k;
+      point(r, t, i, j, k);
+      const long long e = ext(g, i, j, k);
+      const double mk = __ldg(g.mask + (i - 1) + (long long)(j - 1) * g.ni);
+      if (MODE == kPM) {
+        const T a = tr.p[e] * air_p[e];
+        const T b = tr.m[e] * air_m[e];
+        s0 += (double)a * mk;
+        s1 += (double)b * mk;
+      } else if (MODE == kFlux) {
+        const T a = tr.fo[e] * air_m[e];
+        const T b = tr.fi[e] * air_m[e];
+        s0 += (double)a * mk;
+        s1 += (double)b * mk;
+      } else if (MODE == kWei) {
+        const T a = bc_weight<T>(tr, e, sd) * air_m[e];
+        s0 += (double)a * mk;
+      } else {
+        const T a = tr.m[e] * air_m[e];
+        s0 += (double)a * mk;
+      }
+    }
+  }
+  __shared__ double red[2][kThreads];
+  red[0][threadIdx.x] = s0;
+  red[1][threadIdx.x] = s1;
+  __syncthreads();
+  for (int o = kThreads / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + o];
+      red[1][threadIdx.x] += red[1][threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[((long long)q * kBlocks + blockIdx.x) * 2 + 0] = red[0][0];
+    part[((long long)q * kBlocks + blockIdx.x) * 2 + 1] = red[1][0];
+  }
+}
+
+// almost_zero (modelutils almost_zero.F90:16-36), bit for bit
+__device__ __forceinline__ bool almost_zero(double a) {
+  long long bits = __double_as_longlong(a);
+  if (bits < 0) bits = (long long)(0x80000000ULL - (unsigned long long)bits);
+  return bits >= -1 && bits <= 1;
+}
+
+enum Stage { kAfterPM = 0, kAfterFlux = 1, kAfterWei = 2, kAfterBcR = 3, kAfterBc = 4 };
+
+// one thread per tracer: partials in index order, then the scalar formulas
+template <int STAGE>
+__global__ void k_finish(const double* __restrict__ part, State* __restrict__ st, int ntr,
+                         double* __restrict__ deficit, double* __restrict__ diag) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= ntr) return;
+  double s0 = 0.0, s1 = 0.0;
+  for (int b = 0; b < kBlocks; b++) {
+    s0 += part[((long long)q * kBlocks + b) * 2 + 0];
+    s1 += part[((long long)q * kBlocks + b) * 2 + 1];
+  }
+  State& S = st[q];
+  if (STAGE == kAfterPM) {
+    S = State{};
+    S.mass_p = s0;
+    S.mass_m = s1;
+  } else if (STAGE == kAfterFlux) {
+    S.fo = s0;
+    S.fi = s1;
+  } else if (STAGE == kAfterWei) {
+    S.wei = s0;
+    S.skip = almost_zero(s0) ? 1 : 0;
+    S.lambda = S.skip ? 0.0 : S.def / s0;
+  } else if (STAGE == kAfterBcR) {
+    if (!S.skip) {
+      S.bc_r = s0;
+      S.prop = S.tot_p / s0;
+    }
+  } else {
+    if (!S.skip) {
+      S.bc = s0;
+      deficit[q] = s0 - S.tot_p;  // Bermejo_Conde.F90:225-243
+    }
+    if (diag) {
+      double* d = diag + 8 * q;
+      d[0] = S.mass_p; d[1] = S.mass_m; d[2] = S.fo; d[3] = S.fi;
+      d[4] = S.wei; d[5] = S.lambda; d[6] = S.bc_r; d[7] = S.bc;
+    }
+  }
+  if (STAGE == kAfterFlux) {  // Bermejo_Conde.F90:70-84 (the flux stage always runs, sums 0 without fluxes)
+    const double bflux = S.fi - S.fo;
+    const double mp = S.mass_p - deficit[q];
+    S.tot_p = mp + bflux;
+    S.def = S.mass_m - S.tot_p;
+  }
+}
+
+// m - lambda w, clipped to the bound box when min_max (Bermejo_Conde.F90:163-199)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_correct(const Tr<T>* __restrict__ trs, const State* __restrict__ st,
+                                                      Region r, Geo g, int min_max) {
+  const int q = blockIdx.y;
+  if (st[q].skip) return;
+  const Tr<T> tr = trs[q];
+  const double lambda = st[q].lambda, sd = sign1(st[q].def);
+  const long long n = r.n();
+  for (long long t = blockIdx.x * (long long)kThreads + threadIdx.x; t < n; t += (long long)gridDim.x * kThreads) {
+    int i, j, k;
+    point(r, t, i, j, k);
+    const long long e = ext(g, i, j, k);
+    const double corr = lambda * (double)bc_weight<T>(tr, e, sd);
+    if (!min_max) {
+      tr.m[e] = (T)((double)tr.m[e] - corr);
+    } else {
+      const T wrk = (T)((double)tr.m[e] - corr);
+      T v = wrk;
+      if (corr > 0.0 && wrk < tr.mn[e]) v = tr.mn[e];
+      if (corr < 0.0 && wrk > tr.mx[e]) v = tr.mx[e];
+      tr.m[e] = v;
+    }
+  }
+}
+
+// proportional rescale after the clipped correction (Bermejo_Conde.F90:203-222)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_scale(const Tr<T>* __restrict__ trs, const State* __restrict__ st,
+                                                    Region r, Geo g) {
+  const int q = blockIdx.y;
+  if (st[q].skip) return;
+  T* m = trs[q].m;
+  const double prop = st[q].prop;
+  const long long n = r.n();
+  for (long long t = blockIdx.x * (long long)kThreads + threadIdx.x; t < n; t += (long long)gridDim.x * kThreads) {
+    int i, j, k;
+    point(r, t, i, j, k);
+    const long long e = ext(g, i, j, k);
+    m[e] = (T)(prop * (double)m[e]);
+  }
+}
+
+}  // namespace mass
+}  // namespace adz
+
+namespace {
+
+using namespace adz::mass;
+
+template <typename T>
+int run_bc(int ntr, const adzc_bc_tracer* in, const void* airm_p, const void* airm_m, const double* mask,
+           int min_max, double* deficit, double* diag, const Region& core, const Region& brange, const Geo& g,
+           void* scratch, cudaStream_t s) {
+  // scratch: tracer descriptors | states | partials
+  Tr<T>* d_tr = (Tr<T>*)scratch;
+  State* d_st = (State*)((char*)scratch + ((ntr * sizeof(Tr<T>) + 255) & ~size_t(255)));
+  double* d_part =
+      (double*)((char*)d_st + ((ntr * sizeof(State) + 255) & ~size_t(255)));
+  std::vector<Tr<T>> h(ntr);
+  for (int q = 0; q < ntr; q++) {
+    h[q].p = (const T*)in[q].p;
+    h[q].m = (T*)in[q].m;
+    h[q].lin = (const T*)in[q].lin;
+    h[q].mn = (const T*)in[q].min;
+    h[q].mx = (const T*)in[q].max;
+    h[q].fo = (const T*)in[q].fo;
+    h[q].fi = (const T*)in[q].fi;
+    h[q].pkps = (const T*)in[q].pkps;
+    h[q].weight = in[q].weight;
+    h[q].p_exp = in[q].p_exp;
+  }
+  if (cudaMemcpyAsync(d_tr, h.data(), ntr * sizeof(Tr<T>), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return ADZC_ERR_CUDA;
+  const dim3 rg(kBlocks, ntr);
+  const T* ap = (const T*)airm_p;
+  const T* am = (const T*)airm_m;
+  const int fb = (ntr + 127) / 128;
+  const long long n = core.n();
+  const dim3 eg((unsigned)std::max<long long>(1, std::min<long long>((n + kThreads - 1) / kThreads, 1024)), ntr);
+  Geo gm = g;
+  gm.mask = mask;
+  k_reduce<T, kPM><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, ap, am, d_part);
+  k_finish<kAfterPM><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
+  k_reduce<T, kFlux><<<rg, kThreads, 0, s>>>(d_tr, d_st, brange, gm, ap, am, d_part);
+  k_finish<kAfterFlux><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
+  k_reduce<T, kWei><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, ap, am, d_part);
+  k_finish<kAfterWei><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
+  k_correct<T><<<eg, kThreads, 0, s>>>(d_tr, d_st, core, gm, min_max);
+  if (min_max) {
+    k_reduce<T, kM><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, ap, am, d_part);
+    k_finish<kAfterBcR><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
+    k_scale<T><<<eg, kThreads, 0, s>>>(d_tr, d_st, core, gm);
+  }
+  k_reduce<T, kM><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, ap, am, d_part);
+  k_finish<kAfterBc><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
+  return cudaGetLastError() == cudaSuccess ? ADZC_OK : ADZC_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" int adzc_bermejo_conde(adzc_handle* h, int prec, int ntr, const adzc_bc_tracer* tracers,
+                                  const void* airm_p, const void* airm_m, const double* mask, int min_max,
+                                  double* deficit, double* diag, void* stream) {
+  adz::DGrid D;
+  adzc_info I;
+  adzc_grid G;
+  int niter = 0, cold = 0;
+  if (!h || (prec != ADZC_REF32 && prec != ADZC_MIXED && prec != ADZC_FP64) || ntr < 1 || !tracers || !airm_p ||
+      !airm_m || !mask || !deficit || adz_internal_view(h, &D, &I, &G, &niter, &cold) != ADZC_OK)
+    return adz_internal_fail(ADZC_ERR_ARG);
+  for (int q = 0; q < ntr; q++) {
+    const adzc_bc_tracer& t = tracers[q];
+    if (!t.p || !t.m || !t.lin || (min_max && (!t.min || !t.max)) || t.weight < 1 || t.weight > 3 ||
+        (t.weight == 3 && !t.pkps) || (!t.fo) != (!t.fi) || !std::isfinite(t.p_exp))
+      return adz_internal_fail(ADZC_ERR_ARG);
+  }
+  // core region (B/adz_post_tr.F90:146-152) and the LAM flux range (b set, all levels)
+  Region core{1 + (G.west ? G.pil_w : 0), 0, 1 + (G.south ? G.pil_s : 0), 0, I.k0t, 0};
+  core.nx = D.ni - (G.east ? G.pil_e : 0) - core.i0 + 1;
+  core.ny = D.nj - (G.north ? G.pil_n : 0) - core.j0 + 1;
+  core.nz = D.nk - I.k0t + 1;
+  Region br{I.i0b, I.inb - I.i0b + 1, I.j0b, I.jnb - I.j0b + 1, 1, D.nk};
+  if (core.nx <= 0 || core.ny <= 0 || core.nz <= 0) return adz_internal_fail(ADZC_ERR_ARG);
+  Geo g{D.lminx, D.lminy, D.nit, D.ni, D.nij, mask};
+  const size_t ts = prec == ADZC_FP64 ? sizeof(Tr<double>) : sizeof(Tr<float>);
+  const size_t bytes = ((ntr * ts + 255) & ~size_t(255)) + ((ntr * sizeof(State) + 255) & ~size_t(255)) +
+                       (size_t)ntr * kBlocks * 2 * sizeof(double);
+  void* scratch = nullptr;
+  if (adz_internal_aux(h, bytes, &scratch) != ADZC_OK) return adz_internal_fail(ADZC_ERR_ALLOC);
+  const int st = prec == ADZC_FP64 ? run_bc<double>(ntr, tracers, airm_p, airm_m, mask, min_max, deficit, diag, core,
+                                                     br, g, scratch, (cudaStream_t)stream)
+                                   : run_bc<float>(ntr, tracers, airm_p, airm_m, mask, min_max, deficit, diag, core,
+                                                   br, g, scratch, (cudaStream_t)stream);
+  return st == ADZC_OK ? ADZC_OK : adz_internal_fail(st);
+}

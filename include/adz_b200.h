@@ -293,6 +293,34 @@ int adzc_mlp_adam(adzc_mlp *t, float lr, void *stream);
  * last adzc_mlp_grad (1 float); synchronises the stream */
 int adzc_mlp_read(adzc_mlp *t, int what, float *host_out, void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* Bermejo-Conde mass fixer                                                   */
+/* ------------------------------------------------------------------------ */
+/* After the interpolation of mass-conserving tracers (B/adz_post_tr.F90:140-236,
+ * B/Bermejo_Conde.F90:16-251, B/mass_tr_PM.F90, B/mass_tr_X.F90): restores
+ * each tracer's air-mass-weighted total over the core region (the tile minus
+ * its pilot zones, levels k0t..nk) to its value before advection, plus the
+ * LAM boundary flux when given, by adding lambda * w where the high-order
+ * value departs from the low-order one.  All arrays are DEVICE arrays in the
+ * ext layout of the handle, of the precision's field type (double for
+ * ADZC_FP64, float otherwise); mask is the (ni, nj) FP64 area mask
+ * (geomh_mask_8).  deficit: DEVICE array of ntr epsilons carried between
+ * steps (in: previous step, out: this step; start at 0).  diag: NULL or
+ * DEVICE ntr x 8 doubles receiving mass_p, mass_m, mass_fo, mass_fi,
+ * mass_wei, lambda, mass_bc_r, mass_bc.  Nothing synchronises the stream. */
+typedef struct {
+  const void *p;              /* tracer before advection (time P)                 */
+  void *m;                    /* tracer after advection (time M), fixed in place  */
+  const void *lin, *min, *max;/* Adz_post of m: adzc_tricub post arrays           */
+  const void *fo, *fi;        /* NULL, or LAM flux out / in (Adz_BC_LAM_flux 1)   */
+  const void *pkps;           /* weight 3 only                                    */
+  int weight;                 /* 1 additive, 2 multiplicative, 3 additive * pkps  */
+  double p_exp;               /* exponent of |high - low| (adz_BC_pexp_list)      */
+} adzc_bc_tracer;
+int adzc_bermejo_conde(adzc_handle *h, int prec, int ntr, const adzc_bc_tracer *tracers, const void *airm_p,
+                       const void *airm_m, const double *mask, int min_max, double *deficit, double *diag,
+                       void *stream);
+
 /* One whole advection step that allocates no device memory.  No counterpart
  * in the reference (its Fortran drivers use automatic arrays).
  *

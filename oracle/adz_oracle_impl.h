@@ -504,6 +504,119 @@ void SFX(orc_tricub_qv)(const orc_set *s, const REAL *pos, int m, const REAL *co
   }
 }
 
+/* almost_zero (modelutils almost_zero.F90:16-36), bit for bit, including its
+ * 32-bit constant for negative values */
+static int SFX(almost_zero)(double a) {
+  long long bits;
+  memcpy(&bits, &a, 8);
+  if (bits < 0) bits = (long long)((unsigned long long)0x80000000ULL - (unsigned long long)bits);
+  return bits >= -1 && bits <= 1;
+}
+
+static double SFX(fsign1)(double x) { return signbit(x) ? -1.0 : 1.0; } /* sign(ONE_8, x) */
+
+/* sum over the core region of t * air * mask, the product t * air in REAL */
+static double SFX(bc_mass)(const orc_set *s, const REAL *t, const REAL *air, const double *mask, int i0, int in,
+                           int j0, int jn, int k0, int k1) {
+  const int ni = s->g.ni;
+  double c = 0.0;
+  for (int k = k0; k <= k1; k++)
+    for (int j = j0; j <= jn; j++)
+      for (int i = i0; i <= in; i++) {
+        const long e = EXT(i, j, k);
+        const REAL ta = t[e] * air[e];
+        c = c + ta * mask[(i - 1) + (long)(j - 1) * ni];
+      }
+  return c;
+}
+
+void SFX(orc_bermejo_conde)(const orc_set *s, const REAL *p, REAL *m, const REAL *lin, const REAL *mn,
+                            const REAL *mx, const REAL *fo, const REAL *fi, const REAL *pkps, int weight,
+                            double p_exp, int min_max, const REAL *airm_p, const REAL *airm_m, const double *mask,
+                            double *deficit, double *diag) {
+  const orc_grid *g = &s->g;
+  const int nk = g->nk;
+  /* adz_post_tr.F90:146-152: core limits */
+  const int i0 = 1 + (g->west ? g->pil_w : 0), in = g->ni - (g->east ? g->pil_e : 0);
+  const int j0 = 1 + (g->south ? g->pil_s : 0), jn = g->nj - (g->north ? g->pil_n : 0);
+  const int k0 = s->k0t;
+  /* mass_tr_PM */
+  double mass_p = SFX(bc_mass)(s, p, airm_p, mask, i0, in, j0, jn, k0, nk);
+  const double mass_m = SFX(bc_mass)(s, m, airm_m, mask, i0, in, j0, jn, k0, nk);
+  double mass_fo = 0.0, mass_fi = 0.0;
+  if (fo && fi) {
+    mass_fo = SFX(bc_mass)(s, fo, airm_m, mask, s->i0b, s->inb, s->j0b, s->jnb, 1, nk);
+    mass_fi = SFX(bc_mass)(s, fi, airm_m, mask, s->i0b, s->inb, s->j0b, s->jnb, 1, nk);
+  }
+  if (diag) { diag[0] = mass_p; diag[1] = mass_m; diag[2] = mass_fo; diag[3] = mass_fi; }
+  /* Bermejo_Conde.F90:70-84 */
+  const double mass_bflux = mass_fi - mass_fo;
+  mass_p = mass_p - *deficit;
+  const double mass_tot_p = mass_p + mass_bflux, mass_tot_m = mass_m;
+  double def = mass_tot_m - mass_tot_p;
+  const double sd = SFX(fsign1)(def);
+  const int ni = g->ni, nj = g->nj;
+  /* weights (Bermejo_Conde.F90:87-137), REAL storage; mass_tr_X kind 1 */
+  REAL *w = (REAL *)calloc((size_t)s->nit * s->njt * nk, sizeof(REAL));
+  for (int k = k0; k <= nk; k++)
+    for (int j = j0; j <= jn; j++)
+      for (int i = i0; i <= in; i++) {
+        const long e = EXT(i, j, k);
+        const double hml = (double)(REAL)(m[e] - lin[e]);
+        REAL wv = 0;
+        if ((int)sd == (int)SFX(fsign1)(hml)) {
+          const double a = fabs(hml);
+          const double pw = (p_exp == 1.0) ? a : pow(a, p_exp);
+          if (weight == 1) wv = (REAL)(pw * sd);
+          else if (weight == 2) wv = (REAL)(pw * sd * (double)(m[e] > (REAL)0 ? m[e] : (REAL)0));
+          else wv = (REAL)(pw * sd * (double)pkps[e]);
+        }
+        w[e] = wv;
+      }
+  const double mass_wei = SFX(bc_mass)(s, w, airm_m, mask, i0, in, j0, jn, k0, nk);
+  if (diag) diag[4] = mass_wei;
+  (void)nj;
+  if (SFX(almost_zero)(mass_wei)) { /* Bermejo_Conde.F90:150-158: tracer left as it is */
+    if (diag) { diag[5] = 0.0; diag[6] = 0.0; diag[7] = 0.0; }
+    free(w);
+    return;
+  }
+  const double lambda = def / mass_wei;
+  if (diag) diag[5] = lambda;
+  for (int k = k0; k <= nk; k++)
+    for (int j = j0; j <= jn; j++)
+      for (int i = i0; i <= in; i++) {
+        const long e = EXT(i, j, k);
+        const double corr = lambda * (double)w[e];
+        if (!min_max) {
+          m[e] = (REAL)((double)m[e] - corr);
+        } else {
+          const REAL wrk = (REAL)((double)m[e] - corr);
+          m[e] = wrk;
+          if (corr > 0.0 && wrk < mn[e]) m[e] = mn[e];
+          if (corr < 0.0 && wrk > mx[e]) m[e] = mx[e];
+        }
+      }
+  free(w);
+  if (min_max) { /* Bermejo_Conde.F90:203-222 */
+    const double mass_bc_r = SFX(bc_mass)(s, m, airm_m, mask, i0, in, j0, jn, k0, nk);
+    if (diag) diag[6] = mass_bc_r;
+    const double prop = mass_tot_p / mass_bc_r;
+    for (int k = k0; k <= nk; k++)
+      for (int j = j0; j <= jn; j++)
+        for (int i = i0; i <= in; i++) {
+          const long e = EXT(i, j, k);
+          m[e] = (REAL)(prop * (double)m[e]);
+        }
+  } else if (diag) {
+    diag[6] = 0.0;
+  }
+  /* Bermejo_Conde.F90:225-243: epsilon for the next step */
+  const double mass_bc = SFX(bc_mass)(s, m, airm_m, mask, i0, in, j0, jn, k0, nk);
+  if (diag) diag[7] = mass_bc;
+  *deficit = mass_bc - mass_tot_p;
+}
+
 #undef EXT
 #undef ARR
 #undef WP

@@ -144,6 +144,24 @@ void orc_tricub_qv_f32(const orc_set *s, const float *pos, int m, const float *c
 void orc_tricub_qv_f64(const orc_set *s, const double *pos, int m, const double *const *srcs, double *const *dsts,
                        int clip, double *const *lin, double *const *mn, double *const *mx);
 
+/* Bermejo-Conde mass fixer for one tracer (Bermejo_Conde.F90:16-251 with
+ * mass_tr_PM.F90 and mass_tr_X.F90), single domain (the MPI_Allgather sums
+ * of one rank).  Arrays in the ext layout; mask (ni, nj) is geomh_mask_8.
+ * Core region: 1+pil_w..ni-pil_e, 1+pil_s..nj-pil_n (pilots of edge tiles),
+ * levels k0t..nk.  fo/fi (may be NULL): LAM flux masses over the b range,
+ * levels 1..nk.  weight 1/2/3, p_exp, min_max as adz_BC_weight,
+ * adz_BC_pexp_list(n), adz_BC_min_max_L.  *deficit: in the previous step's
+ * epsilon, out this step's.  diag[8] (may be NULL): mass_p, mass_m, mass_fo,
+ * mass_fi, mass_wei, lambda, mass_bc_r, mass_bc. */
+void orc_bermejo_conde_f32(const orc_set *s, const float *p, float *m, const float *lin, const float *mn,
+                           const float *mx, const float *fo, const float *fi, const float *pkps, int weight,
+                           double p_exp, int min_max, const float *airm_p, const float *airm_m, const double *mask,
+                           double *deficit, double *diag);
+void orc_bermejo_conde_f64(const orc_set *s, const double *p, double *m, const double *lin, const double *mn,
+                           const double *mx, const double *fo, const double *fi, const double *pkps, int weight,
+                           double p_exp, int min_max, const double *airm_p, const double *airm_m,
+                           const double *mask, double *deficit, double *diag);
+
 /* number of points of a position set (0=q/pm, 1=u, 2=v, 3=t) */
 long orc_set_npoints(const orc_set *s, int set);
 

@@ -108,6 +108,8 @@ class _Lib:
                                                         C.c_int, C.c_int, vp, vp, vp]
             getattr(L, f"orc_tricub_qv_{sfx}").argtypes = [C.POINTER(OrcSet), vp, C.c_int, vp, vp, C.c_int,
                                                            vp, vp, vp]
+            getattr(L, f"orc_bermejo_conde_{sfx}").argtypes = [C.POINTER(OrcSet)] + [vp] * 8 + [
+                C.c_int, C.c_double, C.c_int, vp, vp, vp, vp, vp]
 
 
 _LIBS: dict[str, _Lib] = {}
@@ -375,6 +377,23 @@ class Step:
         if post:
             return dsts, tuple(extra)
         return dsts
+
+    def bermejo_conde(self, p, m, lin, mn, mx, airm_p, airm_m, mask, deficit=0.0, weight=1, p_exp=1.0,
+                      min_max=True, fo=None, fi=None, pkps=None):
+        """Bermejo-Conde on one tracer (ext arrays of the Step's precision);
+        returns (fixed m, new deficit, diag[8])."""
+        A = lambda x: None if x is None else np.ascontiguousarray(x, dtype=self.dt)  # noqa: E731
+        arrs = [A(x) for x in (p, m, lin, mn, mx, fo, fi, pkps)]
+        arrs[1] = arrs[1].copy()  # fixed in place: never the caller's array
+        am, bm = A(airm_p), A(airm_m)
+        mk = np.ascontiguousarray(mask, dtype=np.float64)
+        d = C.c_double(deficit)
+        diag = np.zeros(8, np.float64)
+        P = lambda x: None if x is None else x.ctypes.data  # noqa: E731
+        getattr(self.L, f"orc_bermejo_conde_{self.prec}")(
+            C.byref(self.s), *(P(x) for x in arrs), int(weight), float(p_exp), int(min_max), am.ctypes.data,
+            bm.ctypes.data, mk.ctypes.data, C.byref(d), diag.ctypes.data)
+        return arrs[1], d.value, diag
 
     def step(self, inp, niter=None):
         """Trajectory, then u@pmu, v@pmv, w@pt, tracers@pt (clip if cfg.mono)."""

@@ -1,0 +1,108 @@
+"""Bermejo-Conde mass fixer (adzc_bermejo_conde) against the restatement
+(oracle/adz_oracle_impl.h: orc_bermejo_conde) on the same inputs: tracers
+after a real advection step with their post arrays (mono 2), synthetic air
+masses and area mask.  Tolerances: masses and diagnostics 1e-12 relative
+(FP64 sums in another order); fixed fields within 2 units in the last place
+of the field type, plus the correction times the relative difference of the
+two lambdas (a quotient of a cancelling difference of sums: up to ~1e-12);
+the deficit carried to the next step within 1e-12 of the tracer mass.  The
+fixed total must equal the total before advection to the field type's
+rounding."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(prec_name, ntr=3):
+    from gem_b200 import adz as A, synth
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for -m gpu tests")
+    prec = A.PREC_NAMES[prec_name]
+    dt = A._field_dtype(prec)
+    cfg = synth.config_small(56, 48, 20)
+    cfg.ntracers, cfg.tracer_kind = ntr, "lognormal"
+    inp = synth.make_inputs(cfg, device="cuda", dtype=dt)
+    ad = A.Adz.from_config(cfg)
+    px, wp = ad.new_state(prec)
+    ad.adz_inittraj(prec, px, wp)
+    ad.adz_traject(prec, cfg.dt, inp, px, wp)
+    trs = inp["tracers"]
+    z = lambda: torch.zeros(ad.ext_shape, dtype=dt, device="cuda")  # noqa: E731
+    m = [z() for _ in trs]
+    post = ([z() for _ in trs], [z() for _ in trs], [z() for _ in trs])
+    ad.adz_tricub_hlt(prec, A.SET_T, trs, m, mono=[2] * len(trs), post=post)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    shp = ad.ext_shape
+    airm_p = (1.0 + 0.2 * torch.rand(shp, generator=g, device="cuda", dtype=torch.float64)).to(dt)
+    airm_m = (airm_p.double() * (1.0 + 0.01 * torch.rand(shp, generator=g, device="cuda", dtype=torch.float64))).to(dt)
+    mask = (cfg.dx ** 2 * (0.5 + torch.rand((cfg.nj, cfg.ni), generator=g, device="cuda", dtype=torch.float64)))
+    torch.cuda.synchronize()
+    return A, cfg, prec, ad, trs, m, post, airm_p, airm_m, mask
+
+
+def _np(t):
+    return t.cpu().numpy()
+
+
+def _close(a, b, before, ulps, dlam):
+    """a, b agree to ulps units in the last place of the value, plus the
+    correction m - before times the relative difference of the two lambdas
+    (a quotient of two FP64 sums, summed in different orders)."""
+    a, b = np.asarray(a), np.asarray(b)
+    eps = np.finfo(a.dtype).eps
+    tol = ulps * eps * np.maximum(np.abs(a), np.abs(b)) + (dlam + 4 * eps) * np.abs(b - before)
+    return np.all(np.abs(a - b) <= tol + np.finfo(a.dtype).tiny)
+
+
+@pytest.mark.parametrize("prec_name,weight,p_exp,min_max", [("mixed", 1, 1.0, True), ("ref32", 2, 2.0, True),
+                                                             ("fp64", 1, 1.0, False), ("mixed", 1, 1.0, False)])
+def test_bermejo_conde_vs_oracle(prec_name, weight, p_exp, min_max):
+    A, cfg, prec, ad, trs, m, post, airm_p, airm_m, mask = _case(prec_name)
+    lin, mn, mx = post
+    ntr = len(trs)
+    # tracer 0 made smooth in its last step: high and low order equal -> no correction (almost_zero)
+    m[0].copy_(lin[0])
+    src = [dict(p=trs[q], m=m[q], lin=lin[q], min=mn[q], max=mx[q], weight=weight, p_exp=p_exp) for q in range(ntr)]
+    before = [_np(t).copy() for t in m]
+    deficit = torch.tensor([0.0, 1e-3, -2e-3][:ntr], dtype=torch.float64, device="cuda")
+    d0 = _np(deficit).copy()
+    diag = torch.zeros((ntr, 8), dtype=torch.float64, device="cuda")
+    A.bermejo_conde(ad, prec, src, airm_p, airm_m, mask, deficit, min_max=min_max, diag=diag)
+    torch.cuda.synchronize()
+    st = O.Step(cfg, kind="oracle", prec="f32" if prec != A.FP64 else "f64")
+    g_diag, g_def = _np(diag), _np(deficit)
+    for q in range(ntr):
+        o_m, o_def, o_diag = st.bermejo_conde(_np(trs[q]), before[q], _np(lin[q]), _np(mn[q]), _np(mx[q]),
+                                              _np(airm_p), _np(airm_m), _np(mask), deficit=d0[q], weight=weight,
+                                              p_exp=p_exp, min_max=min_max)
+        scale = max(abs(o_diag[0]), abs(o_diag[1]))
+        masses = [0, 1, 2, 3, 4, 6, 7]
+        assert np.all(np.abs(g_diag[q][masses] - o_diag[masses]) <= 1e-12 * scale), (q, g_diag[q], o_diag)
+        assert abs(g_diag[q][5] - o_diag[5]) <= 1e-10 * abs(o_diag[5]), (q, g_diag[q][5], o_diag[5])
+        assert abs(g_def[q] - o_def) <= 1e-12 * scale
+        gm = _np(m[q])
+        bad = np.argmax(np.abs(gm - o_m))
+        dlam = abs(g_diag[q][5] - o_diag[5]) / max(abs(o_diag[5]), 1e-300)
+        assert _close(gm, o_m, before[q], 2 if p_exp == 1.0 else 4, dlam), (
+            q, np.unravel_index(bad, gm.shape), gm.flat[bad], o_m.flat[bad], before[q].flat[bad],
+            int(np.sum(gm != o_m)))
+    # tracer 0: nothing to fix, epsilon carried unchanged
+    assert np.array_equal(_np(m[0]), before[0]) and g_def[0] == d0[0]
+    # the fixed tracers hold the mass they had before advection (minus the old epsilon)
+    for q in range(1, ntr):
+        assert abs(g_diag[q][7] - (g_diag[q][0] - d0[q])) <= 1e-6 * abs(g_diag[q][0])
+
+
+def test_bermejo_conde_rejects_bad_arguments():
+    A, cfg, prec, ad, trs, m, post, airm_p, airm_m, mask = _case("mixed", ntr=1)
+    deficit = torch.zeros(1, dtype=torch.float64, device="cuda")
+    bad = [dict(p=trs[0], m=m[0], lin=post[0][0], min=post[1][0], max=post[2][0], weight=4)]
+    with pytest.raises(A.AdzError):
+        A.bermejo_conde(ad, prec, bad, airm_p, airm_m, mask, deficit)
+    bad = [dict(p=trs[0], m=m[0], lin=post[0][0], weight=1)]  # min/max needed when min_max
+    with pytest.raises(A.AdzError):
+        A.bermejo_conde(ad, prec, bad, airm_p, airm_m, mask, deficit, min_max=True)
