@@ -106,6 +106,9 @@ def lib() -> C.CDLL:
         L.adzc_batch_status.argtypes = [vp, i, vp]
         L.adzc_batch_destroy.argtypes = [vp]
         L.adzc_bermejo_conde.argtypes = [vp, i, i, vp, vp, vp, vp, i, vp, vp, vp]
+        L.adzc_cfl.argtypes = [vp, vp, vp, vp, vp]
+        L.adzc_state_save.argtypes = [vp, i, vp, vp, C.c_char_p]
+        L.adzc_state_load.argtypes = [vp, i, vp, vp, C.c_char_p]
         L.adzc_error_string.restype = C.c_char_p
         L.Vsearch_setup.restype = vp
         L.Vsearch_setup.argtypes = [vp, i, i, i]
@@ -293,6 +296,22 @@ class Adz:
                                       C.cast(_ptr_array(dsts), C.c_void_p), mono_arr, _stream(stream)),
                "adzc_tricub_sets")
 
+    def adz_cfl(self, wpxyz, stream=None):
+        """Maximum Courant numbers (horizontal, vertical, 3-D) and their global
+        (i, j, k), as adz_cfl prints them."""
+        cfl = torch.zeros(3, dtype=torch.float64, device=wpxyz.device)
+        idx = torch.zeros(9, dtype=torch.int32, device=wpxyz.device)
+        _check(lib().adzc_cfl(self.h, wpxyz.data_ptr(), cfl.data_ptr(), idx.data_ptr(), _stream(stream)), "adzc_cfl")
+        return cfl.cpu().numpy(), idx.cpu().numpy().reshape(3, 3)
+
+    def state_save(self, prec: int, pxyzm, wpxyz, path: str):
+        _check(lib().adzc_state_save(self.h, prec, None if pxyzm is None else pxyzm.data_ptr(), wpxyz.data_ptr(),
+                                     path.encode()), "adzc_state_save")
+
+    def state_load(self, prec: int, pxyzm, wpxyz, path: str):
+        _check(lib().adzc_state_load(self.h, prec, None if pxyzm is None else pxyzm.data_ptr(), wpxyz.data_ptr(),
+                                     path.encode()), "adzc_state_load")
+
     def status(self, reset=True, stream=None) -> int:
         return lib().adzc_status(self.h, 1 if reset else 0, _stream(stream))
 
@@ -357,6 +376,22 @@ class Batch:
         r, b, n = C.c_int(), C.c_int(), C.c_longlong()
         _check(lib().adzc_batch_query(self.h, C.byref(r), C.byref(b), C.byref(n)), "adzc_batch_query")
         return {"rows_per_item": r.value, "blocks_per_sm": b.value, "items": n.value}
+
+    def adz_cfl(self, wpxyz, stream=None):
+        """Maximum Courant numbers (horizontal, vertical, 3-D) and their global
+        (i, j, k), as adz_cfl prints them."""
+        cfl = torch.zeros(3, dtype=torch.float64, device=wpxyz.device)
+        idx = torch.zeros(9, dtype=torch.int32, device=wpxyz.device)
+        _check(lib().adzc_cfl(self.h, wpxyz.data_ptr(), cfl.data_ptr(), idx.data_ptr(), _stream(stream)), "adzc_cfl")
+        return cfl.cpu().numpy(), idx.cpu().numpy().reshape(3, 3)
+
+    def state_save(self, prec: int, pxyzm, wpxyz, path: str):
+        _check(lib().adzc_state_save(self.h, prec, None if pxyzm is None else pxyzm.data_ptr(), wpxyz.data_ptr(),
+                                     path.encode()), "adzc_state_save")
+
+    def state_load(self, prec: int, pxyzm, wpxyz, path: str):
+        _check(lib().adzc_state_load(self.h, prec, None if pxyzm is None else pxyzm.data_ptr(), wpxyz.data_ptr(),
+                                     path.encode()), "adzc_state_load")
 
     def status(self, reset=True, stream=None) -> int:
         return lib().adzc_batch_status(self.h, 1 if reset else 0, _stream(stream))

@@ -206,6 +206,7 @@ extern "C" const char* adzc_error_string(int st) {
     case ADZC_ERR_ALLOC: return "allocation failed";
     case ADZC_ERR_NODEVICE: return "no CUDA device";
     case ADZC_ERR_SIZE: return "size above capacity";
+    case ADZC_ERR_IO: return "file missing, unreadable or not matching";
     default: return "unknown status";
   }
 }
@@ -942,4 +943,9 @@ int adz_internal_aux(adzc_handle* h, size_t bytes, void** p) {
   if (ensure(&h->d_aux, &h->aux_bytes, bytes) != ADZC_OK) return ADZC_ERR_ALLOC;
   *p = h->d_aux;
   return ADZC_OK;
+}
+
+void adz_internal_set_iteration(adzc_handle* h, int cold, int niter) {
+  h->cold = cold ? 1 : 0;
+  h->niter = niter > 0 ? niter : std::max(1, h->g.itraj);
 }

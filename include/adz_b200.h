@@ -48,6 +48,7 @@ extern "C" {
 #define ADZC_ERR_ALLOC      7  /* device or host allocation failed              */
 #define ADZC_ERR_NODEVICE   8  /* no usable CUDA device                         */
 #define ADZC_ERR_SIZE       9  /* request larger than a fixed capacity          */
+#define ADZC_ERR_IO        10  /* file missing, unreadable or not matching      */
 
 #define ADZC_REF32 0
 #define ADZC_FP64  1
@@ -320,6 +321,25 @@ typedef struct {
 int adzc_bermejo_conde(adzc_handle *h, int prec, int ntr, const adzc_bc_tracer *tracers, const void *airm_p,
                        const void *airm_m, const double *mask, int min_max, double *deficit, double *diag,
                        void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* Diagnostics and restart state                                              */
+/* ------------------------------------------------------------------------ */
+/* adz_cfl / adz_courant (B/adz_cfl.F90:47-189): maximum Courant numbers of
+ * the departure points in wpxyz over Adz_i0:in, j0:jn, k0:nk, bit-exact with
+ * the reference (FP64, first point of equal maxima in k, j, i order).
+ * DEVICE outputs: cfl[3] (horizontal, vertical, 3-D), idx[9] (global i, j, k
+ * of each maximum, as cfl_i(1:3, 1:3)). */
+int adzc_cfl(adzc_handle *h, const double *wpxyz, double *cfl, int *idx, void *stream);
+
+/* Trajectory state for a restart: Adz_wpxyz, Adz_pxyzm (REF32) and the
+ * handle's iteration state (cold start pending, Adz_niter), which the
+ * reference keeps through its memory manager's restart flag
+ * (B/adz_set.F90:343-360).  The file format is this library's own (a 64-byte
+ * header, then the device arrays).  Load checks precision and dimensions
+ * (ADZC_ERR_IO otherwise).  Both synchronise the device. */
+int adzc_state_save(adzc_handle *h, int prec, const void *pxyzm, const double *wpxyz, const char *path);
+int adzc_state_load(adzc_handle *h, int prec, void *pxyzm, double *wpxyz, const char *path);
 
 /* One whole advection step that allocates no device memory.  No counterpart
  * in the reference (its Fortran drivers use automatic arrays).

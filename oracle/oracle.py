@@ -405,3 +405,32 @@ class Step:
         if inp.get("tracers"):
             out["tracers"] = self.tricub(3, inp["tracers"], mono=self.cfg.mono, clip=self.cfg.mono)
         return out
+
+
+def adz_cfl(wpxyz, i0, in_, j0, jn, k0, nk, i0g=1, j0g=1):
+    """adz_courant (src/gemdyn/src/base/adz_cfl.F90:63-189) on one domain:
+    maximum horizontal, vertical and 3-D Courant numbers of the departure
+    points, FP64 in the reference's order, first maximum in loop order
+    (k, j, i); returns (cfl[3], idx[3, 3] global i, j, k)."""
+    wp = np.asarray(wpxyz, np.float64)
+    best = [(0.0, (0, 0, 0)) for _ in range(3)]
+    kk = np.arange(k0, nk + 1)
+    jj = np.arange(j0, jn + 1)
+    ii = np.arange(i0, in_ + 1)
+    sl = (slice(k0 - 1, nk), slice(j0 + 1, jn + 2), slice(i0 + 1, in_ + 2))
+    x = np.abs(wp[0][sl] - float(i0g) + 1.0 - ii[None, None, :].astype(np.float64))
+    y = np.abs(wp[1][sl] - float(j0g) + 1.0 - jj[None, :, None].astype(np.float64))
+    z = np.abs(wp[2][sl] - kk[:, None, None].astype(np.float64))
+    vals = [np.sqrt(x * x + y * y), z, np.sqrt(x * x + y * y + z * z)]
+    cfl = np.zeros(3)
+    idx = np.zeros((3, 3), np.int64)
+    for q, v in enumerate(vals):
+        flat = v.reshape(-1)
+        n = int(np.argmax(flat))  # first of equal maxima in (k, j, i) order
+        if flat[n] > 0.0:
+            k, j, i = np.unravel_index(n, v.shape)
+            cfl[q] = flat[n]
+            idx[q] = (ii[i] + i0g - 1, jj[j] + j0g - 1, kk[k])
+        else:
+            idx[q] = (i0g - 1, j0g - 1, 0)
+    return cfl, idx
