@@ -107,6 +107,7 @@ def lib() -> C.CDLL:
         L.adzc_batch_destroy.argtypes = [vp]
         L.adzc_bermejo_conde.argtypes = [vp, i, i, vp, vp, vp, vp, i, vp, vp, vp]
         L.adzc_cfl.argtypes = [vp, vp, vp, vp, vp]
+        L.adzc_ilmc.argtypes = [vp, i, i, vp, vp, vp, vp, i, i, C.POINTER(C.c_int), vp]
         L.adzc_state_save.argtypes = [vp, i, vp, vp, C.c_char_p]
         L.adzc_state_load.argtypes = [vp, i, vp, vp, C.c_char_p]
         L.adzc_error_string.restype = C.c_char_p
@@ -420,3 +421,12 @@ def bermejo_conde(adz: Adz, prec: int, tracers, airm_p, airm_m, mask, deficit, m
                                     airm_m.data_ptr(), mask.data_ptr(), int(min_max), deficit.data_ptr(),
                                     None if diag is None else diag.data_ptr(), _stream(stream)),
            "adzc_bermejo_conde")
+
+
+def ilmc(adz: Adz, prec: int, fields, mins, maxs, air, sweep_max=2, min_max=True, stream=None) -> int:
+    """ILMC filter (adzc_ilmc) of tracers in place; returns the rounds used."""
+    rounds = C.c_int(0)
+    _check(lib().adzc_ilmc(adz.h, prec, len(fields), C.cast(_ptr_array(fields), C.c_void_p),
+                           C.cast(_ptr_array(mins), C.c_void_p), C.cast(_ptr_array(maxs), C.c_void_p),
+                           air.data_ptr(), int(sweep_max), int(min_max), C.byref(rounds), _stream(stream)), "adzc_ilmc")
+    return rounds.value

@@ -322,6 +322,18 @@ int adzc_bermejo_conde(adzc_handle *h, int prec, int ntr, const adzc_bc_tracer *
                        const void *airm_m, const double *mask, int min_max, double *deficit, double *diag,
                        void *stream);
 
+/* ILMC shape-preserving filter (B/ILMC_LAM.F90:16-388, B/ilmc_lam_loop.inc)
+ * of ntr tracers f[q] (DEVICE, ext layout, fixed in place) with bounds
+ * mn[q]/mx[q] (the Adz_post min/max of adzc_tricub) and air mass air:
+ * single LAM domain (the arrival range i0..in, j0..jn, levels k0t..nk),
+ * sweeps 1..sweep_max (1-4, adz_ILMC_sweep_max), then the clip to the bounds
+ * when min_max (adz_ILMC_min_max_L).  Bit-exact with the reference's
+ * sequential loop order, run in parallel rounds of points whose
+ * neighbourhoods do not overlap; rounds (may be NULL) receives the largest
+ * number of rounds a tracer needed.  Synchronises the stream once per round. */
+int adzc_ilmc(adzc_handle *h, int prec, int ntr, void *const *f, const void *const *mn, const void *const *mx,
+              const void *air, int sweep_max, int min_max, int *rounds, void *stream);
+
 /* ------------------------------------------------------------------------ */
 /* Diagnostics and restart state                                              */
 /* ------------------------------------------------------------------------ */

@@ -617,6 +617,91 @@ void SFX(orc_bermejo_conde)(const orc_set *s, const REAL *p, REAL *m, const REAL
   *deficit = mass_bc - mass_tot_p;
 }
 
+/* neighbour shell of (i,j,k) at one sweep, in the order of the reference's
+ * sweep_rd lists (ILMC_LAM.F90:118-169): jx, then kx, then ix */
+static int SFX(ilmc_shell)(int i, int j, int k, int sweep, int il, int ir, int jl, int jr, int k0, int nk,
+                           int *ix_out, int *jx_out, int *kx_out) {
+  int n = 0;
+  const int kxm = (k - sweep > k0) ? k - sweep : k0, kxp = (k + sweep < nk) ? k + sweep : nk;
+  const int j1 = (j - sweep > jl) ? j - sweep : jl, j2 = (j + sweep < jr) ? j + sweep : jr;
+  const int i1 = (i - sweep > il) ? i - sweep : il, i2 = (i + sweep < ir) ? i + sweep : ir;
+  for (int jx = j1; jx <= j2; jx++)
+    for (int kx = kxm; kx <= kxp; kx++) {
+      const int limit_i = (jx != j - sweep && jx != j + sweep) && (kx > k - sweep && kx < k + sweep);
+      for (int ix = i1; ix <= i2; ix++) {
+        if (limit_i && ix != i - sweep && ix != i + sweep) continue;
+        ix_out[n] = ix;
+        jx_out[n] = jx;
+        kx_out[n] = kx;
+        n++;
+      }
+    }
+  return n;
+}
+
+void SFX(orc_ilmc)(const orc_set *s, REAL *f, const REAL *mn, const REAL *mx, const REAL *air, int sweep_max,
+                   int min_max) {
+  const int nk = s->g.nk;
+  const int il = s->i0, ir = s->in, jl = s->j0, jr = s->jn, k0 = s->k0t;
+  int ixs[400], jxs[400], kxs[400];
+  REAL cap[400];
+  for (int k = k0; k <= nk; k++) /* ilmc_lam_loop.inc */
+    for (int j = jl; j <= jr; j++)
+      for (int i = il; i <= ir; i++) {
+        const long e = EXT(i, j, k);
+        REAL o_shoot = SFX(rmax)((REAL)0, f[e] - mx[e]);
+        REAL u_shoot = SFX(rmax)((REAL)0, mn[e] - f[e]);
+        if (o_shoot == (REAL)0 && u_shoot == (REAL)0) continue;
+        for (int sweep = 1; sweep <= sweep_max; sweep++) {
+          const int nc = SFX(ilmc_shell)(i, j, k, sweep, il, ir, jl, jr, k0, nk, ixs, jxs, kxs);
+          REAL msum = 0;
+          if (o_shoot > (REAL)0) {
+            for (int q = 0; q < nc; q++) {
+              const long r = EXT(ixs[q], jxs[q], kxs[q]);
+              cap[q] = SFX(rmax)((REAL)0, mx[r] - f[r]);
+              msum = cap[q] * air[r] + msum;
+            }
+            const REAL use = SFX(rmin)(msum, o_shoot * air[e]);
+            if (use > (REAL)0) {
+              f[e] = SFX(rmax)(f[e] - (REAL)(use / air[e]), mn[e]);
+              o_shoot = SFX(rmax)((REAL)0, f[e] - mx[e]);
+              const REAL ratio = use / msum;
+              for (int q = 0; q < nc; q++)
+                if (cap[q] > (REAL)0) {
+                  const long r = EXT(ixs[q], jxs[q], kxs[q]);
+                  f[r] = SFX(rmin)(f[r] + (REAL)(cap[q] * ratio), mx[r]);
+                }
+            }
+          } else {
+            for (int q = 0; q < nc; q++) {
+              const long r = EXT(ixs[q], jxs[q], kxs[q]);
+              cap[q] = SFX(rmax)((REAL)0, f[r] - mn[r]);
+              msum = cap[q] * air[r] + msum;
+            }
+            const REAL use = SFX(rmin)(msum, u_shoot * air[e]);
+            if (use > (REAL)0) {
+              f[e] = SFX(rmin)(f[e] + (REAL)(use / air[e]), mx[e]);
+              u_shoot = SFX(rmax)((REAL)0, mn[e] - f[e]);
+              const REAL ratio = use / msum;
+              for (int q = 0; q < nc; q++)
+                if (cap[q] > (REAL)0) {
+                  const long r = EXT(ixs[q], jxs[q], kxs[q]);
+                  f[r] = SFX(rmax)(f[r] - (REAL)(cap[q] * ratio), mn[r]);
+                }
+            }
+          }
+        }
+      }
+  if (min_max) /* ILMC_LAM.F90:186-208 */
+    for (int k = k0; k <= nk; k++)
+      for (int j = jl; j <= jr; j++)
+        for (int i = il; i <= ir; i++) {
+          const long e = EXT(i, j, k);
+          if (f[e] < mn[e]) f[e] = mn[e];
+          if (f[e] > mx[e]) f[e] = mx[e];
+        }
+}
+
 #undef EXT
 #undef ARR
 #undef WP

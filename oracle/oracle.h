@@ -162,6 +162,16 @@ void orc_bermejo_conde_f64(const orc_set *s, const double *p, double *m, const d
                            double p_exp, int min_max, const double *airm_p, const double *airm_m,
                            const double *mask, double *deficit, double *diag);
 
+/* ILMC shape-preserving filter (ILMC_LAM.F90:16-388 with ilmc_lam_loop.inc),
+ * single LAM domain: points i0..in, j0..jn (the arrival range), levels
+ * k0t..nk, in that loop order; sweeps 1..sweep_max (<= 4) of neighbour shells
+ * enumerated as the reference's sweep_rd lists; then, if min_max, the clip
+ * to [min, max].  f fixed in place (ext layout). */
+void orc_ilmc_f32(const orc_set *s, float *f, const float *mn, const float *mx, const float *air, int sweep_max,
+                  int min_max);
+void orc_ilmc_f64(const orc_set *s, double *f, const double *mn, const double *mx, const double *air,
+                  int sweep_max, int min_max);
+
 /* number of points of a position set (0=q/pm, 1=u, 2=v, 3=t) */
 long orc_set_npoints(const orc_set *s, int set);
 

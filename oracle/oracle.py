@@ -108,6 +108,7 @@ class _Lib:
                                                         C.c_int, C.c_int, vp, vp, vp]
             getattr(L, f"orc_tricub_qv_{sfx}").argtypes = [C.POINTER(OrcSet), vp, C.c_int, vp, vp, C.c_int,
                                                            vp, vp, vp]
+            getattr(L, f"orc_ilmc_{sfx}").argtypes = [C.POINTER(OrcSet), vp, vp, vp, vp, C.c_int, C.c_int]
             getattr(L, f"orc_bermejo_conde_{sfx}").argtypes = [C.POINTER(OrcSet)] + [vp] * 8 + [
                 C.c_int, C.c_double, C.c_int, vp, vp, vp, vp, vp]
 
@@ -394,6 +395,16 @@ class Step:
             C.byref(self.s), *(P(x) for x in arrs), int(weight), float(p_exp), int(min_max), am.ctypes.data,
             bm.ctypes.data, mk.ctypes.data, C.byref(d), diag.ctypes.data)
         return arrs[1], d.value, diag
+
+    def ilmc(self, f, mn, mx, air, sweep_max=2, min_max=True):
+        """ILMC on one tracer (ext arrays of the Step's precision); returns the
+        filtered copy."""
+        A = lambda x: np.ascontiguousarray(x, dtype=self.dt)  # noqa: E731
+        out = A(f).copy()
+        a = [A(x) for x in (mn, mx, air)]
+        getattr(self.L, f"orc_ilmc_{self.prec}")(C.byref(self.s), out.ctypes.data, *(x.ctypes.data for x in a),
+                                                 int(sweep_max), int(min_max))
+        return out
 
     def step(self, inp, niter=None):
         """Trajectory, then u@pmu, v@pmv, w@pt, tracers@pt (clip if cfg.mono)."""
