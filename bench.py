@@ -314,6 +314,11 @@ def run_product(args):
         torch.cuda.empty_cache()
         tsum = measure_tracers(args, timed, ws, rank)
 
+    psum = None
+    if not args.no_post:
+        torch.cuda.empty_cache()
+        psum = measure_post(args, timed, ws, rank)
+
     gsum = None
     if not args.no_guess and os.path.exists(args.guess_weights):
         torch.cuda.empty_cache()
@@ -340,7 +345,7 @@ def run_product(args):
                           "achieved_gbs": step_bytes / (ms32 * 1e-3) / 1e9,
                           "frac": step_bytes / (ms32 * 1e-3) / 1e9 / hbm},
         "e2e": e2e, "gpu_launches": LAUNCHES_PER_STEP * args.steps, "clocks": clk, "cpu_baseline": cpu,
-        "tracers8": tsum, "batch": batch, "learned_guess": gsum,
+        "tracers8": tsum, "post": psum, "batch": batch, "learned_guess": gsum,
     }
     if rank == 0:
         print(json.dumps(line))
@@ -436,6 +441,69 @@ def measure_tracers(args, timed, ws, rank):
     out["step_roofline"] = {"algorithmic_bytes_per_point": 160.0,
                             "achieved_gbs": 160.0 * cfg.npoints / (out["mixed_ms_per_step"] * 1e-3) / 1e9}
     out["step_roofline"]["frac"] = out["step_roofline"]["achieved_gbs"] / hbm
+    return out
+
+
+def measure_post(args, timed, ws, rank):
+    """The passes after the interpolation on the multi-tracer workload (8
+    log-normal tracers, 1024x1024x80, MIXED): BICUBH_QV instead of the
+    tricubic at the thermo set, the Bermejo-Conde mass fixer (clipped
+    correction and proportional rescale), the ILMC filter (2 sweeps, then
+    the clip), and the CFL diagnostic; each timed alone."""
+    from gem_b200 import adz, synth
+    prec = adz.MIXED
+    ni, nj, nk = args.size
+    cfg = synth.config_mixed(ni, nj, nk, seed=tile_seed(rank), ntracers=8)
+    data = synth.make_inputs(cfg, device="cuda", dtype=torch.float32)
+    ad = adz.Adz.from_config(cfg)
+    px, wp = ad.new_state(prec)
+    ad.adz_inittraj(prec, px, wp)
+    ad.adz_traject(prec, cfg.dt, data, px, wp)
+    trs = data["tracers"]
+    z = lambda: torch.zeros(ad.ext_shape, dtype=torch.float32, device="cuda")  # noqa: E731
+    m = [z() for _ in trs]
+    lin, mn, mx = [z() for _ in trs], [z() for _ in trs], [z() for _ in trs]
+    K, W = max(3, min(args.steps, 10)), args.warmup
+    out = {"workload": f"{len(trs)} log-normal tracers at {ni}x{nj}x{nk}, MIXED", "ms": {}}
+
+    def tricub():
+        ad.adz_tricub_hlt(prec, adz.SET_T, trs, m, mono=[2] * len(trs), post=(lin, mn, mx))
+
+    def qv():
+        ad.adz_tricub_hlt(prec, adz.SET_T, trs, m, mono=[2 | adz.QV] * len(trs), post=(lin, mn, mx))
+    out["ms"]["tricubic_t_set"] = timed(tricub, K, W)[0]
+    out["ms"]["bicubh_qv_t_set"] = timed(qv, K, W)[0]
+    g = torch.Generator(device="cuda").manual_seed(5)
+    airm_p = 1.0 + 0.2 * torch.rand(ad.ext_shape, generator=g, device="cuda")
+    airm_m = airm_p * (1.0 + 0.01 * torch.rand(ad.ext_shape, generator=g, device="cuda"))
+    mask = torch.full((nj, ni), cfg.dx ** 2, dtype=torch.float64, device="cuda")
+    deficit = torch.zeros(len(trs), dtype=torch.float64, device="cuda")
+    tricub()
+    base = [t.clone() for t in m]
+    spec = [dict(p=trs[q], m=m[q], lin=lin[q], min=mn[q], max=mx[q]) for q in range(len(trs))]
+
+    def restore():
+        for t, b in zip(m, base):
+            t.copy_(b)
+
+    def bc():
+        restore()
+        adz.bermejo_conde(ad, prec, spec, airm_p, airm_m, mask, deficit)
+    out["ms"]["bermejo_conde_incl_restore"] = timed(bc, K, W)[0]
+    out["ms"]["restore_only"] = timed(restore, K, W)[0]
+    viol = sum(int(((b < n_) | (b > x_)).sum()) for b, n_, x_ in zip(base, mn, mx))
+    rounds = []
+
+    def ilmc():
+        restore()
+        rounds.append(adz.ilmc(ad, prec, m, mn, mx, airm_m, sweep_max=2, min_max=True))
+    out["ms"]["ilmc_incl_restore"] = timed(ilmc, K, W)[0]
+    out["ilmc"] = {"violating_points": viol, "points": cfg.npoints * len(trs), "rounds": max(rounds)}
+    out["ms"]["cfl"] = timed(lambda: ad.adz_cfl(wp), K, W)[0]
+    if ad.status() != 0:
+        raise RuntimeError("device status set during the post-processing measurement")
+    del data, m, lin, mn, mx, base
+    torch.cuda.empty_cache()
     return out
 
 
@@ -540,6 +608,7 @@ def main():
     ap.add_argument("--batch-domains", type=int, default=16)
     ap.add_argument("--no-guess", action="store_true", help="skip the learned-guess cold-start measurement")
     ap.add_argument("--no-tracers", action="store_true", help="skip the 8-tracer mono measurement")
+    ap.add_argument("--no-post", action="store_true", help="skip the QV / mass-fixer / ILMC / CFL measurement")
     ap.add_argument("--guess-weights", default=os.path.join(ROOT, "gem_b200", "data", "guess_mlp.npz"))
     ap.add_argument("--only", choices=["mixed"], default=None,
                     help="run the mixed-precision path alone (small profiling runs)")

@@ -5,18 +5,23 @@
 //
 // The reference visits the points in loop order (k, then j, then i) and
 // every visit changes the point's neighbourhood, so later visits see earlier
-// results.  This file keeps that order exactly and still runs in parallel:
-// a point's visit reads and writes only the cube of radius sweep_max around
-// it, so two visits commute unless the points are within 2 * sweep_max of
-// each other (Chebyshev).  Work runs in rounds; in each round every pending
-// point with no earlier pending point within 2 * sweep_max is visited (their
-// cubes are disjoint), then those points leave the pending set.  The earliest
-// pending point is always ready, so every round makes progress, and the
-// result is bit-for-bit the sequential one.  Only points outside their bounds
-// at the start are pending: a visit never pushes a neighbour out of its
-// bounds (the reference clamps every neighbour update), so no other point can
-// become one.  Built with -fmad=false: the REAL arithmetic is the
-// reference's, without contraction.
+// results.  This file keeps that order exactly and still runs in parallel.
+// A visit reads and writes only the cube of radius S = sweep_max around its
+// point, so a visit can depend only on earlier points within R = 2 S
+// (Chebyshev).  The region is cut into tiles of one row and 8 columns
+// (8 >= R for S <= 4), numbered (k, j, it); every earlier point within R of a
+// tile's point lies in the same tile (handled in order by one thread) or in a
+// tile of strictly smaller wavefront number
+//     t = (2 R + 2) k + 2 j + it
+// (a level below: at most R rows and one tile column away; the same level: an
+// earlier row, at most one tile column away; the same row: the tile before).
+// Tiles of one wavefront therefore never interact, and running the wavefronts
+// in increasing t, each tile by one warp in loop order, reproduces the
+// sequential result bit for bit.  Within a visit the lanes split the shell's
+// loads and updates; lane 0 forms the capacity sum in the reference's order.  The reference's visit of a point inside its
+// bounds does nothing, so each thread visits only the points it finds outside.
+// Built with -fmad=false: the REAL arithmetic is the reference's, without
+// contraction.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -55,149 +60,126 @@ __device__ __forceinline__ T rmax(T a, T b) { return a > b ? a : b; }
 template <typename T>
 __device__ __forceinline__ T rmin(T a, T b) { return a < b ? a : b; }
 
-// the neighbour shell of one sweep, in the order of the reference's sweep_rd
-// lists (B/ILMC_LAM.F90:118-169): jx, then kx, then ix
-template <typename Fn>
-__device__ __forceinline__ void shell(const Box& b, int i, int j, int k, int sweep, Fn fn) {
-  const int kxm = max(k - sweep, b.k0), kxp = min(k + sweep, b.nk);
-  const int j1 = max(j - sweep, b.jl), j2 = min(j + sweep, b.jr);
-  const int i1 = max(i - sweep, b.il), i2 = min(i + sweep, b.ir);
-  int q = 0;
-  for (int jx = j1; jx <= j2; jx++)
-    for (int kx = kxm; kx <= kxp; kx++) {
-      const bool limit_i = (jx != j - sweep && jx != j + sweep) && (kx > k - sweep && kx < k + sweep);
-      for (int ix = i1; ix <= i2; ix++) {
-        if (limit_i && ix != i - sweep && ix != i + sweep) continue;
-        fn(q++, ext(b, ix, jx, kx));
-      }
-    }
-}
+constexpr int kTile = 8;    // columns per tile, >= R = 2 sweep_max for sweep_max <= 4
+constexpr int kWarps = 4;   // tiles (warps) per block of k_wave
 
-// one visit of B/ilmc_lam_loop.inc
 template <typename T>
-__device__ void visit(const Box& b, T* f, const T* mn, const T* mx, const T* air, int sweep_max, int i, int j,
-                      int k) {
+struct Fields {
+  T* f[ADZC_ILMC_MAX_TRACERS];
+  const T* mn[ADZC_ILMC_MAX_TRACERS];
+  const T* mx[ADZC_ILMC_MAX_TRACERS];
+};
+
+// the unclipped shells of sweeps 1..4 in the order of the reference's
+// sweep_rd lists (jx, then kx, then ix; offsets di, dj, dk), concatenated;
+// a shell clipped to the region is this list filtered to the region, in the
+// same order (the inclusion test of a cell depends only on its offsets)
+constexpr int kShellTotal = 26 + 98 + 218 + 386;
+__constant__ signed char c_shell[kShellTotal][3];
+__constant__ int c_shell_start[5];
+
+// one visit by a warp: lane l owns the cells l, l + 32, ... of each shell;
+// lane 0 forms the capacity sum in the reference's order (bit-exact)
+template <typename T>
+__device__ void visit_warp(const Box& b, T* f, const T* mn, const T* mx, const T* air, int sweep_max, int i, int j,
+                           int k, int lane, T* cap, T* prod, long long* cell) {
   const long long e = ext(b, i, j, k);
   T o_shoot = rmax((T)0, f[e] - mx[e]);
   T u_shoot = rmax((T)0, mn[e] - f[e]);
   if (o_shoot == (T)0 && u_shoot == (T)0) return;
-  T cap[kMaxShell];
   const bool over = o_shoot > (T)0;
   for (int sweep = 1; sweep <= sweep_max; sweep++) {
-    T msum = 0;
-    shell(b, i, j, k, sweep, [&](int q, long long r) {
-      cap[q] = over ? rmax((T)0, mx[r] - f[r]) : rmax((T)0, f[r] - mn[r]);
-      msum = cap[q] * air[r] + msum;
-    });
-    const T use = rmin(msum, (over ? o_shoot : u_shoot) * air[e]);
-    if (use > (T)0) {
-      if (over) {
-        f[e] = rmax(f[e] - (T)(use / air[e]), mn[e]);
-        o_shoot = rmax((T)0, f[e] - mx[e]);
-      } else {
-        f[e] = rmin(f[e] + (T)(use / air[e]), mx[e]);
-        u_shoot = rmax((T)0, mn[e] - f[e]);
+    const int q0 = c_shell_start[sweep - 1], nq = c_shell_start[sweep] - q0;
+    for (int q = lane; q < nq; q += 32) {
+      const int ix = i + c_shell[q0 + q][0], jx = j + c_shell[q0 + q][1], kx = k + c_shell[q0 + q][2];
+      const bool in = ix >= b.il && ix <= b.ir && jx >= b.jl && jx <= b.jr && kx >= b.k0 && kx <= b.nk;
+      long long r = -1;
+      T c = 0, pr = 0;
+      if (in) {
+        r = ext(b, ix, jx, kx);
+        c = over ? rmax((T)0, mx[r] - f[r]) : rmax((T)0, f[r] - mn[r]);
+        pr = c * air[r];
       }
-      const T ratio = use / msum;
-      shell(b, i, j, k, sweep, [&](int q, long long r) {
-        if (cap[q] > (T)0) f[r] = over ? rmin(f[r] + (T)(cap[q] * ratio), mx[r]) : rmax(f[r] - (T)(cap[q] * ratio), mn[r]);
-      });
+      cell[q] = r;
+      cap[q] = c;
+      prod[q] = pr;
     }
-  }
-}
-
-// pending points: outside their bounds at the start
-template <typename T>
-__global__ void __launch_bounds__(256) k_mark(Box b, const T* __restrict__ f, const T* __restrict__ mn,
-                                              const T* __restrict__ mx, unsigned char* __restrict__ pend,
-                                              int* __restrict__ list, unsigned* __restrict__ count) {
-  const long long n = b.n();
-  for (long long o = blockIdx.x * 256LL + threadIdx.x; o < n; o += (long long)gridDim.x * 256) {
-    int i, j, k;
-    coords(b, o, i, j, k);
-    const long long e = ext(b, i, j, k);
-    const bool v = rmax((T)0, f[e] - mx[e]) != (T)0 || rmax((T)0, mn[e] - f[e]) != (T)0;
-    pend[o] = v ? 1 : 0;
-    if (v) list[atomicAdd(count, 1u)] = (int)o;
-  }
-}
-
-// ready: pending, and no earlier pending point within 2 sweep_max
-__global__ void __launch_bounds__(256) k_ready(Box b, int sweep_max, const unsigned char* __restrict__ pend,
-                                               const int* __restrict__ list, unsigned nlist,
-                                               unsigned char* __restrict__ ready) {
-  const unsigned q = blockIdx.x * 256u + threadIdx.x;
-  if (q >= nlist) return;
-  const long long o = list[q];
-  if (!pend[o]) {
-    ready[q] = 0;
-    return;
-  }
-  int i, j, k;
-  coords(b, o, i, j, k);
-  const int R = 2 * sweep_max, bx = b.bx(), by = b.by();
-  bool ok = true;
-  for (int kx = max(k - R, b.k0); kx <= k && ok; kx++)
-    for (int jx = max(j - R, b.jl); jx <= min(j + R, b.jr) && ok; jx++) {
-      if (kx == k && jx > j) break;
-      const int iend = (kx == k && jx == j) ? i - 1 : min(i + R, b.ir);
-      const long long row = (long long)(jx - b.jl) * bx + (long long)(kx - b.k0) * bx * by - b.il;
-      for (int ix = max(i - R, b.il); ix <= iend; ix++)
-        if (pend[row + ix]) {
-          ok = false;
-          break;
+    __syncwarp();
+    T ratio = 0;
+    int go = 0;
+    if (lane == 0) {
+      T msum = 0;
+      for (int q = 0; q < nq; q++)
+        if (cell[q] >= 0) msum = prod[q] + msum;
+      const T use = rmin(msum, (over ? o_shoot : u_shoot) * air[e]);
+      if (use > (T)0) {
+        if (over) {
+          f[e] = rmax(f[e] - (T)(use / air[e]), mn[e]);
+          o_shoot = rmax((T)0, f[e] - mx[e]);
+        } else {
+          f[e] = rmin(f[e] + (T)(use / air[e]), mx[e]);
+          u_shoot = rmax((T)0, mn[e] - f[e]);
         }
+        ratio = use / msum;
+        go = 1;
+      }
     }
-  ready[q] = ok ? 1 : 0;
+    go = __shfl_sync(0xffffffffu, go, 0);
+    ratio = __shfl_sync(0xffffffffu, ratio, 0);
+    o_shoot = __shfl_sync(0xffffffffu, o_shoot, 0);
+    u_shoot = __shfl_sync(0xffffffffu, u_shoot, 0);
+    if (go)
+      for (int q = lane; q < nq; q += 32) {
+        const long long r = cell[q];
+        if (r >= 0 && cap[q] > (T)0)
+          f[r] = over ? rmin(f[r] + (T)(cap[q] * ratio), mx[r]) : rmax(f[r] - (T)(cap[q] * ratio), mn[r]);
+      }
+    __syncwarp();
+  }
 }
 
+// one wavefront t: warp (tracer, level, tile column) finds its row from t
 template <typename T>
-__global__ void __launch_bounds__(128) k_visit(Box b, T* f, const T* __restrict__ mn, const T* __restrict__ mx,
-                                               const T* __restrict__ air, int sweep_max,
-                                               const int* __restrict__ list, unsigned nlist,
-                                               const unsigned char* __restrict__ ready) {
-  const unsigned q = blockIdx.x * 128u + threadIdx.x;
-  if (q >= nlist || !ready[q]) return;
-  int i, j, k;
-  coords(b, list[q], i, j, k);
-  visit<T>(b, f, mn, mx, air, sweep_max, i, j, k);
-}
-
-__global__ void __launch_bounds__(256) k_retire(unsigned char* __restrict__ pend, const int* __restrict__ list,
-                                                unsigned nlist, const unsigned char* __restrict__ ready,
-                                                unsigned* __restrict__ remaining) {
-  const unsigned q = blockIdx.x * 256u + threadIdx.x;
-  if (q >= nlist) return;
-  if (ready[q]) pend[list[q]] = 0;
-  else if (pend[list[q]]) atomicAdd(remaining, 1u);
-}
-
-// the rest in loop order on one thread (only after the round limit)
-template <typename T>
-__global__ void k_sequential(Box b, T* f, const T* mn, const T* mx, const T* air, int sweep_max,
-                             const unsigned char* pend) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  const long long n = b.n();
-  for (long long o = 0; o < n; o++)
-    if (pend[o]) {
-      int i, j, k;
-      coords(b, o, i, j, k);
-      visit<T>(b, f, mn, mx, air, sweep_max, i, j, k);
+__global__ void __launch_bounds__(32 * kWarps) k_wave(Box b, Fields<T> fl, int ntr, const T* __restrict__ air,
+                                                      int sweep_max, int t, int c1, int ntile) {
+  __shared__ T s_cap[kWarps][kMaxShell];
+  __shared__ T s_prod[kWarps][kMaxShell];
+  __shared__ long long s_cell[kWarps][kMaxShell];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nz = b.nk - b.k0 + 1, ny = b.by();
+  const long long n = (long long)ntr * nz * ntile;
+  for (long long g = (long long)blockIdx.x * kWarps + w; g < n; g += (long long)gridDim.x * kWarps) {
+    const int it = (int)(g % ntile);
+    const int kk = (int)((g / ntile) % nz);
+    const int tr = (int)(g / ((long long)ntile * nz));
+    const int rem = t - c1 * kk - it;
+    if (rem < 0 || (rem & 1) || (rem >> 1) >= ny) continue;  // warp-uniform
+    const int j = b.jl + (rem >> 1), k = b.k0 + kk;
+    const int i0 = b.il + it * kTile, i1 = min(i0 + kTile - 1, b.ir);
+    T* f = fl.f[tr];
+    const T* mn = fl.mn[tr];
+    const T* mx = fl.mx[tr];
+    for (int i = i0; i <= i1; i++) {
+      const long long e = ext(b, i, j, k);
+      if (f[e] > mx[e] || f[e] < mn[e]) visit_warp<T>(b, f, mn, mx, air, sweep_max, i, j, k, lane, s_cap[w], s_prod[w], s_cell[w]);
+      __syncwarp();
     }
+  }
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_clip(Box b, T* __restrict__ f, const T* __restrict__ mn,
                                               const T* __restrict__ mx) {
-  const long long n = b.n();
-  for (long long o = blockIdx.x * 256LL + threadIdx.x; o < n; o += (long long)gridDim.x * 256) {
-    int i, j, k;
-    coords(b, o, i, j, k);
-    const long long e = ext(b, i, j, k);
-    T v = f[e];
-    if (v < mn[e]) v = mn[e];
-    if (v > mx[e]) v = mx[e];
-    f[e] = v;
+  const int by = b.by();
+  for (long long row = blockIdx.x; row < (long long)by * (b.nk - b.k0 + 1); row += gridDim.x) {
+    const int j = b.jl + (int)(row % by), k = b.k0 + (int)(row / by);
+    for (int i = b.il + threadIdx.x; i <= b.ir; i += blockDim.x) {
+      const long long e = ext(b, i, j, k);
+      T v = f[e];
+      if (v < mn[e]) v = mn[e];
+      if (v > mx[e]) v = mx[e];
+      f[e] = v;
+    }
   }
 }
 
@@ -208,39 +190,61 @@ namespace {
 
 using namespace adz::ilmc;
 
-constexpr int kMaxRounds = 4096;
+// the reference's sweep_rd order for an unclipped point (B/ILMC_LAM.F90:118-169)
+struct ShellTable {
+  signed char off[kShellTotal][3];
+  int start[5];
+  ShellTable() {
+    int n = 0;
+    start[0] = 0;
+    for (int sw = 1; sw <= 4; sw++) {
+      for (int dj = -sw; dj <= sw; dj++)
+        for (int dk = -sw; dk <= sw; dk++) {
+          const bool limit_i = (dj != -sw && dj != sw) && (dk > -sw && dk < sw);
+          for (int di = -sw; di <= sw; di++) {
+            if (limit_i && di != -sw && di != sw) continue;
+            off[n][0] = (signed char)di;
+            off[n][1] = (signed char)dj;
+            off[n][2] = (signed char)dk;
+            n++;
+          }
+        }
+      start[sw] = n;
+    }
+  }
+};
+
+int upload_shells(cudaStream_t s) {
+  static const ShellTable tab;
+  if (cudaMemcpyToSymbolAsync(c_shell, tab.off, sizeof(tab.off), 0, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyToSymbolAsync(c_shell_start, tab.start, sizeof(tab.start), 0, cudaMemcpyHostToDevice, s) !=
+          cudaSuccess)
+    return ADZC_ERR_CUDA;
+  return ADZC_OK;
+}
 
 template <typename T>
-int run_ilmc(const Box& b, T* f, const T* mn, const T* mx, const T* air, int sweep_max, int min_max, char* scratch,
-             int* rounds, cudaStream_t s) {
-  const long long n = b.n();
-  unsigned char* pend = (unsigned char*)scratch;
-  int* list = (int*)(scratch + ((n + 255) & ~255LL));
-  unsigned char* ready = (unsigned char*)(list + ((n + 63) & ~63LL));
-  unsigned* counters = (unsigned*)(ready + ((n + 255) & ~255LL));  // [0] list length, [1] remaining
-  const int gb = (int)std::min<long long>((n + 255) / 256, 148LL * 32);
-  if (cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned), s) != cudaSuccess) return ADZC_ERR_CUDA;
-  k_mark<T><<<gb, 256, 0, s>>>(b, f, mn, mx, pend, list, counters);
-  unsigned nlist = 0;
-  if (cudaMemcpyAsync(&nlist, counters, sizeof(unsigned), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess)
-    return ADZC_ERR_CUDA;
-  int r = 0;
-  unsigned remaining = nlist;
-  while (remaining > 0 && r < kMaxRounds) {
-    const unsigned g = (nlist + 255) / 256;
-    k_ready<<<g, 256, 0, s>>>(b, sweep_max, pend, list, nlist, ready);
-    k_visit<T><<<(nlist + 127) / 128, 128, 0, s>>>(b, f, mn, mx, air, sweep_max, list, nlist, ready);
-    if (cudaMemsetAsync(counters + 1, 0, sizeof(unsigned), s) != cudaSuccess) return ADZC_ERR_CUDA;
-    k_retire<<<g, 256, 0, s>>>(pend, list, nlist, ready, counters + 1);
-    if (cudaMemcpyAsync(&remaining, counters + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess)
-      return ADZC_ERR_CUDA;
-    r++;
+int run_ilmc(const Box& b, int ntr, void* const* f, const void* const* mn, const void* const* mx, const T* air,
+             int sweep_max, int min_max, int* waves, cudaStream_t s) {
+  if (upload_shells(s) != ADZC_OK) return ADZC_ERR_CUDA;
+  Fields<T> fl{};
+  for (int q = 0; q < ntr; q++) {
+    fl.f[q] = (T*)f[q];
+    fl.mn[q] = (const T*)mn[q];
+    fl.mx[q] = (const T*)mx[q];
   }
-  if (remaining > 0) k_sequential<T><<<1, 1, 0, s>>>(b, f, mn, mx, air, sweep_max, pend);
-  if (min_max) k_clip<T><<<gb, 256, 0, s>>>(b, f, mn, mx);
-  if (rounds) *rounds = r + (remaining > 0 ? 1 : 0);
+  const int R = 2 * sweep_max, c1 = 2 * R + 2;
+  const int nz = b.nk - b.k0 + 1, ny = b.by(), ntile = (b.bx() + kTile - 1) / kTile;
+  const int nwave = c1 * (nz - 1) + 2 * (ny - 1) + (ntile - 1) + 1;
+  const long long ntiles = (long long)ntr * nz * ntile;
+  const int grid = (int)std::max<long long>(1, std::min<long long>((ntiles + kWarps - 1) / kWarps, 148LL * 32));
+  for (int t = 0; t < nwave; t++) k_wave<T><<<grid, 32 * kWarps, 0, s>>>(b, fl, ntr, air, sweep_max, t, c1, ntile);
+  if (min_max) {
+    const long long rows = (long long)ny * nz;
+    const int gr = (int)std::min<long long>(rows, 148LL * 16);
+    for (int q = 0; q < ntr; q++) k_clip<T><<<gr, 256, 0, s>>>(b, fl.f[q], fl.mn[q], fl.mx[q]);
+  }
+  if (waves) *waves = nwave;
   return cudaGetLastError() == cudaSuccess ? ADZC_OK : ADZC_ERR_CUDA;
 }
 
@@ -253,30 +257,21 @@ extern "C" int adzc_ilmc(adzc_handle* h, int prec, int ntr, void* const* f, cons
   adzc_info I;
   adzc_grid G;
   int niter = 0, cold = 0;
-  if (!h || (prec != ADZC_REF32 && prec != ADZC_MIXED && prec != ADZC_FP64) || ntr < 0 || (ntr > 0 && (!f || !mn || !mx)) ||
-      !air || sweep_max < 1 || sweep_max > 4 || adz_internal_view(h, &D, &I, &G, &niter, &cold) != ADZC_OK)
+  if (!h || (prec != ADZC_REF32 && prec != ADZC_MIXED && prec != ADZC_FP64) || ntr < 0 ||
+      ntr > ADZC_ILMC_MAX_TRACERS || (ntr > 0 && (!f || !mn || !mx)) || !air || sweep_max < 1 || sweep_max > 4 ||
+      adz_internal_view(h, &D, &I, &G, &niter, &cold) != ADZC_OK)
     return adz_internal_fail(ADZC_ERR_ARG);
   for (int q = 0; q < ntr; q++)
     if (!f[q] || !mn[q] || !mx[q]) return adz_internal_fail(ADZC_ERR_ARG);
+  if (rounds) *rounds = 0;
+  if (ntr == 0) return ADZC_OK;
   // single LAM domain: il..ir, jl..jr = Adz_i0..Adz_in, Adz_j0..Adz_jn (B/ILMC_LAM.F90:57-63), levels k0t..nk
   Box b{I.i0, I.in, I.j0, I.jn, I.k0t, D.nk, D.lminx, D.lminy, D.nit, D.nij};
-  const long long n = b.n();
-  if (n <= 0 || n > (1LL << 31) - 1) return adz_internal_fail(ADZC_ERR_SIZE);
-  const size_t bytes = ((n + 255) & ~255LL) + 4 * ((n + 63) & ~63LL) + ((n + 255) & ~255LL) + 256;
-  void* scratch = nullptr;
-  if (adz_internal_aux(h, bytes, &scratch) != ADZC_OK) return adz_internal_fail(ADZC_ERR_ALLOC);
+  if (b.n() <= 0) return adz_internal_fail(ADZC_ERR_ARG);
   const cudaStream_t s = (cudaStream_t)stream;
-  int total = 0;
-  for (int q = 0; q < ntr; q++) {
-    int r = 0;
-    const int st = prec == ADZC_FP64
-                       ? run_ilmc<double>(b, (double*)f[q], (const double*)mn[q], (const double*)mx[q],
-                                          (const double*)air, sweep_max, min_max, (char*)scratch, &r, s)
-                       : run_ilmc<float>(b, (float*)f[q], (const float*)mn[q], (const float*)mx[q],
-                                         (const float*)air, sweep_max, min_max, (char*)scratch, &r, s);
-    if (st != ADZC_OK) return adz_internal_fail(st);
-    total = std::max(total, r);
-  }
-  if (rounds) *rounds = total;
-  return ADZC_OK;
+  const int st = prec == ADZC_FP64 ? run_ilmc<double>(b, ntr, f, mn, mx, (const double*)air, sweep_max, min_max,
+                                                      rounds, s)
+                                   : run_ilmc<float>(b, ntr, f, mn, mx, (const float*)air, sweep_max, min_max,
+                                                     rounds, s);
+  return st == ADZC_OK ? ADZC_OK : adz_internal_fail(st);
 }

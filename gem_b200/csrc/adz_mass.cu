@@ -58,12 +58,6 @@ struct Geo {
   const double* mask;  // (ni, nj)
 };
 
-__device__ __forceinline__ void point(const Region& r, long long t, int& i, int& j, int& k) {
-  i = r.i0 + (int)(t % r.nx);
-  j = r.j0 + (int)((t / r.nx) % r.ny);
-  k = r.k0 + (int)(t / ((long long)r.nx * r.ny));
-}
-
 __device__ __forceinline__ long long ext(const Geo& g, int i, int j, int k) {
   return (long long)(i - g.lminx) + (long long)(j - g.lminy) * g.nit + (long long)(k - 1) * g.nij;
 }
@@ -92,16 +86,17 @@ __global__ void __launch_bounds__(kThreads) k_reduce(const Tr<T>* __restrict__ t
                                                      const T* __restrict__ air_m, double* __restrict__ part) {
   const int q = blockIdx.y;
   const Tr<T> tr = trs[q];
-  const long long n = r.n();
-  const long long chunk = (n + kBlocks - 1) / kBlocks;
-  const long long b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+  // block b owns a fixed slice of the region's rows (j, k); threads stride over i
+  const long long rows = (long long)r.ny * r.nz;
+  const long long chunk = (rows + kBlocks - 1) / kBlocks;
+  const long long r0 = blockIdx.x * chunk, r1 = min(rows, r0 + chunk);
   double s0 = 0.0, s1 = 0.0;
   const bool skip = (MODE == kM || MODE == kWei) && st[q].skip;
   const double sd = MODE == kWei ? sign1(st[q].def) : 1.0;
-  if (!skip && !(MODE == kFlux && (!tr.fo || !tr.fi))) {
-    for (long long t = b0 + threadIdx.x; t < b1; t += kThreads) {
-      int i, j, k;
-      point(r, t, i, j, k);
+  if (!skip && !(MODE == kFlux && (!tr.fo || !tr.fi)) && r.nx > 0) {
+    for (long long row = r0; row < r1; row++)
+    for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) {
+      const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
       const long long e = ext(g, i, j, k);
       const double mk = __ldg(g.mask + (i - 1) + (long long)(j - 1) * g.ni);
       if (MODE == kPM) {
@@ -204,10 +199,10 @@ __global__ void __launch_bounds__(kThreads) k_correct(const Tr<T>* __restrict__ 
   if (st[q].skip) return;
   const Tr<T> tr = trs[q];
   const double lambda = st[q].lambda, sd = sign1(st[q].def);
-  const long long n = r.n();
-  for (long long t = blockIdx.x * (long long)kThreads + threadIdx.x; t < n; t += (long long)gridDim.x * kThreads) {
-    int i, j, k;
-    point(r, t, i, j, k);
+  const long long rows = (long long)r.ny * r.nz;
+  for (long long row = blockIdx.x; row < rows; row += gridDim.x)
+  for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) {
+    const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
     const long long e = ext(g, i, j, k);
     const double corr = lambda * (double)bc_weight<T>(tr, e, sd);
     if (!min_max) {
@@ -230,10 +225,10 @@ __global__ void __launch_bounds__(kThreads) k_scale(const Tr<T>* __restrict__ tr
   if (st[q].skip) return;
   T* m = trs[q].m;
   const double prop = st[q].prop;
-  const long long n = r.n();
-  for (long long t = blockIdx.x * (long long)kThreads + threadIdx.x; t < n; t += (long long)gridDim.x * kThreads) {
-    int i, j, k;
-    point(r, t, i, j, k);
+  const long long rows = (long long)r.ny * r.nz;
+  for (long long row = blockIdx.x; row < rows; row += gridDim.x)
+  for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) {
+    const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
     const long long e = ext(g, i, j, k);
     m[e] = (T)(prop * (double)m[e]);
   }
@@ -274,8 +269,8 @@ int run_bc(int ntr, const adzc_bc_tracer* in, const void* airm_p, const void* ai
   const T* ap = (const T*)airm_p;
   const T* am = (const T*)airm_m;
   const int fb = (ntr + 127) / 128;
-  const long long n = core.n();
-  const dim3 eg((unsigned)std::max<long long>(1, std::min<long long>((n + kThreads - 1) / kThreads, 1024)), ntr);
+  const long long crows = (long long)core.ny * core.nz;
+  const dim3 eg((unsigned)std::max<long long>(1, std::min<long long>(crows, 2048)), ntr);
   Geo gm = g;
   gm.mask = mask;
   k_reduce<T, kPM><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, ap, am, d_part);

@@ -328,9 +328,11 @@ int adzc_bermejo_conde(adzc_handle *h, int prec, int ntr, const adzc_bc_tracer *
  * single LAM domain (the arrival range i0..in, j0..jn, levels k0t..nk),
  * sweeps 1..sweep_max (1-4, adz_ILMC_sweep_max), then the clip to the bounds
  * when min_max (adz_ILMC_min_max_L).  Bit-exact with the reference's
- * sequential loop order, run in parallel rounds of points whose
- * neighbourhoods do not overlap; rounds (may be NULL) receives the largest
- * number of rounds a tracer needed.  Synchronises the stream once per round. */
+ * sequential loop order, run as wavefronts of row tiles whose neighbourhoods
+ * never interact, all tracers (at most ADZC_ILMC_MAX_TRACERS) together;
+ * rounds (may be NULL) receives the number of wavefronts.  Does not
+ * synchronise the stream. */
+#define ADZC_ILMC_MAX_TRACERS 32
 int adzc_ilmc(adzc_handle *h, int prec, int ntr, void *const *f, const void *const *mn, const void *const *mx,
               const void *air, int sweep_max, int min_max, int *rounds, void *stream);
 
