@@ -34,6 +34,7 @@
 struct adzc_batch {
   int prec = 0, ndom = 0;
   std::vector<adz::BDom> doms;
+  adz::BatchParams* params = nullptr;  // the domains' grid-constant descriptors
   std::vector<adzc_handle*> handles;
   adz::BDom* d_doms = nullptr;
   adz::BItem* d_items = nullptr;
@@ -98,10 +99,10 @@ cudaError_t enqueue(adzc_batch* b, cudaStream_t s) {
   if ((e = cudaMemsetAsync(b->d_done, 0, 2 * b->ndom * sizeof(unsigned), s)) != cudaSuccess) return e;
   const int grid = b->bps * b->sms;
   if (b->prec == ADZC_FP64)
-    return adz::launch_batch<adz::kFp64>(b->variant, grid, b->d_doms, b->d_items, b->nitems, b->d_need, b->d_next,
-                                         b->d_done, b->d_status, s);
-  return adz::launch_batch<adz::kMixed>(b->variant, grid, b->d_doms, b->d_items, b->nitems, b->d_need, b->d_next,
-                                        b->d_done, b->d_status, s);
+    return adz::launch_batch<adz::kFp64>(b->variant, grid, *b->params, b->d_doms, b->d_items, b->nitems, b->d_need,
+                                         b->d_next, b->d_done, b->d_status, s);
+  return adz::launch_batch<adz::kMixed>(b->variant, grid, *b->params, b->d_doms, b->d_items, b->nitems, b->d_need,
+                                        b->d_next, b->d_done, b->d_status, s);
 }
 
 int resident(const adzc_batch* b, int variant) {
@@ -141,6 +142,7 @@ extern "C" int adzc_batch_destroy(adzc_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->cap) cudaStreamDestroy(b->cap);
+  delete b->params;
   cudaFree(b->d_doms);
   cudaFree(b->d_items);
   cudaFree(b->d_need);
@@ -153,6 +155,7 @@ extern "C" int adzc_batch_destroy(adzc_batch* b) {
 
 extern "C" int adzc_batch_create(int prec, int ndom, const adzc_domain* doms, adzc_batch** out) {
   if (!out || ndom < 1 || !doms || (prec != ADZC_FP64 && prec != ADZC_MIXED)) return adz_internal_fail(ADZC_ERR_ARG);
+  if (ndom > ADZC_BATCH_MAX_DOMAINS) return adz_internal_fail(ADZC_ERR_SIZE);
   auto* b = new (std::nothrow) adzc_batch();
   if (!b) return adz_internal_fail(ADZC_ERR_ALLOC);
   b->prec = prec;
@@ -243,6 +246,20 @@ extern "C" int adzc_batch_create(int prec, int ndom, const adzc_domain* doms, ad
       f0 += nf;
     }
     b->handles.push_back(in.h);
+  }
+  b->params = new (std::nothrow) adz::BatchParams();
+  if (!b->params) {
+    adzc_batch_destroy(b);
+    return adz_internal_fail(ADZC_ERR_ALLOC);
+  }
+  for (int d = 0; d < ndom; d++) {
+    adz::BDomC& C = b->params->d[d];
+    C.g = b->doms[d].g;
+    C.uu = b->doms[d].uu;
+    C.vv = b->doms[d].vv;
+    C.ww = b->doms[d].ww;
+    C.ta = b->doms[d].ta;
+    C.sa = b->doms[d].sa;
   }
   if (cudaMalloc(&b->d_doms, ndom * sizeof(adz::BDom)) != cudaSuccess ||
       cudaMalloc(&b->d_need, 2 * ndom * sizeof(unsigned)) != cudaSuccess ||

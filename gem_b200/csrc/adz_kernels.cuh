@@ -405,11 +405,11 @@ __global__ void ADZ_TRAJ_BOUNDS k_traject_tol(DGrid g, TrajArgs a, double tol, i
 
 // ---------------------------------------------------------------------------
 // position of arrival point (i,j,k) of a set, adz_interp_traj.F90:45-187
-// CG: read the trajectory arrays around L1 (ld.global.cg), for a kernel that
+// CG: read the trajectory arrays through the coherent path (ld.global.ca), for a kernel that
 // wrote them itself earlier in the same launch
 template <typename T, bool CG>
 __device__ __forceinline__ T ld_traj(const T* p) {
-  if (CG) return __ldcg(p);
+  if (CG) return __ldca(p);  // coherent (not the read-only path), L1-cached after the acquire
   return *p;
 }
 
@@ -700,17 +700,14 @@ __device__ __forceinline__ void block_copy(T* dst, const T* src) {
 // MINB: minimum resident blocks per SM handed to ptxas (register budget);
 // the autotuner picks the variant
 template <int PREC, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_batch(const BDom* __restrict__ doms, const BItem* __restrict__ items,
+__global__ void __launch_bounds__(128, MINB) k_batch(const __grid_constant__ BatchParams P,
+                                                     const BDom* __restrict__ doms, const BItem* __restrict__ items,
                                                      long long nitems, const unsigned* __restrict__ need,
                                                      unsigned long long* __restrict__ next,
                                                      unsigned* __restrict__ done, int* __restrict__ status) {
   __shared__ long long cur;
   __shared__ int dep_ok;
-  __shared__ DGrid sg;
-  __shared__ TrajArgs sta;
-  __shared__ SetArgs ssa;
   __shared__ FieldPtrs sfp;
-  __shared__ const void* swind[4];
   __shared__ int sset, srange[5];
   for (;;) {
     if (threadIdx.x == 0) cur = (long long)atomicAdd(next, 1ull);
@@ -737,32 +734,26 @@ __global__ void __launch_bounds__(128, MINB) k_batch(const BDom* __restrict__ do
         }
       }
     }
-    {
+    if (item.phase == 2) {  // field group of the item: global descriptor -> shared
       const BDom& D = doms[item.dom];
-      block_copy(&sg, &D.g);
-      if (item.phase == 0 && threadIdx.x < 4)
-        swind[threadIdx.x] = threadIdx.x == 0 ? D.uu : threadIdx.x == 1 ? D.vv : threadIdx.x == 2 ? D.ww : D.ta.uvw_d;
-      if (item.phase == 1) block_copy(&sta, &D.ta);
-      if (item.phase == 2) {
-        block_copy(&ssa, &D.sa);
-        block_copy(&sfp, &D.gfp[item.group]);
-        if (threadIdx.x < 5) srange[threadIdx.x] = D.grange[item.group][threadIdx.x];
-        if (threadIdx.x == 5) sset = D.gset[item.group];
-      }
+      block_copy(&sfp, &D.gfp[item.group]);
+      if (threadIdx.x < 5) srange[threadIdx.x] = D.grange[item.group][threadIdx.x];
+      if (threadIdx.x == 5) sset = D.gset[item.group];
     }
     __syncthreads();
     if (dep_ok) {
+      const BDomC& C = P.d[item.dom];  // constant bank
       const long long end = item.start + item.count;
       if (item.phase == 0) {
         using F = typename Types<PREC>::F;
         for (long long e = item.start + threadIdx.x; e < end; e += blockDim.x)
-          prepare_cell<PREC>(sg, (const F*)swind[0], (const F*)swind[1], (const F*)swind[2], (F*)swind[3], e);
+          prepare_cell<PREC>(C.g, (const F*)C.uu, (const F*)C.vv, (const F*)C.ww, (F*)C.ta.uvw_d, e);
       } else if (item.phase == 1) {
-        const long long plane = (long long)sg.ni * sg.nj;
+        const long long plane = (long long)C.g.ni * C.g.nj;
         for (long long t = item.start + threadIdx.x; t < end; t += blockDim.x) {
-          const int i = (int)(t % sg.ni) + 1, j = (int)((t / sg.ni) % sg.nj) + 1;
-          const int k = (int)(t / plane) + sta.k00;
-          traject_point<PREC, true>(sg, sta, i, j, k);
+          const int i = (int)(t % C.g.ni) + 1, j = (int)((t / C.g.ni) % C.g.nj) + 1;
+          const int k = (int)(t / plane) + C.ta.k00;
+          traject_point<PREC, true>(C.g, C.ta, i, j, k);
         }
       } else {
         const int nx = srange[1], ny = srange[3];
@@ -770,7 +761,7 @@ __global__ void __launch_bounds__(128, MINB) k_batch(const BDom* __restrict__ do
         for (long long t = item.start + threadIdx.x; t < end; t += blockDim.x) {
           const int i = (int)(t % nx) + srange[0], j = (int)((t / nx) % ny) + srange[2];
           const int k = (int)(t / plane) + srange[4];
-          set_point<PREC, true>(sg, sset, ssa, sfp, i, j, k);
+          set_point<PREC, true>(C.g, sset, C.sa, sfp, i, j, k);
         }
       }
     }
@@ -859,18 +850,18 @@ struct BatchMinB {
 };
 
 template <int PREC>
-cudaError_t launch_batch(int variant, int grid, const BDom* doms, const BItem* items, long long nitems,
-                         const unsigned* need, unsigned long long* next, unsigned* done, int* status,
-                         cudaStream_t s) {
+cudaError_t launch_batch(int variant, int grid, const BatchParams& P, const BDom* doms, const BItem* items,
+                         long long nitems, const unsigned* need, unsigned long long* next, unsigned* done,
+                         int* status, cudaStream_t s) {
   if constexpr (PREC == kRef32) {
     return cudaErrorNotSupported;
   } else {
     if (variant == 1)
-      k_batch<PREC, BatchMinB<PREC, 1>::value><<<grid, 128, 0, s>>>(doms, items, nitems, need, next, done, status);
+      k_batch<PREC, BatchMinB<PREC, 1>::value><<<grid, 128, 0, s>>>(P, doms, items, nitems, need, next, done, status);
     else if (variant == 2)
-      k_batch<PREC, BatchMinB<PREC, 2>::value><<<grid, 128, 0, s>>>(doms, items, nitems, need, next, done, status);
+      k_batch<PREC, BatchMinB<PREC, 2>::value><<<grid, 128, 0, s>>>(P, doms, items, nitems, need, next, done, status);
     else
-      k_batch<PREC, BatchMinB<PREC, 0>::value><<<grid, 128, 0, s>>>(doms, items, nitems, need, next, done, status);
+      k_batch<PREC, BatchMinB<PREC, 0>::value><<<grid, 128, 0, s>>>(P, doms, items, nitems, need, next, done, status);
     return cudaGetLastError();
   }
 }
@@ -900,7 +891,8 @@ int batch_resident_blocks(int variant) {
   template cudaError_t launch_interp_pos<P>(const DZtab&, int, int, const void*, const FieldPtrs&, cudaStream_t); \
   template cudaError_t launch_qv_set<P>(const DGrid&, int, int, int, int, int, int, const SetArgs&,               \
                                         const FieldPtrs&, cudaStream_t);                                          \
-  template cudaError_t launch_batch<P>(int, int, const BDom*, const BItem*, long long, const unsigned*,           \
+  template cudaError_t launch_batch<P>(int, int, const BatchParams&, const BDom*, const BItem*, long long,       \
+                                       const unsigned*,                                                             \
                                        unsigned long long*, unsigned*, int*, cudaStream_t);                        \
   template int batch_resident_blocks<P>(int);
 

@@ -1,6 +1,7 @@
 // Plain data structures shared by the kernels and the host C-ABI code
 // (no device code here, so g++ can compile the host side).
 #pragma once
+#include "../../include/adz_b200.h"
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -146,6 +147,22 @@ struct BDom {
   FieldPtrs gfp[kMaxGroups];
 };
 
+// per-domain descriptors of the batch kernel, passed as one grid-constant
+// kernel parameter (read from the constant bank, never aliased by stores)
+struct BDomC {
+  DGrid g;
+  const void* uu;
+  const void* vv;
+  const void* ww;
+  TrajArgs ta;
+  SetArgs sa;
+};
+constexpr int kBatchMaxDomains = ADZC_BATCH_MAX_DOMAINS;
+struct BatchParams {
+  BDomC d[kBatchMaxDomains];
+};
+static_assert(sizeof(BatchParams) <= 32000, "kernel parameter limit");
+
 struct BItem {
   int dom, phase, group, pad;
   long long start, count;
@@ -153,7 +170,8 @@ struct BItem {
 
 constexpr int kBatchVariants = 3;  // register budgets of the batch kernel
 template <int PREC>
-cudaError_t launch_batch(int variant, int grid, const BDom* doms, const BItem* items, long long nitems,
+cudaError_t launch_batch(int variant, int grid, const BatchParams& P, const BDom* doms, const BItem* items,
+                         long long nitems,
                          const unsigned* need, unsigned long long* next, unsigned* done, int* status,
                          cudaStream_t s);
 template <int PREC>

@@ -224,6 +224,7 @@ typedef struct {
 
 typedef struct adzc_batch adzc_batch;
 
+#define ADZC_BATCH_MAX_DOMAINS 40  /* more: ADZC_ERR_SIZE */
 int adzc_batch_create(int prec, int ndom, const adzc_domain *doms, adzc_batch **out);
 /* autotuner: times candidate tile heights (rows per work item) and resident
  * blocks per SM on these domains, keeps the fastest and re-captures the graph.
