@@ -307,7 +307,12 @@ def run_product(args):
     if not args.no_batch:
         del d32, outs32, tro32, step32, px, wp, srcs, dsts
         torch.cuda.empty_cache()
-        batch = measure_batch(args, timed, ws)
+        from gem_b200 import synth
+        batch = measure_batch(args, timed, ws, synth.config_batch(n=args.batch_domains, seed=2024),
+                              "uneven LAM domains (256-1024 squared, 40-80 levels, 1-20 tracers, mono)")
+        batch["small_domains"] = measure_batch(
+            args, timed, ws, synth.config_batch(n=40, seed=2025, size=(48, 160), levels=(20, 80), tracers=(1, 8)),
+            "small LAM domains (48-160 squared, 20-80 levels, 1-8 tracers, mono)")
 
     tsum = None
     if not args.no_tracers:
@@ -358,16 +363,14 @@ def run_product(args):
 LAUNCHES_PER_STEP = 5
 
 
-def measure_batch(args, timed, ws):
-    """Independent limited-area domains of uneven size (256-1024 squared,
-    40-80 levels, 1-20 log-normal tracers, own flow phase, U0 and dt) in one
-    persistent launch per step, replayed from a CUDA graph after the
-    autotuner picked its tile height, register budget and resident blocks;
-    beside it the same domains stepped one after another through the
-    per-domain entry points."""
+def measure_batch(args, timed, ws, cfgs, label):
+    """Independent limited-area domains of uneven size (each with its own
+    levels, log-normal tracers, flow phase, U0 and dt) in one persistent
+    launch per step, replayed from a CUDA graph after the autotuner picked
+    its tile height, register budget and resident blocks; beside it the same
+    domains stepped one after another through the per-domain entry points."""
     from gem_b200 import adz, synth
     prec = adz.MIXED
-    cfgs = synth.config_batch(n=args.batch_domains, seed=2024)
     doms, spec = [], []
     for cfg in cfgs:
         ad = adz.Adz.from_config(cfg)
@@ -398,7 +401,7 @@ def measure_batch(args, timed, ws):
     ms_s, _ = timed(sequential, args.steps, args.warmup)
     # per domain: winds, trajectory, u set, v set, thermo set in groups of 16 fields
     seq_launches = sum(4 + (len(d[4]) - 2 + 15) // 16 for d in doms)
-    out = {"workload": f"{len(cfgs)} uneven LAM domains (256-1024 squared, 40-80 levels, 1-20 tracers, mono)",
+    out = {"workload": f"{len(cfgs)} {label}",
            "points_per_step": npts, "value": npts * ws / (ms_b * 1e-3), "unit": "grid-points/s",
            "ms_per_step": ms_b, "launches_per_step": 1, "plan": batch.query(), "tune_s": tune_s,
            "sequential_ms_per_step": ms_s, "sequential_launches_per_step": seq_launches,
