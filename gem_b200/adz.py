@@ -110,6 +110,9 @@ def lib() -> C.CDLL:
         L.adzc_ilmc.argtypes = [vp, i, i, vp, vp, vp, vp, i, i, C.POINTER(C.c_int), vp]
         L.adzc_state_save.argtypes = [vp, i, vp, vp, C.c_char_p]
         L.adzc_state_load.argtypes = [vp, i, vp, vp, C.c_char_p]
+        L.adzc_halo_layout.argtypes = [vp, i, vp]
+        L.adzc_halo_pack.argtypes = [vp, i, vp, vp, vp]
+        L.adzc_halo_unpack.argtypes = [vp, i, vp, vp, vp]
         L.adzc_error_string.restype = C.c_char_p
         L.Vsearch_setup.restype = vp
         L.Vsearch_setup.argtypes = [vp, i, i, i]
@@ -217,16 +220,23 @@ class Adz:
         self.ni, self.nj, self.nk = grid.ni, grid.nj, grid.nk
 
     @classmethod
-    def from_config(cls, cfg, lam=True, i0g=1, j0g=1, schm_advec=1):
-        """adz_set for a synthetic LAM tile (gem_b200.synth.Config)."""
+    def from_config(cls, cfg, lam=True, i0g=None, j0g=None, schm_advec=1, edges=None):
+        """adz_set for a synthetic LAM tile (gem_b200.synth.Config).  The
+        tile starts at global (i0g, j0g) (default: the config's tile origin)
+        and touches the LAM edges flagged in ``edges`` = (west, east, south,
+        north) (default: all of them when ``lam``); pilot zones lie on those
+        edges only."""
         from . import synth
         ga = synth.grid_arrays(cfg)
         keep = {k: np.ascontiguousarray(ga[k], dtype=np.float64) for k in ("cy", "zm", "zt", "zx")}
         e = 1 if lam else 0
+        w, ea, so, no = edges if edges is not None else (e, e, e, e)
         p = cfg.pil if lam else 0
+        i0g = cfg.gi0 if i0g is None else i0g
+        j0g = cfg.gj0 if j0g is None else j0g
         P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
         g = AdzcGrid(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk, maxcfl=cfg.maxcfl, i0g=i0g, j0g=j0g,
-                     west=e, east=e, south=e, north=e, pil_w=p, pil_e=p, pil_s=p, pil_n=p,
+                     west=w, east=ea, south=so, north=no, pil_w=p * w, pil_e=p * ea, pil_s=p * so, pil_n=p * no,
                      lam_gbpil_t=0, bc_lam_flux=1, schm_advec=schm_advec, itraj=cfg.niter, slt_winds=0,
                      bA_m=0.6, bA=0.6, inv_rayt=ga["inv_rayt"], inv_hx=ga["inv_hx"], inv_hy=ga["inv_hy"],
                      cy=P(keep["cy"]), zm=P(keep["zm"]), zt=P(keep["zt"]), zx=P(keep["zx"]),
@@ -377,22 +387,6 @@ class Batch:
         r, b, n = C.c_int(), C.c_int(), C.c_longlong()
         _check(lib().adzc_batch_query(self.h, C.byref(r), C.byref(b), C.byref(n)), "adzc_batch_query")
         return {"rows_per_item": r.value, "blocks_per_sm": b.value, "items": n.value}
-
-    def adz_cfl(self, wpxyz, stream=None):
-        """Maximum Courant numbers (horizontal, vertical, 3-D) and their global
-        (i, j, k), as adz_cfl prints them."""
-        cfl = torch.zeros(3, dtype=torch.float64, device=wpxyz.device)
-        idx = torch.zeros(9, dtype=torch.int32, device=wpxyz.device)
-        _check(lib().adzc_cfl(self.h, wpxyz.data_ptr(), cfl.data_ptr(), idx.data_ptr(), _stream(stream)), "adzc_cfl")
-        return cfl.cpu().numpy(), idx.cpu().numpy().reshape(3, 3)
-
-    def state_save(self, prec: int, pxyzm, wpxyz, path: str):
-        _check(lib().adzc_state_save(self.h, prec, None if pxyzm is None else pxyzm.data_ptr(), wpxyz.data_ptr(),
-                                     path.encode()), "adzc_state_save")
-
-    def state_load(self, prec: int, pxyzm, wpxyz, path: str):
-        _check(lib().adzc_state_load(self.h, prec, None if pxyzm is None else pxyzm.data_ptr(), wpxyz.data_ptr(),
-                                     path.encode()), "adzc_state_load")
 
     def status(self, reset=True, stream=None) -> int:
         return lib().adzc_batch_status(self.h, 1 if reset else 0, _stream(stream))

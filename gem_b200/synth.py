@@ -117,7 +117,18 @@ class Config:
     mono: bool = False
     phase: tuple = (0.0, 0.0)
     t_now: float = 0.0
+    # tile of a larger domain: global index of local (1,1) and the global
+    # extents (0: the tile is the whole domain); the flow and the tracers are
+    # functions of the global position
+    gi0: int = 1
+    gj0: int = 1
+    gni: int = 0
+    gnj: int = 0
     extra: dict = field(default_factory=dict)
+
+    @property
+    def domain(self) -> tuple:
+        return (self.gni or self.ni, self.gnj or self.nj)
 
     @property
     def halo(self) -> int:
@@ -190,15 +201,15 @@ def config_cold(ni=1024, nj=1024, nk=80, seed=4321) -> Config:
 def _coords(cfg: Config, device, dtype):
     H = cfg.halo
     nit, njt = cfg.ni + 2 * H, cfg.nj + 2 * H
-    i = torch.arange(1 - H, cfg.ni + H + 1, device=device, dtype=dtype)
-    j = torch.arange(1 - H, cfg.nj + H + 1, device=device, dtype=dtype)
+    i = torch.arange(1 - H, cfg.ni + H + 1, device=device, dtype=dtype) + (cfg.gi0 - 1)
+    j = torch.arange(1 - H, cfg.nj + H + 1, device=device, dtype=dtype) + (cfg.gj0 - 1)
     x = (i - 1) * cfg.dx
     y = (j - 1) * cfg.dx
     return x, y, nit, njt
 
 
 def _flow(cfg: Config, x, y, z, t, comp):
-    Lx, Ly = cfg.ni * cfg.dx, cfg.nj * cfg.dx
+    Lx, Ly = cfg.domain[0] * cfg.dx, cfg.domain[1] * cfg.dx
     ph = cfg.phase
     ct = math.cos(math.pi * t / cfg.period)
     X = x.view(1, 1, -1) / Lx + ph[0]
@@ -249,7 +260,7 @@ def make_inputs(cfg: Config, device="cpu", dtype=torch.float64, with_fields=True
     out["src_w"] = _flow(cfg, x, y, zt, t1, 2).expand(shp).to(dtype).contiguous()
     tr = []
     rng = np.random.default_rng(cfg.seed + 7)
-    Lx, Ly = cfg.ni * cfg.dx, cfg.nj * cfg.dx
+    Lx, Ly = cfg.domain[0] * cfg.dx, cfg.domain[1] * cfg.dx
     H = cfg.levels.ztop
     for n in range(cfg.ntracers):
         kind = cfg.tracer_kind

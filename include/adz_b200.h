@@ -356,6 +356,44 @@ int adzc_cfl(adzc_handle *h, const double *wpxyz, double *cfl, int *idx, void *s
 int adzc_state_save(adzc_handle *h, int prec, const void *pxyzm, const double *wpxyz, const char *path);
 int adzc_state_load(adzc_handle *h, int prec, void *pxyzm, double *wpxyz, const char *path);
 
+/* ------------------------------------------------------------------------ */
+/* Halo exchange between tiles                                                */
+/* ------------------------------------------------------------------------ */
+/* The rpn_comm_xch_halo calls of the path, non-periodic, in a 2-D tile
+ * decomposition: the departure winds (B/dynstep.F90:52-53, width
+ * Adz_halox), the tracer sources (B/adz_interp_hlt.F90:87-88, same width)
+ * and Adz_wpxyz (B/adz_traject.F90:121-122, width 2, between the trajectory
+ * and the position sets).  The library packs a tile's halo strips into one
+ * buffer and unpacks the neighbours' strips from another, one launch each;
+ * the caller moves the bytes (NCCL send/recv, MPI, a device copy).
+ *
+ * Neighbours sit in slots q = 3*(dy+1) + (dx+1), dx, dy in -1..1 (dx = +1:
+ * larger i, dy = +1: larger j); slot 4 is the tile itself and is never used.
+ * Segment q of the send buffer holds the strip of this tile's interior that
+ * the neighbour in slot q needs; segment q of the receive buffer is filled
+ * from that neighbour's send segment 8 - q.  Both buffers have the layout
+ * adzc_halo_layout returns.  A strip spans i = 1-hx..0, 1..ni or
+ * ni+1..ni+hx (receive) and 1..hx, 1..ni or ni-hx+1..ni (send) by dx, the
+ * same in j by dy, every plane and every array; inside a segment the order is
+ * array, plane, j, i (i fastest).  Corner strips come from the diagonal
+ * neighbours in the same exchange; inside the global domain this gives what
+ * the two-pass (x, then y) exchange gives.  Absent neighbours (domain edges)
+ * have empty segments and leave the halo untouched. */
+typedef struct {
+  int minx, maxx, miny, maxy;     /* array bounds; the interior is 1..ni, 1..nj    */
+  int ni, nj;
+  long long nplanes;              /* product of the trailing extents (nk, 3*nk)    */
+  int hx, hy;                     /* widths exchanged: 1..1-minx, 1..ni            */
+  int elem;                       /* bytes per element: 4 or 8                     */
+  int nbr[9];                     /* 1 when the neighbour in slot q exists         */
+} adzc_halo;
+#define ADZC_HALO_MAX_ARRAYS 64
+/* off[10]: byte offset of each segment in a buffer, off[9] the total. */
+int adzc_halo_layout(const adzc_halo *x, int narrays, long long *off);
+/* arrays: HOST array of narrays DEVICE pointers (element (minx, miny, 1)). */
+int adzc_halo_pack(const adzc_halo *x, int narrays, const void *const *arrays, void *sendbuf, void *stream);
+int adzc_halo_unpack(const adzc_halo *x, int narrays, void *const *arrays, const void *recvbuf, void *stream);
+
 /* One whole advection step that allocates no device memory.  No counterpart
  * in the reference (its Fortran drivers use automatic arrays).
  *

@@ -1,0 +1,178 @@
+"""Halo exchange between tiles, host side (no GPU): the library's buffer
+layout against the oracle (oracle/halo_oracle.py), argument checks, the
+oracle's pack/route/unpack against its own statement of the exchange, and
+gem_b200.halo's point-to-point transfer as gloo ranks on the CPU (2x2 tiles:
+edge and corner neighbours; 3x1: a rank with two neighbours).  Packing on the
+CPU ranks is the oracle's; the library's pack and unpack kernels are checked
+on the GPU (tests/test_gpu_halo.py)."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+import torch
+import torch.multiprocessing as mp
+
+from oracle import halo_oracle as HO
+
+
+def _desc(ni, nj, bounds, nplanes, hx, hy, elem, nbr):
+    from gem_b200 import halo
+    return halo.AdzcHalo(minx=bounds[0], maxx=bounds[1], miny=bounds[2], maxy=bounds[3], ni=ni, nj=nj,
+                         nplanes=nplanes, hx=hx, hy=hy, elem=elem, nbr=(C.c_int * 9)(*nbr))
+
+
+@pytest.mark.parametrize("ni,nj,h,nplanes,narrays,elem,nbr", [
+    (24, 20, 4, 10, 3, 4, [1] * 9),
+    (17, 33, 2, 6, 1, 8, [0, 1, 0, 1, 0, 1, 0, 0, 0]),
+    (5, 4, 4, 3, 13, 4, [0, 0, 0, 0, 0, 1, 0, 1, 1]),
+    (9, 9, 1, 1, 64, 8, [1, 0, 1, 0, 0, 0, 1, 0, 1]),
+])
+def test_layout_matches_oracle(ni, nj, h, nplanes, narrays, elem, nbr):
+    from gem_b200 import adz
+    d = _desc(ni, nj, (1 - h, ni + h, 1 - h, nj + h), nplanes, h, h, elem, nbr)
+    off = (C.c_longlong * 10)()
+    assert adz.lib().adzc_halo_layout(C.byref(d), narrays, off) == 0
+    nb = [0 if q == 4 else nbr[q] for q in range(9)]
+    assert [o // elem for o in off] == HO.layout(ni, nj, h, h, nplanes, narrays, nb)
+
+
+def test_layout_rejects_bad_descriptors():
+    from gem_b200 import adz
+    off = (C.c_longlong * 10)()
+    ok = dict(ni=8, nj=8, bounds=(-3, 12, -3, 12), nplanes=2, hx=4, hy=4, elem=4, nbr=[1] * 9)
+    assert adz.lib().adzc_halo_layout(C.byref(_desc(**ok)), 1, off) == 0
+    bad = [dict(ok, hx=5), dict(ok, bounds=(-2, 12, -3, 12)), dict(ok, elem=2), dict(ok, nplanes=0),
+           dict(ok, ni=3), dict(ok, bounds=(-3, 11, -3, 12))]
+    for b in bad:
+        assert adz.lib().adzc_halo_layout(C.byref(_desc(**b)), 1, off) == 1, b
+    assert adz.lib().adzc_halo_layout(C.byref(_desc(**ok)), 0, off) == 1
+    assert adz.lib().adzc_halo_layout(C.byref(_desc(**ok)), 65, off) == 1
+
+
+def _tiles(decomp, h, nplanes, narrays, seed, dtype=np.float32):
+    """Tile arrays cut from seeded global arrays (ext bounds 1-h:n+h), with
+    the halo cells inside the domain poisoned with NaN."""
+    rng = np.random.default_rng(seed)
+    G = [rng.standard_normal((nplanes, decomp.gnj + 2 * h, decomp.gni + 2 * h)).astype(dtype)
+         for _ in range(narrays)]
+    out = []
+    for r in range(decomp.size):
+        t = decomp.tile(r)
+        arrs = []
+        for g in G:
+            a = g[:, t.j0g - 1:t.j0g - 1 + t.nj + 2 * h, t.i0g - 1:t.i0g - 1 + t.ni + 2 * h].copy()
+            for j in range(1 - h, t.nj + h + 1):
+                for i in range(1 - h, t.ni + h + 1):
+                    gi, gj = t.i0g - 1 + i, t.j0g - 1 + j
+                    inside = 1 <= i <= t.ni and 1 <= j <= t.nj
+                    if not inside and 1 <= gi <= decomp.gni and 1 <= gj <= decomp.gnj:
+                        a[:, j + h - 1, i + h - 1] = np.nan
+            arrs.append(a)
+        out.append(arrs)
+    return G, out
+
+
+def _expected(decomp, tiles, h, k):
+    bounds_of = lambda ni, nj: (1 - h, ni + h, 1 - h, nj + h)  # noqa: E731
+    tl = [(decomp.tile(r).i0g, decomp.tile(r).j0g, decomp.tile(r).ni, decomp.tile(r).nj, tiles[r][k])
+          for r in range(decomp.size)]
+    return HO.expected(tl, bounds_of, decomp.gni, decomp.gnj, h, h)
+
+
+@pytest.mark.parametrize("gni,gnj,npx,npy", [(23, 17, 3, 2), (12, 30, 1, 3), (16, 16, 2, 2)])
+def test_oracle_route_equals_statement(gni, gnj, npx, npy):
+    from gem_b200.halo import Decomposition
+    D = Decomposition(gni, gnj, npx, npy)
+    h, nplanes, narrays = 3, 4, 2
+    G, tiles = _tiles(D, h, nplanes, narrays, seed=11)
+    bufs = []
+    for r in range(D.size):
+        t = D.tile(r)
+        nbr = [0 if p is None else 1 for p in D.neighbours(r)]
+        bufs.append((HO.pack(tiles[r], (1 - h, t.ni + h, 1 - h, t.nj + h), t.ni, t.nj, h, h, nbr), nbr))
+    for r in range(D.size):
+        t = D.tile(r)
+        nbr = bufs[r][1]
+        off = HO.layout(t.ni, t.nj, h, h, nplanes, narrays, nbr)
+        recv = np.empty(off[9], dtype=np.float32)
+        for q, peer in enumerate(D.neighbours(r)):
+            if peer is None:
+                continue
+            pt = D.tile(peer)
+            poff = HO.layout(pt.ni, pt.nj, h, h, nplanes, narrays, bufs[peer][1])
+            recv[off[q]:off[q + 1]] = bufs[peer][0][poff[8 - q]:poff[9 - q]]
+        HO.unpack(tiles[r], recv, (1 - h, t.ni + h, 1 - h, t.nj + h), t.ni, t.nj, h, h, nbr)
+    for k in range(narrays):
+        exp = _expected(D, tiles, h, k)
+        for r in range(D.size):
+            np.testing.assert_array_equal(tiles[r][k], exp[r])
+            t = D.tile(r)
+            # interior-domain cells equal the global array's
+            g = G[k][:, t.j0g - 1:t.j0g - 1 + t.nj + 2 * h, t.i0g - 1:t.i0g - 1 + t.ni + 2 * h]
+            assert np.array_equal(tiles[r][k], g, equal_nan=True)
+
+
+def test_decomposition_neighbours():
+    from gem_b200.halo import Decomposition, slot
+    D = Decomposition(100, 60, 4, 3)
+    assert sum(D.tile(r).ni for r in range(4)) == 100
+    assert [D.tile(r).i0g for r in range(4)] == [1, 26, 51, 76]
+    for r in range(D.size):
+        for q, p in enumerate(D.neighbours(r)):
+            if p is not None:
+                assert D.neighbours(p)[8 - q] == r
+    assert D.tile(5).edges == (0, 0, 0, 0) and D.tile(0).edges == (1, 0, 1, 0)
+    assert slot(-1, -1) == 0 and slot(1, 1) == 8 and slot(0, 1) == 7
+    assert Decomposition.grid_for(8) == (4, 2) and Decomposition.grid_for(2) == (2, 1)
+
+
+def _worker(rank, ws, port, npx, npy, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(ws), RANK=str(rank))
+    import datetime
+    import torch.distributed as dist
+    from gem_b200 import halo
+    dist.init_process_group("gloo", rank=rank, world_size=ws, timeout=datetime.timedelta(seconds=60))
+    D = halo.Decomposition(21, 14, npx, npy)
+    h, nplanes, narrays = 4, 3, 2
+    _, tiles = _tiles(D, h, nplanes, narrays, seed=5)
+    t = D.tile(rank)
+    bounds = (1 - h, t.ni + h, 1 - h, t.nj + h)
+    nbr = [0 if p is None else 1 for p in D.neighbours(rank)]
+
+    class OracleExchange(halo.HaloExchange):  # the CPU ranks pack with the oracle
+        def pack(self, arrays, stream=None):
+            self.send.copy_(torch.from_numpy(HO.pack([a.numpy() for a in arrays], bounds, t.ni, t.nj, h, h, nbr)))
+
+        def unpack(self, arrays, stream=None):
+            HO.unpack([a.numpy() for a in arrays], self.recv.numpy(), bounds, t.ni, t.nj, h, h, nbr)
+
+    ex = OracleExchange(D, rank, bounds, nplanes, h, h, torch.float32, narrays, device="cpu")
+    mine = [torch.from_numpy(a) for a in tiles[rank]]
+    ex.exchange(mine)
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, [a.numpy() for a in mine]))
+
+
+@pytest.mark.skipif(not torch.distributed.is_gloo_available(), reason="gloo backend missing")
+@pytest.mark.parametrize("npx,npy", [(2, 2), (3, 1)])
+def test_gloo_ranks_exchange(npx, npy):
+    from gem_b200.halo import Decomposition
+    ws = npx * npy
+    port = 29600 + (os.getpid() % 1500) + 7 * npx
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, ws, port, npx, npy, q)) for r in range(ws)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=180) for _ in range(ws))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    D = Decomposition(21, 14, npx, npy)
+    _, tiles = _tiles(D, 4, 3, 2, seed=5)
+    for k in range(2):
+        exp = _expected(D, tiles, 4, k)
+        for r in range(ws):
+            np.testing.assert_array_equal(res[r][k], exp[r])
