@@ -182,7 +182,7 @@ def run_product(args):
     ws, rank, local = dist_init()
     torch.cuda.set_device(local)
     ni, nj, nk = args.size
-    cfg = synth.config_large(ni, nj, nk, seed=tile_seed(rank), ntracers=args.ntr)
+    cfg, tile, decomp = tile_config(args.size, rank, ws, args.ntr)
     npts = cfg.npoints
     inp64 = synth.make_inputs(cfg, device="cuda", dtype=torch.float64)
     keys = ["uu_ext", "vv_ext", "ww_ext", "ut0", "vt0", "zdt0", "src_u", "src_v", "src_w"]
@@ -192,8 +192,9 @@ def run_product(args):
         o["tracers"] = [t.to(dt) for t in d["tracers"]]
         return o
 
-    ad = adz.Adz.from_config(cfg)
+    ad = adz.Adz.from_config(cfg, edges=tile.edges)
     results = {}
+    barrier(ws)  # first collective of the group, before any point-to-point batch
 
     def make_step(prec, data):
         px, wp = ad.new_state(prec)
@@ -201,9 +202,15 @@ def run_product(args):
         dt = adz._field_dtype(prec)
         outs = {k: torch.zeros(ad.ext_shape, dtype=dt, device="cuda") for k in ("u", "v", "w")}
         tro = [torch.zeros(ad.ext_shape, dtype=dt, device="cuda") for _ in data["tracers"]]
+        if ws > 1:  # a tile of one decomposed domain: halo exchanges inside the step
+            from gem_b200.halo import TiledStep
+            tiled = TiledStep(decomp, rank, ad, prec, len(data["tracers"]))
 
-        def step():
-            adz.step_fused(ad, prec, cfg.dt, data, data, data["tracers"], px, wp, outs, tro, cfg.mono)
+            def step():
+                tiled(cfg.dt, data, data, data["tracers"], px, wp, outs, tro, cfg.mono)
+        else:
+            def step():
+                adz.step_fused(ad, prec, cfg.dt, data, data, data["tracers"], px, wp, outs, tro, cfg.mono)
         step()  # cold start: 6 iterations, untimed
         return step, outs, tro
 
@@ -341,7 +348,9 @@ def run_product(args):
         "config": {"workload": f"adz step {ni}x{nj}x{nk} LAM tile, u,v,w+{args.ntr} cosine-bell tracers, "
                                "2 trajectory iterations, dt=60 s, dx=2.5 km, 80 stretched levels",
                    "points_per_step": npts, "l2": "inputs larger than L2 (no flush)", "parallelism":
-                   f"{ws} independent tiles (one per GPU)" if ws > 1 else "1 tile"},
+                   (f"{decomp.npx}x{decomp.npy} tiles of one {decomp.gni}x{decomp.gnj} domain, one per GPU; "
+                    "halo exchange (NCCL send/recv) of winds and sources, then of wpxyz, every step")
+                   if ws > 1 else "1 tile"},
         "fp64_value": npts * ws / (ms64 * 1e-3), "fp64_ms_per_step": ms64, "speedup_vs_fp64": ms64 / ms32,
         "per_launch_ms": per,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -349,7 +358,8 @@ def run_product(args):
         "step_roofline": {"algorithmic_bytes_per_point": step_bytes / npts,
                           "achieved_gbs": step_bytes / (ms32 * 1e-3) / 1e9,
                           "frac": step_bytes / (ms32 * 1e-3) / 1e9 / hbm},
-        "e2e": e2e, "gpu_launches": LAUNCHES_PER_STEP * args.steps, "clocks": clk, "cpu_baseline": cpu,
+        "e2e": e2e, "gpu_launches": (LAUNCHES_PER_STEP + (HALO_LAUNCHES_PER_STEP if ws > 1 else 0)) * args.steps,
+        "clocks": clk, "cpu_baseline": cpu,
         "tracers8": tsum, "post": psum, "batch": batch, "learned_guess": gsum,
     }
     if rank == 0:
@@ -361,6 +371,22 @@ def run_product(args):
 # kernels of one MIXED step: departure winds, trajectory, and one
 # interpolation launch per position set (u, v, then w + tracers at thermo points)
 LAUNCHES_PER_STEP = 5
+HALO_LAUNCHES_PER_STEP = 4  # pack + unpack of the two exchanges (N > 1)
+
+
+def tile_config(size, rank, ws, ntr):
+    """The bench tile of a rank: one ni x nj x nk tile of an (npx ni) x
+    (npy nj) domain cut into npx x npy = ws tiles, the flow and tracers
+    functions of the global position, the noise seeded per rank."""
+    from gem_b200 import synth
+    from gem_b200.halo import Decomposition
+    ni, nj, nk = size
+    npx, npy = Decomposition.grid_for(ws)
+    decomp = Decomposition(ni * npx, nj * npy, npx, npy)
+    tile = decomp.tile(rank)
+    cfg = synth.config_large(ni, nj, nk, seed=tile_seed(rank), ntracers=ntr)
+    cfg.gi0, cfg.gj0, cfg.gni, cfg.gnj = tile.i0g, tile.j0g, decomp.gni, decomp.gnj
+    return cfg, tile, decomp
 
 
 def measure_batch(args, timed, ws, cfgs, label):

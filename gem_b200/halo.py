@@ -167,12 +167,13 @@ class HaloExchange:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
 
-    def exchange(self, arrays, stream=None):
-        """pack, transfer, unpack: the halos of ``arrays`` now hold the
-        neighbours' interior values."""
-        self.pack(arrays, stream)
+    def exchange(self, arrays):
+        """pack, transfer, unpack on the current stream (the one the
+        point-to-point batch orders itself after): the halos of ``arrays``
+        now hold the neighbours' interior values."""
+        self.pack(arrays)
         self.transfer()
-        self.unpack(arrays, stream)
+        self.unpack(arrays)
 
 
 def ext_exchange(decomp: Decomposition, rank: int, ad: A.Adz, dtype, narrays: int, device="cuda", group=None):
@@ -187,3 +188,38 @@ def wpxyz_exchange(decomp: Decomposition, rank: int, ad: A.Adz, device="cuda", g
     """Exchange of Adz_wpxyz (-1:ni+2, -1:nj+2, nk, 3), width 2."""
     bounds = (-1, ad.ni + 2, -1, ad.nj + 2)
     return HaloExchange(decomp, rank, bounds, 3 * ad.nk, 2, 2, torch.float64, 1, device, group)
+
+
+WIND_KEYS = ("uu_ext", "vv_ext", "ww_ext", "ut0", "vt0", "zdt0")
+
+
+class TiledStep:
+    """One advection step of a tile of a decomposed domain (adz_main with its
+    halo exchanges):
+
+    1. exchange the winds and the sources (width Adz_halox): departure winds
+       as dynstep.F90:52-53, sources as adz_interp_hlt.F90:87-88, and the
+       arrival winds, whose halo the host model fills with its own exchange
+       before the step;
+    2. adzc_traject;
+    3. exchange Adz_wpxyz, width 2 (adz_traject.F90:121-122);
+    4. adzc_tricub_sets: u@pmu, v@pmv, w and the tracers @pt.
+
+    Packing, unpacking and the step run on the current CUDA stream; the
+    transfers are torch.distributed point-to-point batches in the
+    process group ``group``."""
+
+    def __init__(self, decomp: Decomposition, rank: int, ad: A.Adz, prec: int, ntracers: int, device="cuda",
+                 group=None):
+        self.ad, self.prec = ad, prec
+        self.ex = ext_exchange(decomp, rank, ad, A._field_dtype(prec), len(WIND_KEYS) + 3 + ntracers, device, group)
+        self.exw = wpxyz_exchange(decomp, rank, ad, device, group)
+
+    def __call__(self, dt, winds, fields, tracers, pxyzm, wpxyz, outs, tr_outs, mono, niter=0):
+        srcs = [fields["src_u"], fields["src_v"], fields["src_w"]] + list(tracers)
+        self.ex.exchange([winds[k] for k in WIND_KEYS] + srcs)
+        self.ad.adz_traject(self.prec, dt, winds, pxyzm, wpxyz, niter)
+        self.exw.exchange([wpxyz])
+        dsts = [outs["u"], outs["v"], outs["w"]] + list(tr_outs)
+        monos = [0, 0, 0] + [1 if mono else 0] * len(tracers)
+        self.ad.adz_tricub_sets(self.prec, [0, 1, 1, 1 + len(tracers)], srcs, dsts, monos)

@@ -176,3 +176,19 @@ def test_gloo_ranks_exchange(npx, npy):
         exp = _expected(D, tiles, 4, k)
         for r in range(ws):
             np.testing.assert_array_equal(res[r][k], exp[r])
+
+
+@pytest.mark.parametrize("ws", [1, 2, 4, 8])
+def test_bench_tiles_form_one_domain(ws):
+    import bench
+    tiles = [bench.tile_config((64, 48, 10), r, ws, 2) for r in range(ws)]
+    decomp = tiles[0][2]
+    assert decomp.size == ws and decomp.gni == 64 * decomp.npx and decomp.gnj == 48 * decomp.npy
+    seen = set()
+    for r, (cfg, tile, _) in enumerate(tiles):
+        assert (cfg.ni, cfg.nj, cfg.nk) == (64, 48, 10) and (tile.ni, tile.nj) == (64, 48)
+        assert (cfg.gi0, cfg.gj0, cfg.gni, cfg.gnj) == (tile.i0g, tile.j0g, decomp.gni, decomp.gnj)
+        seen.add((tile.i0g, tile.j0g))
+    assert len(seen) == ws and len({c.seed for c, _, _ in tiles}) == ws
+    if ws == 1:
+        assert tiles[0][1].edges == (1, 1, 1, 1)
