@@ -34,6 +34,14 @@
 #else
 #define ADZ_SET_BOUNDS __launch_bounds__(128)
 #endif
+#ifndef ADZ_QV_MINB
+#define ADZ_QV_MINB 0
+#endif
+#if ADZ_QV_MINB > 0
+#define ADZ_QV_BOUNDS __launch_bounds__(128, ADZ_QV_MINB)
+#else
+#define ADZ_QV_BOUNDS __launch_bounds__(128)
+#endif
 
 // MIXED stores the departure winds as three component planes (u, v, w) instead
 // of interleaved triplets: each component gather is then a run of consecutive
@@ -605,7 +613,7 @@ __device__ __forceinline__ void qv_point(const DGrid& g, const SetArgs& a, const
 }
 
 template <int PREC>
-__global__ void __launch_bounds__(128) k_qv_set(DGrid g, int i0, int nx, int j0, int ny, int k0, int nz, SetArgs a,
+__global__ void ADZ_QV_BOUNDS k_qv_set(DGrid g, int i0, int nx, int j0, int ny, int k0, int nz, SetArgs a,
                                                 FieldPtrs fp) {
   const long long nplane = (long long)nx * ny;
   const long long n = nplane * nz;
