@@ -103,6 +103,8 @@ def lib() -> C.CDLL:
         L.adzc_batch_tune.argtypes = [vp, vp]
         L.adzc_batch_step.argtypes = [vp, vp]
         L.adzc_batch_query.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
+        L.adzc_batch_plan.argtypes = [vp, C.POINTER(C.c_int)]
+        L.adzc_batch_select.argtypes = [vp, i, i]
         L.adzc_batch_status.argtypes = [vp, i, vp]
         L.adzc_batch_destroy.argtypes = [vp]
         L.adzc_bermejo_conde.argtypes = [vp, i, i, vp, vp, vp, vp, i, vp, vp, vp]
@@ -383,10 +385,19 @@ class Batch:
     def step(self, stream=None):
         _check(lib().adzc_batch_step(self.h, _stream(stream)), "adzc_batch_step")
 
+    PHASED = 3  # plan of select(): one persistent launch per phase
+
+    def select(self, rows: int, plan: int):
+        """Pin a plan: rows per work item and 0..2 (register budget of the
+        one-launch kernel) or Batch.PHASED."""
+        _check(lib().adzc_batch_select(self.h, int(rows), int(plan)), "adzc_batch_select")
+
     def query(self):
-        r, b, n = C.c_int(), C.c_int(), C.c_longlong()
+        r, b, n, p = C.c_int(), C.c_int(), C.c_longlong(), C.c_int()
         _check(lib().adzc_batch_query(self.h, C.byref(r), C.byref(b), C.byref(n)), "adzc_batch_query")
-        return {"rows_per_item": r.value, "blocks_per_sm": b.value, "items": n.value}
+        _check(lib().adzc_batch_plan(self.h, C.byref(p)), "adzc_batch_plan")
+        return {"rows_per_item": r.value, "blocks_per_sm": b.value, "items": n.value,
+                "plan": "phased (one launch per phase)" if p.value else "one launch"}
 
     def status(self, reset=True, stream=None) -> int:
         return lib().adzc_batch_status(self.h, 1 if reset else 0, _stream(stream))

@@ -16,6 +16,11 @@
 // (rows * row length points); adzc_batch_tune times candidate row counts and
 // resident block counts and keeps the fastest.  The tuned launch is captured
 // in a CUDA graph (counter reset + persistent kernel) and replayed per step.
+//
+// The phased plan runs the same items as three persistent launches in the
+// graph, one per phase, each kernel with the register budget of the
+// per-domain kernel of its phase; launch order replaces the dependency waits.
+// The tuner weighs it against the one-launch kernel's budgets.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,6 +50,9 @@ struct adzc_batch {
   unsigned* d_done = nullptr;
   int* d_status = nullptr;
   int rows = 8, bps = 4, sms = 148, variant = 0;
+  int phased = 0;           // the phased plan: one launch per phase
+  long long pstart[4] = {}; // first item of each phase, total
+  int pgrid[3] = {};        // persistent grid of each phased launch
   cudaStream_t cap = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -56,6 +64,7 @@ int build_items(adzc_batch* b, int rows) {
   std::vector<adz::BItem> items;
   std::vector<unsigned> need(2 * b->ndom, 0);
   for (int phase = 0; phase < 3; phase++) {
+    b->pstart[phase] = (long long)items.size();
     for (int d = 0; d < b->ndom; d++) {
       const adz::BDom& D = b->doms[d];
       auto push = [&](int group, long long n, long long chunk) {
@@ -89,12 +98,21 @@ int build_items(adzc_batch* b, int rows) {
       cudaMemcpy(b->d_need, need.data(), need.size() * sizeof(unsigned), cudaMemcpyHostToDevice) != cudaSuccess)
     return ADZC_ERR_CUDA;
   b->nitems = (long long)items.size();
+  b->pstart[3] = b->nitems;
   b->rows = rows;
   return ADZC_OK;
 }
 
 cudaError_t enqueue(adzc_batch* b, cudaStream_t s) {
   cudaError_t e;
+  if (b->phased) {
+    if ((e = cudaMemsetAsync(b->d_next + 1, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
+    if (b->prec == ADZC_FP64)
+      return adz::launch_batch_phased<adz::kFp64>(b->pgrid, *b->params, b->d_doms, b->d_items, b->pstart,
+                                                  b->d_next + 1, s);
+    return adz::launch_batch_phased<adz::kMixed>(b->pgrid, *b->params, b->d_doms, b->d_items, b->pstart,
+                                                 b->d_next + 1, s);
+  }
   if ((e = cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(b->d_done, 0, 2 * b->ndom * sizeof(unsigned), s)) != cudaSuccess) return e;
   const int grid = b->bps * b->sms;
@@ -165,6 +183,11 @@ extern "C" int adzc_batch_create(int prec, int ndom, const adzc_domain* doms, ad
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
   b->bps = std::max(1, resident(b, 0));
+  for (int p = 0; p < 3; p++) {
+    const int r = b->prec == ADZC_FP64 ? adz::batch_phase_resident_blocks<adz::kFp64>(p)
+                                       : adz::batch_phase_resident_blocks<adz::kMixed>(p);
+    b->pgrid[p] = std::max(1, r) * b->sms;
+  }
   for (int d = 0; d < ndom; d++) {
     const adzc_domain& in = doms[d];
     adz::BDom& D = b->doms[d];
@@ -263,7 +286,7 @@ extern "C" int adzc_batch_create(int prec, int ndom, const adzc_domain* doms, ad
   }
   if (cudaMalloc(&b->d_doms, ndom * sizeof(adz::BDom)) != cudaSuccess ||
       cudaMalloc(&b->d_need, 2 * ndom * sizeof(unsigned)) != cudaSuccess ||
-      cudaMalloc(&b->d_next, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&b->d_next, 4 * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&b->d_done, 2 * ndom * sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&b->d_status, sizeof(int)) != cudaSuccess ||
       cudaMemcpy(b->d_doms, b->doms.data(), ndom * sizeof(adz::BDom), cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -294,16 +317,22 @@ extern "C" int adzc_batch_tune(adzc_batch* b, void* stream) {
   const cudaStream_t s = (cudaStream_t)stream;
   const int rows_c[] = {2, 8, 32};
   float best = 1e30f;
-  int br = b->rows, bb = b->bps, bv = b->variant;
+  int br = b->rows, bb = b->bps, bv = b->variant, bp = b->phased;
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
   int st = ADZC_OK;
-  for (int v = 0; v < adz::kBatchVariants && st == ADZC_OK; v++) {
-    const int res = resident(b, v);  // persistent: every block resident
+  // variants 0..kBatchVariants-1: the one-launch kernel's register budgets;
+  // kBatchVariants: the phased plan
+  for (int v = 0; v <= adz::kBatchVariants && st == ADZC_OK; v++) {
+    const bool ph = v == adz::kBatchVariants;
+    const int res = ph ? b->bps : resident(b, v);  // persistent: every block resident
     if (res < 1) continue;
     for (int r : rows_c) {
-      b->variant = v;
-      b->bps = res;
+      b->phased = ph ? 1 : 0;
+      if (!ph) {
+        b->variant = v;
+        b->bps = res;
+      }
       if (build_items(b, r) != ADZC_OK || enqueue(b, s) != cudaSuccess) {
         st = ADZC_ERR_CUDA;
         break;
@@ -320,8 +349,11 @@ extern "C" int adzc_batch_tune(adzc_batch* b, void* stream) {
       if (ms < best) {
         best = ms;
         br = r;
-        bb = res;
-        bv = v;
+        bp = ph ? 1 : 0;
+        if (!ph) {
+          bb = res;
+          bv = v;
+        }
       }
     }
   }
@@ -329,6 +361,7 @@ extern "C" int adzc_batch_tune(adzc_batch* b, void* stream) {
   cudaEventDestroy(e1);
   b->bps = bb;
   b->variant = bv;
+  b->phased = bp;
   if (st == ADZC_OK) st = build_items(b, br);
   if (st == ADZC_OK) st = capture(b);
   record(b);
@@ -338,8 +371,30 @@ extern "C" int adzc_batch_tune(adzc_batch* b, void* stream) {
 extern "C" int adzc_batch_query(const adzc_batch* b, int* rows, int* blocks_per_sm, long long* nitems) {
   if (!b) return adz_internal_fail(ADZC_ERR_ARG);
   if (rows) *rows = b->rows;
-  if (blocks_per_sm) *blocks_per_sm = b->bps;
+  if (blocks_per_sm) *blocks_per_sm = b->phased ? b->pgrid[1] / b->sms : b->bps;
   if (nitems) *nitems = b->nitems;
+  return ADZC_OK;
+}
+
+extern "C" int adzc_batch_select(adzc_batch* b, int rows, int plan) {
+  if (!b || rows < 1 || plan < 0 || plan > adz::kBatchVariants) return adz_internal_fail(ADZC_ERR_ARG);
+  if (plan < adz::kBatchVariants) {
+    const int res = resident(b, plan);
+    if (res < 1) return adz_internal_fail(ADZC_ERR_ARG);
+    b->variant = plan;
+    b->bps = res;
+    b->phased = 0;
+  } else {
+    b->phased = 1;
+  }
+  int st = build_items(b, rows);
+  if (st == ADZC_OK) st = capture(b);
+  return st == ADZC_OK ? ADZC_OK : adz_internal_fail(st);
+}
+
+extern "C" int adzc_batch_plan(const adzc_batch* b, int* phased) {
+  if (!b || !phased) return adz_internal_fail(ADZC_ERR_ARG);
+  *phased = b->phased;
   return ADZC_OK;
 }
 

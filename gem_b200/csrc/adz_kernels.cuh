@@ -781,6 +781,74 @@ __global__ void __launch_bounds__(128, MINB) k_batch(const __grid_constant__ Bat
   }
 }
 
+// One phase of the batch per launch (the phased plan).  The previous phase
+// of every domain completed with the previous launch, so there is no
+// dependency wait, and data it wrote is read through the read-only path.
+template <int PREC, int PH>
+__device__ __forceinline__ void batch_phase_body(const BatchParams& P, const BDom* __restrict__ doms,
+                                                 const BItem* __restrict__ items, long long nitems,
+                                                 unsigned long long* __restrict__ next) {
+  __shared__ long long cur;
+  __shared__ FieldPtrs sfp;
+  __shared__ int sset, srange[5];
+  for (;;) {
+    if (threadIdx.x == 0) cur = (long long)atomicAdd(next, 1ull);
+    __syncthreads();
+    const long long it = cur;
+    if (it >= nitems) break;
+    const BItem item = items[it];
+    if (PH == 2) {
+      const BDom& D = doms[item.dom];
+      block_copy(&sfp, &D.gfp[item.group]);
+      if (threadIdx.x < 5) srange[threadIdx.x] = D.grange[item.group][threadIdx.x];
+      if (threadIdx.x == 5) sset = D.gset[item.group];
+      __syncthreads();
+    }
+    const BDomC& C = P.d[item.dom];
+    const long long end = item.start + item.count;
+    if (PH == 0) {
+      using F = typename Types<PREC>::F;
+      for (long long e = item.start + threadIdx.x; e < end; e += blockDim.x)
+        prepare_cell<PREC>(C.g, (const F*)C.uu, (const F*)C.vv, (const F*)C.ww, (F*)C.ta.uvw_d, e);
+    } else if (PH == 1) {
+      const long long plane = (long long)C.g.ni * C.g.nj;
+      for (long long t = item.start + threadIdx.x; t < end; t += blockDim.x) {
+        const int i = (int)(t % C.g.ni) + 1, j = (int)((t / C.g.ni) % C.g.nj) + 1;
+        const int k = (int)(t / plane) + C.ta.k00;
+        traject_point<PREC, false>(C.g, C.ta, i, j, k);
+      }
+    } else {
+      const int nx = srange[1], ny = srange[3];
+      const long long plane = (long long)nx * ny;
+      for (long long t = item.start + threadIdx.x; t < end; t += blockDim.x) {
+        const int i = (int)(t % nx) + srange[0], j = (int)((t / nx) % ny) + srange[2];
+        const int k = (int)(t / plane) + srange[4];
+        set_point<PREC, false>(C.g, sset, C.sa, sfp, i, j, k);
+      }
+    }
+    __syncthreads();  // every thread is done with cur and sfp
+  }
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(128) k_batch_p0(const __grid_constant__ BatchParams P, const BDom* __restrict__ doms,
+                                                  const BItem* __restrict__ items, long long nitems,
+                                                  unsigned long long* __restrict__ next) {
+  batch_phase_body<PREC, 0>(P, doms, items, nitems, next);
+}
+template <int PREC>
+__global__ void ADZ_TRAJ_BOUNDS k_batch_p1(const __grid_constant__ BatchParams P, const BDom* __restrict__ doms,
+                                           const BItem* __restrict__ items, long long nitems,
+                                           unsigned long long* __restrict__ next) {
+  batch_phase_body<PREC, 1>(P, doms, items, nitems, next);
+}
+template <int PREC>
+__global__ void ADZ_SET_BOUNDS k_batch_p2(const __grid_constant__ BatchParams P, const BDom* __restrict__ doms,
+                                          const BItem* __restrict__ items, long long nitems,
+                                          unsigned long long* __restrict__ next) {
+  batch_phase_body<PREC, 2>(P, doms, items, nitems, next);
+}
+
 // ---------------------------------------------------------------------------
 // launchers (host)
 inline int grid_for(long long n, int block, int max_blocks = 148 * 64) {
@@ -875,6 +943,36 @@ cudaError_t launch_batch(int variant, int grid, const BatchParams& P, const BDom
 }
 
 template <int PREC>
+cudaError_t launch_batch_phased(const int* grid, const BatchParams& P, const BDom* doms, const BItem* items,
+                                const long long* pstart, unsigned long long* next, cudaStream_t s) {
+  if constexpr (PREC == kRef32) {
+    return cudaErrorNotSupported;
+  } else {
+    if (pstart[1] > pstart[0])
+      k_batch_p0<PREC><<<grid[0], 128, 0, s>>>(P, doms, items + pstart[0], pstart[1] - pstart[0], next);
+    if (pstart[2] > pstart[1])
+      k_batch_p1<PREC><<<grid[1], 128, 0, s>>>(P, doms, items + pstart[1], pstart[2] - pstart[1], next + 1);
+    if (pstart[3] > pstart[2])
+      k_batch_p2<PREC><<<grid[2], 128, 0, s>>>(P, doms, items + pstart[2], pstart[3] - pstart[2], next + 2);
+    return cudaGetLastError();
+  }
+}
+
+template <int PREC>
+int batch_phase_resident_blocks(int phase) {
+  if constexpr (PREC == kRef32) {
+    return 0;
+  } else {
+    const void* f = phase == 0 ? (const void*)k_batch_p0<PREC>
+                    : phase == 1 ? (const void*)k_batch_p1<PREC>
+                                 : (const void*)k_batch_p2<PREC>;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, 128, 0) != cudaSuccess) return 0;
+    return n;
+  }
+}
+
+template <int PREC>
 int batch_resident_blocks(int variant) {
   if constexpr (PREC == kRef32) {
     return 0;
@@ -902,6 +1000,9 @@ int batch_resident_blocks(int variant) {
   template cudaError_t launch_batch<P>(int, int, const BatchParams&, const BDom*, const BItem*, long long,       \
                                        const unsigned*,                                                             \
                                        unsigned long long*, unsigned*, int*, cudaStream_t);                        \
-  template int batch_resident_blocks<P>(int);
+  template int batch_resident_blocks<P>(int);                                                                   \
+  template cudaError_t launch_batch_phased<P>(const int*, const BatchParams&, const BDom*, const BItem*,           \
+                                              const long long*, unsigned long long*, cudaStream_t);                \
+  template int batch_phase_resident_blocks<P>(int);
 
 }  // namespace adz

@@ -176,5 +176,13 @@ cudaError_t launch_batch(int variant, int grid, const BatchParams& P, const BDom
                          cudaStream_t s);
 template <int PREC>
 int batch_resident_blocks(int variant);  // blocks of 128 threads resident per SM
+// the phased plan: one persistent launch per phase (items[pstart[p], pstart[p+1])),
+// each with the register budget of the per-domain kernel of that phase;
+// next[3] are the phases' queue counters
+template <int PREC>
+cudaError_t launch_batch_phased(const int* grid, const BatchParams& P, const BDom* doms, const BItem* items,
+                                const long long* pstart, unsigned long long* next, cudaStream_t s);
+template <int PREC>
+int batch_phase_resident_blocks(int phase);
 
 }  // namespace adz

@@ -209,7 +209,11 @@ int adzc_status(adzc_handle *h, int reset, void *stream);
  * start (adzc_inittraj + one adzc_traject).  The batch steps every domain as
  * adzc_traject + adzc_tricub on each set would (B/adz_main.F90 and
  * B/adz_tracers.F90 for many limited-area domains at once) in ONE persistent
- * kernel launch, replayed from a CUDA graph.  ADZC_FP64 or ADZC_MIXED. */
+ * kernel launch, replayed from a CUDA graph.  ADZC_FP64 or ADZC_MIXED.
+ * The autotuner may instead pick the phased plan: three persistent launches
+ * per step in the same graph (departure winds, trajectories, interpolations
+ * of every domain), each with the register budget of the per-domain kernel
+ * of that phase. */
 typedef struct {
   adzc_handle *h;
   double dt;
@@ -226,12 +230,20 @@ typedef struct adzc_batch adzc_batch;
 
 #define ADZC_BATCH_MAX_DOMAINS 40  /* more: ADZC_ERR_SIZE */
 int adzc_batch_create(int prec, int ndom, const adzc_domain *doms, adzc_batch **out);
-/* autotuner: times candidate tile heights (rows per work item) and resident
- * blocks per SM on these domains, keeps the fastest and re-captures the graph.
- * The timed launches are real steps: they advance the domains' positions. */
+/* autotuner: times candidate tile heights (rows per work item), register
+ * budgets (resident blocks per SM) of the one-launch kernel and the phased
+ * plan on these domains, keeps the fastest and re-captures the graph.  The
+ * timed launches are real steps: they advance the domains' positions. */
 int adzc_batch_tune(adzc_batch *b, void *stream);
 int adzc_batch_step(adzc_batch *b, void *stream);
+/* the plan in use; blocks_per_sm of the one-launch kernel (phased plan: of
+ * its trajectory launch); phased: 1 for the phased plan (may be NULL) */
 int adzc_batch_query(const adzc_batch *b, int *rows_per_item, int *blocks_per_sm, long long *nitems);
+int adzc_batch_plan(const adzc_batch *b, int *phased);
+/* pin a plan instead of tuning: rows per work item, plan 0..2 = register
+ * budget of the one-launch kernel, 3 = phased; re-captures the graph */
+#define ADZC_BATCH_PHASED 3
+int adzc_batch_select(adzc_batch *b, int rows_per_item, int plan);
 /* synchronises; ADZC_ERR_TIMEOUT when a dependency wait gave up, else the
  * first non-zero status of the domains' handles */
 int adzc_batch_status(adzc_batch *b, int reset, void *stream);

@@ -69,8 +69,11 @@ def _compare(a, b, what):
         assert np.array_equal(_bits(x), _bits(y)), f"{what}: array {q} differs"
 
 
-@pytest.mark.parametrize("precname", ["mixed", "fp64"])
-def test_batch_matches_per_domain_steps(precname):
+@pytest.mark.parametrize("precname,plan", [("mixed", None), ("fp64", None), ("mixed", (8, 2)), ("mixed", (2, 3)),
+                                           ("fp64", (32, 3))])
+def test_batch_matches_per_domain_steps(precname, plan):
+    """plan None: the default one-launch plan; (rows, 0..2): that register
+    budget of the one-launch kernel; (rows, 3): the phased plan."""
     from gem_b200 import adz as A
     prec = A.PREC_NAMES[precname]
     adz, doms = _domains(prec)
@@ -78,8 +81,13 @@ def test_batch_matches_per_domain_steps(precname):
     wps_b = [wp.clone() for (_, _, _, wp) in doms]
     outs_b = [_outs(ad, inp, dt) for (_, ad, inp, _) in doms]
     batch = _batch(adz, prec, doms, wps_b, outs_b)
+    if plan is not None:
+        batch.select(*plan)
     q = batch.query()
     assert q["items"] > 0 and q["blocks_per_sm"] >= 1
+    assert q["plan"].startswith("phased") == (plan is not None and plan[1] == adz.Batch.PHASED)
+    if plan is not None:
+        assert q["rows_per_item"] == plan[0]
     for step in range(2):
         batch.step()
         assert batch.status() == 0
@@ -132,6 +140,10 @@ def test_batch_rejects_bad_domains():
     outs = [_outs(ad, inp, dt) for (_, ad, inp, _) in doms]
     with pytest.raises(adz.AdzError):
         adz.Batch(A.REF32, [])  # no domains / REF32 not batched
+    ok = _batch(adz, A.MIXED, doms, wps, outs)
+    for rows, plan in ((0, 0), (8, -1), (8, 4)):
+        with pytest.raises(adz.AdzError):
+            ok.select(rows, plan)
     # a handle still in its cold start is refused
     cfg, _, inp, _ = doms[0]
     fresh = adz.Adz.from_config(cfg)
