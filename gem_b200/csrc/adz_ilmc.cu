@@ -8,8 +8,8 @@
 // results.  This file keeps that order exactly and still runs in parallel.
 // A visit reads and writes only the cube of radius S = sweep_max around its
 // point, so a visit can depend only on earlier points within R = 2 S
-// (Chebyshev).  The region is cut into tiles of one row and 8 columns
-// (8 >= R for S <= 4), numbered (k, j, it); every earlier point within R of a
+// (Chebyshev).  The region is cut into tiles of one row and R columns,
+// numbered (k, j, it); every earlier point within R of a
 // tile's point lies in the same tile (handled in order by one thread) or in a
 // tile of strictly smaller wavefront number
 //     t = (2 R + 2) k + 2 j + it
@@ -18,8 +18,15 @@
 // Tiles of one wavefront therefore never interact, and running the wavefronts
 // in increasing t, each tile by one warp in loop order, reproduces the
 // sequential result bit for bit.  Within a visit the lanes split the shell's
-// loads and updates; lane 0 forms the capacity sum in the reference's order.  The reference's visit of a point inside its
-// bounds does nothing, so each thread visits only the points it finds outside.
+// loads and updates; lane 0 forms the capacity sum in the reference's order.
+//
+// A visit moves a neighbour only toward its bounds (it gains up to its max or
+// loses down to its min) and its own point into them, so a point inside its
+// bounds when the filter starts stays inside, and the reference's visit of it
+// does nothing.  Candidate tiles (a point outside its bounds at the start)
+// are therefore listed per wavefront once (count, scan, scatter), each wave
+// launch visits only its listed tiles, and a warp loads a tile's 8 points at
+// once and visits, in order, only those that were outside.
 // Built with -fmad=false: the REAL arithmetic is the reference's, without
 // contraction.
 #include <cuda_runtime.h>
@@ -34,7 +41,6 @@
 namespace adz {
 namespace ilmc {
 
-constexpr int kMaxShell = 400;  // sweep_max <= 4 (the reference's sweep_max(400))
 
 struct Box {
   int il, ir, jl, jr, k0, nk;
@@ -60,8 +66,10 @@ __device__ __forceinline__ T rmax(T a, T b) { return a > b ? a : b; }
 template <typename T>
 __device__ __forceinline__ T rmin(T a, T b) { return a < b ? a : b; }
 
-constexpr int kTile = 8;    // columns per tile, >= R = 2 sweep_max for sweep_max <= 4
 constexpr int kWarps = 4;   // tiles (warps) per block of k_wave
+// columns per tile: R = 2 sweep_max, the narrowest width the wavefront order
+// allows (a tile's visits are sequential, so narrow tiles shorten each wave)
+inline int tile_width(int sweep_max) { return 2 * sweep_max; }
 
 template <typename T>
 struct Fields {
@@ -108,9 +116,11 @@ __device__ void visit_warp(const Box& b, T* f, const T* mn, const T* mx, const T
     T ratio = 0;
     int go = 0;
     if (lane == 0) {
+      // the reference skips cells outside the region; their prod is +0 and
+      // msum >= +0, so adding it leaves msum unchanged bit for bit
       T msum = 0;
-      for (int q = 0; q < nq; q++)
-        if (cell[q] >= 0) msum = prod[q] + msum;
+#pragma unroll 8
+      for (int q = 0; q < nq; q++) msum = prod[q] + msum;
       const T use = rmin(msum, (over ? o_shoot : u_shoot) * air[e]);
       if (use > (T)0) {
         if (over) {
@@ -138,30 +148,98 @@ __device__ void visit_warp(const Box& b, T* f, const T* mn, const T* mx, const T
   }
 }
 
-// one wavefront t: warp (tracer, level, tile column) finds its row from t
-template <typename T>
-__global__ void __launch_bounds__(32 * kWarps) k_wave(Box b, Fields<T> fl, int ntr, const T* __restrict__ air,
-                                                      int sweep_max, int t, int c1, int ntile) {
-  __shared__ T s_cap[kWarps][kMaxShell];
-  __shared__ T s_prod[kWarps][kMaxShell];
-  __shared__ long long s_cell[kWarps][kMaxShell];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+// tile id (tracer, level, tile column) and the row it has in wavefront t
+__device__ __forceinline__ int tile_row(int t, int c1, int kk, int it) { return (t - c1 * kk - it) >> 1; }
+
+// candidate tiles per wavefront.  pass 0 counts them, pass 1 lists their ids
+// (order inside a wave is free: its tiles never interact)
+template <typename T, int PASS>
+__global__ void __launch_bounds__(256) k_candidates(Box b, Fields<T> fl, int ntr, int c1, int ntile, int tw,
+                                                    int* __restrict__ count, const int* __restrict__ wstart,
+                                                    int* __restrict__ list) {
   const int nz = b.nk - b.k0 + 1, ny = b.by();
-  const long long n = (long long)ntr * nz * ntile;
-  for (long long g = (long long)blockIdx.x * kWarps + w; g < n; g += (long long)gridDim.x * kWarps) {
+  const long long n = (long long)ntr * nz * ny * ntile;
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < n; g += (long long)gridDim.x * blockDim.x) {
     const int it = (int)(g % ntile);
-    const int kk = (int)((g / ntile) % nz);
-    const int tr = (int)(g / ((long long)ntile * nz));
-    const int rem = t - c1 * kk - it;
-    if (rem < 0 || (rem & 1) || (rem >> 1) >= ny) continue;  // warp-uniform
-    const int j = b.jl + (rem >> 1), k = b.k0 + kk;
-    const int i0 = b.il + it * kTile, i1 = min(i0 + kTile - 1, b.ir);
+    const int jr = (int)((g / ntile) % ny);
+    const long long rest = g / ((long long)ntile * ny);
+    const int kk = (int)(rest % nz), tr = (int)(rest / nz);
+    const int j = b.jl + jr, k = b.k0 + kk;
+    const int i0 = b.il + it * tw, i1 = min(i0 + tw - 1, b.ir);
+    const T* f = fl.f[tr];
+    const T* mn = fl.mn[tr];
+    const T* mx = fl.mx[tr];
+    bool any = false;
+    for (int i = i0; i <= i1; i++) {
+      const long long e = ext(b, i, j, k);
+      const T v = f[e];
+      any |= (v > mx[e]) || (v < mn[e]);
+    }
+    if (!any) continue;
+    const int t = c1 * kk + 2 * jr + it;
+    if (PASS == 0) {
+      atomicAdd(count + t, 1);
+    } else {
+      list[wstart[t] + atomicAdd(count + t, 1)] = (tr * nz + kk) * ntile + it;
+    }
+  }
+}
+
+// exclusive scan of the per-wave counts (one block): wstart[0..n]
+__global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ count, int n, int* __restrict__ wstart) {
+  __shared__ int part[1024];
+  const int per = (n + 1023) / 1024, a = threadIdx.x * per, z = min(a + per, n);
+  int sum = 0;
+  for (int q = a; q < z; q++) sum += count[q];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {  // inclusive Hillis-Steele
+    const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = part[threadIdx.x] - sum;
+  for (int q = a; q < z; q++) {
+    wstart[q] = run;
+    run += count[q];
+  }
+  if (threadIdx.x == 1023) wstart[n] = part[1023];
+}
+
+// one wavefront t: a warp per listed tile, its points in loop order
+template <typename T>
+__global__ void __launch_bounds__(32 * kWarps) k_wave(Box b, Fields<T> fl, const T* __restrict__ air, int sweep_max,
+                                                      int t, int c1, int ntile, int tw, int nshell,
+                                                      const int* __restrict__ wstart, const int* __restrict__ list) {
+  // dynamic shared memory: cell[kWarps][nshell] (8 B), then cap and prod
+  // [kWarps][2][nshell] (T)
+  extern __shared__ long long s_dyn[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  long long* s_cell = s_dyn + (size_t)w * nshell;
+  T* s_cap = reinterpret_cast<T*>(s_dyn + (size_t)kWarps * nshell) + (size_t)w * 2 * nshell;
+  T* s_prod = s_cap + nshell;
+  const int nz = b.nk - b.k0 + 1;
+  const int beg = wstart[t], end = wstart[t + 1];
+  for (int q = beg + blockIdx.x * kWarps + w; q < end; q += gridDim.x * kWarps) {
+    const int id = list[q];
+    const int it = id % ntile, kk = (id / ntile) % nz, tr = id / (ntile * nz);
+    const int j = b.jl + tile_row(t, c1, kk, it), k = b.k0 + kk;
+    const int i0 = b.il + it * tw, i1 = min(i0 + tw - 1, b.ir);
     T* f = fl.f[tr];
     const T* mn = fl.mn[tr];
     const T* mx = fl.mx[tr];
-    for (int i = i0; i <= i1; i++) {
-      const long long e = ext(b, i, j, k);
-      if (f[e] > mx[e] || f[e] < mn[e]) visit_warp<T>(b, f, mn, mx, air, sweep_max, i, j, k, lane, s_cap[w], s_prod[w], s_cell[w]);
+    bool out = false;
+    if (lane < tw && i0 + lane <= i1) {
+      const long long e = ext(b, i0 + lane, j, k);
+      const T v = f[e];
+      out = (v > mx[e]) || (v < mn[e]);
+    }
+    unsigned todo = __ballot_sync(0xffffffffu, out);
+    while (todo) {
+      const int l = __ffs(todo) - 1;
+      todo &= todo - 1;
+      visit_warp<T>(b, f, mn, mx, air, sweep_max, i0 + l, j, k, lane, s_cap, s_prod, s_cell);
       __syncwarp();
     }
   }
@@ -214,6 +292,16 @@ struct ShellTable {
   }
 };
 
+// largest shell of sweeps 1..sweep_max (the reference's sweep counts)
+int c_shell_len(int sweep_max) {
+  int m = 0;
+  for (int sw = 1; sw <= sweep_max; sw++) {
+    const int side = 2 * sw + 1, inner = 2 * sw - 1;
+    m = std::max(m, side * side * side - inner * inner * inner);
+  }
+  return m;
+}
+
 int upload_shells(cudaStream_t s) {
   static const ShellTable tab;
   if (cudaMemcpyToSymbolAsync(c_shell, tab.off, sizeof(tab.off), 0, cudaMemcpyHostToDevice, s) != cudaSuccess ||
@@ -224,8 +312,8 @@ int upload_shells(cudaStream_t s) {
 }
 
 template <typename T>
-int run_ilmc(const Box& b, int ntr, void* const* f, const void* const* mn, const void* const* mx, const T* air,
-             int sweep_max, int min_max, int* waves, cudaStream_t s) {
+int run_ilmc(adzc_handle* h, const Box& b, int ntr, void* const* f, const void* const* mn, const void* const* mx,
+             const T* air, int sweep_max, int min_max, int* waves, cudaStream_t s) {
   if (upload_shells(s) != ADZC_OK) return ADZC_ERR_CUDA;
   Fields<T> fl{};
   for (int q = 0; q < ntr; q++) {
@@ -234,11 +322,33 @@ int run_ilmc(const Box& b, int ntr, void* const* f, const void* const* mn, const
     fl.mx[q] = (const T*)mx[q];
   }
   const int R = 2 * sweep_max, c1 = 2 * R + 2;
-  const int nz = b.nk - b.k0 + 1, ny = b.by(), ntile = (b.bx() + kTile - 1) / kTile;
+  const int tw = tile_width(sweep_max);
+  const int nz = b.nk - b.k0 + 1, ny = b.by(), ntile = (b.bx() + tw - 1) / tw;
   const int nwave = c1 * (nz - 1) + 2 * (ny - 1) + (ntile - 1) + 1;
-  const long long ntiles = (long long)ntr * nz * ntile;
-  const int grid = (int)std::max<long long>(1, std::min<long long>((ntiles + kWarps - 1) / kWarps, 148LL * 32));
-  for (int t = 0; t < nwave; t++) k_wave<T><<<grid, 32 * kWarps, 0, s>>>(b, fl, ntr, air, sweep_max, t, c1, ntile);
+  const long long ntiles = (long long)ntr * nz * ny * ntile;
+  if ((long long)ntr * nz * ntile > (1LL << 31) - 1 || ntiles > (1LL << 31) - 1) return ADZC_ERR_SIZE;
+  // scratch: count[nwave], wstart[nwave + 1], list[ntiles] (ints)
+  void* scratch = nullptr;
+  const size_t nint = (size_t)nwave * 2 + 1 + (size_t)ntiles;
+  if (adz_internal_aux(h, nint * sizeof(int), &scratch) != ADZC_OK) return ADZC_ERR_ALLOC;
+  int* count = (int*)scratch;
+  int* wstart = count + nwave;
+  int* list = wstart + nwave + 1;
+  const int gc = (int)std::max<long long>(1, std::min<long long>((ntiles + 255) / 256, 148LL * 16));
+  if (cudaMemsetAsync(count, 0, (size_t)nwave * sizeof(int), s) != cudaSuccess) return ADZC_ERR_CUDA;
+  k_candidates<T, 0><<<gc, 256, 0, s>>>(b, fl, ntr, c1, ntile, tw, count, nullptr, nullptr);
+  k_scan<<<1, 1024, 0, s>>>(count, nwave, wstart);
+  if (cudaMemsetAsync(count, 0, (size_t)nwave * sizeof(int), s) != cudaSuccess) return ADZC_ERR_CUDA;
+  k_candidates<T, 1><<<gc, 256, 0, s>>>(b, fl, ntr, c1, ntile, tw, count, wstart, list);
+  const int nshell = c_shell_len(sweep_max);
+  const size_t smem = (size_t)kWarps * nshell * (sizeof(long long) + 2 * sizeof(T));
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wave<T>, 32 * kWarps, smem) != cudaSuccess ||
+      per_sm < 1)
+    return ADZC_ERR_CUDA;
+  const int grid = per_sm * 148;
+  for (int t = 0; t < nwave; t++)
+    k_wave<T><<<grid, 32 * kWarps, smem, s>>>(b, fl, air, sweep_max, t, c1, ntile, tw, nshell, wstart, list);
   if (min_max) {
     const long long rows = (long long)ny * nz;
     const int gr = (int)std::min<long long>(rows, 148LL * 16);
@@ -269,9 +379,9 @@ extern "C" int adzc_ilmc(adzc_handle* h, int prec, int ntr, void* const* f, cons
   Box b{I.i0, I.in, I.j0, I.jn, I.k0t, D.nk, D.lminx, D.lminy, D.nit, D.nij};
   if (b.n() <= 0) return adz_internal_fail(ADZC_ERR_ARG);
   const cudaStream_t s = (cudaStream_t)stream;
-  const int st = prec == ADZC_FP64 ? run_ilmc<double>(b, ntr, f, mn, mx, (const double*)air, sweep_max, min_max,
-                                                      rounds, s)
-                                   : run_ilmc<float>(b, ntr, f, mn, mx, (const float*)air, sweep_max, min_max,
+  const int st = prec == ADZC_FP64 ? run_ilmc<double>(h, b, ntr, f, mn, mx, (const double*)air, sweep_max,
+                                                      min_max, rounds, s)
+                                   : run_ilmc<float>(h, b, ntr, f, mn, mx, (const float*)air, sweep_max, min_max,
                                                      rounds, s);
   return st == ADZC_OK ? ADZC_OK : adz_internal_fail(st);
 }

@@ -24,7 +24,7 @@ def _fields(st, dt, frac, seed):
 
 @pytest.mark.parametrize("prec_name,frac,sweeps,min_max", [("mixed", 0.01, 2, True), ("fp64", 0.01, 2, False),
                                                             ("ref32", 0.2, 2, True), ("mixed", 0.05, 1, False),
-                                                            ("fp64", 0.05, 3, True)])
+                                                            ("fp64", 0.05, 3, True), ("mixed", 0.2, 4, True)])
 def test_ilmc_bit_exact(prec_name, frac, sweeps, min_max):
     from gem_b200 import adz as A, synth
     from oracle import oracle as O
