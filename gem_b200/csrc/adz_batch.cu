@@ -306,6 +306,7 @@ extern "C" int adzc_batch_create(int prec, int ndom, const adzc_domain* doms, ad
 }
 
 extern "C" int adzc_batch_step(adzc_batch* b, void* stream) {
+  AdzRange nvtx_range("ADZ_MAIN batch");
   if (!b || !b->exec) return adz_internal_fail(ADZC_ERR_ARG);
   if (cudaGraphLaunch(b->exec, (cudaStream_t)stream) != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
   record(b);
@@ -313,6 +314,7 @@ extern "C" int adzc_batch_step(adzc_batch* b, void* stream) {
 }
 
 extern "C" int adzc_batch_tune(adzc_batch* b, void* stream) {
+  AdzRange nvtx_range("ADZ_MAIN batch tune");
   if (!b) return adz_internal_fail(ADZC_ERR_ARG);
   const cudaStream_t s = (cudaStream_t)stream;
   const int rows_c[] = {2, 8, 32};

@@ -124,6 +124,7 @@ __global__ void k_cfl_final(const Best* __restrict__ part, int nblk, int i0, int
 }  // namespace adz
 
 extern "C" int adzc_cfl(adzc_handle* h, const double* wpxyz, double* cfl, int* idx, void* stream) {
+  AdzRange nvtx_range("adz_cfl");
   using namespace adz::diag;
   adz::DGrid D;
   adzc_info I;

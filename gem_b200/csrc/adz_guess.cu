@@ -554,6 +554,7 @@ extern "C" int adzc_guess_features(adzc_handle* h, double dt, const void* uu_ext
 
 extern "C" int adzc_guess_apply(adzc_handle* h, const adzc_guess* net, double dt, const void* uu_ext,
                                 const void* vv_ext, const void* ww_ext, double* wpxyz, float* disp, void* stream) {
+  AdzRange nvtx_range("adz guess");
   using namespace adz::guess;
   adz::DGrid D;
   adzc_info I;
@@ -591,6 +592,7 @@ extern "C" int adzc_traject_tol(adzc_handle* h, int prec, double dt, double tol,
                                 const void* uu_ext, const void* vv_ext, const void* ww_ext, const void* ut0,
                                 const void* vt0, const void* zdt0, double* wpxyz, unsigned char* iters,
                                 unsigned long long* stats, void* stream) {
+  AdzRange nvtx_range("adz_traject tol");
   adz::DGrid D;
   adzc_info I;
   adzc_grid G;

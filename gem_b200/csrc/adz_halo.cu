@@ -129,10 +129,12 @@ extern "C" int adzc_halo_layout(const adzc_halo* x, int narrays, long long* off)
 
 extern "C" int adzc_halo_pack(const adzc_halo* x, int narrays, const void* const* arrays, void* sendbuf,
                               void* stream) {
+  AdzRange nvtx_range("rpn_comm_xch_halo pack");
   return adz::halo::run(x, narrays, arrays, sendbuf, true, stream);
 }
 
 extern "C" int adzc_halo_unpack(const adzc_halo* x, int narrays, void* const* arrays, const void* recvbuf,
                                 void* stream) {
+  AdzRange nvtx_range("rpn_comm_xch_halo unpack");
   return adz::halo::run(x, narrays, (const void* const*)arrays, const_cast<void*>(recvbuf), false, stream);
 }

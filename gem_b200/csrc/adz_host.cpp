@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/adz_b200.h"
+#include "adz_internal.h"
 #include "adz_types.h"
 
 namespace {
@@ -255,16 +256,19 @@ static int run_interp(const ztab* lv, int prec, int kind, void* d, void* l, void
 
 extern "C" int adzc_tricublin_m_n(const ztab* lv, int prec, void* d, const void* const* fs, const void* pxyz, int n,
                                   int m, void* stream) {
+  AdzRange nvtx_range("TRICUBLIN");
   return run_interp(lv, prec, 0, d, nullptr, nullptr, nullptr, fs, pxyz, n, m, 0, (cudaStream_t)stream);
 }
 
 extern "C" int adzc_tricublin_mono_m_n(const ztab* lv, int prec, void* d, void* l, void* mi, void* ma,
                                        const void* const* fs, const void* pxyz, int n, int m, int box, void* stream) {
+  AdzRange nvtx_range("TRICUBLIN mono");
   return run_interp(lv, prec, 1, d, l, mi, ma, fs, pxyz, n, m, box, (cudaStream_t)stream);
 }
 
 extern "C" int adzc_tricublin_zyx3_n(const ztab* lv, int prec, void* d, const void* f3, const void* pxyz, int n,
                                      void* stream) {
+  AdzRange nvtx_range("TRICUBLIN zyx3");
   const void* fs[1] = {f3};
   if (!f3) return fail(ADZC_ERR_ARG);
   return run_interp(lv, prec, 2, d, nullptr, nullptr, nullptr, fs, pxyz, n, 1, 0, (cudaStream_t)stream);
@@ -564,6 +568,7 @@ static int ensure(void** p, size_t* have, size_t need) {
 }
 
 extern "C" int adzc_inittraj(adzc_handle* h, int prec, void* pxyzm, double* wpxyz, void* stream) {
+  AdzRange nvtx_range("adz_inittraj");
   if (!h || !check_prec(prec) || !wpxyz || (prec == ADZC_REF32 && !pxyzm)) return fail(ADZC_ERR_ARG);
   ADZ_CK(dispatch_init(prec, h->dg, (float*)pxyzm, wpxyz, (cudaStream_t)stream));
   h->niter = std::max(6, h->g.itraj);  // B/adz_inittraj.F90:25
@@ -574,6 +579,7 @@ extern "C" int adzc_inittraj(adzc_handle* h, int prec, void* pxyzm, double* wpxy
 extern "C" int adzc_traject(adzc_handle* h, int prec, double dt, int niter, const void* uu_ext, const void* vv_ext,
                             const void* ww_ext, const void* ut0, const void* vt0, const void* zdt0, void* pxyzm,
                             double* wpxyz, void* stream) {
+  AdzRange nvtx_range("adz_traject");
   if (!h || !check_prec(prec) || !uu_ext || !vv_ext || !ww_ext || !ut0 || !vt0 || !zdt0 || !wpxyz ||
       (prec == ADZC_REF32 && !pxyzm))
     return fail(ADZC_ERR_ARG);
@@ -610,6 +616,7 @@ extern "C" int adzc_traject(adzc_handle* h, int prec, double dt, int niter, cons
 
 extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const void* const* srcs, void* const* dsts,
                            const int* mono, void* const* lin, void* const* mn, void* const* mx, void* stream) {
+  AdzRange nvtx_range("adz_tricub_hlt");
   if (!h || !check_prec(prec) || set < 0 || set > 3 || nfields < 0 || (nfields > 0 && (!srcs || !dsts)))
     return fail(ADZC_ERR_ARG);
   if (h->last_prec != prec || !h->wpxyz) return fail(ADZC_ERR_ARG);
@@ -669,6 +676,7 @@ extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const
 
 extern "C" int adzc_tricub_sets(adzc_handle* h, int prec, const int* nfields, const void* const* srcs,
                                 void* const* dsts, const int* mono, void* stream) {
+  AdzRange nvtx_range("ADZ_MAIN sets");
   if (!h || !check_prec(prec) || !nfields) return fail(ADZC_ERR_ARG);
   if (h->last_prec != prec || !h->wpxyz) return fail(ADZC_ERR_ARG);
   int ntot = 0;
@@ -894,7 +902,6 @@ extern "C" void Tricublin_zyx3_n(float* d, float* f3, pxpypz* pxyz, ztab* lv, in
 // ---------------------------------------------------------------------------
 // accessors used by the no-allocation entry point (adz_noalloc.cu)
 // ---------------------------------------------------------------------------
-#include "adz_internal.h"
 
 int adz_internal_view(const adzc_handle* h, adz::DGrid* dg, adzc_info* info, adzc_grid* g, int* niter, int* cold) {
   if (!h) return ADZC_ERR_ARG;

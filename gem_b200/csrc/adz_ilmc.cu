@@ -363,6 +363,7 @@ int run_ilmc(adzc_handle* h, const Box& b, int ntr, void* const* f, const void* 
 extern "C" int adzc_ilmc(adzc_handle* h, int prec, int ntr, void* const* f, const void* const* mn,
                          const void* const* mx, const void* air, int sweep_max, int min_max, int* rounds,
                          void* stream) {
+  AdzRange nvtx_range("ILMC_LAM");
   adz::DGrid D;
   adzc_info I;
   adzc_grid G;

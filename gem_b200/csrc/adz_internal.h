@@ -1,6 +1,8 @@
 // Internal accessors between the host C-ABI translation units (not part of
 // the public ABI).
 #pragma once
+#include <nvtx3/nvToolsExt.h>
+
 #include <cstddef>
 #include "../../include/adz_b200.h"
 #include "adz_types.h"
@@ -22,3 +24,13 @@ int adz_internal_scratch(adzc_handle* h, int prec, void** uvw, void** wdep);
 int adz_internal_aux(adzc_handle* h, size_t bytes, void** p);
 // restore the iteration state (cold start pending, Adz_niter) from a restart
 void adz_internal_set_iteration(adzc_handle* h, int cold, int niter);
+
+// NVTX range over a C-ABI call (host enqueue time), named after the reference
+// routine or gtmg timer it stands for (B/adz_tracers.F90:34-111,
+// B/tstpdyn.F90:116); visible to nsys/ncu, a no-op without a tool attached
+struct AdzRange {
+  explicit AdzRange(const char* name) { nvtxRangePushA(name); }
+  ~AdzRange() { nvtxRangePop(); }
+  AdzRange(const AdzRange&) = delete;
+  AdzRange& operator=(const AdzRange&) = delete;
+};

@@ -295,6 +295,7 @@ int run_bc(int ntr, const adzc_bc_tracer* in, const void* airm_p, const void* ai
 extern "C" int adzc_bermejo_conde(adzc_handle* h, int prec, int ntr, const adzc_bc_tracer* tracers,
                                   const void* airm_p, const void* airm_m, const double* mask, int min_max,
                                   double* deficit, double* diag, void* stream) {
+  AdzRange nvtx_range("Bermejo_Conde");
   adz::DGrid D;
   adzc_info I;
   adzc_grid G;

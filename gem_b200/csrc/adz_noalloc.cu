@@ -74,6 +74,7 @@ extern "C" int adzc_step_noalloc(adzc_handle* h, int prec, double dt, int niter,
                                  const void* vv_ext, const void* ww_ext, const void* ut0, const void* vt0,
                                  const void* zdt0, void* pxyzm, double* wpxyz, const int* nfields,
                                  const void* const* srcs, void* const* dsts, const int* mono, void* stream) {
+  AdzRange nvtx_range("ADZ_MAIN");
   if (!h || (prec != ADZC_REF32 && prec != ADZC_FP64 && prec != ADZC_MIXED) || !uu_ext || !vv_ext || !ww_ext ||
       !ut0 || !vt0 || !zdt0 || !wpxyz || (prec == ADZC_REF32 && !pxyzm) || !nfields)
     return adz_internal_fail(ADZC_ERR_ARG);

@@ -210,6 +210,46 @@ def test_step_ref32_bit_exact(A, shape):
         assert np.array_equal(_bits(a.cpu().numpy()[m]), _bits(b[m]))
 
 
+@pytest.mark.parametrize("lam", [True, False])
+def test_cfl_above_maxcfl_clips(A, lam):
+    """Winds of about twice maxcfl grid lengths per step.  Departure points are
+    clipped to the adz_set bounds: on a LAM-edge tile the BCS_BASE bounds, on
+    an interior tile the halo (B/adz_set.F90:123-160, B/adz_traject.F90:94-98).
+    No stencil leaves the extended array (status 0, nothing read out of
+    bounds), and the REF32 step stays bit-exact with the reference."""
+    from gem_b200 import synth
+    cfg = synth.config_small(48, 40, 20)
+    cfg.u0 = 2.0 * cfg.maxcfl * cfg.dx / cfg.dt
+    cfg.phase = (0.5, 0.25)  # strongest eastward wind on the west edge: departures leave the tile
+    cfg.mono = True
+    np_in, dev = _inputs(cfg, torch.float32)
+    kind = "ref" if O.have_ref() else "oracle"
+    st = O.Step(cfg, kind=kind, prec="f32", lam=lam)
+    st.inittraj()
+    ad = A.Adz.from_config(cfg, lam=lam)
+    px, wp = ad.new_state(A.REF32)
+    ad.adz_inittraj(A.REF32, px, wp)
+    for _ in range(2):
+        o_out = st.step(np_in)
+        outs = {k: torch.full(ad.ext_shape, float("nan"), dtype=torch.float32, device="cuda") for k in ("u", "v", "w")}
+        tro = [torch.full(ad.ext_shape, float("nan"), dtype=torch.float32, device="cuda") for _ in dev["tracers"]]
+        A.step_fused(ad, A.REF32, cfg.dt, dev, dev, dev["tracers"], px, wp, outs, tro, cfg.mono)
+    assert ad.status() == 0
+    torch.cuda.synchronize()
+    pxc = px.cpu().numpy()
+    lo, hi = np.float32(ad.info.iminposx), np.float32(ad.info.imaxposx)
+    clipped = int(np.sum(pxc[..., 0] == lo) + np.sum(pxc[..., 0] == hi))
+    assert clipped > 0  # the clip is exercised
+    assert np.array_equal(_bits(pxc), _bits(st.pxyzm))
+    assert np.array_equal(_bits(wp.cpu().numpy()), _bits(st.wpxyz))
+    for k, s in (("u", 1), ("v", 2), ("w", 3)):
+        m = ad.range_mask(s).numpy()
+        assert np.array_equal(_bits(outs[k].cpu().numpy()[m]), _bits(o_out[k][m])), k
+    m = ad.range_mask(3).numpy()
+    for a, b in zip(tro, o_out["tracers"]):
+        assert np.array_equal(_bits(a.cpu().numpy()[m]), _bits(b[m]))
+
+
 def test_step_fp64_bit_exact_stretched_levels(A):
     from gem_b200 import synth
     cfg = synth.config_large(96, 80, 80)
