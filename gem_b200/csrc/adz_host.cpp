@@ -74,6 +74,14 @@ cudaError_t dispatch_set(int prec, const adz::DGrid& g, int set, int i0, int nx,
     default: return adz::launch_tricub_set<adz::kMixed>(g, set, i0, nx, j0, ny, k0, nz, a, fp, s);
   }
 }
+cudaError_t dispatch_parts(int prec, const adz::DGrid& g, const adz::SetArgs& a, const adz::SetParts& sp,
+                           cudaStream_t s) {
+  switch (prec) {
+    case ADZC_REF32: return adz::launch_tricub_parts<adz::kRef32>(g, a, sp, s);
+    case ADZC_FP64: return adz::launch_tricub_parts<adz::kFp64>(g, a, sp, s);
+    default: return adz::launch_tricub_parts<adz::kMixed>(g, a, sp, s);
+  }
+}
 cudaError_t dispatch_pos(int prec, const adz::DZtab& lv, int kind, int n, const void* pos, const adz::FieldPtrs& fp,
                          cudaStream_t s) {
   switch (prec) {
@@ -614,23 +622,25 @@ extern "C" int adzc_traject(adzc_handle* h, int prec, double dt, int niter, cons
   return ADZC_OK;
 }
 
-extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const void* const* srcs, void* const* dsts,
-                           const int* mono, void* const* lin, void* const* mn, void* const* mx, void* stream) {
-  AdzRange nvtx_range("adz_tricub_hlt");
-  if (!h || !check_prec(prec) || set < 0 || set > 3 || nfields < 0 || (nfields > 0 && (!srcs || !dsts)))
-    return fail(ADZC_ERR_ARG);
-  if (h->last_prec != prec || !h->wpxyz) return fail(ADZC_ERR_ARG);
+namespace {
+
+// arrival points of a position set (B/adz_set.F90:94-114)
+void set_box(const adzc_handle* h, int set, int& i0, int& nx, int& j0, int& ny, int& k0, int& nz) {
   const adzc_info& I = h->info;
-  const adz::DGrid& D = h->dg;
-  int i0, i1, j0, j1, k0;
+  int i1, j1;
   switch (set) {
     case ADZC_SET_Q: i0 = I.i0; i1 = I.in; j0 = I.j0; j1 = I.jn; k0 = I.k0; break;
     case ADZC_SET_U: i0 = I.i0u; i1 = I.inu; j0 = I.j0; j1 = I.jn; k0 = I.k0; break;
     case ADZC_SET_V: i0 = I.i0; i1 = I.in; j0 = I.j0v; j1 = I.jnv; k0 = I.k0; break;
     default: i0 = I.i0; i1 = I.in; j0 = I.j0; j1 = I.jn; k0 = I.k0t; break;
   }
-  const int nx = i1 - i0 + 1, ny = j1 - j0 + 1, nz = D.nk - k0 + 1;
-  if (nx <= 0 || ny <= 0 || nz <= 0 || nfields == 0) return ADZC_OK;
+  nx = i1 - i0 + 1;
+  ny = j1 - j0 + 1;
+  nz = h->dg.nk - k0 + 1;
+}
+
+adz::SetArgs set_args(const adzc_handle* h) {
+  const adzc_info& I = h->info;
   adz::SetArgs a{};
   a.wpxyz = h->wpxyz;
   a.pxyzm = h->pxyzm;
@@ -639,12 +649,33 @@ extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const
   a.dt = h->dt;
   a.k00 = std::max(I.k0t - 1, 1);  // B/adz_interp_traj.F90:39-40
   if (h->g.bc_lam_flux != 0 && I.k0 > 1) a.k00 = 1;
+  return a;
+}
+
+// a mono flag of adzc_tricub: 0..2, | ADZC_QV on set T only
+bool mono_ok(int mv, int set) {
+  if ((mv & ~(3 | ADZC_QV)) != 0 || (mv & 3) == 3) return false;
+  return !((mv & ADZC_QV) && set != ADZC_SET_T);
+}
+
+}  // namespace
+
+extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const void* const* srcs, void* const* dsts,
+                           const int* mono, void* const* lin, void* const* mn, void* const* mx, void* stream) {
+  AdzRange nvtx_range("adz_tricub_hlt");
+  if (!h || !check_prec(prec) || set < 0 || set > 3 || nfields < 0 || (nfields > 0 && (!srcs || !dsts)))
+    return fail(ADZC_ERR_ARG);
+  if (h->last_prec != prec || !h->wpxyz) return fail(ADZC_ERR_ARG);
+  const adz::DGrid& D = h->dg;
+  int i0, nx, j0, ny, k0, nz;
+  set_box(h, set, i0, nx, j0, ny, k0, nz);
+  if (nx <= 0 || ny <= 0 || nz <= 0 || nfields == 0) return ADZC_OK;
+  const adz::SetArgs a = set_args(h);
   // tricubic fields, then BICUBH_QV fields (set t only), in groups of kMaxFields
   std::vector<int> groups[2];
   for (int f = 0; f < nfields; f++) {
     const int mv = mono ? mono[f] : 0;
-    if ((mv & ~(3 | ADZC_QV)) != 0 || (mv & 3) == 3) return fail(ADZC_ERR_ARG);
-    if ((mv & ADZC_QV) && set != ADZC_SET_T) return fail(ADZC_ERR_ARG);
+    if (!mono_ok(mv, set)) return fail(ADZC_ERR_ARG);
     if (!srcs[f] || !dsts[f]) return fail(ADZC_ERR_ARG);
     groups[(mv & ADZC_QV) ? 1 : 0].push_back(f);
   }
@@ -686,18 +717,55 @@ extern "C" int adzc_tricub_sets(adzc_handle* h, int prec, const int* nfields, co
   }
   if (ntot == 0) return ADZC_OK;
   if (!srcs || !dsts) return fail(ADZC_ERR_ARG);
-  for (int f = 0; f < ntot; f++)
-    if (!srcs[f] || !dsts[f]) return fail(ADZC_ERR_ARG);
-  // one launch per set (and per chunk of fields)
-  int f0 = 0;
-  for (int q = 0; q < 4; q++) {
-    if (nfields[q] > 0) {
-      const int st = adzc_tricub(h, prec, q, nfields[q], srcs + f0, dsts + f0, mono ? mono + f0 : nullptr, nullptr,
-                                 nullptr, nullptr, stream);
-      if (st != ADZC_OK) return st;
-    }
-    f0 += nfields[q];
+  for (int f = 0, set = 0, left = nfields[0]; f < ntot; f++, left--) {
+    while (left == 0) left = nfields[++set];
+    if (!srcs[f] || !dsts[f] || !mono_ok(mono ? mono[f] : 0, set)) return fail(ADZC_ERR_ARG);
   }
+  // every tricubic field group of every set in one interleaved launch
+  // (k_tricub_parts); BICUBH_QV fields of set t after it
+  const adz::SetArgs a = set_args(h);
+  const cudaStream_t s = (cudaStream_t)stream;
+  adz::SetParts sp{};
+  std::vector<const void*> qv_src;
+  std::vector<void*> qv_dst;
+  std::vector<int> qv_mono;
+  int f0 = 0;
+  for (int set = 0; set < 4; set++) {
+    const int nf = nfields[set];
+    int i0, nx, j0, ny, k0, nz;
+    set_box(h, set, i0, nx, j0, ny, k0, nz);
+    const bool empty = nx <= 0 || ny <= 0 || nz <= 0;
+    adz::SetPart* part = nullptr;
+    for (int f = f0; f < f0 + nf && !empty; f++) {
+      const int mv = mono ? mono[f] : 0;
+      if (mv & ADZC_QV) {
+        qv_src.push_back(srcs[f]);
+        qv_dst.push_back(dsts[f]);
+        qv_mono.push_back(mv);
+        continue;
+      }
+      if (!part || part->fp.nf == adz::kMaxFields) {
+        if (sp.n == adz::kMaxParts) {
+          ADZ_CK(dispatch_parts(prec, h->dg, a, sp, s));
+          sp = adz::SetParts{};
+        }
+        part = &sp.p[sp.n++];
+        part->set = set;
+        part->i0 = i0; part->nx = nx; part->j0 = j0; part->ny = ny; part->k0 = k0; part->nz = nz;
+      }
+      adz::FieldPtrs& fp = part->fp;
+      const int q = fp.nf++;
+      fp.src[q] = srcs[f];
+      fp.dst[q] = dsts[f];
+      if ((mv & 3) != 0) fp.mono_mask |= 1u << q;
+      if ((mv & 3) == 1) fp.clip_mask |= 1u << q;
+    }
+    f0 += nf;
+  }
+  if (sp.n > 0) ADZ_CK(dispatch_parts(prec, h->dg, a, sp, s));
+  if (!qv_src.empty())
+    return adzc_tricub(h, prec, ADZC_SET_T, (int)qv_src.size(), qv_src.data(), qv_dst.data(), qv_mono.data(),
+                       nullptr, nullptr, nullptr, stream);
   return ADZC_OK;
 }
 

@@ -566,6 +566,23 @@ __global__ void ADZ_SET_BOUNDS k_tricub_set(DGrid g, int set, int i0, int nx, in
   }
 }
 
+// the tricubic groups of several sets in one launch.  Consecutive blocks
+// take consecutive parts (u, v, t ...), so every SM runs a mix of the
+// issue-bound one-field sets and the load-bound multi-field set at once;
+// each thread interpolates one arrival point of its part as k_tricub_set does
+template <int PREC>
+__global__ void ADZ_SET_BOUNDS k_tricub_parts(DGrid g, SetArgs a, const __grid_constant__ SetParts sp) {
+  const int q = (int)(blockIdx.x % (unsigned)sp.n);
+  const SetPart& P = sp.p[q];
+  const long long t = (long long)(blockIdx.x / (unsigned)sp.n) * blockDim.x + threadIdx.x;
+  const long long nplane = (long long)P.nx * P.ny;
+  if (t >= nplane * P.nz) return;
+  const int i = (int)(t % P.nx) + P.i0;
+  const int j = (int)((t / P.nx) % P.ny) + P.j0;
+  const int k = (int)(t / nplane) + P.k0;
+  set_point<PREC>(g, P.set, a, P.fp, i, j, k);
+}
+
 // BICUBH_QV fields at position set t (adz_interp_hlt.F90:113-116 with
 // F_QV_L): lin/min/max of the inner 2x2x2 box always formed, written where
 // asked; clip as adz_post_tr.F90:81-94
@@ -899,6 +916,21 @@ cudaError_t launch_tricub_set(const DGrid& g, int set, int i0, int nx, int j0, i
 }
 
 template <int PREC>
+cudaError_t launch_tricub_parts(const DGrid& g, const SetArgs& a, const SetParts& sp, cudaStream_t s) {
+  if (sp.n < 1 || sp.n > kMaxParts) return cudaErrorInvalidValue;
+  long long most = 0;  // blocks of the largest part
+  for (int q = 0; q < sp.n; q++) {
+    const long long n = (long long)sp.p[q].nx * sp.p[q].ny * sp.p[q].nz;
+    most = n > most ? n : most;
+  }
+  const long long blocks = (most + 127) / 128 * sp.n;
+  if (blocks < 1) return cudaSuccess;
+  if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+  k_tricub_parts<PREC><<<(unsigned)blocks, 128, 0, s>>>(g, a, sp);
+  return cudaGetLastError();
+}
+
+template <int PREC>
 cudaError_t launch_qv_set(const DGrid& g, int i0, int nx, int j0, int ny, int k0, int nz, const SetArgs& a,
                           const FieldPtrs& fp, cudaStream_t s) {
   const long long n = (long long)nx * ny * nz;
@@ -995,6 +1027,7 @@ int batch_resident_blocks(int variant) {
   template cudaError_t launch_tricub_set<P>(const DGrid&, int, int, int, int, int, int, int, const SetArgs&,       \
                                             const FieldPtrs&, cudaStream_t);                                       \
   template cudaError_t launch_interp_pos<P>(const DZtab&, int, int, const void*, const FieldPtrs&, cudaStream_t); \
+  template cudaError_t launch_tricub_parts<P>(const DGrid&, const SetArgs&, const SetParts&, cudaStream_t);       \
   template cudaError_t launch_qv_set<P>(const DGrid&, int, int, int, int, int, int, const SetArgs&,               \
                                         const FieldPtrs&, cudaStream_t);                                          \
   template cudaError_t launch_batch<P>(int, int, const BatchParams&, const BDom*, const BItem*, long long,       \

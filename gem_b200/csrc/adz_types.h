@@ -81,6 +81,17 @@ struct FieldPtrs {
   long long ostride;   // explicit-position kernels: output element stride per point
 };
 
+// the tricubic field groups of several position sets in one launch
+struct SetPart {
+  FieldPtrs fp;
+  int set, i0, nx, j0, ny, k0, nz, pad;
+};
+constexpr int kMaxParts = 8;
+struct SetParts {
+  SetPart p[kMaxParts];
+  int n;
+};
+
 struct TrajArgs {
   const void* uvw_d;  // ext, 3 interleaved
   const void* ut0;
@@ -169,6 +180,8 @@ struct BItem {
 };
 
 constexpr int kBatchVariants = 3;  // register budgets of the batch kernel
+template <int PREC>
+cudaError_t launch_tricub_parts(const DGrid& g, const SetArgs& a, const SetParts& sp, cudaStream_t s);
 template <int PREC>
 cudaError_t launch_batch(int variant, int grid, const BatchParams& P, const BDom* doms, const BItem* items,
                          long long nitems,
