@@ -388,7 +388,7 @@ def run_product(args):
 
 # kernels of one MIXED step: departure winds, trajectory, and one
 # interpolation launch per position set (u, v, then w + tracers at thermo points)
-LAUNCHES_PER_STEP = 5
+LAUNCHES_PER_STEP = 3  # k_prepare, k_traject, k_tricub_parts (every set's field groups)
 HALO_LAUNCHES_PER_STEP = 4  # pack + unpack of the two exchanges (N > 1)
 
 
