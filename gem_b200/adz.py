@@ -112,6 +112,7 @@ def lib() -> C.CDLL:
         L.adzc_ilmc.argtypes = [vp, i, i, vp, vp, vp, vp, i, i, C.POINTER(C.c_int), vp]
         L.adzc_state_save.argtypes = [vp, i, vp, vp, C.c_char_p]
         L.adzc_state_load.argtypes = [vp, i, vp, vp, C.c_char_p]
+        L.adzc_slt_winds.argtypes = [vp, vp, vp]
         L.adzc_halo_layout.argtypes = [vp, i, vp]
         L.adzc_halo_pack.argtypes = [vp, i, vp, vp, vp]
         L.adzc_halo_unpack.argtypes = [vp, i, vp, vp, vp]
@@ -222,7 +223,8 @@ class Adz:
         self.ni, self.nj, self.nk = grid.ni, grid.nj, grid.nk
 
     @classmethod
-    def from_config(cls, cfg, lam=True, i0g=None, j0g=None, schm_advec=1, edges=None):
+    def from_config(cls, cfg, lam=True, i0g=None, j0g=None, schm_advec=1, edges=None, slt_winds=False,
+                    lam_gbpil_t=0):
         """adz_set for a synthetic LAM tile (gem_b200.synth.Config).  The
         tile starts at global (i0g, j0g) (default: the config's tile origin)
         and touches the LAM edges flagged in ``edges`` = (west, east, south,
@@ -239,7 +241,8 @@ class Adz:
         P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
         g = AdzcGrid(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk, maxcfl=cfg.maxcfl, i0g=i0g, j0g=j0g,
                      west=w, east=ea, south=so, north=no, pil_w=p * w, pil_e=p * ea, pil_s=p * so, pil_n=p * no,
-                     lam_gbpil_t=0, bc_lam_flux=1, schm_advec=schm_advec, itraj=cfg.niter, slt_winds=0,
+                     lam_gbpil_t=lam_gbpil_t, bc_lam_flux=1, schm_advec=schm_advec, itraj=cfg.niter,
+                     slt_winds=1 if slt_winds else 0,
                      bA_m=0.6, bA=0.6, inv_rayt=ga["inv_rayt"], inv_hx=ga["inv_hx"], inv_hy=ga["inv_hy"],
                      cy=P(keep["cy"]), zm=P(keep["zm"]), zt=P(keep["zt"]), zx=P(keep["zx"]),
                      zmin=ga["zmin"], zmax=ga["zmax"], wmstar_nk=ga["wmstar_nk"], idz_t_nkm1=ga["idz_t_nkm1"])
@@ -287,6 +290,13 @@ class Adz:
                                   *(winds[k].data_ptr() for k in ("uu_ext", "vv_ext", "ww_ext", "ut0", "vt0", "zdt0")),
                                   None if pxyzm is None else pxyzm.data_ptr(), wpxyz.data_ptr(), _stream(stream)),
                "adzc_traject")
+
+    def set_slt_winds(self, uslt=None, vslt=None):
+        """Adz_uslt, Adz_vslt (nj, ni) device tensors of the field type for
+        the top-level pt positions when slt_winds is set; None to clear."""
+        self._slt = (uslt, vslt)
+        _check(lib().adzc_slt_winds(self.h, None if uslt is None else uslt.data_ptr(),
+                                    None if vslt is None else vslt.data_ptr()), "adzc_slt_winds")
 
     def adz_tricub_hlt(self, prec: int, set_id: int, srcs, dsts, mono=None, post=None, stream=None):
         """Interpolate srcs at position set set_id into dsts (ext layout).

@@ -313,6 +313,10 @@ struct adzc_handle {
   const float* pxyzm = nullptr;
   const void* zdt0 = nullptr;
   adz::DtSplit dt{};
+  // Adz_uslt, Adz_vslt (ni, nj): surface-layer winds of the top-level pt
+  // positions when the grid's slt_winds is set (adzc_slt_winds)
+  const void* uslt = nullptr;
+  const void* vslt = nullptr;
 };
 
 static int build_search(const std::vector<double>& z, int nk, double sig, const std::vector<double>& delz,
@@ -649,6 +653,8 @@ adz::SetArgs set_args(const adzc_handle* h) {
   a.dt = h->dt;
   a.k00 = std::max(I.k0t - 1, 1);  // B/adz_interp_traj.F90:39-40
   if (h->g.bc_lam_flux != 0 && I.k0 > 1) a.k00 = 1;
+  a.uslt = h->uslt;
+  a.vslt = h->vslt;
   return a;
 }
 
@@ -659,6 +665,13 @@ bool mono_ok(int mv, int set) {
 }
 
 }  // namespace
+
+extern "C" int adzc_slt_winds(adzc_handle* h, const void* uslt, const void* vslt) {
+  if (!h || (!uslt) != (!vslt)) return fail(ADZC_ERR_ARG);
+  h->uslt = uslt;
+  h->vslt = vslt;
+  return ADZC_OK;
+}
 
 extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const void* const* srcs, void* const* dsts,
                            const int* mono, void* const* lin, void* const* mn, void* const* mx, void* stream) {
@@ -989,6 +1002,11 @@ void adz_internal_after_traject(adzc_handle* h) {
 }
 
 adz::DtSplit adz_internal_dt_split(const adzc_grid& g, double dt) { return dt_split(g, dt); }
+
+void adz_internal_slt(const adzc_handle* h, const void** uslt, const void** vslt) {
+  *uslt = h ? h->uslt : nullptr;
+  *vslt = h ? h->vslt : nullptr;
+}
 
 void adz_internal_record_positions(adzc_handle* h, int prec, double* wpxyz, const void* zdt0, const adz::DtSplit& dt) {
   adz_internal_after_traject(h);

@@ -253,6 +253,11 @@ def make_inputs(cfg: Config, device="cpu", dtype=torch.float64, with_fields=True
     out["ut0"] = (_flow(cfg, xu, y, zm, t0, 0).expand(shp) + noise()).to(dtype).contiguous()
     out["vt0"] = (_flow(cfg, x, yv, zm, t0, 1).expand(shp) + noise()).to(dtype).contiguous()
     out["zdt0"] = (_flow(cfg, x, y, zt, t0, 2).expand(shp) + noise(cfg.noise_w)).to(dtype).contiguous()
+    # surface-layer winds Adz_uslt, Adz_vslt (nj, ni): the lowest momentum
+    # level's winds, weakened as near the ground
+    i0 = j0 = cfg.halo
+    out["uslt"] = (0.7 * out["uu_ext"][-1, j0:j0 + cfg.nj, i0:i0 + cfg.ni].to(torch.float64)).to(dtype).contiguous()
+    out["vslt"] = (0.7 * out["vv_ext"][-1, j0:j0 + cfg.nj, i0:i0 + cfg.ni].to(torch.float64)).to(dtype).contiguous()
     if not with_fields:
         return out
     out["src_u"] = _flow(cfg, xu, y, zm, t1, 0).expand(shp).to(dtype).contiguous()

@@ -191,6 +191,15 @@ int adzc_traject(adzc_handle *h, int prec, double dt, int niter, const void *uu_
 int adzc_tricub(adzc_handle *h, int prec, int set, int nfields, const void *const *srcs, void *const *dsts,
                 const int *mono, void *const *lin, void *const *mn, void *const *mx, void *stream);
 
+/* Adz_uslt, Adz_vslt: DEVICE arrays (ni, nj) of the field type holding the
+ * surface-layer winds.  When the grid sets slt_winds, the top-level points
+ * of set T (k = nk) take their horizontal positions from them
+ * (B/adz_interp_traj.F90:123-133); without them (or with NULL, NULL) those
+ * points use the wpxyz extrapolation, as the reference does when the
+ * physics does not provide the fields (B/adz_set.F90:364-370).  Used by
+ * the adzc_tricub*, adzc_step_noalloc and batch calls that follow. */
+int adzc_slt_winds(adzc_handle *h, const void *uslt, const void *vslt);
+
 /* Every position set of the last trajectory in one call: nfields[4] fields
  * for sets Q, U, V, T, srcs/dsts/mono holding all sets' entries in that order
  * (HOST arrays of DEVICE pointers; mono may be NULL).  Same results as

@@ -252,7 +252,7 @@ class RefKernels:
 # --------------------------------------------------------------------------
 # driver restatement: one advection step (adz_main + adz_tracers subset)
 # --------------------------------------------------------------------------
-def make_grid(cfg, i0g=1, j0g=1, lam=True, slt_winds=False, schm_advec=1):
+def make_grid(cfg, i0g=1, j0g=1, lam=True, slt_winds=False, schm_advec=1, lam_gbpil_t=0):
     """orc_grid for a synth.Config tile (LAM tile touching all four edges)."""
     from gem_b200 import synth
     ga = synth.grid_arrays(cfg)
@@ -261,7 +261,7 @@ def make_grid(cfg, i0g=1, j0g=1, lam=True, slt_winds=False, schm_advec=1):
     p = cfg.pil if lam else 0
     g = OrcGrid(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk, maxcfl=cfg.maxcfl, i0g=i0g, j0g=j0g,
                 west=e, east=e, south=e, north=e, pil_w=p, pil_e=p, pil_s=p, pil_n=p,
-                lam_gbpil_t=0, bc_lam_flux=1, schm_advec=schm_advec, itraj=cfg.niter,
+                lam_gbpil_t=lam_gbpil_t, bc_lam_flux=1, schm_advec=schm_advec, itraj=cfg.niter,
                 slt_winds=1 if slt_winds else 0, bA_m=0.6, bA=0.6, inv_rayt=ga["inv_rayt"],
                 inv_hx=ga["inv_hx"], inv_hy=ga["inv_hy"],
                 cy=keep["cy"].ctypes.data_as(C.POINTER(C.c_double)),
@@ -334,9 +334,13 @@ class Step:
             self.vv_arr.ctypes.data, self.ww_arr.ctypes.data, self.uvw_dep.ctypes.data,
             self.pxyzm.ctypes.data, self.wpxyz.ctypes.data)
         self.cold = False
+        # Adz_uslt, Adz_vslt (nj, ni), used when the grid sets slt_winds
+        slt = [np.ascontiguousarray(inp[k], dtype=self.dt) if inp.get(k) is not None else None
+               for k in ("uslt", "vslt")]
+        self._slt = slt
         getattr(self.L, f"orc_interp_traj_{P}")(
             C.byref(self.s), self.cfg.dt, self.wpxyz.ctypes.data, self.uvw_dep.ctypes.data,
-            a["zdt0"].ctypes.data, self.pxyzm.ctypes.data, None, None,
+            a["zdt0"].ctypes.data, self.pxyzm.ctypes.data, *(None if x is None else x.ctypes.data for x in slt),
             *(self.sets[q].ctypes.data for q in range(4)))
 
     def tricub(self, set_id, srcs, mono=False, clip=False, post=False):

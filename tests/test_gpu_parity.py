@@ -210,6 +210,58 @@ def test_step_ref32_bit_exact(A, shape):
         assert np.array_equal(_bits(a.cpu().numpy()[m]), _bits(b[m]))
 
 
+@pytest.mark.parametrize("branch", ["schm_advec2", "schm_advec3", "slt_winds", "lam_gbpil_t"])
+def test_step_ref32_reference_branches(A, branch):
+    """The less common switches of the path, REF32 bit-exact with the
+    reference interpolator and the driver restatement:
+    Schm_advec 2 and 3 (dt split with the off-centering weights,
+    B/adz_traject.F90:38-59), Adz_slt_winds (surface-layer winds for the
+    top-level pt positions, B/adz_interp_traj.F90:123-133) and
+    Lam_gbpil_t > 0 (a top pilot: k0 > 1, B/adz_set.F90:94-114)."""
+    from gem_b200 import synth
+    cfg = synth.config_small(40, 36, 24)
+    cfg.mono = True
+    kw = {"schm_advec2": dict(schm_advec=2), "schm_advec3": dict(schm_advec=3),
+          "slt_winds": dict(slt_winds=True), "lam_gbpil_t": dict(lam_gbpil_t=4)}[branch]
+    np_in, dev = _inputs(cfg, torch.float32)
+    kind = "ref" if O.have_ref() else "oracle"
+    st = O.Step(cfg, kind=kind, prec="f32", **kw)
+    st.inittraj()
+    ad = A.Adz.from_config(cfg, **kw)
+    if branch == "slt_winds":
+        ad.set_slt_winds(dev["uslt"], dev["vslt"])
+    px, wp = ad.new_state(A.REF32)
+    ad.adz_inittraj(A.REF32, px, wp)
+    for _ in range(2):
+        o_out = st.step(np_in)
+        outs = {k: torch.full(ad.ext_shape, float("nan"), dtype=torch.float32, device="cuda") for k in ("u", "v", "w")}
+        tro = [torch.full(ad.ext_shape, float("nan"), dtype=torch.float32, device="cuda") for _ in dev["tracers"]]
+        A.step_fused(ad, A.REF32, cfg.dt, dev, dev, dev["tracers"], px, wp, outs, tro, cfg.mono)
+    assert ad.status() == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(_bits(px.cpu().numpy()), _bits(st.pxyzm))
+    assert np.array_equal(_bits(wp.cpu().numpy()), _bits(st.wpxyz))
+    for k, s in (("u", 1), ("v", 2), ("w", 3)):
+        m = ad.range_mask(s).numpy()
+        assert m.any()
+        assert np.array_equal(_bits(outs[k].cpu().numpy()[m]), _bits(o_out[k][m])), k
+    m = ad.range_mask(3).numpy()
+    for a, b in zip(tro, o_out["tracers"]):
+        assert np.array_equal(_bits(a.cpu().numpy()[m]), _bits(b[m]))
+    if branch == "slt_winds":  # the switch changes the top-level results
+        ad2 = A.Adz.from_config(cfg)
+        px2, wp2 = ad2.new_state(A.REF32)
+        ad2.adz_inittraj(A.REF32, px2, wp2)
+        o2 = [torch.zeros(ad.ext_shape, dtype=torch.float32, device="cuda") for _ in range(3)]
+        for _ in range(2):
+            A.step_fused(ad2, A.REF32, cfg.dt, dev, dev, [], px2, wp2, dict(zip("uvw", o2)), [], cfg.mono)
+        torch.cuda.synchronize()
+        top = np.zeros(ad.ext_shape, bool)
+        top[-1] = True
+        mw = ad.range_mask(3).numpy() & top
+        assert not np.array_equal(_bits(o2[2].cpu().numpy()[mw]), _bits(outs["w"].cpu().numpy()[mw]))
+
+
 @pytest.mark.parametrize("lam", [True, False])
 def test_cfl_above_maxcfl_clips(A, lam):
     """Winds of about twice maxcfl grid lengths per step.  Departure points are
