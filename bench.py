@@ -563,8 +563,8 @@ def measure_batch(args, timed, ws, cfgs, label):
             ad.adz_traject(prec, cfg.dt, inp, None, wp)
             ad.adz_tricub_sets(prec, [0, 1, 1, len(srcs) - 2], srcs, dsts, mono)
     ms_s, _ = timed(sequential, args.steps, args.warmup)
-    # per domain: winds, trajectory, u set, v set, thermo set in groups of 16 fields
-    seq_launches = sum(4 + (len(d[4]) - 2 + 15) // 16 for d in doms)
+    # per domain: winds, trajectory, and every set's field groups in one launch
+    seq_launches = 3 * len(doms)
     out = {"workload": f"{len(cfgs)} {label}",
            "points_per_step": npts, "value": npts * ws / (ms_b * 1e-3), "unit": "grid-points/s",
            "ms_per_step": ms_b, "launches_per_step": 1, "plan": batch.query(), "tune_s": tune_s,
