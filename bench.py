@@ -37,9 +37,9 @@ HBM_FALLBACK_GBS = 6650.0
 TENSOR_FALLBACK_TFLOPS = 1590.0
 # DRAM bytes (read + write) per arrival point of each MIXED launch, from the
 # ncu capture of the 384x384x80 case with u, v, w + 4 tracers
-# (profiles/k_tricub_set_k_traject_mixed_384x384x80.md); traffic grows in
+# (profiles/k_traject_k_tricub_parts_mixed_384x384x80.md); traffic grows in
 # proportion to the points, so it scales to the benched tile
-MEASURED_TRAFFIC_PER_POINT = {"traject": 74.2, "sets": 122.8}
+MEASURED_TRAFFIC_PER_POINT = {"traject": 74.25, "sets": 89.77}
 
 
 def peaks():
@@ -262,6 +262,15 @@ def run_product(args):
         acc = accuracy(ad, [outs32["u"], outs32["v"], outs32["w"]] + tro32, wp32, ref64)
         del ref64
         torch.cuda.empty_cache()
+    # the reference's own arithmetic (REF32, bit-exact with the CPU reference) on the same inputs
+    ms_ref32 = float("nan")
+    if args.only is None:
+        step_r, o_r, t_r, _ = make_step(adz.REF32, d32)
+        ms_ref32, _ = timed(step_r, max(3, min(args.steps, 10)), args.warmup)
+        if ad.status() != 0:
+            raise RuntimeError("device status set during the REF32 steps")
+        del step_r, o_r, t_r
+        torch.cuda.empty_cache()
 
     # per-launch durations of one step (events between the API calls)
     s = torch.cuda.current_stream()
@@ -369,6 +378,7 @@ def run_product(args):
                     "halo exchange (NCCL send/recv) of winds and sources, then of wpxyz, every step")
                    if ws > 1 else "1 tile"},
         "fp64_value": npts * ws / (ms64 * 1e-3), "fp64_ms_per_step": ms64, "speedup_vs_fp64": ms64 / ms32,
+        "ref32_value": npts * ws / (ms_ref32 * 1e-3), "ref32_ms_per_step": ms_ref32,
         "per_launch_ms": per,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind},
