@@ -302,6 +302,40 @@ def test_cfl_above_maxcfl_clips(A, lam):
         assert np.array_equal(_bits(a.cpu().numpy()[m]), _bits(b[m]))
 
 
+def test_step_ref32_bit_exact_full_size(A):
+    """The benchmark tile itself: 1024x1024x80 (84 M arrival points, ext
+    arrays of 85 M cells), u, v, w + 4 tracers, a cold and a warm step, REF32
+    bit-exact with the reference-linked oracle on every point of every set.
+    The oracle runs on all host cores."""
+    from gem_b200 import synth
+    cfg = synth.config_large(1024, 1024, 80)
+    cfg.mono = True
+    g = synth.make_inputs(cfg, device="cuda", dtype=torch.float32)
+    dev = g
+    np_in = {k: (v.cpu().numpy() if torch.is_tensor(v) else [t.cpu().numpy() for t in v]) for k, v in g.items()}
+    kind = "ref" if O.have_ref() else "oracle"
+    st = O.Step(cfg, kind=kind, prec="f32", threads=os.cpu_count() or 1)
+    st.inittraj()
+    ad = A.Adz.from_config(cfg)
+    px, wp = ad.new_state(A.REF32)
+    ad.adz_inittraj(A.REF32, px, wp)
+    outs = {k: torch.zeros(ad.ext_shape, dtype=torch.float32, device="cuda") for k in ("u", "v", "w")}
+    tro = [torch.zeros(ad.ext_shape, dtype=torch.float32, device="cuda") for _ in dev["tracers"]]
+    for _ in range(2):
+        o_out = st.step(np_in)
+        A.step_fused(ad, A.REF32, cfg.dt, dev, dev, dev["tracers"], px, wp, outs, tro, cfg.mono)
+    assert ad.status() == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(_bits(px.cpu().numpy()), _bits(st.pxyzm))
+    assert np.array_equal(_bits(wp.cpu().numpy()), _bits(st.wpxyz))
+    for k, s in (("u", 1), ("v", 2), ("w", 3)):
+        m = ad.range_mask(s).numpy()
+        assert np.array_equal(_bits(outs[k].cpu().numpy()[m]), _bits(o_out[k][m])), k
+    m = ad.range_mask(3).numpy()
+    for a, b in zip(tro, o_out["tracers"]):
+        assert np.array_equal(_bits(a.cpu().numpy()[m]), _bits(b[m]))
+
+
 def test_step_fp64_bit_exact_stretched_levels(A):
     from gem_b200 import synth
     cfg = synth.config_large(96, 80, 80)
