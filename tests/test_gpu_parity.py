@@ -302,31 +302,36 @@ def test_cfl_above_maxcfl_clips(A, lam):
         assert np.array_equal(_bits(a.cpu().numpy()[m]), _bits(b[m]))
 
 
-def test_step_ref32_bit_exact_full_size(A):
+@pytest.mark.parametrize("prec_name", ["ref32", "fp64"])
+def test_step_bit_exact_full_size(A, prec_name):
     """The benchmark tile itself: 1024x1024x80 (84 M arrival points, ext
-    arrays of 85 M cells), u, v, w + 4 tracers, a cold and a warm step, REF32
-    bit-exact with the reference-linked oracle on every point of every set.
-    The oracle runs on all host cores."""
+    arrays of 85 M cells), u, v, w + 4 tracers, a cold and a warm step, bit
+    for bit on every point of every set: REF32 against the reference-linked
+    oracle, FP64 against the FP64 oracle.  The oracle runs on all host cores."""
     from gem_b200 import synth
+    prec = A.PREC_NAMES[prec_name]
+    dt = A._field_dtype(prec)
     cfg = synth.config_large(1024, 1024, 80)
     cfg.mono = True
-    g = synth.make_inputs(cfg, device="cuda", dtype=torch.float32)
-    dev = g
-    np_in = {k: (v.cpu().numpy() if torch.is_tensor(v) else [t.cpu().numpy() for t in v]) for k, v in g.items()}
-    kind = "ref" if O.have_ref() else "oracle"
-    st = O.Step(cfg, kind=kind, prec="f32", threads=os.cpu_count() or 1)
+    dev = synth.make_inputs(cfg, device="cuda", dtype=dt)
+    np_in = {k: (v.cpu().numpy() if torch.is_tensor(v) else [t.cpu().numpy() for t in v]) for k, v in dev.items()}
+    if prec == A.REF32:
+        st = O.Step(cfg, kind="ref" if O.have_ref() else "oracle", prec="f32", threads=os.cpu_count() or 1)
+    else:
+        st = O.Step(cfg, kind="oracle", prec="f64", threads=os.cpu_count() or 1)
     st.inittraj()
     ad = A.Adz.from_config(cfg)
-    px, wp = ad.new_state(A.REF32)
-    ad.adz_inittraj(A.REF32, px, wp)
-    outs = {k: torch.zeros(ad.ext_shape, dtype=torch.float32, device="cuda") for k in ("u", "v", "w")}
-    tro = [torch.zeros(ad.ext_shape, dtype=torch.float32, device="cuda") for _ in dev["tracers"]]
+    px, wp = ad.new_state(prec)
+    ad.adz_inittraj(prec, px, wp)
+    outs = {k: torch.zeros(ad.ext_shape, dtype=dt, device="cuda") for k in ("u", "v", "w")}
+    tro = [torch.zeros(ad.ext_shape, dtype=dt, device="cuda") for _ in dev["tracers"]]
     for _ in range(2):
         o_out = st.step(np_in)
-        A.step_fused(ad, A.REF32, cfg.dt, dev, dev, dev["tracers"], px, wp, outs, tro, cfg.mono)
+        A.step_fused(ad, prec, cfg.dt, dev, dev, dev["tracers"], px, wp, outs, tro, cfg.mono)
     assert ad.status() == 0
     torch.cuda.synchronize()
-    assert np.array_equal(_bits(px.cpu().numpy()), _bits(st.pxyzm))
+    if prec == A.REF32:
+        assert np.array_equal(_bits(px.cpu().numpy()), _bits(st.pxyzm))
     assert np.array_equal(_bits(wp.cpu().numpy()), _bits(st.wpxyz))
     for k, s in (("u", 1), ("v", 2), ("w", 3)):
         m = ad.range_mask(s).numpy()
