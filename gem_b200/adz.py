@@ -113,6 +113,7 @@ def lib() -> C.CDLL:
         L.adzc_state_save.argtypes = [vp, i, vp, vp, C.c_char_p]
         L.adzc_state_load.argtypes = [vp, i, vp, vp, C.c_char_p]
         L.adzc_slt_winds.argtypes = [vp, vp, vp]
+        L.adzc_rhs_perturbation.argtypes = [vp, vp, i]
         L.adzc_halo_layout.argtypes = [vp, i, vp]
         L.adzc_halo_pack.argtypes = [vp, i, vp, vp, vp]
         L.adzc_halo_unpack.argtypes = [vp, i, vp, vp, vp]
@@ -297,6 +298,14 @@ class Adz:
         self._slt = (uslt, vslt)
         _check(lib().adzc_slt_winds(self.h, None if uslt is None else uslt.data_ptr(),
                                     None if vslt is None else vslt.data_ptr()), "adzc_slt_winds")
+
+    def set_rhs_perturbation(self, mcrhsint=None):
+        """mcrhsint (nj, ni) device tensor of the field type: every later
+        interpolation writes value + mcrhsint * |value - lin|; None clears."""
+        self._pert = mcrhsint
+        ld = 0 if mcrhsint is None else mcrhsint.stride(0)
+        _check(lib().adzc_rhs_perturbation(self.h, None if mcrhsint is None else mcrhsint.data_ptr(), ld),
+               "adzc_rhs_perturbation")
 
     def adz_tricub_hlt(self, prec: int, set_id: int, srcs, dsts, mono=None, post=None, stream=None):
         """Interpolate srcs at position set set_id into dsts (ext layout).

@@ -317,6 +317,10 @@ struct adzc_handle {
   // positions when the grid's slt_winds is set (adzc_slt_winds)
   const void* uslt = nullptr;
   const void* vslt = nullptr;
+  // mcrhsint (field type, element (1,1), row stride pert_ld): the ensemble
+  // perturbation of every interpolation while set (adzc_rhs_perturbation)
+  const void* pert = nullptr;
+  int pert_ld = 0;
 };
 
 static int build_search(const std::vector<double>& z, int nk, double sig, const std::vector<double>& delz,
@@ -655,6 +659,8 @@ adz::SetArgs set_args(const adzc_handle* h) {
   if (h->g.bc_lam_flux != 0 && I.k0 > 1) a.k00 = 1;
   a.uslt = h->uslt;
   a.vslt = h->vslt;
+  a.pert = h->pert;
+  a.pert_ld = h->pert_ld;
   return a;
 }
 
@@ -670,6 +676,13 @@ extern "C" int adzc_slt_winds(adzc_handle* h, const void* uslt, const void* vslt
   if (!h || (!uslt) != (!vslt)) return fail(ADZC_ERR_ARG);
   h->uslt = uslt;
   h->vslt = vslt;
+  return ADZC_OK;
+}
+
+extern "C" int adzc_rhs_perturbation(adzc_handle* h, const void* mcrhsint, int ld) {
+  if (!h || (mcrhsint && ld < h->g.ni)) return fail(ADZC_ERR_ARG);
+  h->pert = mcrhsint;
+  h->pert_ld = mcrhsint ? ld : 0;
   return ADZC_OK;
 }
 
@@ -1003,9 +1016,11 @@ void adz_internal_after_traject(adzc_handle* h) {
 
 adz::DtSplit adz_internal_dt_split(const adzc_grid& g, double dt) { return dt_split(g, dt); }
 
-void adz_internal_slt(const adzc_handle* h, const void** uslt, const void** vslt) {
-  *uslt = h ? h->uslt : nullptr;
-  *vslt = h ? h->vslt : nullptr;
+void adz_internal_set_inputs(const adzc_handle* h, adz::SetArgs* a) {
+  a->uslt = h ? h->uslt : nullptr;
+  a->vslt = h ? h->vslt : nullptr;
+  a->pert = h ? h->pert : nullptr;
+  a->pert_ld = h ? h->pert_ld : 0;
 }
 
 void adz_internal_record_positions(adzc_handle* h, int prec, double* wpxyz, const void* zdt0, const adz::DtSplit& dt) {

@@ -22,8 +22,10 @@ int adz_internal_fail(int status);
 int adz_internal_scratch(adzc_handle* h, int prec, void** uvw, void** wdep);
 // a handle-owned device buffer of at least bytes for auxiliary passes (mass fixers)
 int adz_internal_aux(adzc_handle* h, size_t bytes, void** p);
-// the surface-layer winds registered with adzc_slt_winds (NULL when none)
-void adz_internal_slt(const adzc_handle* h, const void** uslt, const void** vslt);
+// the optional inputs of the position sets registered on the handle: the
+// surface-layer winds (adzc_slt_winds) and the perturbation pattern
+// (adzc_rhs_perturbation); NULL when not set
+void adz_internal_set_inputs(const adzc_handle* h, adz::SetArgs* a);
 // restore the iteration state (cold start pending, Adz_niter) from a restart
 void adz_internal_set_iteration(adzc_handle* h, int cold, int niter);
 

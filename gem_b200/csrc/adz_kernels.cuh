@@ -501,6 +501,15 @@ __device__ __forceinline__ void set_position(const DGrid& g, const SetArgs& a, i
   pz = zindx_t(g, ztv);
 }
 
+// the ensemble perturbation pattern mcrhsint(i, j) (adz_interp_hlt.F90:99,
+// 125-133): dst = value + mcrhsint * |value - lin|, before any clip
+template <typename T>
+__device__ __forceinline__ T pert_at(const SetArgs& a, int i, int j) {
+  return __ldg((const T*)a.pert + (long long)(i - 1) + (long long)(j - 1) * a.pert_ld);
+}
+__device__ __forceinline__ float fabs_(float x) { return fabsf(x); }
+__device__ __forceinline__ double fabs_(double x) { return fabs(x); }
+
 template <int PREC, bool CG = false>
 __device__ __forceinline__ void set_point(const DGrid& g, int set, const SetArgs& a, const FieldPtrs& fp, int i,
                                           int j, int k) {
@@ -516,13 +525,16 @@ __device__ __forceinline__ void set_point(const DGrid& g, int set, const SetArgs
     if (!stencil_ok(g, w.off)) { raise_status(g.status, kErrHalo); return; }
     for (int q = 0; q < fp.nf; q++) {
       const float* f = (const float*)fp.src[q] + e111 + w.off;
-      if ((fp.mono_mask >> q) & 1u) {
+      if (((fp.mono_mask >> q) & 1u) || a.pert) {
         float d, lin, mn, mx;
         interp_mono_mixed(f, w, lv.ni, lv.nij, d, lin, mn, mx);
+        if (a.pert) d = d + pert_at<float>(a, i, j) * fabsf(d - lin);
         if ((fp.clip_mask >> q) & 1u) d = fmaxf(mn, fminf(mx, d));
-        if (fp.lin[q]) ((float*)fp.lin[q])[e] = fmaxf(mn, fminf(mx, lin));
-        if (fp.mn[q]) ((float*)fp.mn[q])[e] = mn;
-        if (fp.mx[q]) ((float*)fp.mx[q])[e] = mx;
+        if ((fp.mono_mask >> q) & 1u) {  // post arrays of mono fields
+          if (fp.lin[q]) ((float*)fp.lin[q])[e] = fmaxf(mn, fminf(mx, lin));
+          if (fp.mn[q]) ((float*)fp.mn[q])[e] = mn;
+          if (fp.mx[q]) ((float*)fp.mx[q])[e] = mx;
+        }
         ((float*)fp.dst[q])[e] = d;
       } else {
         ((float*)fp.dst[q])[e] = interp1_mixed(f, w, lv.ni, lv.nij);
@@ -536,15 +548,19 @@ __device__ __forceinline__ void set_point(const DGrid& g, int set, const SetArgs
     if (!stencil_ok(g, off)) { raise_status(g.status, kErrHalo); return; }
     for (int q = 0; q < fp.nf; q++) {
       const F* f = (const F*)fp.src[q] + e111 + off;
-      if ((fp.mono_mask >> q) & 1u) {
+      if (((fp.mono_mask >> q) & 1u) || a.pert) {
         double d, lin, mn, mx;
         interp_mono_exact<F>(f, c, lv.ni, lv.nij, zl, fp.box222 != 0, d, lin, mn, mx);
         F df = (F)d, lf = (F)lin, mnf = (F)mn, mxf = (F)mx;
+        // mcrhsint perturbation in the field type (adz_interp_hlt.F90:125-133)
+        if (a.pert) df = df + pert_at<F>(a, i, j) * fabs_(df - lf);
         // Adz_post lin/min/max (adz_interp_hlt.F90:156-158), clip of adz_post_tr.F90:86-89
         if ((fp.clip_mask >> q) & 1u) df = (mnf > ((mxf < df) ? mxf : df)) ? mnf : ((mxf < df) ? mxf : df);
-        if (fp.lin[q]) ((F*)fp.lin[q])[e] = (mnf > ((mxf < lf) ? mxf : lf)) ? mnf : ((mxf < lf) ? mxf : lf);
-        if (fp.mn[q]) ((F*)fp.mn[q])[e] = mnf;
-        if (fp.mx[q]) ((F*)fp.mx[q])[e] = mxf;
+        if ((fp.mono_mask >> q) & 1u) {  // post arrays of mono fields
+          if (fp.lin[q]) ((F*)fp.lin[q])[e] = (mnf > ((mxf < lf) ? mxf : lf)) ? mnf : ((mxf < lf) ? mxf : lf);
+          if (fp.mn[q]) ((F*)fp.mn[q])[e] = mnf;
+          if (fp.mx[q]) ((F*)fp.mx[q])[e] = mxf;
+        }
         ((F*)fp.dst[q])[e] = df;
       } else {
         ((F*)fp.dst[q])[e] = (F)interp1_exact<F>(f, c, lv.ni, lv.nij, zl);
@@ -610,6 +626,7 @@ __device__ __forceinline__ void qv_point(const DGrid& g, const SetArgs& a, const
     for (int q = 0; q < fp.nf; q++) {
       float d, lin, mn, mx;
       interp_qv_mixed((const float*)fp.src[q] + base, g.nit, g.nij, c, w, d, lin, mn, mx);
+      if (a.pert) d = d + pert_at<float>(a, i, j) * fabsf(d - lin);
       if ((fp.clip_mask >> q) & 1u) d = fmaxf(mn, fminf(mx, d));
       if (fp.lin[q]) ((float*)fp.lin[q])[e] = fmaxf(mn, fminf(mx, lin));
       if (fp.mn[q]) ((float*)fp.mn[q])[e] = mn;
@@ -620,6 +637,7 @@ __device__ __forceinline__ void qv_point(const DGrid& g, const SetArgs& a, const
     for (int q = 0; q < fp.nf; q++) {
       F d, lin, mn, mx;
       interp_qv_exact<F>((const F*)fp.src[q] + base, g.nit, g.nij, c, d, lin, mn, mx);
+      if (a.pert) d = d + pert_at<F>(a, i, j) * fabs_(d - lin);
       if ((fp.clip_mask >> q) & 1u) d = (mn > ((mx < d) ? mx : d)) ? mn : ((mx < d) ? mx : d);
       if (fp.lin[q]) ((F*)fp.lin[q])[e] = (mn > ((mx < lin) ? mx : lin)) ? mn : ((mx < lin) ? mx : lin);
       if (fp.mn[q]) ((F*)fp.mn[q])[e] = mn;

@@ -133,7 +133,7 @@ extern "C" int adzc_step_noalloc(adzc_handle* h, int prec, double dt, int niter,
   sa.dt = a.dt;
   sa.k00 = std::max(I.k0t - 1, 1);
   if (G.bc_lam_flux != 0 && I.k0 > 1) sa.k00 = 1;
-  adz_internal_slt(h, &sa.uslt, &sa.vslt);
+  adz_internal_set_inputs(h, &sa);
   int f0 = 0;
   for (int set = 0; set < 4; set++) {
     const int nf = nfields[set];

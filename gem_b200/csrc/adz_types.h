@@ -111,8 +111,10 @@ struct SetArgs {
   const void* zdt0;
   const void* uslt;    // optional surface-layer winds (ni,nj)
   const void* vslt;
+  const void* pert;    // optional mcrhsint (field type, element (1,1), row stride pert_ld)
   DtSplit dt;
   int k00;             // interp_traj k00
+  int pert_ld;
 };
 
 

@@ -305,8 +305,15 @@ void SFX(orc_interp_traj)(const orc_set *s, double dt, const double *wpxyz, cons
 
 /* adz_tricub_hlt (adz_interp_hlt.F90:98-182) plus the clip of
  * adz_post_tr.F90:81-94: one kernel call per k-plane of the set's range. */
-void SFX(orc_tricub)(const orc_set *s, int set, const REAL *pos, int m, const REAL *const *srcs, REAL *const *dsts,
-                     int mono, int clip, REAL *const *lin, REAL *const *mn, REAL *const *mx) {
+static REAL SFX(rabs)(REAL x) { return IS_F32 ? (REAL)fabsf((float)x) : (REAL)fabs((double)x); }
+
+/* pert: mcrhsint (element (1,1), rows ld apart) or NULL; when set, every
+ * field takes the mono path for its trilinear value and dst = value +
+ * mcrhsint(i,j) * abs(value - lin) in REAL, before the clip
+ * (adz_interp_hlt.F90:99-100, 125-133) */
+void SFX(orc_tricub_p)(const orc_set *s, int set, const REAL *pos, int m, const REAL *const *srcs,
+                       REAL *const *dsts, int mono, int clip, REAL *const *lin, REAL *const *mn, REAL *const *mx,
+                       const REAL *pert, int ld) {
   int r[5];
   set_range(s, set, r);
   const int nk = s->g.nk;
@@ -322,19 +329,20 @@ void SFX(orc_tricub)(const orc_set *s, int set, const REAL *pos, int m, const RE
 #pragma omp for schedule(static)
     for (int k = r[4]; k <= nk; k++) {
       const REAL *p = pos + 3 * (long)(k - r[4]) * np;
+      const int linmima = mono || pert;
 #if IS_F32
 #ifdef ORC_USE_REF
       void *zt = (set == 3) ? ref_ztab_t_of(s) : ref_ztab_m_of(s);
-      if (mono) Tricublin_mono_zyx_m_n(wrk, wl, wmi, wma, fs, (pxpypz *)p, zt, (int)np, m);
+      if (linmima) Tricublin_mono_zyx_m_n(wrk, wl, wmi, wma, fs, (pxpypz *)p, zt, (int)np, m);
       else Tricublin_zyx1_m_n(wrk, fs, (pxpypz *)p, zt, (int)np, m);
 #else
       const orc_ztab *zt = (set == 3) ? s->ztab_t : s->ztab_m;
-      if (mono) orc_mono_m_n_f32(wrk, wl, wmi, wma, (const float *const *)fs, p, zt, (int)np, m, 0);
+      if (linmima) orc_mono_m_n_f32(wrk, wl, wmi, wma, (const float *const *)fs, p, zt, (int)np, m, 0);
       else orc_zyx1_m_n_f32(wrk, (const float *const *)fs, p, zt, (int)np, m);
 #endif
 #else
       const orc_ztab *zt = (set == 3) ? s->ztab_t : s->ztab_m;
-      if (mono) orc_mono_m_n_f64(wrk, wl, wmi, wma, (const double *const *)fs, p, zt, (int)np, m);
+      if (linmima) orc_mono_m_n_f64(wrk, wl, wmi, wma, (const double *const *)fs, p, zt, (int)np, m);
       else orc_zyx1_m_n_f64(wrk, (const double *const *)fs, p, zt, (int)np, m);
 #endif
       for (int q = 0; q < m; q++)
@@ -343,6 +351,10 @@ void SFX(orc_tricub)(const orc_set *s, int set, const REAL *pos, int m, const RE
             long w = q * np + (i - r[0]) + (j - r[2]) * nx;
             long e = EXT(i, j, k);
             REAL d = wrk[w];
+            if (pert) {
+              const REAL pt = pert[(i - 1) + (long)(j - 1) * ld] * SFX(rabs)(d - wl[w]);
+              d = d + pt;
+            }
             if (mono) {
               REAL lo = wmi[w], hi = wma[w];
               if (lin && lin[q]) lin[q][e] = SFX(rmax)(lo, SFX(rmin)(hi, wl[w]));
@@ -356,6 +368,11 @@ void SFX(orc_tricub)(const orc_set *s, int set, const REAL *pos, int m, const RE
     free(fs);
     free(wrk);
   }
+}
+
+void SFX(orc_tricub)(const orc_set *s, int set, const REAL *pos, int m, const REAL *const *srcs, REAL *const *dsts,
+                     int mono, int clip, REAL *const *lin, REAL *const *mn, REAL *const *mx) {
+  SFX(orc_tricub_p)(s, set, pos, m, srcs, dsts, mono, clip, lin, mn, mx, NULL, 0);
 }
 
 /* BICUBH_QV at one position: bicubHQV_lin_mono.F90:66-147 (coefficients)
@@ -475,8 +492,8 @@ static void SFX(qv_point)(const REAL *src, long ni, const double cx[4], const do
 
 /* adz_tricub_hlt with F_QV_L (adz_interp_hlt.F90:113-116 and the scatter of
  * :119-158) on position set t, plus the clip of adz_post_tr.F90:81-94. */
-void SFX(orc_tricub_qv)(const orc_set *s, const REAL *pos, int m, const REAL *const *srcs, REAL *const *dsts,
-                        int clip, REAL *const *lin, REAL *const *mn, REAL *const *mx) {
+void SFX(orc_tricub_qv_p)(const orc_set *s, const REAL *pos, int m, const REAL *const *srcs, REAL *const *dsts,
+                          int clip, REAL *const *lin, REAL *const *mn, REAL *const *mx, const REAL *pert, int ld) {
   int r[5];
   set_range(s, 3, r);
   const int nk = s->g.nk;
@@ -494,6 +511,10 @@ void SFX(orc_tricub_qv)(const orc_set *s, const REAL *pos, int m, const REAL *co
         for (int q = 0; q < m; q++) {
           REAL d, l, lo, hi;
           SFX(qv_point)(srcs[q] + o, s->nit, cx, cy, qz, lx, ly, lz, po, &d, &l, &lo, &hi);
+          if (pert) {
+            const REAL pt = pert[(i - 1) + (long)(j - 1) * ld] * SFX(rabs)(d - l);
+            d = d + pt;
+          }
           if (lin && lin[q]) lin[q][e] = SFX(rmax)(lo, SFX(rmin)(hi, l));
           if (mn && mn[q]) mn[q][e] = lo;
           if (mx && mx[q]) mx[q][e] = hi;
@@ -502,6 +523,11 @@ void SFX(orc_tricub_qv)(const orc_set *s, const REAL *pos, int m, const REAL *co
         }
       }
   }
+}
+
+void SFX(orc_tricub_qv)(const orc_set *s, const REAL *pos, int m, const REAL *const *srcs, REAL *const *dsts,
+                        int clip, REAL *const *lin, REAL *const *mn, REAL *const *mx) {
+  SFX(orc_tricub_qv_p)(s, pos, m, srcs, dsts, clip, lin, mn, mx, NULL, 0);
 }
 
 /* almost_zero (modelutils almost_zero.F90:16-36), bit for bit, including its

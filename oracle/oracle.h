@@ -144,6 +144,21 @@ void orc_tricub_qv_f32(const orc_set *s, const float *pos, int m, const float *c
 void orc_tricub_qv_f64(const orc_set *s, const double *pos, int m, const double *const *srcs, double *const *dsts,
                        int clip, double *const *lin, double *const *mn, double *const *mx);
 
+/* the same with the ensemble perturbation mcrhsint (element (1,1), rows ld
+ * apart; NULL: none): dst = value + mcrhsint * abs(value - lin) before the
+ * clip (adz_interp_hlt.F90:99-100, 125-133) */
+void orc_tricub_p_f32(const orc_set *s, int set, const float *pos, int m, const float *const *srcs,
+                      float *const *dsts, int mono, int clip, float *const *lin, float *const *mn, float *const *mx,
+                      const float *pert, int ld);
+void orc_tricub_p_f64(const orc_set *s, int set, const double *pos, int m, const double *const *srcs,
+                      double *const *dsts, int mono, int clip, double *const *lin, double *const *mn,
+                      double *const *mx, const double *pert, int ld);
+void orc_tricub_qv_p_f32(const orc_set *s, const float *pos, int m, const float *const *srcs, float *const *dsts,
+                         int clip, float *const *lin, float *const *mn, float *const *mx, const float *pert, int ld);
+void orc_tricub_qv_p_f64(const orc_set *s, const double *pos, int m, const double *const *srcs,
+                         double *const *dsts, int clip, double *const *lin, double *const *mn, double *const *mx,
+                         const double *pert, int ld);
+
 /* Bermejo-Conde mass fixer for one tracer (Bermejo_Conde.F90:16-251 with
  * mass_tr_PM.F90 and mass_tr_X.F90), single domain (the MPI_Allgather sums
  * of one rank).  Arrays in the ext layout; mask (ni, nj) is geomh_mask_8.

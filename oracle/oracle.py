@@ -108,6 +108,10 @@ class _Lib:
                                                         C.c_int, C.c_int, vp, vp, vp]
             getattr(L, f"orc_tricub_qv_{sfx}").argtypes = [C.POINTER(OrcSet), vp, C.c_int, vp, vp, C.c_int,
                                                            vp, vp, vp]
+            getattr(L, f"orc_tricub_p_{sfx}").argtypes = [C.POINTER(OrcSet), C.c_int, vp, C.c_int, vp, vp,
+                                                          C.c_int, C.c_int, vp, vp, vp, vp, C.c_int]
+            getattr(L, f"orc_tricub_qv_p_{sfx}").argtypes = [C.POINTER(OrcSet), vp, C.c_int, vp, vp, C.c_int,
+                                                             vp, vp, vp, vp, C.c_int]
             getattr(L, f"orc_ilmc_{sfx}").argtypes = [C.POINTER(OrcSet), vp, vp, vp, vp, C.c_int, C.c_int]
             getattr(L, f"orc_bermejo_conde_{sfx}").argtypes = [C.POINTER(OrcSet)] + [vp] * 8 + [
                 C.c_int, C.c_double, C.c_int, vp, vp, vp, vp, vp]
@@ -343,6 +347,15 @@ class Step:
             a["zdt0"].ctypes.data, self.pxyzm.ctypes.data, *(None if x is None else x.ctypes.data for x in slt),
             *(self.sets[q].ctypes.data for q in range(4)))
 
+    def set_rhs_perturbation(self, mcrhsint=None):
+        """mcrhsint (nj, ni) or None: the ensemble perturbation of every
+        later interpolation (adz_interp_hlt.F90:99-133)."""
+        self._pert = None if mcrhsint is None else np.ascontiguousarray(mcrhsint, dtype=self.dt)
+
+    def _pert_args(self):
+        p = getattr(self, "_pert", None)
+        return (None, 0) if p is None else (p.ctypes.data, p.shape[1])
+
     def tricub(self, set_id, srcs, mono=False, clip=False, post=False):
         """adz_tricub_hlt on position set set_id (0=q,1=u,2=v,3=t); returns the
         destination arrays (ext layout, range written, NaN elsewhere) and, if
@@ -359,9 +372,10 @@ class Step:
             mn = [np.full(self.ext_shape, np.nan, self.dt) for _ in range(m)]
             mx = [np.full(self.ext_shape, np.nan, self.dt) for _ in range(m)]
             lp, mnp, mxp = (C.cast(_ptrs(z, ct), C.c_void_p) for z in (lin, mn, mx))
-        getattr(self.L, f"orc_tricub_{self.prec}")(
+        pert, ld = self._pert_args()
+        getattr(self.L, f"orc_tricub_p_{self.prec}")(
             C.byref(self.s), set_id, self.sets[set_id].ctypes.data, m, C.cast(sp, C.c_void_p),
-            C.cast(dp, C.c_void_p), int(mono), int(clip), lp, mnp, mxp)
+            C.cast(dp, C.c_void_p), int(mono), int(clip), lp, mnp, mxp, pert, ld)
         if post:
             return dsts, (lin, mn, mx)
         return dsts
@@ -376,9 +390,10 @@ class Step:
         ct = C.c_float if self.prec == "f32" else C.c_double
         extra = [[np.full(self.ext_shape, np.nan, self.dt) for _ in range(m)] for _ in range(3)]
         ptr = [C.cast(_ptrs(z, ct), C.c_void_p) for z in extra]
-        getattr(self.L, f"orc_tricub_qv_{self.prec}")(
+        pert, ld = self._pert_args()
+        getattr(self.L, f"orc_tricub_qv_p_{self.prec}")(
             C.byref(self.s), self.sets[3].ctypes.data, m, C.cast(_ptrs(srcs, ct), C.c_void_p),
-            C.cast(_ptrs(dsts, ct), C.c_void_p), int(clip), *ptr)
+            C.cast(_ptrs(dsts, ct), C.c_void_p), int(clip), *ptr, pert, ld)
         if post:
             return dsts, tuple(extra)
         return dsts

@@ -210,19 +210,21 @@ def test_step_ref32_bit_exact(A, shape):
         assert np.array_equal(_bits(a.cpu().numpy()[m]), _bits(b[m]))
 
 
-@pytest.mark.parametrize("branch", ["schm_advec2", "schm_advec3", "slt_winds", "lam_gbpil_t"])
+@pytest.mark.parametrize("branch", ["schm_advec2", "schm_advec3", "slt_winds", "lam_gbpil_t", "mcrhsint"])
 def test_step_ref32_reference_branches(A, branch):
     """The less common switches of the path, REF32 bit-exact with the
     reference interpolator and the driver restatement:
     Schm_advec 2 and 3 (dt split with the off-centering weights,
     B/adz_traject.F90:38-59), Adz_slt_winds (surface-layer winds for the
     top-level pt positions, B/adz_interp_traj.F90:123-133) and
-    Lam_gbpil_t > 0 (a top pilot: k0 > 1, B/adz_set.F90:94-114)."""
+    Lam_gbpil_t > 0 (a top pilot: k0 > 1, B/adz_set.F90:94-114) and the
+    ensemble perturbation mcrhsint of every interpolation
+    (B/adz_interp_hlt.F90:99-133, momentum and tracers, before the clip)."""
     from gem_b200 import synth
     cfg = synth.config_small(40, 36, 24)
     cfg.mono = True
     kw = {"schm_advec2": dict(schm_advec=2), "schm_advec3": dict(schm_advec=3),
-          "slt_winds": dict(slt_winds=True), "lam_gbpil_t": dict(lam_gbpil_t=4)}[branch]
+          "slt_winds": dict(slt_winds=True), "lam_gbpil_t": dict(lam_gbpil_t=4), "mcrhsint": {}}[branch]
     np_in, dev = _inputs(cfg, torch.float32)
     kind = "ref" if O.have_ref() else "oracle"
     st = O.Step(cfg, kind=kind, prec="f32", **kw)
@@ -230,6 +232,10 @@ def test_step_ref32_reference_branches(A, branch):
     ad = A.Adz.from_config(cfg, **kw)
     if branch == "slt_winds":
         ad.set_slt_winds(dev["uslt"], dev["vslt"])
+    if branch == "mcrhsint":
+        mc = np.random.default_rng(23).uniform(-0.5, 0.5, (cfg.nj, cfg.ni)).astype(np.float32)
+        st.set_rhs_perturbation(mc)
+        ad.set_rhs_perturbation(torch.from_numpy(mc).cuda())
     px, wp = ad.new_state(A.REF32)
     ad.adz_inittraj(A.REF32, px, wp)
     for _ in range(2):
@@ -248,6 +254,13 @@ def test_step_ref32_reference_branches(A, branch):
     m = ad.range_mask(3).numpy()
     for a, b in zip(tro, o_out["tracers"]):
         assert np.array_equal(_bits(a.cpu().numpy()[m]), _bits(b[m]))
+    if branch == "mcrhsint":  # the pattern changes the results
+        ad.set_rhs_perturbation(None)
+        plain = torch.zeros(ad.ext_shape, dtype=torch.float32, device="cuda")
+        ad.adz_tricub_hlt(A.REF32, A.SET_U, [dev["src_u"]], [plain])
+        torch.cuda.synchronize()
+        m = ad.range_mask(1).numpy()
+        assert not np.array_equal(_bits(plain.cpu().numpy()[m]), _bits(outs["u"].cpu().numpy()[m]))
     if branch == "slt_winds":  # the switch changes the top-level results
         ad2 = A.Adz.from_config(cfg)
         px2, wp2 = ad2.new_state(A.REF32)

@@ -28,7 +28,7 @@ def _case(shape=(48, 40, 24), stretched=True):
     return cfg
 
 
-def _run(prec_name, cfg, clip=True):
+def _run(prec_name, cfg, clip=True, pert=False):
     from gem_b200 import adz as A, synth
     if not torch.cuda.is_available():
         pytest.fail("CUDA device required for -m gpu tests")
@@ -42,11 +42,17 @@ def _run(prec_name, cfg, clip=True):
     # oracle
     st = O.Step(cfg, kind="oracle", prec="f32" if prec == A.REF32 else "f64")
     st.inittraj()
+    mc = None
+    if pert:  # ensemble perturbation pattern mcrhsint (nj, ni)
+        mc = np.random.default_rng(17).uniform(-0.5, 0.5, (cfg.nj, cfg.ni)).astype(npd)
+        st.set_rhs_perturbation(mc)
     st.traject({k: v.astype(st.dt) for k, v in np_in.items()})
     o_d, (o_l, o_mn, o_mx) = st.tricub_qv([t.astype(st.dt) for t in trs], clip=clip, post=True)
     # device
     dev = {k: torch.from_numpy(v).cuda() for k, v in np_in.items()}
     ad = A.Adz.from_config(cfg)
+    if pert:
+        ad.set_rhs_perturbation(torch.from_numpy(mc).cuda())
     px, wp = ad.new_state(prec)
     ad.adz_inittraj(prec, px, wp)
     ad.adz_traject(prec, cfg.dt, dev, px, wp)
@@ -64,10 +70,11 @@ def _run(prec_name, cfg, clip=True):
     return A, ad, m, g, o
 
 
-@pytest.mark.parametrize("prec_name", ["ref32", "fp64"])
-def test_qv_bit_exact(prec_name):
+@pytest.mark.parametrize("prec_name,pert", [("ref32", False), ("fp64", False), ("ref32", True), ("fp64", True)])
+def test_qv_bit_exact(prec_name, pert):
+    """pert: with the ensemble perturbation mcrhsint set (adz_interp_hlt.F90:99-133)"""
     cfg = _case()
-    A, ad, m, g, o = _run(prec_name, cfg)
+    A, ad, m, g, o = _run(prec_name, cfg, pert=pert)
     for gi, oi in zip(g, o):
         for a, b in zip(gi, oi):
             assert np.isnan(a[~m]).all()
