@@ -225,6 +225,10 @@ extern "C" int adzc_batch_create(int prec, int ndom, const adzc_domain* doms, ad
     D.sa.k00 = std::max(I.k0t - 1, 1);
     if (G.bc_lam_flux != 0 && I.k0 > 1) D.sa.k00 = 1;
     adz_internal_set_inputs(in.h, &D.sa);
+    if (D.sa.pert) {  // the batch kernels carry no perturbation: step such a domain on its own
+      adzc_batch_destroy(b);
+      return adz_internal_fail(ADZC_ERR_ARG);
+    }
     const int r[4][5] = {{I.i0, I.in, I.j0, I.jn, I.k0},
                          {I.i0u, I.inu, I.j0, I.jn, I.k0},
                          {I.i0, I.in, I.j0v, I.jnv, I.k0},

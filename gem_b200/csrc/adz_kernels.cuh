@@ -510,7 +510,9 @@ __device__ __forceinline__ T pert_at(const SetArgs& a, int i, int j) {
 __device__ __forceinline__ float fabs_(float x) { return fabsf(x); }
 __device__ __forceinline__ double fabs_(double x) { return fabs(x); }
 
-template <int PREC, bool CG = false>
+// PERT: the mcrhsint perturbation is set (a.pert); a separate instantiation,
+// so the common path carries none of it
+template <int PREC, bool CG = false, bool PERT = false>
 __device__ __forceinline__ void set_point(const DGrid& g, int set, const SetArgs& a, const FieldPtrs& fp, int i,
                                           int j, int k) {
   using F = typename Types<PREC>::F;
@@ -525,10 +527,10 @@ __device__ __forceinline__ void set_point(const DGrid& g, int set, const SetArgs
     if (!stencil_ok(g, w.off)) { raise_status(g.status, kErrHalo); return; }
     for (int q = 0; q < fp.nf; q++) {
       const float* f = (const float*)fp.src[q] + e111 + w.off;
-      if (((fp.mono_mask >> q) & 1u) || a.pert) {
+      if (((fp.mono_mask >> q) & 1u) || PERT) {
         float d, lin, mn, mx;
         interp_mono_mixed(f, w, lv.ni, lv.nij, d, lin, mn, mx);
-        if (a.pert) d = d + pert_at<float>(a, i, j) * fabsf(d - lin);
+        if (PERT) d = d + pert_at<float>(a, i, j) * fabsf(d - lin);
         if ((fp.clip_mask >> q) & 1u) d = fmaxf(mn, fminf(mx, d));
         if ((fp.mono_mask >> q) & 1u) {  // post arrays of mono fields
           if (fp.lin[q]) ((float*)fp.lin[q])[e] = fmaxf(mn, fminf(mx, lin));
@@ -548,12 +550,12 @@ __device__ __forceinline__ void set_point(const DGrid& g, int set, const SetArgs
     if (!stencil_ok(g, off)) { raise_status(g.status, kErrHalo); return; }
     for (int q = 0; q < fp.nf; q++) {
       const F* f = (const F*)fp.src[q] + e111 + off;
-      if (((fp.mono_mask >> q) & 1u) || a.pert) {
+      if (((fp.mono_mask >> q) & 1u) || PERT) {
         double d, lin, mn, mx;
         interp_mono_exact<F>(f, c, lv.ni, lv.nij, zl, fp.box222 != 0, d, lin, mn, mx);
         F df = (F)d, lf = (F)lin, mnf = (F)mn, mxf = (F)mx;
         // mcrhsint perturbation in the field type (adz_interp_hlt.F90:125-133)
-        if (a.pert) df = df + pert_at<F>(a, i, j) * fabs_(df - lf);
+        if (PERT) df = df + pert_at<F>(a, i, j) * fabs_(df - lf);
         // Adz_post lin/min/max (adz_interp_hlt.F90:156-158), clip of adz_post_tr.F90:86-89
         if ((fp.clip_mask >> q) & 1u) df = (mnf > ((mxf < df) ? mxf : df)) ? mnf : ((mxf < df) ? mxf : df);
         if ((fp.mono_mask >> q) & 1u) {  // post arrays of mono fields
@@ -569,7 +571,7 @@ __device__ __forceinline__ void set_point(const DGrid& g, int set, const SetArgs
   }
 }
 
-template <int PREC>
+template <int PREC, bool PERT>
 __global__ void ADZ_SET_BOUNDS k_tricub_set(DGrid g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
                                             SetArgs a, FieldPtrs fp) {
   const long long nplane = (long long)nx * ny;
@@ -578,7 +580,7 @@ __global__ void ADZ_SET_BOUNDS k_tricub_set(DGrid g, int set, int i0, int nx, in
     const int i = (int)(t % nx) + i0;
     const int j = (int)((t / nx) % ny) + j0;
     const int k = (int)(t / nplane) + k0;
-    set_point<PREC>(g, set, a, fp, i, j, k);
+    set_point<PREC, false, PERT>(g, set, a, fp, i, j, k);
   }
 }
 
@@ -586,7 +588,7 @@ __global__ void ADZ_SET_BOUNDS k_tricub_set(DGrid g, int set, int i0, int nx, in
 // take consecutive parts (u, v, t ...), so every SM runs a mix of the
 // issue-bound one-field sets and the load-bound multi-field set at once;
 // each thread interpolates one arrival point of its part as k_tricub_set does
-template <int PREC>
+template <int PREC, bool PERT>
 __global__ void ADZ_SET_BOUNDS k_tricub_parts(DGrid g, SetArgs a, const __grid_constant__ SetParts sp) {
   const int q = (int)(blockIdx.x % (unsigned)sp.n);
   const SetPart& P = sp.p[q];
@@ -596,13 +598,13 @@ __global__ void ADZ_SET_BOUNDS k_tricub_parts(DGrid g, SetArgs a, const __grid_c
   const int i = (int)(t % P.nx) + P.i0;
   const int j = (int)((t / P.nx) % P.ny) + P.j0;
   const int k = (int)(t / nplane) + P.k0;
-  set_point<PREC>(g, P.set, a, P.fp, i, j, k);
+  set_point<PREC, false, PERT>(g, P.set, a, P.fp, i, j, k);
 }
 
 // BICUBH_QV fields at position set t (adz_interp_hlt.F90:113-116 with
 // F_QV_L): lin/min/max of the inner 2x2x2 box always formed, written where
 // asked; clip as adz_post_tr.F90:81-94
-template <int PREC>
+template <int PREC, bool PERT>
 __device__ __forceinline__ void qv_point(const DGrid& g, const SetArgs& a, const FieldPtrs& fp, int i, int j, int k) {
   using F = typename Types<PREC>::F;
   double px, py, pz;
@@ -626,7 +628,7 @@ __device__ __forceinline__ void qv_point(const DGrid& g, const SetArgs& a, const
     for (int q = 0; q < fp.nf; q++) {
       float d, lin, mn, mx;
       interp_qv_mixed((const float*)fp.src[q] + base, g.nit, g.nij, c, w, d, lin, mn, mx);
-      if (a.pert) d = d + pert_at<float>(a, i, j) * fabsf(d - lin);
+      if (PERT) d = d + pert_at<float>(a, i, j) * fabsf(d - lin);
       if ((fp.clip_mask >> q) & 1u) d = fmaxf(mn, fminf(mx, d));
       if (fp.lin[q]) ((float*)fp.lin[q])[e] = fmaxf(mn, fminf(mx, lin));
       if (fp.mn[q]) ((float*)fp.mn[q])[e] = mn;
@@ -637,7 +639,7 @@ __device__ __forceinline__ void qv_point(const DGrid& g, const SetArgs& a, const
     for (int q = 0; q < fp.nf; q++) {
       F d, lin, mn, mx;
       interp_qv_exact<F>((const F*)fp.src[q] + base, g.nit, g.nij, c, d, lin, mn, mx);
-      if (a.pert) d = d + pert_at<F>(a, i, j) * fabs_(d - lin);
+      if (PERT) d = d + pert_at<F>(a, i, j) * fabs_(d - lin);
       if ((fp.clip_mask >> q) & 1u) d = (mn > ((mx < d) ? mx : d)) ? mn : ((mx < d) ? mx : d);
       if (fp.lin[q]) ((F*)fp.lin[q])[e] = (mn > ((mx < lin) ? mx : lin)) ? mn : ((mx < lin) ? mx : lin);
       if (fp.mn[q]) ((F*)fp.mn[q])[e] = mn;
@@ -647,7 +649,7 @@ __device__ __forceinline__ void qv_point(const DGrid& g, const SetArgs& a, const
   }
 }
 
-template <int PREC>
+template <int PREC, bool PERT>
 __global__ void ADZ_QV_BOUNDS k_qv_set(DGrid g, int i0, int nx, int j0, int ny, int k0, int nz, SetArgs a,
                                                 FieldPtrs fp) {
   const long long nplane = (long long)nx * ny;
@@ -656,7 +658,7 @@ __global__ void ADZ_QV_BOUNDS k_qv_set(DGrid g, int i0, int nx, int j0, int ny, 
     const int i = (int)(t % nx) + i0;
     const int j = (int)((t / nx) % ny) + j0;
     const int k = (int)(t / nplane) + k0;
-    qv_point<PREC>(g, a, fp, i, j, k);
+    qv_point<PREC, PERT>(g, a, fp, i, j, k);
   }
 }
 
@@ -929,7 +931,8 @@ cudaError_t launch_tricub_set(const DGrid& g, int set, int i0, int nx, int j0, i
                               const SetArgs& a, const FieldPtrs& fp, cudaStream_t s) {
   const long long n = (long long)nx * ny * nz;
   if (n <= 0) return cudaSuccess;
-  k_tricub_set<PREC><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, set, i0, nx, j0, ny, k0, nz, a, fp);
+  if (a.pert) k_tricub_set<PREC, true><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, set, i0, nx, j0, ny, k0, nz, a, fp);
+  else k_tricub_set<PREC, false><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, set, i0, nx, j0, ny, k0, nz, a, fp);
   return cudaGetLastError();
 }
 
@@ -944,7 +947,8 @@ cudaError_t launch_tricub_parts(const DGrid& g, const SetArgs& a, const SetParts
   const long long blocks = (most + 127) / 128 * sp.n;
   if (blocks < 1) return cudaSuccess;
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
-  k_tricub_parts<PREC><<<(unsigned)blocks, 128, 0, s>>>(g, a, sp);
+  if (a.pert) k_tricub_parts<PREC, true><<<(unsigned)blocks, 128, 0, s>>>(g, a, sp);
+  else k_tricub_parts<PREC, false><<<(unsigned)blocks, 128, 0, s>>>(g, a, sp);
   return cudaGetLastError();
 }
 
@@ -953,7 +957,8 @@ cudaError_t launch_qv_set(const DGrid& g, int i0, int nx, int j0, int ny, int k0
                           const FieldPtrs& fp, cudaStream_t s) {
   const long long n = (long long)nx * ny * nz;
   if (n <= 0) return cudaSuccess;
-  k_qv_set<PREC><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, i0, nx, j0, ny, k0, nz, a, fp);
+  if (a.pert) k_qv_set<PREC, true><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, i0, nx, j0, ny, k0, nz, a, fp);
+  else k_qv_set<PREC, false><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, i0, nx, j0, ny, k0, nz, a, fp);
   return cudaGetLastError();
 }
 

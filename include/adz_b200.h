@@ -203,10 +203,10 @@ int adzc_slt_winds(adzc_handle *h, const void *uslt, const void *vslt);
 /* mcrhsint, the ensemble perturbation pattern (B/ens_setmem.F90:47): a
  * DEVICE array of the field type, element (1,1) at mcrhsint, rows ld >= ni
  * elements apart.  While set, every interpolation of the handle (adzc_tricub*,
- * adzc_step_noalloc, batches) writes value + mcrhsint(i,j) * |value - lin|
+ * adzc_step_noalloc) writes value + mcrhsint(i,j) * |value - lin|
  * (lin the trilinear value of the inner box), before any clip, as
  * adz_tricub_hlt does when mcrhsint is associated (B/adz_interp_hlt.F90:99-133).
- * NULL clears it. */
+ * NULL clears it.  adzc_batch_create refuses a handle with a pattern set. */
 int adzc_rhs_perturbation(adzc_handle *h, const void *mcrhsint, int ld);
 
 /* Every position set of the last trajectory in one call: nfields[4] fields
