@@ -25,7 +25,7 @@
 namespace adz {
 namespace mass {
 
-constexpr int kBlocks = 256;   // blocks per tracer in a reduction
+constexpr int kBlocks = 1024;  // blocks per tracer in every pass (each owns a fixed slice of rows)
 constexpr int kThreads = 256;
 
 template <typename T>
@@ -43,7 +43,7 @@ struct Tr {
 };
 
 struct State {
-  double mass_p, mass_m, fo, fi, tot_p, def, wei, lambda, bc_r, prop, bc;
+  double mass_p, mass_m, fo, fi, tot_p, def, wei, lambda, bc_r, prop, bc, wei_pos, wei_neg;
   int skip;
 };
 
@@ -77,62 +77,70 @@ __device__ __forceinline__ T bc_weight(const Tr<T>& tr, long long e, double sd) 
   return (T)(pw * sd * (double)tr.pkps[e]);
 }
 
-enum Mode { kPM = 0, kFlux = 1, kWei = 2, kM = 3 };
+enum Mode { kPMW = 0, kFlux = 1 };
+constexpr int kSums = 4;  // partial sums per block
 
-// block partial sums of one or two masses; blockIdx.y = tracer
-template <typename T, int MODE>
-__global__ void __launch_bounds__(kThreads) k_reduce(const Tr<T>* __restrict__ trs, const State* __restrict__ st,
-                                                     Region r, Geo g, const T* __restrict__ air_p,
-                                                     const T* __restrict__ air_m, double* __restrict__ part) {
-  const int q = blockIdx.y;
-  const Tr<T> tr = trs[q];
-  // block b owns a fixed slice of the region's rows (j, k); threads stride over i
+// block-wide tree sum of up to kSums values per thread (fixed order), into
+// part[(q * kBlocks + block) * kSums + c]
+__device__ __forceinline__ void block_sums(const double* v, int nv, int q, double* __restrict__ part) {
+  __shared__ double red[kSums][kThreads];
+  for (int c = 0; c < nv; c++) red[c][threadIdx.x] = v[c];
+  __syncthreads();
+  for (int o = kThreads / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int c = 0; c < nv; c++) red[c][threadIdx.x] += red[c][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int c = 0; c < nv; c++) part[((long long)q * kBlocks + blockIdx.x) * kSums + c] = red[c][0];
+}
+
+// the rows (j, k) a block owns in every pass, so each sum keeps its order
+__device__ __forceinline__ void block_rows(const Region& r, long long& r0, long long& r1) {
   const long long rows = (long long)r.ny * r.nz;
   const long long chunk = (rows + kBlocks - 1) / kBlocks;
-  const long long r0 = blockIdx.x * chunk, r1 = min(rows, r0 + chunk);
-  double s0 = 0.0, s1 = 0.0;
-  const bool skip = (MODE == kM || MODE == kWei) && st[q].skip;
-  const double sd = MODE == kWei ? sign1(st[q].def) : 1.0;
-  if (!skip && !(MODE == kFlux && (!tr.fo || !tr.fi)) && r.nx > 0) {
+  r0 = blockIdx.x * chunk;
+  r1 = min(rows, r0 + chunk);
+}
+
+// masses before the correction and the weight sums of both deficit signs in
+// one read of the fields (kPMW), or the boundary fluxes (kFlux); blockIdx.y
+// = tracer.  A point's weight is non-zero for one sign only, and its value is
+// the one bc_weight gives for that sign.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kThreads) k_reduce(const Tr<T>* __restrict__ trs, Region r, Geo g,
+                                                     const T* __restrict__ air_p, const T* __restrict__ air_m,
+                                                     double* __restrict__ part) {
+  const int q = blockIdx.y;
+  const Tr<T> tr = trs[q];
+  long long r0, r1;
+  block_rows(r, r0, r1);
+  double v[kSums] = {0.0, 0.0, 0.0, 0.0};
+  if (!(MODE == kFlux && (!tr.fo || !tr.fi)) && r.nx > 0) {
     for (long long row = r0; row < r1; row++)
+#pragma unroll 4
     for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) {
       const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
       const long long e = ext(g, i, j, k);
       const double mk = __ldg(g.mask + (i - 1) + (long long)(j - 1) * g.ni);
-      if (MODE == kPM) {
+      if (MODE == kPMW) {
         const T a = tr.p[e] * air_p[e];
         const T b = tr.m[e] * air_m[e];
-        s0 += (double)a * mk;
-        s1 += (double)b * mk;
-      } else if (MODE == kFlux) {
+        v[0] += (double)a * mk;
+        v[1] += (double)b * mk;
+        const double sd = sign1((double)(T)(tr.m[e] - tr.lin[e]));
+        const T w = bc_weight<T>(tr, e, sd) * air_m[e];
+        if (sd > 0.0) v[2] += (double)w * mk;
+        else v[3] += (double)w * mk;
+      } else {
         const T a = tr.fo[e] * air_m[e];
         const T b = tr.fi[e] * air_m[e];
-        s0 += (double)a * mk;
-        s1 += (double)b * mk;
-      } else if (MODE == kWei) {
-        const T a = bc_weight<T>(tr, e, sd) * air_m[e];
-        s0 += (double)a * mk;
-      } else {
-        const T a = tr.m[e] * air_m[e];
-        s0 += (double)a * mk;
+        v[0] += (double)a * mk;
+        v[1] += (double)b * mk;
       }
     }
   }
-  __shared__ double red[2][kThreads];
-  red[0][threadIdx.x] = s0;
-  red[1][threadIdx.x] = s1;
-  __syncthreads();
-  for (int o = kThreads / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) {
-      red[0][threadIdx.x] += red[0][threadIdx.x + o];
-      red[1][threadIdx.x] += red[1][threadIdx.x + o];
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    part[((long long)q * kBlocks + blockIdx.x) * 2 + 0] = red[0][0];
-    part[((long long)q * kBlocks + blockIdx.x) * 2 + 1] = red[1][0];
-  }
+  block_sums(v, MODE == kPMW ? 4 : 2, q, part);
 }
 
 // almost_zero (modelutils almost_zero.F90:16-36), bit for bit
@@ -142,7 +150,7 @@ __device__ __forceinline__ bool almost_zero(double a) {
   return bits >= -1 && bits <= 1;
 }
 
-enum Stage { kAfterPM = 0, kAfterFlux = 1, kAfterWei = 2, kAfterBcR = 3, kAfterBc = 4 };
+enum Stage { kAfterPMW = 0, kAfterFlux = 1, kAfterBcR = 2, kAfterBc = 3 };
 
 // one thread per tracer: partials in index order, then the scalar formulas
 template <int STAGE>
@@ -150,32 +158,35 @@ __global__ void k_finish(const double* __restrict__ part, State* __restrict__ st
                          double* __restrict__ deficit, double* __restrict__ diag) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= ntr) return;
-  double s0 = 0.0, s1 = 0.0;
-  for (int b = 0; b < kBlocks; b++) {
-    s0 += part[((long long)q * kBlocks + b) * 2 + 0];
-    s1 += part[((long long)q * kBlocks + b) * 2 + 1];
-  }
+  double s[kSums] = {0.0, 0.0, 0.0, 0.0};
+  for (int b = 0; b < kBlocks; b++)
+    for (int c = 0; c < kSums; c++) s[c] += part[((long long)q * kBlocks + b) * kSums + c];
   State& S = st[q];
-  if (STAGE == kAfterPM) {
+  if (STAGE == kAfterPMW) {
     S = State{};
-    S.mass_p = s0;
-    S.mass_m = s1;
-  } else if (STAGE == kAfterFlux) {
-    S.fo = s0;
-    S.fi = s1;
-  } else if (STAGE == kAfterWei) {
-    S.wei = s0;
-    S.skip = almost_zero(s0) ? 1 : 0;
-    S.lambda = S.skip ? 0.0 : S.def / s0;
+    S.mass_p = s[0];
+    S.mass_m = s[1];
+    S.wei_pos = s[2];
+    S.wei_neg = s[3];
+  } else if (STAGE == kAfterFlux) {  // Bermejo_Conde.F90:70-84, then the weight sum of the deficit's sign
+    S.fo = s[0];
+    S.fi = s[1];
+    const double bflux = S.fi - S.fo;
+    const double mp = S.mass_p - deficit[q];
+    S.tot_p = mp + bflux;
+    S.def = S.mass_m - S.tot_p;
+    S.wei = sign1(S.def) > 0.0 ? S.wei_pos : S.wei_neg;
+    S.skip = almost_zero(S.wei) ? 1 : 0;
+    S.lambda = S.skip ? 0.0 : S.def / S.wei;
   } else if (STAGE == kAfterBcR) {
     if (!S.skip) {
-      S.bc_r = s0;
-      S.prop = S.tot_p / s0;
+      S.bc_r = s[0];
+      S.prop = S.tot_p / s[0];
     }
   } else {
     if (!S.skip) {
-      S.bc = s0;
-      deficit[q] = s0 - S.tot_p;  // Bermejo_Conde.F90:225-243
+      S.bc = s[0];
+      deficit[q] = s[0] - S.tot_p;  // Bermejo_Conde.F90:225-243
     }
     if (diag) {
       double* d = diag + 8 * q;
@@ -183,55 +194,71 @@ __global__ void k_finish(const double* __restrict__ part, State* __restrict__ st
       d[4] = S.wei; d[5] = S.lambda; d[6] = S.bc_r; d[7] = S.bc;
     }
   }
-  if (STAGE == kAfterFlux) {  // Bermejo_Conde.F90:70-84 (the flux stage always runs, sums 0 without fluxes)
-    const double bflux = S.fi - S.fo;
-    const double mp = S.mass_p - deficit[q];
-    S.tot_p = mp + bflux;
-    S.def = S.mass_m - S.tot_p;
-  }
 }
 
-// m - lambda w, clipped to the bound box when min_max (Bermejo_Conde.F90:163-199)
+// m - lambda w, clipped to the bound box when min_max (Bermejo_Conde.F90:163-199),
+// and the mass of the corrected field in the same pass
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_correct(const Tr<T>* __restrict__ trs, const State* __restrict__ st,
-                                                      Region r, Geo g, int min_max) {
+                                                      Region r, Geo g, const T* __restrict__ air_m, int min_max,
+                                                      double* __restrict__ part) {
   const int q = blockIdx.y;
-  if (st[q].skip) return;
   const Tr<T> tr = trs[q];
+  const bool skip = st[q].skip;
   const double lambda = st[q].lambda, sd = sign1(st[q].def);
-  const long long rows = (long long)r.ny * r.nz;
-  for (long long row = blockIdx.x; row < rows; row += gridDim.x)
-  for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) {
-    const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
-    const long long e = ext(g, i, j, k);
-    const double corr = lambda * (double)bc_weight<T>(tr, e, sd);
-    if (!min_max) {
-      tr.m[e] = (T)((double)tr.m[e] - corr);
-    } else {
-      const T wrk = (T)((double)tr.m[e] - corr);
-      T v = wrk;
-      if (corr > 0.0 && wrk < tr.mn[e]) v = tr.mn[e];
-      if (corr < 0.0 && wrk > tr.mx[e]) v = tr.mx[e];
-      tr.m[e] = v;
+  long long r0, r1;
+  block_rows(r, r0, r1);
+  double v = 0.0;
+  if (!skip && r.nx > 0) {
+    for (long long row = r0; row < r1; row++)
+#pragma unroll 4
+    for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) {
+      const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
+      const long long e = ext(g, i, j, k);
+      const double corr = lambda * (double)bc_weight<T>(tr, e, sd);
+      T nv;
+      if (!min_max) {
+        nv = (T)((double)tr.m[e] - corr);
+      } else {
+        const T wrk = (T)((double)tr.m[e] - corr);
+        nv = wrk;
+        if (corr > 0.0 && wrk < tr.mn[e]) nv = tr.mn[e];
+        if (corr < 0.0 && wrk > tr.mx[e]) nv = tr.mx[e];
+      }
+      tr.m[e] = nv;
+      const T a = nv * air_m[e];
+      v += (double)a * __ldg(g.mask + (i - 1) + (long long)(j - 1) * g.ni);
     }
   }
+  block_sums(&v, 1, q, part);
 }
 
-// proportional rescale after the clipped correction (Bermejo_Conde.F90:203-222)
+// proportional rescale after the clipped correction (Bermejo_Conde.F90:203-222),
+// and the final mass in the same pass
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_scale(const Tr<T>* __restrict__ trs, const State* __restrict__ st,
-                                                    Region r, Geo g) {
+                                                    Region r, Geo g, const T* __restrict__ air_m,
+                                                    double* __restrict__ part) {
   const int q = blockIdx.y;
-  if (st[q].skip) return;
   T* m = trs[q].m;
+  const bool skip = st[q].skip;
   const double prop = st[q].prop;
-  const long long rows = (long long)r.ny * r.nz;
-  for (long long row = blockIdx.x; row < rows; row += gridDim.x)
-  for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) {
-    const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
-    const long long e = ext(g, i, j, k);
-    m[e] = (T)(prop * (double)m[e]);
+  long long r0, r1;
+  block_rows(r, r0, r1);
+  double v = 0.0;
+  if (!skip && r.nx > 0) {
+    for (long long row = r0; row < r1; row++)
+#pragma unroll 4
+    for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) {
+      const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
+      const long long e = ext(g, i, j, k);
+      const T nv = (T)(prop * (double)m[e]);
+      m[e] = nv;
+      const T a = nv * air_m[e];
+      v += (double)a * __ldg(g.mask + (i - 1) + (long long)(j - 1) * g.ni);
+    }
   }
+  block_sums(&v, 1, q, part);
 }
 
 }  // namespace mass
@@ -269,23 +296,19 @@ int run_bc(int ntr, const adzc_bc_tracer* in, const void* airm_p, const void* ai
   const T* ap = (const T*)airm_p;
   const T* am = (const T*)airm_m;
   const int fb = (ntr + 127) / 128;
-  const long long crows = (long long)core.ny * core.nz;
-  const dim3 eg((unsigned)std::max<long long>(1, std::min<long long>(crows, 2048)), ntr);
   Geo gm = g;
   gm.mask = mask;
-  k_reduce<T, kPM><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, ap, am, d_part);
-  k_finish<kAfterPM><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
-  k_reduce<T, kFlux><<<rg, kThreads, 0, s>>>(d_tr, d_st, brange, gm, ap, am, d_part);
+  // four passes over the fields: masses and weights; fluxes (boundary only);
+  // correction with its mass; rescale with the final mass (clipped only)
+  k_reduce<T, kPMW><<<rg, kThreads, 0, s>>>(d_tr, core, gm, ap, am, d_part);
+  k_finish<kAfterPMW><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
+  k_reduce<T, kFlux><<<rg, kThreads, 0, s>>>(d_tr, brange, gm, ap, am, d_part);
   k_finish<kAfterFlux><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
-  k_reduce<T, kWei><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, ap, am, d_part);
-  k_finish<kAfterWei><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
-  k_correct<T><<<eg, kThreads, 0, s>>>(d_tr, d_st, core, gm, min_max);
+  k_correct<T><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, am, min_max, d_part);
   if (min_max) {
-    k_reduce<T, kM><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, ap, am, d_part);
     k_finish<kAfterBcR><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
-    k_scale<T><<<eg, kThreads, 0, s>>>(d_tr, d_st, core, gm);
+    k_scale<T><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, am, d_part);
   }
-  k_reduce<T, kM><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, ap, am, d_part);
   k_finish<kAfterBc><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
   return cudaGetLastError() == cudaSuccess ? ADZC_OK : ADZC_ERR_CUDA;
 }
@@ -319,7 +342,7 @@ extern "C" int adzc_bermejo_conde(adzc_handle* h, int prec, int ntr, const adzc_
   Geo g{D.lminx, D.lminy, D.nit, D.ni, D.nij, mask};
   const size_t ts = prec == ADZC_FP64 ? sizeof(Tr<double>) : sizeof(Tr<float>);
   const size_t bytes = ((ntr * ts + 255) & ~size_t(255)) + ((ntr * sizeof(State) + 255) & ~size_t(255)) +
-                       (size_t)ntr * kBlocks * 2 * sizeof(double);
+                       (size_t)ntr * kBlocks * kSums * sizeof(double);
   void* scratch = nullptr;
   if (adz_internal_aux(h, bytes, &scratch) != ADZC_OK) return adz_internal_fail(ADZC_ERR_ALLOC);
   const int st = prec == ADZC_FP64 ? run_bc<double>(ntr, tracers, airm_p, airm_m, mask, min_max, deficit, diag, core,
