@@ -105,6 +105,7 @@ def lib() -> C.CDLL:
         L.adzc_batch_query.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
         L.adzc_batch_plan.argtypes = [vp, C.POINTER(C.c_int)]
         L.adzc_batch_select.argtypes = [vp, i, i]
+        L.adzc_batch_inject.argtypes = [vp, i, C.c_longlong]
         L.adzc_batch_status.argtypes = [vp, i, vp]
         L.adzc_batch_destroy.argtypes = [vp]
         L.adzc_bermejo_conde.argtypes = [vp, i, i, vp, vp, vp, vp, i, vp, vp, vp]
@@ -405,6 +406,13 @@ class Batch:
         _check(lib().adzc_batch_step(self.h, _stream(stream)), "adzc_batch_step")
 
     PHASED = 3  # plan of select(): one persistent launch per phase
+    INJECT_SPINS, INJECT_NEED = 1, 2  # inject(): fault injection for failure-path tests
+
+    def inject(self, what: int, value: int):
+        """adzc_batch_inject: INJECT_SPINS sets the wait bound (0: default);
+        INJECT_NEED makes domain 0's trajectory items wait for items that
+        never come (0: clear)."""
+        _check(lib().adzc_batch_inject(self.h, int(what), int(value)), "adzc_batch_inject")
 
     def select(self, rows: int, plan: int):
         """Pin a plan: rows per work item and 0..2 (register budget of the

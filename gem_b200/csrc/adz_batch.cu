@@ -51,6 +51,8 @@ struct adzc_batch {
   int* d_status = nullptr;
   int rows = 8, bps = 4, sms = 148, variant = 0;
   int phased = 0;           // the phased plan: one launch per phase
+  unsigned long long spins = adz::kDepSpins;  // bound of a dependency wait
+  long long inject_need = 0;  // fault injection: extra items domain 0's trajectory waits for
   long long pstart[4] = {}; // first item of each phase, total
   int pgrid[3] = {};        // persistent grid of each phased launch
   cudaStream_t cap = nullptr;
@@ -88,6 +90,7 @@ int build_items(adzc_batch* b, int rows) {
         }
     }
   }
+  need[0] += (unsigned)b->inject_need;  // fault injection (adzc_batch_inject): items that never come
   if (items.size() > b->items_cap) {
     cudaFree(b->d_items);
     b->d_items = nullptr;
@@ -118,9 +121,9 @@ cudaError_t enqueue(adzc_batch* b, cudaStream_t s) {
   const int grid = b->bps * b->sms;
   if (b->prec == ADZC_FP64)
     return adz::launch_batch<adz::kFp64>(b->variant, grid, *b->params, b->d_doms, b->d_items, b->nitems, b->d_need,
-                                         b->d_next, b->d_done, b->d_status, s);
+                                         b->d_next, b->d_done, b->d_status, b->spins, s);
   return adz::launch_batch<adz::kMixed>(b->variant, grid, *b->params, b->d_doms, b->d_items, b->nitems, b->d_need,
-                                        b->d_next, b->d_done, b->d_status, s);
+                                        b->d_next, b->d_done, b->d_status, b->spins, s);
 }
 
 int resident(const adzc_batch* b, int variant) {
@@ -395,6 +398,21 @@ extern "C" int adzc_batch_select(adzc_batch* b, int rows, int plan) {
     b->phased = 1;
   }
   int st = build_items(b, rows);
+  if (st == ADZC_OK) st = capture(b);
+  return st == ADZC_OK ? ADZC_OK : adz_internal_fail(st);
+}
+
+extern "C" int adzc_batch_inject(adzc_batch* b, int what, long long value) {
+  if (!b || value < 0) return adz_internal_fail(ADZC_ERR_ARG);
+  if (what == ADZC_INJECT_SPINS) {
+    b->spins = value > 0 ? (unsigned long long)value : adz::kDepSpins;
+  } else if (what == ADZC_INJECT_NEED) {
+    if (value > 1000000) return adz_internal_fail(ADZC_ERR_ARG);
+    b->inject_need = value;
+  } else {
+    return adz_internal_fail(ADZC_ERR_ARG);
+  }
+  int st = build_items(b, b->rows);
   if (st == ADZC_OK) st = capture(b);
   return st == ADZC_OK ? ADZC_OK : adz_internal_fail(st);
 }

@@ -731,7 +731,6 @@ __global__ void __launch_bounds__(128) k_interp_pos(DZtab lv, int n, const void*
 // persistent batch kernel: work items (domain, phase, group, first, count) taken
 // from an atomic queue; phase p>0 items wait (bounded) on the per-domain count
 // of completed phase p-1 items.  Item list and host side: adz_batch.cu.
-constexpr unsigned long long kDepSpins = 1ull << 24;  // >= 1 s of 64 ns sleeps
 
 // block-wide copy of a descriptor into shared memory (8-byte words)
 template <typename T>
@@ -749,7 +748,8 @@ __global__ void __launch_bounds__(128, MINB) k_batch(const __grid_constant__ Bat
                                                      const BDom* __restrict__ doms, const BItem* __restrict__ items,
                                                      long long nitems, const unsigned* __restrict__ need,
                                                      unsigned long long* __restrict__ next,
-                                                     unsigned* __restrict__ done, int* __restrict__ status) {
+                                                     unsigned* __restrict__ done, int* __restrict__ status,
+                                                     unsigned long long max_spins) {
   __shared__ long long cur;
   __shared__ int dep_ok;
   __shared__ FieldPtrs sfp;
@@ -769,7 +769,7 @@ __global__ void __launch_bounds__(128, MINB) k_batch(const __grid_constant__ Bat
         unsigned v;
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(d) : "memory");
         while (v < target) {
-          if (++spins > kDepSpins) {
+          if (++spins > max_spins) {
             dep_ok = 0;
             atomicOr(status, kErrTimeout);
             break;
@@ -983,16 +983,16 @@ struct BatchMinB {
 template <int PREC>
 cudaError_t launch_batch(int variant, int grid, const BatchParams& P, const BDom* doms, const BItem* items,
                          long long nitems, const unsigned* need, unsigned long long* next, unsigned* done,
-                         int* status, cudaStream_t s) {
+                         int* status, unsigned long long max_spins, cudaStream_t s) {
   if constexpr (PREC == kRef32) {
     return cudaErrorNotSupported;
   } else {
     if (variant == 1)
-      k_batch<PREC, BatchMinB<PREC, 1>::value><<<grid, 128, 0, s>>>(P, doms, items, nitems, need, next, done, status);
+      k_batch<PREC, BatchMinB<PREC, 1>::value><<<grid, 128, 0, s>>>(P, doms, items, nitems, need, next, done, status, max_spins);
     else if (variant == 2)
-      k_batch<PREC, BatchMinB<PREC, 2>::value><<<grid, 128, 0, s>>>(P, doms, items, nitems, need, next, done, status);
+      k_batch<PREC, BatchMinB<PREC, 2>::value><<<grid, 128, 0, s>>>(P, doms, items, nitems, need, next, done, status, max_spins);
     else
-      k_batch<PREC, BatchMinB<PREC, 0>::value><<<grid, 128, 0, s>>>(P, doms, items, nitems, need, next, done, status);
+      k_batch<PREC, BatchMinB<PREC, 0>::value><<<grid, 128, 0, s>>>(P, doms, items, nitems, need, next, done, status, max_spins);
     return cudaGetLastError();
   }
 }
@@ -1055,7 +1055,7 @@ int batch_resident_blocks(int variant) {
                                         const FieldPtrs&, cudaStream_t);                                          \
   template cudaError_t launch_batch<P>(int, int, const BatchParams&, const BDom*, const BItem*, long long,       \
                                        const unsigned*,                                                             \
-                                       unsigned long long*, unsigned*, int*, cudaStream_t);                        \
+                                       unsigned long long*, unsigned*, int*, unsigned long long, cudaStream_t);    \
   template int batch_resident_blocks<P>(int);                                                                   \
   template cudaError_t launch_batch_phased<P>(const int*, const BatchParams&, const BDom*, const BItem*,           \
                                               const long long*, unsigned long long*, cudaStream_t);                \

@@ -184,11 +184,13 @@ struct BItem {
 constexpr int kBatchVariants = 3;  // register budgets of the batch kernel
 template <int PREC>
 cudaError_t launch_tricub_parts(const DGrid& g, const SetArgs& a, const SetParts& sp, cudaStream_t s);
+// bound of a dependency wait of the batch kernel: >= 1 s of 64 ns sleeps
+constexpr unsigned long long kDepSpins = 1ull << 24;
 template <int PREC>
 cudaError_t launch_batch(int variant, int grid, const BatchParams& P, const BDom* doms, const BItem* items,
                          long long nitems,
                          const unsigned* need, unsigned long long* next, unsigned* done, int* status,
-                         cudaStream_t s);
+                         unsigned long long max_spins, cudaStream_t s);
 template <int PREC>
 int batch_resident_blocks(int variant);  // blocks of 128 threads resident per SM
 // the phased plan: one persistent launch per phase (items[pstart[p], pstart[p+1])),

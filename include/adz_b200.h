@@ -262,6 +262,16 @@ int adzc_batch_plan(const adzc_batch *b, int *phased);
  * budget of the one-launch kernel, 3 = phased; re-captures the graph */
 #define ADZC_BATCH_PHASED 3
 int adzc_batch_select(adzc_batch *b, int rows_per_item, int plan);
+/* Fault injection for tests of the failure path, on the host (no GPU fault).
+ * ADZC_INJECT_SPINS: bound of a dependency wait of the one-launch kernel, in
+ * iterations of a 64 ns sleep (0: the default, >= 1 s).  ADZC_INJECT_NEED:
+ * domain 0's trajectory items also wait for value departure-wind items that
+ * do not exist, so their waits run out: the kernel skips them, raises
+ * ADZC_ERR_TIMEOUT (adzc_batch_status) and completes (0 clears).  Both
+ * re-capture the graph; the phased plan has no waits. */
+#define ADZC_INJECT_SPINS 1
+#define ADZC_INJECT_NEED 2
+int adzc_batch_inject(adzc_batch *b, int what, long long value);
 /* synchronises; ADZC_ERR_TIMEOUT when a dependency wait gave up, else the
  * first non-zero status of the domains' handles */
 int adzc_batch_status(adzc_batch *b, int reset, void *stream);

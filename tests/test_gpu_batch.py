@@ -151,3 +151,42 @@ def test_batch_rejects_bad_domains():
     with pytest.raises(adz.AdzError):
         adz.Batch(A.MIXED, [dict(adz=fresh, dt=cfg.dt, winds=inp, wpxyz=wps[0], nfields=[0, 1, 1, 1 + ntr],
                                  srcs=_sources(inp), dsts=outs[0], mono=[0, 0, 0] + [1] * ntr)])
+
+
+def test_batch_wait_times_out_and_recovers():
+    """Failure detection without a GPU fault: domain 0's trajectory items are
+    made to wait for departure-wind items that do not exist (host-side
+    injection) under a short wait bound.  The waits run out, the kernel skips
+    those items and completes, the host reads ADZC_ERR_TIMEOUT, and the next
+    step (fault cleared, same positions) is bit-exact with the per-domain
+    entry points: the context stays usable."""
+    import time
+    from gem_b200 import adz as A
+    prec = A.MIXED
+    adz, doms = _domains(prec, n=2, seed=13)
+    dt = adz._field_dtype(prec)
+    wps_b = [wp.clone() for (_, _, _, wp) in doms]
+    outs_b = [_outs(ad, inp, dt) for (_, ad, inp, _) in doms]
+    batch = _batch(adz, prec, doms, wps_b, outs_b)
+    batch.select(8, 0)  # the one-launch plan: the phased plan has no waits
+    batch.inject(adz.Batch.INJECT_SPINS, 4096)
+    batch.inject(adz.Batch.INJECT_NEED, 1)
+    t0 = time.time()
+    batch.step()
+    assert batch.status() == 6  # ADZC_ERR_TIMEOUT
+    assert time.time() - t0 < 60
+    assert batch.status() == 0  # read and reset
+    batch.inject(adz.Batch.INJECT_NEED, 0)
+    batch.inject(adz.Batch.INJECT_SPINS, 0)
+    for (_, _, _, wp), wb in zip(doms, wps_b):
+        wb.copy_(wp)
+    batch.step()
+    assert batch.status() == 0
+    snaps_b = [_snap(wp, o) for wp, o in zip(wps_b, outs_b)]
+    for d, (cfg, ad, inp, wp) in enumerate(doms):
+        o = _outs(ad, inp, dt)
+        _regular_step(adz, prec, cfg, ad, inp, wp, o)
+        assert ad.status() == 0
+        _compare(_snap(wp, o), snaps_b[d], f"after recovery, domain {d}")
+    with pytest.raises(adz.AdzError):
+        batch.inject(9, 1)
