@@ -114,6 +114,7 @@ def lib() -> C.CDLL:
         L.adzc_state_save.argtypes = [vp, i, vp, vp, C.c_char_p]
         L.adzc_state_load.argtypes = [vp, i, vp, vp, C.c_char_p]
         L.adzc_slt_winds.argtypes = [vp, vp, vp]
+        L.adzc_bc_lam_flux.argtypes = [vp, i, i, vp, vp, vp, vp]
         L.adzc_rhs_perturbation.argtypes = [vp, vp, i]
         L.adzc_halo_layout.argtypes = [vp, i, vp]
         L.adzc_halo_pack.argtypes = [vp, i, vp, vp, vp]
@@ -299,6 +300,13 @@ class Adz:
         self._slt = (uslt, vslt)
         _check(lib().adzc_slt_winds(self.h, None if uslt is None else uslt.data_ptr(),
                                     None if vslt is None else vslt.data_ptr()), "adzc_slt_winds")
+
+    def bc_lam_flux(self, prec: int, srcs, fo, fi, stream=None):
+        """adz_BC_LAM_Aranami_hlt: FLUX_out / FLUX_in of the tracers srcs into
+        fo, fi (ext tensors of the field type)."""
+        _check(lib().adzc_bc_lam_flux(self.h, prec, len(srcs), C.cast(_ptr_array(srcs), C.c_void_p),
+                                      C.cast(_ptr_array(fo), C.c_void_p), C.cast(_ptr_array(fi), C.c_void_p),
+                                      _stream(stream)), "adzc_bc_lam_flux")
 
     def set_rhs_perturbation(self, mcrhsint=None):
         """mcrhsint (nj, ni) device tensor of the field type: every later

@@ -47,7 +47,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     common = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]
     objs = []
-    units = [("adz_exact.cu", ["-fmad=false"]), ("adz_mixed.cu", ["-fmad=true"]), ("adz_noalloc.cu", []), ("adz_batch.cu", []), ("adz_guess.cu", []), ("adz_train.cu", []), ("adz_mass.cu", []), ("adz_diag.cu", []), ("adz_ilmc.cu", ["-fmad=false"]), ("adz_halo.cu", [])]
+    units = [("adz_exact.cu", ["-fmad=false"]), ("adz_mixed.cu", ["-fmad=true"]), ("adz_noalloc.cu", []), ("adz_batch.cu", []), ("adz_guess.cu", []), ("adz_train.cu", []), ("adz_mass.cu", []), ("adz_diag.cu", []), ("adz_ilmc.cu", ["-fmad=false"]), ("adz_halo.cu", []), ("adz_bcflux.cu", [])]
     for src, extra in units:
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))
         out = _run([NVCC] + ARCH + common + extra + ["-Xptxas", "-v", "-c", os.path.join(CSRC, src), "-o", obj])

@@ -1,0 +1,85 @@
+// LAM boundary fluxes of Aranami et al. (2015) (B/adz_BC_LAM_Aranami_hlt.F90:
+// 18-236, masks of B/adz_BC_LAM_setup.F90:18-92): the masked copies of a
+// tracer and the zeroing of the interpolated fluxes.  The interpolation
+// between them is the set-t kernel over range b (adzc_bc_lam_flux).
+//
+// mask_o is 1 on the core (levels k0t..nk and, on each LAM edge the tile
+// touches, the span inside its pilot zone); mask_i is 1 on the rest of the
+// domain; both are 0 outside the domain.  They are functions of the global
+// position, so a tile of a decomposition gets what the reference's halo
+// exchange of the masks gives.  The copies select (mask ? value : 0), which
+// is the reference's mask * value for finite values and 0 where the reference
+// never writes.
+#include <cuda_runtime.h>
+
+#include "adz_types.h"
+
+namespace adz {
+namespace bcflux {
+
+__device__ __forceinline__ bool in_domain(const BcMask& m, int i, int j) {
+  return (!m.west || i >= 1) && (!m.east || i <= m.ni) && (!m.south || j >= 1) && (!m.north || j <= m.nj);
+}
+__device__ __forceinline__ bool in_core(const BcMask& m, int i, int j, int k) {
+  const bool cx = (!m.west || i >= 1 + m.pil_w) && (!m.east || i <= m.ni - m.pil_e);
+  const bool cy = (!m.south || j >= 1 + m.pil_s) && (!m.north || j <= m.nj - m.pil_n);
+  return cx && cy && k >= m.k0t;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_bc_mask(BcMask m, const T* __restrict__ src, T* __restrict__ mo,
+                                                 T* __restrict__ mi) {
+  const long long plane = (long long)m.nit * m.njt, n = plane * m.nk;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int i = m.lminx + (int)(e % m.nit), j = m.lminy + (int)((e / m.nit) % m.njt), k = 1 + (int)(e / plane);
+    const bool dom = in_domain(m, i, j), core = dom && in_core(m, i, j, k);
+    const T v = src[e];
+    mo[e] = core ? v : (T)0;
+    mi[e] = (dom && !core) ? v : (T)0;
+  }
+}
+
+// FLUX_out = 0 on the core; FLUX_in = 0 on the pilot zones (levels k0t..nk)
+// and above k0t on range b (B/adz_BC_LAM_Aranami_hlt.F90:160-226)
+template <typename T>
+__global__ void __launch_bounds__(256) k_bc_zero(BcMask m, T* __restrict__ fo, T* __restrict__ fi) {
+  const long long plane = (long long)m.ni * m.nj, n = plane * m.nk;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(t % m.ni), j = 1 + (int)((t / m.ni) % m.nj), k = 1 + (int)(t / plane);
+    const long long e = (long long)(i - m.lminx) + (long long)(j - m.lminy) * m.nit + (long long)(k - 1) * m.nit * m.njt;
+    if (k >= m.k0t) {
+      if (j >= 1 + m.pil_s && j <= m.nj - m.pil_n && i >= 1 + m.pil_w && i <= m.ni - m.pil_e) fo[e] = (T)0;
+      if ((m.north && j >= m.nj - m.pil_n + 1) || (m.east && i >= m.ni - m.pil_e + 1) || (m.south && j <= m.pil_s) ||
+          (m.west && i <= m.pil_w))
+        fi[e] = (T)0;
+    } else if (i >= m.i0b && i <= m.inb && j >= m.j0b && j <= m.jnb) {
+      fi[e] = (T)0;
+    }
+  }
+}
+
+inline int grid_of(long long n) {
+  long long b = (n + 255) / 256;
+  return (int)(b < 1 ? 1 : (b > 148LL * 32 ? 148LL * 32 : b));
+}
+
+}  // namespace bcflux
+
+template <typename T>
+cudaError_t launch_bc_mask(const BcMask& m, const void* src, void* mo, void* mi, cudaStream_t s) {
+  const long long n = (long long)m.nit * m.njt * m.nk;
+  bcflux::k_bc_mask<T><<<bcflux::grid_of(n), 256, 0, s>>>(m, (const T*)src, (T*)mo, (T*)mi);
+  return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_bc_zero(const BcMask& m, void* fo, void* fi, cudaStream_t s) {
+  const long long n = (long long)m.ni * m.nj * m.nk;
+  bcflux::k_bc_zero<T><<<bcflux::grid_of(n), 256, 0, s>>>(m, (T*)fo, (T*)fi);
+  return cudaGetLastError();
+}
+template cudaError_t launch_bc_mask<float>(const BcMask&, const void*, void*, void*, cudaStream_t);
+template cudaError_t launch_bc_mask<double>(const BcMask&, const void*, void*, void*, cudaStream_t);
+template cudaError_t launch_bc_zero<float>(const BcMask&, void*, void*, cudaStream_t);
+template cudaError_t launch_bc_zero<double>(const BcMask&, void*, void*, cudaStream_t);
+
+}  // namespace adz

@@ -731,6 +731,52 @@ extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const
   return ADZC_OK;
 }
 
+extern "C" int adzc_bc_lam_flux(adzc_handle* h, int prec, int ntr, const void* const* srcs, void* const* fo,
+                                void* const* fi, void* stream) {
+  AdzRange nvtx_range("adz_BC_LAM_Aranami_hlt");
+  if (!h || !check_prec(prec) || ntr < 0 || (ntr > 0 && (!srcs || !fo || !fi))) return fail(ADZC_ERR_ARG);
+  if (h->last_prec != prec || !h->wpxyz) return fail(ADZC_ERR_ARG);
+  if (h->g.bc_lam_flux == 0) return fail(ADZC_ERR_ARG);  // the range b positions need k00 = 1
+  for (int q = 0; q < ntr; q++)
+    if (!srcs[q] || !fo[q] || !fi[q]) return fail(ADZC_ERR_ARG);
+  if (ntr == 0) return ADZC_OK;
+  const adzc_info& I = h->info;
+  const adz::DGrid& D = h->dg;
+  adz::BcMask m{D.lminx, D.lminy, D.nit, D.njt, D.nk, D.ni, D.nj, h->g.west, h->g.east, h->g.south, h->g.north,
+                h->g.pil_w, h->g.pil_e, h->g.pil_s, h->g.pil_n, I.k0t, I.i0b, I.inb, I.j0b, I.jnb};
+  const int nxb = I.inb - I.i0b + 1, nyb = I.jnb - I.j0b + 1;
+  if (nxb <= 0 || nyb <= 0) return ADZC_OK;
+  const size_t fb = prec == ADZC_FP64 ? sizeof(double) : sizeof(float);
+  const size_t ext = (size_t)D.nij * D.nk * fb;
+  constexpr int kChunk = adz::kMaxFields / 2;  // tracers per interpolation launch (out and in fields)
+  void* scratch = nullptr;
+  if (adz_internal_aux(h, 2 * std::min(kChunk, ntr) * ext, &scratch) != ADZC_OK) return fail(ADZC_ERR_ALLOC);
+  adz::SetArgs a = set_args(h);
+  a.pert = nullptr;  // the fluxes are plain interpolations (tricublin_zyx1_m_n)
+  const cudaStream_t s = (cudaStream_t)stream;
+  for (int q0 = 0; q0 < ntr; q0 += kChunk) {
+    const int nf = std::min(kChunk, ntr - q0);
+    adz::FieldPtrs fp{};
+    fp.nf = 2 * nf;
+    for (int q = 0; q < nf; q++) {
+      char* mo = (char*)scratch + (size_t)(2 * q) * ext;
+      char* mi = (char*)scratch + (size_t)(2 * q + 1) * ext;
+      ADZ_CK(prec == ADZC_FP64 ? adz::launch_bc_mask<double>(m, srcs[q0 + q], mo, mi, s)
+                               : adz::launch_bc_mask<float>(m, srcs[q0 + q], mo, mi, s));
+      fp.src[2 * q] = mo;
+      fp.src[2 * q + 1] = mi;
+      fp.dst[2 * q] = fo[q0 + q];
+      fp.dst[2 * q + 1] = fi[q0 + q];
+    }
+    // Adz_pb over (i0b:inb, j0b:jnb, 1:nk): the set-t positions of those points
+    ADZ_CK(dispatch_set(prec, D, ADZC_SET_T, I.i0b, nxb, I.j0b, nyb, 1, D.nk, a, fp, s));
+    for (int q = 0; q < nf; q++)
+      ADZ_CK(prec == ADZC_FP64 ? adz::launch_bc_zero<double>(m, fo[q0 + q], fi[q0 + q], s)
+                               : adz::launch_bc_zero<float>(m, fo[q0 + q], fi[q0 + q], s));
+  }
+  return ADZC_OK;
+}
+
 extern "C" int adzc_tricub_sets(adzc_handle* h, int prec, const int* nfields, const void* const* srcs,
                                 void* const* dsts, const int* mono, void* stream) {
   AdzRange nvtx_range("ADZ_MAIN sets");

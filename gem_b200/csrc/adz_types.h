@@ -184,6 +184,17 @@ struct BItem {
 constexpr int kBatchVariants = 3;  // register budgets of the batch kernel
 template <int PREC>
 cudaError_t launch_tricub_parts(const DGrid& g, const SetArgs& a, const SetParts& sp, cudaStream_t s);
+// the tile geometry of the LAM boundary-flux masks (adz_bcflux.cu)
+struct BcMask {
+  int lminx, lminy, nit, njt, nk, ni, nj;
+  int west, east, south, north, pil_w, pil_e, pil_s, pil_n, k0t;
+  int i0b, inb, j0b, jnb;
+};
+template <typename T>
+cudaError_t launch_bc_mask(const BcMask& m, const void* src, void* mo, void* mi, cudaStream_t s);
+template <typename T>
+cudaError_t launch_bc_zero(const BcMask& m, void* fo, void* fi, cudaStream_t s);
+
 // bound of a dependency wait of the batch kernel: >= 1 s of 64 ns sleeps
 constexpr unsigned long long kDepSpins = 1ull << 24;
 template <int PREC>

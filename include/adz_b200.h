@@ -209,6 +209,17 @@ int adzc_slt_winds(adzc_handle *h, const void *uslt, const void *vslt);
  * NULL clears it.  adzc_batch_create refuses a handle with a pattern set. */
 int adzc_rhs_perturbation(adzc_handle *h, const void *mcrhsint, int ld);
 
+/* LAM boundary fluxes of Aranami et al. (2015), adz_BC_LAM_Aranami_hlt
+ * (B/adz_BC_LAM_Aranami_hlt.F90:18-236 with the masks of
+ * B/adz_BC_LAM_setup.F90:18-92), for the tracers Bermejo-Conde fixes
+ * (mass 1 or 111..139), after the last trajectory.  srcs: ext tracers; fo,
+ * fi: ext arrays receiving FLUX_out and FLUX_in at Adz_pb over Adz_i0b:inb,
+ * Adz_j0b:jnb, 1:nk, then zeroed as the reference does (FLUX_out on the
+ * core, FLUX_in on the pilot zones and above k0t); the fo, fi fields of
+ * adzc_bermejo_conde.  The grid must set bc_lam_flux. */
+int adzc_bc_lam_flux(adzc_handle *h, int prec, int ntr, const void *const *srcs, void *const *fo, void *const *fi,
+                     void *stream);
+
 /* Every position set of the last trajectory in one call: nfields[4] fields
  * for sets Q, U, V, T, srcs/dsts/mono holding all sets' entries in that order
  * (HOST arrays of DEVICE pointers; mono may be NULL).  Same results as

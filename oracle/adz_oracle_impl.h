@@ -159,65 +159,25 @@ static inline double SFX(zindx)(const orc_set *s, double posz) {
   return (posz - zt[nb]) * s->odelz_t[nb] + (double)nb;
 }
 
-/* adz_traject.F90:113-116 (Adz_pm) and adz_interp_traj.F90:16-187 */
-void SFX(orc_interp_traj)(const orc_set *s, double dt, const double *wpxyz, const REAL *uvw_dep, const REAL *zdt0,
-                          const REAL *pxyzm, const REAL *uslt, const REAL *vslt, REAL *pm, REAL *pmu, REAL *pmv,
-                          REAL *pt) {
+/* Adz_pb (adz_interp_traj.F90:105-187) over (i0b:inb, j0b:jnb, 1:nk), point
+ * (i, j, k) at pb + 3 * ((i - i0b) + (j - j0b) * bx + (k - 1) * bx * by);
+ * levels below k00 are left as they are */
+void SFX(orc_pb)(const orc_set *s, double dt, const double *wpxyz, const REAL *uvw_dep, const REAL *zdt0,
+                 const REAL *uslt, const REAL *vslt, REAL *pb) {
   const int ni = s->g.ni, nj = s->g.nj, nk = s->g.nk;
   double dtA, dtzA, dtD, dtzD;
   SFX(dt_split)(s, dt, &dtA, &dtzA, &dtD, &dtzD);
-  const double half = 0.5, aa = -0.0625, bb = 0.5625;
-  const double zmin_b = 0.0, zmax_b = (double)(nk + 1);
+  (void)dtA;
+  (void)dtD;
+  const double half = 0.5;
   const double *zt = s->g.zt;
   int k00 = imax(s->k0t - 1, 1);
   if (s->g.bc_lam_flux != 0 && s->k0 > 1) k00 = 1;
   const double imnx = s->iminposx, imxx = s->imaxposx, imny = s->iminposy, imxy = s->imaxposy;
+  long bx = s->inb - s->i0b + 1, by = s->jnb - s->j0b + 1;
 #define W(i, j, k, c) wpxyz[WP(i, j, k, c)]
 #define UD3(i, j, k) uvw_dep[3 * ARR(i, j, k) + 2]
 #define ZD(i, j, k) zdt0[EXT(i, j, k)]
-  if (pm) {
-    long nx = s->in - s->i0 + 1, ny = s->jn - s->j0 + 1;
-    for (int k = s->k0; k <= nk; k++)
-      for (int j = s->j0; j <= s->jn; j++)
-        for (int i = s->i0; i <= s->in; i++) {
-          long o = (i - s->i0) + (j - s->j0) * nx + (long)(k - s->k0) * nx * ny;
-          for (int c = 0; c < 3; c++) pm[3 * o + c] = pxyzm[3 * ARR(i, j, k) + c];
-        }
-  }
-  if (pmu) {
-    long nx = s->inu - s->i0u + 1, ny = s->jn - s->j0 + 1;
-#pragma omp parallel for num_threads(nthr()) schedule(static)
-    for (int k = s->k0; k <= nk; k++)
-      for (int j = s->j0; j <= s->jn; j++)
-        for (int i = s->i0u; i <= s->inu; i++) {
-          double xt = aa * (W(i - 1, j, k, 1) + W(i + 2, j, k, 1)) + bb * (W(i, j, k, 1) + W(i + 1, j, k, 1)) - 0.5;
-          double yt = aa * (W(i - 1, j, k, 2) + W(i + 2, j, k, 2)) + bb * (W(i, j, k, 2) + W(i + 1, j, k, 2));
-          double ztv = aa * (W(i - 1, j, k, 3) + W(i + 2, j, k, 3)) + bb * (W(i, j, k, 3) + W(i + 1, j, k, 3));
-          long o = (i - s->i0u) + (j - s->j0) * nx + (long)(k - s->k0) * nx * ny;
-          pmu[3 * o + 0] = (REAL)dmin(dmax(xt, imnx), imxx);
-          pmu[3 * o + 1] = (REAL)dmin(dmax(yt, imny), imxy);
-          pmu[3 * o + 2] = (REAL)dmin(dmax(ztv, zmin_b), zmax_b);
-        }
-  }
-  if (pmv) {
-    long nx = s->in - s->i0 + 1, ny = s->jnv - s->j0v + 1;
-#pragma omp parallel for num_threads(nthr()) schedule(static)
-    for (int k = s->k0; k <= nk; k++)
-      for (int j = s->j0v; j <= s->jnv; j++)
-        for (int i = s->i0; i <= s->in; i++) {
-          double xt = aa * (W(i, j - 1, k, 1) + W(i, j + 2, k, 1)) + bb * (W(i, j, k, 1) + W(i, j + 1, k, 1));
-          double yt = aa * (W(i, j - 1, k, 2) + W(i, j + 2, k, 2)) + bb * (W(i, j, k, 2) + W(i, j + 1, k, 2)) - 0.5;
-          double ztv = aa * (W(i, j - 1, k, 3) + W(i, j + 2, k, 3)) + bb * (W(i, j, k, 3) + W(i, j + 1, k, 3));
-          long o = (i - s->i0) + (j - s->j0v) * nx + (long)(k - s->k0) * nx * ny;
-          pmv[3 * o + 0] = (REAL)dmin(dmax(xt, imnx), imxx);
-          pmv[3 * o + 1] = (REAL)dmin(dmax(yt, imny), imxy);
-          pmv[3 * o + 2] = (REAL)dmin(dmax(ztv, zmin_b), zmax_b);
-        }
-  }
-  if (pt) {
-    /* pb over (i0b:inb, j0b:jnb, 1:nk) then pt = pb on the t range */
-    long bx = s->inb - s->i0b + 1, by = s->jnb - s->j0b + 1;
-    REAL *pb = (REAL *)malloc(sizeof(REAL) * 3 * bx * by * nk);
 #define PB(i, j, k) (pb + 3 * ((i - s->i0b) + (j - s->j0b) * bx + (long)((k) - 1) * bx * by))
 #pragma omp parallel for num_threads(nthr()) schedule(static)
     for (int k = imax(k00, 2); k <= nk - 2; k++)
@@ -287,6 +247,73 @@ void SFX(orc_interp_traj)(const orc_set *s, double dt, const double *wpxyz, cons
           p[2] = (REAL)SFX(zindx)(s, ztv);
         }
     }
+#undef PB
+#undef W
+#undef UD3
+#undef ZD
+}
+
+/* adz_traject.F90:113-116 (Adz_pm) and adz_interp_traj.F90:16-187 */
+void SFX(orc_interp_traj)(const orc_set *s, double dt, const double *wpxyz, const REAL *uvw_dep, const REAL *zdt0,
+                          const REAL *pxyzm, const REAL *uslt, const REAL *vslt, REAL *pm, REAL *pmu, REAL *pmv,
+                          REAL *pt) {
+  const int ni = s->g.ni, nj = s->g.nj, nk = s->g.nk;
+  double dtA, dtzA, dtD, dtzD;
+  SFX(dt_split)(s, dt, &dtA, &dtzA, &dtD, &dtzD);
+  const double half = 0.5, aa = -0.0625, bb = 0.5625;
+  const double zmin_b = 0.0, zmax_b = (double)(nk + 1);
+  const double *zt = s->g.zt;
+  int k00 = imax(s->k0t - 1, 1);
+  if (s->g.bc_lam_flux != 0 && s->k0 > 1) k00 = 1;
+  const double imnx = s->iminposx, imxx = s->imaxposx, imny = s->iminposy, imxy = s->imaxposy;
+#define W(i, j, k, c) wpxyz[WP(i, j, k, c)]
+#define UD3(i, j, k) uvw_dep[3 * ARR(i, j, k) + 2]
+#define ZD(i, j, k) zdt0[EXT(i, j, k)]
+  if (pm) {
+    long nx = s->in - s->i0 + 1, ny = s->jn - s->j0 + 1;
+    for (int k = s->k0; k <= nk; k++)
+      for (int j = s->j0; j <= s->jn; j++)
+        for (int i = s->i0; i <= s->in; i++) {
+          long o = (i - s->i0) + (j - s->j0) * nx + (long)(k - s->k0) * nx * ny;
+          for (int c = 0; c < 3; c++) pm[3 * o + c] = pxyzm[3 * ARR(i, j, k) + c];
+        }
+  }
+  if (pmu) {
+    long nx = s->inu - s->i0u + 1, ny = s->jn - s->j0 + 1;
+#pragma omp parallel for num_threads(nthr()) schedule(static)
+    for (int k = s->k0; k <= nk; k++)
+      for (int j = s->j0; j <= s->jn; j++)
+        for (int i = s->i0u; i <= s->inu; i++) {
+          double xt = aa * (W(i - 1, j, k, 1) + W(i + 2, j, k, 1)) + bb * (W(i, j, k, 1) + W(i + 1, j, k, 1)) - 0.5;
+          double yt = aa * (W(i - 1, j, k, 2) + W(i + 2, j, k, 2)) + bb * (W(i, j, k, 2) + W(i + 1, j, k, 2));
+          double ztv = aa * (W(i - 1, j, k, 3) + W(i + 2, j, k, 3)) + bb * (W(i, j, k, 3) + W(i + 1, j, k, 3));
+          long o = (i - s->i0u) + (j - s->j0) * nx + (long)(k - s->k0) * nx * ny;
+          pmu[3 * o + 0] = (REAL)dmin(dmax(xt, imnx), imxx);
+          pmu[3 * o + 1] = (REAL)dmin(dmax(yt, imny), imxy);
+          pmu[3 * o + 2] = (REAL)dmin(dmax(ztv, zmin_b), zmax_b);
+        }
+  }
+  if (pmv) {
+    long nx = s->in - s->i0 + 1, ny = s->jnv - s->j0v + 1;
+#pragma omp parallel for num_threads(nthr()) schedule(static)
+    for (int k = s->k0; k <= nk; k++)
+      for (int j = s->j0v; j <= s->jnv; j++)
+        for (int i = s->i0; i <= s->in; i++) {
+          double xt = aa * (W(i, j - 1, k, 1) + W(i, j + 2, k, 1)) + bb * (W(i, j, k, 1) + W(i, j + 1, k, 1));
+          double yt = aa * (W(i, j - 1, k, 2) + W(i, j + 2, k, 2)) + bb * (W(i, j, k, 2) + W(i, j + 1, k, 2)) - 0.5;
+          double ztv = aa * (W(i, j - 1, k, 3) + W(i, j + 2, k, 3)) + bb * (W(i, j, k, 3) + W(i, j + 1, k, 3));
+          long o = (i - s->i0) + (j - s->j0v) * nx + (long)(k - s->k0) * nx * ny;
+          pmv[3 * o + 0] = (REAL)dmin(dmax(xt, imnx), imxx);
+          pmv[3 * o + 1] = (REAL)dmin(dmax(yt, imny), imxy);
+          pmv[3 * o + 2] = (REAL)dmin(dmax(ztv, zmin_b), zmax_b);
+        }
+  }
+  if (pt) {
+    /* pb over (i0b:inb, j0b:jnb, 1:nk) then pt = pb on the t range */
+    long bx = s->inb - s->i0b + 1, by = s->jnb - s->j0b + 1;
+    REAL *pb = (REAL *)malloc(sizeof(REAL) * 3 * bx * by * nk);
+#define PB(i, j, k) (pb + 3 * ((i - s->i0b) + (j - s->j0b) * bx + (long)((k) - 1) * bx * by))
+    SFX(orc_pb)(s, dt, wpxyz, uvw_dep, zdt0, uslt, vslt, pb);
     long nx = s->in - s->i0 + 1, ny = s->jn - s->j0 + 1;
     for (int k = s->k0t; k <= nk; k++)
       for (int j = s->j0; j <= s->jn; j++)
@@ -528,6 +555,91 @@ void SFX(orc_tricub_qv_p)(const orc_set *s, const REAL *pos, int m, const REAL *
 void SFX(orc_tricub_qv)(const orc_set *s, const REAL *pos, int m, const REAL *const *srcs, REAL *const *dsts,
                         int clip, REAL *const *lin, REAL *const *mn, REAL *const *mx) {
   SFX(orc_tricub_qv_p)(s, pos, m, srcs, dsts, clip, lin, mn, mx, NULL, 0);
+}
+
+/* LAM boundary fluxes of Aranami et al. (2015) (adz_BC_LAM_Aranami_hlt.F90:
+ * 18-236, masks of adz_BC_LAM_setup.F90:18-92), for m tracers: the tracer
+ * times mask_o (1 on the core: k0t..nk and the tile's span inside the pilot
+ * zones of the LAM edges it touches) and times mask_i (1 on the rest of the
+ * domain), both 0 outside the domain, interpolated at Adz_pb over
+ * (i0b:inb, j0b:jnb, 1:nk) on thermo levels, then FLUX_out zeroed on the
+ * core and FLUX_in on the pilot zones and above k0t.  fo, fi: ext layout. */
+static int SFX(in_core)(const orc_set *s, int i, int j, int k) {
+  const orc_grid *g = &s->g;
+  const int cx = (!g->west || i >= 1 + g->pil_w) && (!g->east || i <= g->ni - g->pil_e);
+  const int cy = (!g->south || j >= 1 + g->pil_s) && (!g->north || j <= g->nj - g->pil_n);
+  return cx && cy && k >= s->k0t;
+}
+static int SFX(in_domain)(const orc_set *s, int i, int j) {
+  const orc_grid *g = &s->g;
+  return (!g->west || i >= 1) && (!g->east || i <= g->ni) && (!g->south || j >= 1) && (!g->north || j <= g->nj);
+}
+
+void SFX(orc_bc_lam_flux)(const orc_set *s, double dt, const double *wpxyz, const REAL *uvw_dep, const REAL *zdt0,
+                          const REAL *uslt, const REAL *vslt, int m, const REAL *const *srcs, REAL *const *fo,
+                          REAL *const *fi) {
+  const orc_grid *g = &s->g;
+  const int ni = g->ni, nj = g->nj, nk = g->nk;
+  const long bx = s->inb - s->i0b + 1, by = s->jnb - s->j0b + 1, np = bx * by;
+  const long next = (long)s->nit * s->njt * nk;
+  REAL *pb = (REAL *)malloc(sizeof(REAL) * 3 * np * nk);
+  SFX(orc_pb)(s, dt, wpxyz, uvw_dep, zdt0, uslt, vslt, pb);
+  REAL *masked = (REAL *)malloc(sizeof(REAL) * 2 * next);
+  REAL *wrk = (REAL *)malloc(sizeof(REAL) * 2 * np);
+  const long o111 = EXT(1, 1, 1);
+  for (int q = 0; q < m; q++) {
+    REAL *mo = masked, *mi = masked + next;
+    for (int k = 1; k <= nk; k++)
+      for (int j = s->lminy; j < s->lminy + s->njt; j++)
+        for (int i = s->lminx; i < s->lminx + s->nit; i++) {
+          const long e = EXT(i, j, k);
+          const int dom = SFX(in_domain)(s, i, j), core = dom && SFX(in_core)(s, i, j, k);
+          mo[e] = core ? srcs[q][e] : (REAL)0;
+          mi[e] = (dom && !core) ? srcs[q][e] : (REAL)0;
+        }
+    REAL *fs[2] = {mo + o111, mi + o111};
+    for (int k = 1; k <= nk; k++) {
+      const REAL *p = pb + 3 * (long)(k - 1) * np;
+#if IS_F32
+#ifdef ORC_USE_REF
+      Tricublin_zyx1_m_n(wrk, fs, (pxpypz *)p, ref_ztab_t_of(s), (int)np, 2);
+#else
+      orc_zyx1_m_n_f32(wrk, (const float *const *)fs, p, s->ztab_t, (int)np, 2);
+#endif
+#else
+      orc_zyx1_m_n_f64(wrk, (const double *const *)fs, p, s->ztab_t, (int)np, 2);
+#endif
+      for (int j = s->j0b; j <= s->jnb; j++)
+        for (int i = s->i0b; i <= s->inb; i++) {
+          const long w = (i - s->i0b) + (j - s->j0b) * bx;
+          fo[q][EXT(i, j, k)] = wrk[w];
+          fi[q][EXT(i, j, k)] = wrk[np + w];
+        }
+    }
+    /* zeroing (adz_BC_LAM_Aranami_hlt.F90:160-226) */
+    for (int k = s->k0t; k <= nk; k++) {
+      for (int j = 1 + g->pil_s; j <= nj - g->pil_n; j++)
+        for (int i = 1 + g->pil_w; i <= ni - g->pil_e; i++) fo[q][EXT(i, j, k)] = 0;
+      if (g->north)
+        for (int j = nj - g->pil_n + 1; j <= nj; j++)
+          for (int i = 1; i <= ni; i++) fi[q][EXT(i, j, k)] = 0;
+      if (g->east)
+        for (int j = 1; j <= nj; j++)
+          for (int i = ni - g->pil_e + 1; i <= ni; i++) fi[q][EXT(i, j, k)] = 0;
+      if (g->south)
+        for (int j = 1; j <= g->pil_s; j++)
+          for (int i = 1; i <= ni; i++) fi[q][EXT(i, j, k)] = 0;
+      if (g->west)
+        for (int j = 1; j <= nj; j++)
+          for (int i = 1; i <= g->pil_w; i++) fi[q][EXT(i, j, k)] = 0;
+    }
+    for (int k = 1; k <= s->k0t - 1; k++)
+      for (int j = s->j0b; j <= s->jnb; j++)
+        for (int i = s->i0b; i <= s->inb; i++) fi[q][EXT(i, j, k)] = 0;
+  }
+  free(wrk);
+  free(masked);
+  free(pb);
 }
 
 /* almost_zero (modelutils almost_zero.F90:16-36), bit for bit, including its

@@ -144,6 +144,15 @@ void orc_tricub_qv_f32(const orc_set *s, const float *pos, int m, const float *c
 void orc_tricub_qv_f64(const orc_set *s, const double *pos, int m, const double *const *srcs, double *const *dsts,
                        int clip, double *const *lin, double *const *mn, double *const *mx);
 
+/* LAM boundary fluxes (adz_BC_LAM_Aranami_hlt.F90) of m tracers into fo, fi
+ * (ext layout, range b and the zeroed regions written) */
+void orc_bc_lam_flux_f32(const orc_set *s, double dt, const double *wpxyz, const float *uvw_dep, const float *zdt0,
+                         const float *uslt, const float *vslt, int m, const float *const *srcs, float *const *fo,
+                         float *const *fi);
+void orc_bc_lam_flux_f64(const orc_set *s, double dt, const double *wpxyz, const double *uvw_dep,
+                         const double *zdt0, const double *uslt, const double *vslt, int m,
+                         const double *const *srcs, double *const *fo, double *const *fi);
+
 /* the same with the ensemble perturbation mcrhsint (element (1,1), rows ld
  * apart; NULL: none): dst = value + mcrhsint * abs(value - lin) before the
  * clip (adz_interp_hlt.F90:99-100, 125-133) */

@@ -108,6 +108,8 @@ class _Lib:
                                                         C.c_int, C.c_int, vp, vp, vp]
             getattr(L, f"orc_tricub_qv_{sfx}").argtypes = [C.POINTER(OrcSet), vp, C.c_int, vp, vp, C.c_int,
                                                            vp, vp, vp]
+            getattr(L, f"orc_bc_lam_flux_{sfx}").argtypes = [C.POINTER(OrcSet), C.c_double, vp, vp, vp, vp, vp,
+                                                             C.c_int, vp, vp, vp]
             getattr(L, f"orc_tricub_p_{sfx}").argtypes = [C.POINTER(OrcSet), C.c_int, vp, C.c_int, vp, vp,
                                                           C.c_int, C.c_int, vp, vp, vp, vp, C.c_int]
             getattr(L, f"orc_tricub_qv_p_{sfx}").argtypes = [C.POINTER(OrcSet), vp, C.c_int, vp, vp, C.c_int,
@@ -346,6 +348,21 @@ class Step:
             C.byref(self.s), self.cfg.dt, self.wpxyz.ctypes.data, self.uvw_dep.ctypes.data,
             a["zdt0"].ctypes.data, self.pxyzm.ctypes.data, *(None if x is None else x.ctypes.data for x in slt),
             *(self.sets[q].ctypes.data for q in range(4)))
+
+    def bc_lam_flux(self, srcs):
+        """FLUX_out, FLUX_in of adz_BC_LAM_Aranami_hlt.F90 for the tracers srcs
+        (ext arrays) at the last trajectory's Adz_pb; ext arrays, NaN where
+        not written."""
+        ct = C.c_float if self.prec == "f32" else C.c_double
+        srcs = [np.ascontiguousarray(x, dtype=self.dt) for x in srcs]
+        fo = [np.full(self.ext_shape, np.nan, self.dt) for _ in srcs]
+        fi = [np.full(self.ext_shape, np.nan, self.dt) for _ in srcs]
+        slt = getattr(self, "_slt", [None, None])
+        getattr(self.L, f"orc_bc_lam_flux_{self.prec}")(
+            C.byref(self.s), self.cfg.dt, self.wpxyz.ctypes.data, self.uvw_dep.ctypes.data, self._zdt0.ctypes.data,
+            *(None if x is None else x.ctypes.data for x in slt), len(srcs), C.cast(_ptrs(srcs, ct), C.c_void_p),
+            C.cast(_ptrs(fo, ct), C.c_void_p), C.cast(_ptrs(fi, ct), C.c_void_p))
+        return fo, fi
 
     def set_rhs_perturbation(self, mcrhsint=None):
         """mcrhsint (nj, ni) or None: the ensemble perturbation of every

@@ -44,6 +44,11 @@ def _case(prec_name, ntr=3):
     return A, cfg, prec, ad, trs, m, post, airm_p, airm_m, mask
 
 
+def _bits(a):
+    a = np.ascontiguousarray(a)
+    return a.view(np.int32) if a.dtype == np.float32 else a.view(np.int64)
+
+
 def _np(t):
     return t.cpu().numpy()
 
@@ -106,3 +111,47 @@ def test_bermejo_conde_rejects_bad_arguments():
     bad = [dict(p=trs[0], m=m[0], lin=post[0][0], weight=1)]  # min/max needed when min_max
     with pytest.raises(A.AdzError):
         A.bermejo_conde(ad, prec, bad, airm_p, airm_m, mask, deficit, min_max=True)
+
+
+@pytest.mark.parametrize("prec_name,gbpil", [("ref32", 0), ("fp64", 0), ("ref32", 4)])
+def test_bc_lam_flux_vs_oracle(prec_name, gbpil):
+    """LAM boundary fluxes (adz_BC_LAM_Aranami_hlt.F90) bit for bit against the
+    restatement: the masked tracers interpolated at Adz_pb over range b, then
+    zeroed; every element of fo and fi compared, including which ones are
+    written (NaN elsewhere on both sides).  gbpil: a top pilot (k0t > 1), so
+    FLUX_in is also zeroed above k0t."""
+    from gem_b200 import adz as A, synth
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for -m gpu tests")
+    prec = A.PREC_NAMES[prec_name]
+    dt = A._field_dtype(prec)
+    cfg = synth.config_small(48, 40, 20)
+    cfg.ntracers, cfg.tracer_kind = 3, "lognormal"
+    inp = synth.make_inputs(cfg, dtype=torch.float64)
+    npd = np.float32 if dt == torch.float32 else np.float64
+    keys = ("uu_ext", "vv_ext", "ww_ext", "ut0", "vt0", "zdt0")
+    np_in = {k: inp[k].numpy().astype(npd) for k in keys}
+    trs = [t.numpy().astype(npd) for t in inp["tracers"]]
+    st = O.Step(cfg, kind="ref" if (prec == A.REF32 and O.have_ref()) else "oracle",
+                prec="f32" if prec == A.REF32 else "f64", lam_gbpil_t=gbpil)
+    st.inittraj()
+    st.traject(np_in)
+    o_fo, o_fi = st.bc_lam_flux(trs)
+    ad = A.Adz.from_config(cfg, lam_gbpil_t=gbpil)
+    px, wp = ad.new_state(prec)
+    ad.adz_inittraj(prec, px, wp)
+    ad.adz_traject(prec, cfg.dt, {k: torch.from_numpy(v).cuda() for k, v in np_in.items()}, px, wp)
+    srcs = [torch.from_numpy(t).cuda() for t in trs]
+    nan = lambda: torch.full(ad.ext_shape, float("nan"), dtype=dt, device="cuda")  # noqa: E731
+    fo, fi = [nan() for _ in srcs], [nan() for _ in srcs]
+    ad.bc_lam_flux(prec, srcs, fo, fi)
+    torch.cuda.synchronize()
+    assert ad.status() == 0
+    for g, o in zip(fo + fi, o_fo + o_fi):
+        g = g.cpu().numpy()
+        assert np.array_equal(np.isnan(g), np.isnan(o))
+        w = ~np.isnan(o)
+        assert w.any()
+        assert np.array_equal(_bits(g[w]), _bits(o[w]))
+    # the fluxes are not trivially zero: both carry tracer outside the zeroed parts
+    assert all(np.nanmax(np.abs(o)) > 0 for o in o_fo + o_fi)
