@@ -9,7 +9,8 @@
 // position, so a tile of a decomposition gets what the reference's halo
 // exchange of the masks gives.  The copies select (mask ? value : 0), which
 // is the reference's mask * value for finite values and 0 where the reference
-// never writes.
+// never writes.  Without a tracer the copies are the masks themselves, the
+// PSADJ branch (B/adz_BC_LAM_Aranami_hlt.F90:84-101).
 #include <cuda_runtime.h>
 
 #include "adz_types.h"
@@ -33,7 +34,7 @@ __global__ void __launch_bounds__(256) k_bc_mask(BcMask m, const T* __restrict__
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
     const int i = m.lminx + (int)(e % m.nit), j = m.lminy + (int)((e / m.nit) % m.njt), k = 1 + (int)(e / plane);
     const bool dom = in_domain(m, i, j), core = dom && in_core(m, i, j, k);
-    const T v = src[e];
+    const T v = src ? src[e] : (T)1;  // no tracer: the masks themselves (PSADJ)
     mo[e] = core ? v : (T)0;
     mi[e] = (dom && !core) ? v : (T)0;
   }

@@ -737,8 +737,9 @@ extern "C" int adzc_bc_lam_flux(adzc_handle* h, int prec, int ntr, const void* c
   if (!h || !check_prec(prec) || ntr < 0 || (ntr > 0 && (!srcs || !fo || !fi))) return fail(ADZC_ERR_ARG);
   if (h->last_prec != prec || !h->wpxyz) return fail(ADZC_ERR_ARG);
   if (h->g.bc_lam_flux == 0) return fail(ADZC_ERR_ARG);  // the range b positions need k00 = 1
-  for (int q = 0; q < ntr; q++)
-    if (!srcs[q] || !fo[q] || !fi[q]) return fail(ADZC_ERR_ARG);
+  if (!srcs) return fail(ADZC_ERR_ARG);
+  for (int q = 0; q < ntr; q++)  // srcs[q] NULL: the masks alone (PSADJ)
+    if (!fo[q] || !fi[q]) return fail(ADZC_ERR_ARG);
   if (ntr == 0) return ADZC_OK;
   const adzc_info& I = h->info;
   const adz::DGrid& D = h->dg;

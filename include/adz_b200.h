@@ -216,7 +216,8 @@ int adzc_rhs_perturbation(adzc_handle *h, const void *mcrhsint, int ld);
  * fi: ext arrays receiving FLUX_out and FLUX_in at Adz_pb over Adz_i0b:inb,
  * Adz_j0b:jnb, 1:nk, then zeroed as the reference does (FLUX_out on the
  * core, FLUX_in on the pilot zones and above k0t); the fo, fi fields of
- * adzc_bermejo_conde.  The grid must set bc_lam_flux. */
+ * adzc_bermejo_conde.  srcs[q] NULL interpolates the masks themselves, the
+ * PSADJ branch (:84-101).  The grid must set bc_lam_flux. */
 int adzc_bc_lam_flux(adzc_handle *h, int prec, int ntr, const void *const *srcs, void *const *fo, void *const *fi,
                      void *stream);
 

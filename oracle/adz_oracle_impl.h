@@ -594,8 +594,9 @@ void SFX(orc_bc_lam_flux)(const orc_set *s, double dt, const double *wpxyz, cons
         for (int i = s->lminx; i < s->lminx + s->nit; i++) {
           const long e = EXT(i, j, k);
           const int dom = SFX(in_domain)(s, i, j), core = dom && SFX(in_core)(s, i, j, k);
-          mo[e] = core ? srcs[q][e] : (REAL)0;
-          mi[e] = (dom && !core) ? srcs[q][e] : (REAL)0;
+          const REAL v = srcs[q] ? srcs[q][e] : (REAL)1; /* no tracer: the masks (PSADJ, :84-101) */
+          mo[e] = core ? v : (REAL)0;
+          mi[e] = (dom && !core) ? v : (REAL)0;
         }
     REAL *fs[2] = {mo + o111, mi + o111};
     for (int k = 1; k <= nk; k++) {

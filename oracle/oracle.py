@@ -354,13 +354,15 @@ class Step:
         (ext arrays) at the last trajectory's Adz_pb; ext arrays, NaN where
         not written."""
         ct = C.c_float if self.prec == "f32" else C.c_double
-        srcs = [np.ascontiguousarray(x, dtype=self.dt) for x in srcs]
+        srcs = [None if x is None else np.ascontiguousarray(x, dtype=self.dt) for x in srcs]
         fo = [np.full(self.ext_shape, np.nan, self.dt) for _ in srcs]
         fi = [np.full(self.ext_shape, np.nan, self.dt) for _ in srcs]
+        sp = (C.POINTER(ct) * len(srcs))(*[C.POINTER(ct)() if x is None else x.ctypes.data_as(C.POINTER(ct))
+                                           for x in srcs])
         slt = getattr(self, "_slt", [None, None])
         getattr(self.L, f"orc_bc_lam_flux_{self.prec}")(
             C.byref(self.s), self.cfg.dt, self.wpxyz.ctypes.data, self.uvw_dep.ctypes.data, self._zdt0.ctypes.data,
-            *(None if x is None else x.ctypes.data for x in slt), len(srcs), C.cast(_ptrs(srcs, ct), C.c_void_p),
+            *(None if x is None else x.ctypes.data for x in slt), len(srcs), C.cast(sp, C.c_void_p),
             C.cast(_ptrs(fo, ct), C.c_void_p), C.cast(_ptrs(fi, ct), C.c_void_p))
         return fo, fi
 

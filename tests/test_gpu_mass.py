@@ -113,13 +113,15 @@ def test_bermejo_conde_rejects_bad_arguments():
         A.bermejo_conde(ad, prec, bad, airm_p, airm_m, mask, deficit, min_max=True)
 
 
-@pytest.mark.parametrize("prec_name,gbpil", [("ref32", 0), ("fp64", 0), ("ref32", 4)])
-def test_bc_lam_flux_vs_oracle(prec_name, gbpil):
+@pytest.mark.parametrize("prec_name,gbpil,psadj", [("ref32", 0, False), ("fp64", 0, False), ("ref32", 4, False),
+                                                   ("ref32", 0, True)])
+def test_bc_lam_flux_vs_oracle(prec_name, gbpil, psadj):
     """LAM boundary fluxes (adz_BC_LAM_Aranami_hlt.F90) bit for bit against the
     restatement: the masked tracers interpolated at Adz_pb over range b, then
     zeroed; every element of fo and fi compared, including which ones are
     written (NaN elsewhere on both sides).  gbpil: a top pilot (k0t > 1), so
-    FLUX_in is also zeroed above k0t."""
+    FLUX_in is also zeroed above k0t.  psadj: no tracer, the masks themselves
+    (the PSADJ branch)."""
     from gem_b200 import adz as A, synth
     if not torch.cuda.is_available():
         pytest.fail("CUDA device required for -m gpu tests")
@@ -136,12 +138,14 @@ def test_bc_lam_flux_vs_oracle(prec_name, gbpil):
                 prec="f32" if prec == A.REF32 else "f64", lam_gbpil_t=gbpil)
     st.inittraj()
     st.traject(np_in)
+    if psadj:
+        trs = [None]
     o_fo, o_fi = st.bc_lam_flux(trs)
     ad = A.Adz.from_config(cfg, lam_gbpil_t=gbpil)
     px, wp = ad.new_state(prec)
     ad.adz_inittraj(prec, px, wp)
     ad.adz_traject(prec, cfg.dt, {k: torch.from_numpy(v).cuda() for k, v in np_in.items()}, px, wp)
-    srcs = [torch.from_numpy(t).cuda() for t in trs]
+    srcs = [None if t is None else torch.from_numpy(t).cuda() for t in trs]
     nan = lambda: torch.full(ad.ext_shape, float("nan"), dtype=dt, device="cuda")  # noqa: E731
     fo, fi = [nan() for _ in srcs], [nan() for _ in srcs]
     ad.bc_lam_flux(prec, srcs, fo, fi)
