@@ -355,6 +355,10 @@ extern "C" int adzc_setup(const adzc_grid* gin, adzc_handle** out) {
   const adzc_grid& g = *gin;
   if (g.ni < 1 || g.nj < 1) return fail(ADZC_ERR_ARG);
   if (g.nk < 4) return fail(ADZC_ERR_NK);
+  {  // stencil offsets inside the extended array are 32-bit in the kernels
+    const long long hx = std::max(1, g.maxcfl) + 1;
+    if (((long long)g.ni + 2 * hx) * ((long long)g.nj + 2 * hx) * g.nk > 0x7fffffffLL) return fail(ADZC_ERR_SIZE);
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return fail(ADZC_ERR_NODEVICE);
   auto* h = new (std::nothrow) adzc_handle();

@@ -151,7 +151,10 @@ typedef struct {
 
 typedef struct adzc_handle adzc_handle;
 
-/* adz_set: derive tables on the host and upload them to the current device. */
+/* adz_set: derive tables on the host and upload them to the current device.
+ * The kernels address a stencil inside the extended array with 32-bit
+ * offsets, so a tile whose extended volume (ni + 2 halo) x (nj + 2 halo) x nk
+ * reaches 2^31 cells is refused with ADZC_ERR_SIZE; split it into tiles. */
 int adzc_setup(const adzc_grid *g, adzc_handle **h);
 int adzc_destroy(adzc_handle *h);
 int adzc_query(const adzc_handle *h, adzc_info *info);

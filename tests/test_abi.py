@@ -54,6 +54,13 @@ def test_errors_without_device(L):
     assert L.adzc_setup(None, None) == 1
     assert L.adzc_traject(None, 0, C.c_double(1.0), 1, *([None] * 9)) == 1
     assert L.adzc_tricub(None, 0, 0, 0, None, None, None, None, None, None, None) == 1
+    # a tile whose extended volume needs offsets beyond 32 bits is refused
+    g = adz.AdzcGrid()
+    big = np.zeros(64)
+    g.ni, g.nj, g.nk, g.maxcfl = 60000, 60000, 4, 3
+    g.zm = g.zt = g.zx = g.cy = big.ctypes.data_as(C.POINTER(C.c_double))
+    h = C.c_void_p()
+    assert L.adzc_setup(C.byref(g), C.byref(h)) == 9
     lev = np.linspace(3000.0, 100.0, 3)
     out = C.c_void_p()
     assert L.adzc_ztab_create(lev.ctypes.data, 3, 10, 10, 0, 0, C.byref(out)) == 3  # nk < 4
