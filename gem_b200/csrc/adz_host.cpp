@@ -912,8 +912,13 @@ int stage_inputs(const adzc_ztab* lv, int comp, const float* const* fs, int m, c
   }
   long long lo = (1LL << 62), hi = -(1LL << 62);
   for (int j = 0; j < n; j++) {
+    // the reference takes positions already clipped to the array; a
+    // non-finite or huge one would be truncated differently here and on the
+    // device, so the staged range would not cover what the kernel reads
+    const pxpypz& q = pos[j];
+    if (!(std::fabs(q.px) < 1.0e9f && std::fabs(q.py) < 1.0e9f && std::fabs(q.pz) < 1.0e9f)) return fail(ADZC_ERR_ARG);
     long long a, b;
-    corner_f32(lv, pos[j], &a, &b);
+    corner_f32(lv, q, &a, &b);
     lo = std::min(lo, a);
     hi = std::max(hi, b);
   }

@@ -102,6 +102,15 @@ def test_golden_vectors_level_a_host_pointers(A, vec):
     d3 = np.empty((n, 3), np.float32)
     L.Tricublin_zyx3_n(d3.ctypes.data, f3.ctypes.data, pos.ctypes.data, lv, n)
     assert np.array_equal(_bits(d3), _bits(vec["zyx3"]))
+    # a non-finite position is refused on the host before anything is staged:
+    # the output is left as it was and the thread's status is ADZC_ERR_ARG
+    bad = pos.copy()
+    bad[n // 2, 0] = np.nan
+    d1[:] = 7.0
+    L.Tricublin_zyx1_n(d1.ctypes.data, fields[1].ctypes.data, bad.ctypes.data, lv, n)
+    assert L.adzc_last_error() == 1 and np.all(d1 == 7.0)
+    L.Tricublin_zyx1_n(d1.ctypes.data, fields[1].ctypes.data, pos.ctypes.data, lv, n)
+    assert np.array_equal(_bits(d1), _bits(vec["zyx1"][1]))
 
 
 def test_selftest_kat_through_cuda_library(A):
