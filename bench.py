@@ -365,6 +365,9 @@ def run_product(args):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_reference(args.cpu_size, 2, 1, ntracers=args.ntr)
+        # the same path on one core, on a smaller sample (256x256x80)
+        one = cpu_reference((256, 256, args.cpu_size[2]), 2, 1, threads=1, ntracers=args.ntr)
+        cpu["single_core"] = {k: one[k] for k in ("value", "unit", "cores", "sample", "ms_per_step")}
     value = npts * ws / (ms32 * 1e-3)
     line = {
         "metric": "SL advection grid-points/s at 1024^2x80 (mixed-precision step; plain FP64 GPU drop-in alongside)",
