@@ -578,9 +578,11 @@ def measure_batch(args, timed, ws, cfgs, label):
     ms_s, _ = timed(sequential, args.steps, args.warmup)
     # per domain: winds, trajectory, and every set's field groups in one launch
     seq_launches = 3 * len(doms)
+    plan = batch.query()
+    nl = {"one launch": 1, "phased (one launch per phase)": 3}.get(plan["plan"], seq_launches)
     out = {"workload": f"{len(cfgs)} {label}",
            "points_per_step": npts, "value": npts * ws / (ms_b * 1e-3), "unit": "grid-points/s",
-           "ms_per_step": ms_b, "launches_per_step": 1, "plan": batch.query(), "tune_s": tune_s,
+           "ms_per_step": ms_b, "launches_per_step": nl, "plan": plan, "tune_s": tune_s,
            "sequential_ms_per_step": ms_s, "sequential_launches_per_step": seq_launches,
            "speedup_vs_sequential": ms_s / ms_b, "clocks": clk}
     del batch, doms, spec

@@ -20,7 +20,10 @@
 // The phased plan runs the same items as three persistent launches in the
 // graph, one per phase, each kernel with the register budget of the
 // per-domain kernel of its phase; launch order replaces the dependency waits.
-// The tuner weighs it against the one-launch kernel's budgets.
+// The per-domain plan replays every domain's own launches in turn: departure
+// winds, trajectory and all field groups in one k_tricub_parts launch, as the
+// per-domain entry points run them.  The tuner weighs the phased and
+// per-domain plans against the one-launch kernel's budgets.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -50,7 +53,7 @@ struct adzc_batch {
   unsigned* d_done = nullptr;
   int* d_status = nullptr;
   int rows = 8, bps = 4, sms = 148, variant = 0;
-  int phased = 0;           // the phased plan: one launch per phase
+  int phased = 0;           // 1: the phased plan (one launch per phase); 2: the per-domain launches
   unsigned long long spins = adz::kDepSpins;  // bound of a dependency wait
   long long inject_need = 0;  // fault injection: extra items domain 0's trajectory waits for
   long long pstart[4] = {}; // first item of each phase, total
@@ -106,8 +109,39 @@ int build_items(adzc_batch* b, int rows) {
   return ADZC_OK;
 }
 
+// every domain's own launches in turn (the per-domain plan)
+template <int PREC>
+cudaError_t enqueue_domains(const adzc_batch* b, cudaStream_t s) {
+  for (int d = 0; d < b->ndom; d++) {
+    const adz::BDom& D = b->doms[d];
+    cudaError_t e = adz::launch_prepare<PREC>(D.g, D.uu, D.vv, D.ww, const_cast<void*>(D.ta.uvw_d), s);
+    if (e == cudaSuccess) e = adz::launch_traject<PREC>(D.g, D.ta, s);
+    adz::SetParts sp{};
+    for (int q = 0; q < D.ngroups && e == cudaSuccess; q++) {
+      adz::SetPart& P = sp.p[sp.n++];
+      P.fp = D.gfp[q];
+      P.set = D.gset[q];
+      P.i0 = D.grange[q][0];
+      P.nx = D.grange[q][1];
+      P.j0 = D.grange[q][2];
+      P.ny = D.grange[q][3];
+      P.k0 = D.grange[q][4];
+      P.nz = D.g.nk - P.k0 + 1;
+      if (P.nx <= 0 || P.ny <= 0 || P.nz <= 0) sp.n--;
+      if (sp.n == adz::kMaxParts || (q == D.ngroups - 1 && sp.n > 0)) {
+        e = adz::launch_tricub_parts<PREC>(D.g, D.sa, sp, s);
+        sp = adz::SetParts{};
+      }
+    }
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t enqueue(adzc_batch* b, cudaStream_t s) {
   cudaError_t e;
+  if (b->phased == 2)
+    return b->prec == ADZC_FP64 ? enqueue_domains<adz::kFp64>(b, s) : enqueue_domains<adz::kMixed>(b, s);
   if (b->phased) {
     if ((e = cudaMemsetAsync(b->d_next + 1, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
     if (b->prec == ADZC_FP64)
@@ -367,6 +401,15 @@ extern "C" int adzc_batch_tune(adzc_batch* b, void* stream) {
       }
     }
   }
+  if (st == ADZC_OK) {  // the per-domain launches (rows unused)
+    b->phased = 2;
+    float ms = 0.f;
+    if (enqueue(b, s) != cudaSuccess || cudaEventRecord(e0, s) != cudaSuccess || enqueue(b, s) != cudaSuccess ||
+        enqueue(b, s) != cudaSuccess || cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess)
+      st = ADZC_ERR_CUDA;
+    else if (cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms < best)
+      best = ms, bp = 2;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   b->bps = bb;
@@ -387,7 +430,7 @@ extern "C" int adzc_batch_query(const adzc_batch* b, int* rows, int* blocks_per_
 }
 
 extern "C" int adzc_batch_select(adzc_batch* b, int rows, int plan) {
-  if (!b || rows < 1 || plan < 0 || plan > adz::kBatchVariants) return adz_internal_fail(ADZC_ERR_ARG);
+  if (!b || rows < 1 || plan < 0 || plan > ADZC_BATCH_DOMAINS) return adz_internal_fail(ADZC_ERR_ARG);
   if (plan < adz::kBatchVariants) {
     const int res = resident(b, plan);
     if (res < 1) return adz_internal_fail(ADZC_ERR_ARG);
@@ -395,7 +438,7 @@ extern "C" int adzc_batch_select(adzc_batch* b, int rows, int plan) {
     b->bps = res;
     b->phased = 0;
   } else {
-    b->phased = 1;
+    b->phased = plan == ADZC_BATCH_DOMAINS ? 2 : 1;
   }
   int st = build_items(b, rows);
   if (st == ADZC_OK) st = capture(b);

@@ -270,12 +270,16 @@ int adzc_batch_create(int prec, int ndom, const adzc_domain *doms, adzc_batch **
 int adzc_batch_tune(adzc_batch *b, void *stream);
 int adzc_batch_step(adzc_batch *b, void *stream);
 /* the plan in use; blocks_per_sm of the one-launch kernel (phased plan: of
- * its trajectory launch); phased: 1 for the phased plan (may be NULL) */
+ * its trajectory launch); phased: 1 for the phased plan, 2 for the
+ * per-domain launches (may be NULL) */
 int adzc_batch_query(const adzc_batch *b, int *rows_per_item, int *blocks_per_sm, long long *nitems);
 int adzc_batch_plan(const adzc_batch *b, int *phased);
 /* pin a plan instead of tuning: rows per work item, plan 0..2 = register
- * budget of the one-launch kernel, 3 = phased; re-captures the graph */
+ * budget of the one-launch kernel, 3 = phased, 4 = every domain's own
+ * launches (departure winds, trajectory, all field groups) in turn inside the
+ * graph, rows unused; re-captures the graph */
 #define ADZC_BATCH_PHASED 3
+#define ADZC_BATCH_DOMAINS 4
 int adzc_batch_select(adzc_batch *b, int rows_per_item, int plan);
 /* Fault injection for tests of the failure path, on the host (no GPU fault).
  * ADZC_INJECT_SPINS: bound of a dependency wait of the one-launch kernel, in

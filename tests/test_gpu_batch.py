@@ -70,10 +70,11 @@ def _compare(a, b, what):
 
 
 @pytest.mark.parametrize("precname,plan", [("mixed", None), ("fp64", None), ("mixed", (8, 2)), ("mixed", (2, 3)),
-                                           ("fp64", (32, 3))])
+                                           ("fp64", (32, 3)), ("mixed", (8, 4)), ("fp64", (8, 4))])
 def test_batch_matches_per_domain_steps(precname, plan):
     """plan None: the default one-launch plan; (rows, 0..2): that register
-    budget of the one-launch kernel; (rows, 3): the phased plan."""
+    budget of the one-launch kernel; (rows, 3): the phased plan; (rows, 4):
+    every domain's own launches in the graph."""
     from gem_b200 import adz as A
     prec = A.PREC_NAMES[precname]
     adz, doms = _domains(prec)
@@ -86,6 +87,7 @@ def test_batch_matches_per_domain_steps(precname, plan):
     q = batch.query()
     assert q["items"] > 0 and q["blocks_per_sm"] >= 1
     assert q["plan"].startswith("phased") == (plan is not None and plan[1] == adz.Batch.PHASED)
+    assert q["plan"].startswith("per-domain") == (plan is not None and plan[1] == adz.Batch.DOMAINS)
     if plan is not None:
         assert q["rows_per_item"] == plan[0]
     for step in range(2):
@@ -141,7 +143,7 @@ def test_batch_rejects_bad_domains():
     with pytest.raises(adz.AdzError):
         adz.Batch(A.REF32, [])  # no domains / REF32 not batched
     ok = _batch(adz, A.MIXED, doms, wps, outs)
-    for rows, plan in ((0, 0), (8, -1), (8, 4)):
+    for rows, plan in ((0, 0), (8, -1), (8, 5)):
         with pytest.raises(adz.AdzError):
             ok.select(rows, plan)
     # a handle still in its cold start is refused
