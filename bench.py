@@ -583,6 +583,7 @@ def measure_batch(args, timed, ws, cfgs, label):
     out = {"workload": f"{len(cfgs)} {label}",
            "points_per_step": npts, "value": npts * ws / (ms_b * 1e-3), "unit": "grid-points/s",
            "ms_per_step": ms_b, "launches_per_step": nl, "plan": plan, "tune_s": tune_s,
+           "tuner_ms_per_plan": batch.tuned(),
            "sequential_ms_per_step": ms_s, "sequential_launches_per_step": seq_launches,
            "speedup_vs_sequential": ms_s / ms_b, "clocks": clk}
     del batch, doms, spec

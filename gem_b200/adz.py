@@ -104,6 +104,7 @@ def lib() -> C.CDLL:
         L.adzc_batch_step.argtypes = [vp, vp]
         L.adzc_batch_query.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
         L.adzc_batch_plan.argtypes = [vp, C.POINTER(C.c_int)]
+        L.adzc_batch_tuned.argtypes = [vp, C.POINTER(C.c_float)]
         L.adzc_batch_select.argtypes = [vp, i, i]
         L.adzc_batch_inject.argtypes = [vp, i, C.c_longlong]
         L.adzc_batch_status.argtypes = [vp, i, vp]
@@ -422,6 +423,12 @@ class Batch:
         INJECT_NEED makes domain 0's trajectory items wait for items that
         never come (0: clear)."""
         _check(lib().adzc_batch_inject(self.h, int(what), int(value)), "adzc_batch_inject")
+
+    def tuned(self) -> dict:
+        """The tuner's best ms per step of each plan family (None: not timed)."""
+        ms = (C.c_float * 3)()
+        _check(lib().adzc_batch_tuned(self.h, ms), "adzc_batch_tuned")
+        return {k: (round(v, 3) if v >= 0 else None) for k, v in zip(("one_launch", "phased", "per_domain"), ms)}
 
     def select(self, rows: int, plan: int):
         """Pin a plan: rows per work item and 0..2 (register budget of the

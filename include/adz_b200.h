@@ -280,6 +280,10 @@ int adzc_batch_plan(const adzc_batch *b, int *phased);
  * graph, rows unused; re-captures the graph */
 #define ADZC_BATCH_PHASED 3
 #define ADZC_BATCH_DOMAINS 4
+/* after adzc_batch_tune: the best time per step the tuner measured for each
+ * plan family, ms[0] the one-launch kernel, ms[1] the phased plan, ms[2] the
+ * per-domain launches (-1: not timed) */
+int adzc_batch_tuned(const adzc_batch *b, float ms[3]);
 int adzc_batch_select(adzc_batch *b, int rows_per_item, int plan);
 /* Fault injection for tests of the failure path, on the host (no GPU fault).
  * ADZC_INJECT_SPINS: bound of a dependency wait of the one-launch kernel, in

@@ -116,6 +116,10 @@ def test_batch_tune_then_step():
     assert batch.status() == 0
     q = batch.query()
     assert q["rows_per_item"] in (2, 8, 32)
+    t = batch.tuned()  # every plan family was timed, and the kept plan is the fastest
+    assert all(v is not None and v > 0 for v in t.values())
+    kept = {"one launch": "one_launch", "phased (one launch per phase)": "phased"}.get(q["plan"], "per_domain")
+    assert t[kept] == min(t.values())
     for (_, _, _, wp), wb in zip(doms, wps_b):
         wp.copy_(wb)
     batch.step()
