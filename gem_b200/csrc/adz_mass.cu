@@ -14,8 +14,10 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <new>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/adz_b200.h"
@@ -64,17 +66,32 @@ __device__ __forceinline__ long long ext(const Geo& g, int i, int j, int k) {
 
 __device__ __forceinline__ double sign1(double x) { return signbit(x) ? -1.0 : 1.0; }
 
-// weight of Bermejo_Conde.F90:87-137 (stored as T by the reference)
+// weight of Bermejo_Conde.F90:87-137 (stored as T by the reference) from the
+// point's values m, lin and (weight 3) pkps
 template <typename T>
-__device__ __forceinline__ T bc_weight(const Tr<T>& tr, long long e, double sd) {
-  const T hmlt = tr.m[e] - tr.lin[e];
+__device__ __forceinline__ T bc_weight_v(const Tr<T>& tr, T m, T lin, T pk, double sd) {
+  const T hmlt = m - lin;
   const double hml = (double)hmlt;
   if ((int)sd != (int)sign1(hml)) return (T)0;
   const double a = fabs(hml);
   const double pw = (tr.p_exp == 1.0) ? a : pow(a, tr.p_exp);
   if (tr.weight == 1) return (T)(pw * sd);
-  if (tr.weight == 2) return (T)(pw * sd * (double)(tr.m[e] > (T)0 ? tr.m[e] : (T)0));
-  return (T)(pw * sd * (double)tr.pkps[e]);
+  if (tr.weight == 2) return (T)(pw * sd * (double)(m > (T)0 ? m : (T)0));
+  return (T)(pw * sd * (double)pk);
+}
+template <typename T>
+__device__ __forceinline__ T bc_weight(const Tr<T>& tr, long long e, double sd) {
+  return bc_weight_v<T>(tr, tr.m[e], tr.lin[e], tr.weight == 3 ? tr.pkps[e] : (T)0, sd);
+}
+
+// FP32 fields four cells at a time: every array and every row start of the
+// region is 16-byte aligned (checked on the host), the region's x extent a
+// multiple of 4, the mask's row start 16-byte aligned
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ float c4(const float4& v, int u) { return u == 0 ? v.x : u == 1 ? v.y : u == 2 ? v.z : v.w; }
+__device__ __forceinline__ void mask4(const double* p, double* mk) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p + 2));
+  mk[0] = a.x; mk[1] = a.y; mk[2] = b.x; mk[3] = b.y;
 }
 
 enum Mode { kPMW = 0, kFlux = 1 };
@@ -107,7 +124,7 @@ __device__ __forceinline__ void block_rows(const Region& r, long long& r0, long 
 // one read of the fields (kPMW), or the boundary fluxes (kFlux); blockIdx.y
 // = tracer.  A point's weight is non-zero for one sign only, and its value is
 // the one bc_weight gives for that sign.
-template <typename T, int MODE>
+template <typename T, int MODE, bool VEC>
 __global__ void __launch_bounds__(kThreads) k_reduce(const Tr<T>* __restrict__ trs, Region r, Geo g,
                                                      const T* __restrict__ air_p, const T* __restrict__ air_m,
                                                      double* __restrict__ part) {
@@ -116,7 +133,47 @@ __global__ void __launch_bounds__(kThreads) k_reduce(const Tr<T>* __restrict__ t
   long long r0, r1;
   block_rows(r, r0, r1);
   double v[kSums] = {0.0, 0.0, 0.0, 0.0};
-  if (!(MODE == kFlux && (!tr.fo || !tr.fi)) && r.nx > 0) {
+  if constexpr (VEC && std::is_same<T, float>::value) {
+    if (!(MODE == kFlux && (!tr.fo || !tr.fi)) && r.nx > 0) {
+      const int nx4 = r.nx >> 2;
+      for (long long row = r0; row < r1; row++) {
+        const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
+        const long long e0 = ext(g, r.i0, j, k);
+        const double* mrow = g.mask + (r.i0 - 1) + (long long)(j - 1) * g.ni;
+        for (int c = threadIdx.x; c < nx4; c += kThreads) {
+          const long long e = e0 + 4 * c;
+          double mk[4];
+          mask4(mrow + 4 * c, mk);
+          if (MODE == kPMW) {
+            const float4 p4 = ld4(tr.p + e), ap4 = ld4(air_p + e), m4 = ld4(tr.m + e), am4 = ld4(air_m + e);
+            const float4 l4 = ld4(tr.lin + e);
+            const float4 k4 = tr.weight == 3 ? ld4(tr.pkps + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+              const float mu = c4(m4, u), lu = c4(l4, u), amu = c4(am4, u);
+              const float a = c4(p4, u) * c4(ap4, u);
+              const float b = mu * amu;
+              v[0] += (double)a * mk[u];
+              v[1] += (double)b * mk[u];
+              const double sd = sign1((double)(float)(mu - lu));
+              const float w = bc_weight_v<float>(tr, mu, lu, c4(k4, u), sd) * amu;
+              if (sd > 0.0) v[2] += (double)w * mk[u];
+              else v[3] += (double)w * mk[u];
+            }
+          } else {
+            const float4 o4 = ld4(tr.fo + e), i4 = ld4(tr.fi + e), am4 = ld4(air_m + e);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+              const float a = c4(o4, u) * c4(am4, u);
+              const float b = c4(i4, u) * c4(am4, u);
+              v[0] += (double)a * mk[u];
+              v[1] += (double)b * mk[u];
+            }
+          }
+        }
+      }
+    }
+  } else if (!(MODE == kFlux && (!tr.fo || !tr.fi)) && r.nx > 0) {
     for (long long row = r0; row < r1; row++)
 #pragma unroll 4
     for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) {
@@ -198,7 +255,7 @@ __global__ void k_finish(const double* __restrict__ part, State* __restrict__ st
 
 // m - lambda w, clipped to the bound box when min_max (Bermejo_Conde.F90:163-199),
 // and the mass of the corrected field in the same pass
-template <typename T>
+template <typename T, bool VEC>
 __global__ void __launch_bounds__(kThreads) k_correct(const Tr<T>* __restrict__ trs, const State* __restrict__ st,
                                                       Region r, Geo g, const T* __restrict__ air_m, int min_max,
                                                       double* __restrict__ part) {
@@ -209,7 +266,44 @@ __global__ void __launch_bounds__(kThreads) k_correct(const Tr<T>* __restrict__ 
   long long r0, r1;
   block_rows(r, r0, r1);
   double v = 0.0;
-  if (!skip && r.nx > 0) {
+  if constexpr (VEC && std::is_same<T, float>::value) {
+    if (!skip && r.nx > 0) {
+      const int nx4 = r.nx >> 2;
+      for (long long row = r0; row < r1; row++) {
+        const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
+        const long long e0 = ext(g, r.i0, j, k);
+        const double* mrow = g.mask + (r.i0 - 1) + (long long)(j - 1) * g.ni;
+        for (int c = threadIdx.x; c < nx4; c += kThreads) {
+          const long long e = e0 + 4 * c;
+          double mk[4];
+          mask4(mrow + 4 * c, mk);
+          const float4 m4 = ld4(tr.m + e), l4 = ld4(tr.lin + e), am4 = ld4(air_m + e);
+          const float4 k4 = tr.weight == 3 ? ld4(tr.pkps + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+          const float4 n4 = min_max ? ld4(tr.mn + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+          const float4 x4 = min_max ? ld4(tr.mx + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+          float out[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const float mu = c4(m4, u);
+            const double corr = lambda * (double)bc_weight_v<float>(tr, mu, c4(l4, u), c4(k4, u), sd);
+            float nv;
+            if (!min_max) {
+              nv = (float)((double)mu - corr);
+            } else {
+              const float wrk = (float)((double)mu - corr);
+              nv = wrk;
+              if (corr > 0.0 && wrk < c4(n4, u)) nv = c4(n4, u);
+              if (corr < 0.0 && wrk > c4(x4, u)) nv = c4(x4, u);
+            }
+            out[u] = nv;
+            const float a = nv * c4(am4, u);
+            v += (double)a * mk[u];
+          }
+          *reinterpret_cast<float4*>(tr.m + e) = make_float4(out[0], out[1], out[2], out[3]);
+        }
+      }
+    }
+  } else if (!skip && r.nx > 0) {
     for (long long row = r0; row < r1; row++)
 #pragma unroll 4
     for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) {
@@ -235,7 +329,7 @@ __global__ void __launch_bounds__(kThreads) k_correct(const Tr<T>* __restrict__ 
 
 // proportional rescale after the clipped correction (Bermejo_Conde.F90:203-222),
 // and the final mass in the same pass
-template <typename T>
+template <typename T, bool VEC>
 __global__ void __launch_bounds__(kThreads) k_scale(const Tr<T>* __restrict__ trs, const State* __restrict__ st,
                                                     Region r, Geo g, const T* __restrict__ air_m,
                                                     double* __restrict__ part) {
@@ -246,7 +340,31 @@ __global__ void __launch_bounds__(kThreads) k_scale(const Tr<T>* __restrict__ tr
   long long r0, r1;
   block_rows(r, r0, r1);
   double v = 0.0;
-  if (!skip && r.nx > 0) {
+  if constexpr (VEC && std::is_same<T, float>::value) {
+    if (!skip && r.nx > 0) {
+      const int nx4 = r.nx >> 2;
+      for (long long row = r0; row < r1; row++) {
+        const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
+        const long long e0 = ext(g, r.i0, j, k);
+        const double* mrow = g.mask + (r.i0 - 1) + (long long)(j - 1) * g.ni;
+        for (int c = threadIdx.x; c < nx4; c += kThreads) {
+          const long long e = e0 + 4 * c;
+          double mk[4];
+          mask4(mrow + 4 * c, mk);
+          const float4 m4 = ld4(m + e), am4 = ld4(air_m + e);
+          float out[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const float nv = (float)(prop * (double)c4(m4, u));
+            out[u] = nv;
+            const float a = nv * c4(am4, u);
+            v += (double)a * mk[u];
+          }
+          *reinterpret_cast<float4*>(m + e) = make_float4(out[0], out[1], out[2], out[3]);
+        }
+      }
+    }
+  } else if (!skip && r.nx > 0) {
     for (long long row = r0; row < r1; row++)
 #pragma unroll 4
     for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) {
@@ -267,6 +385,24 @@ __global__ void __launch_bounds__(kThreads) k_scale(const Tr<T>* __restrict__ tr
 namespace {
 
 using namespace adz::mass;
+
+bool al16(const void* p) { return p == nullptr || ((uintptr_t)p & 15) == 0; }
+
+// the four-cell path applies: FP32, every array 16-byte aligned, every row
+// start of the region at a multiple of 4 cells, the mask's rows likewise
+template <typename T>
+bool vec_ok(int ntr, const adzc_bc_tracer* in, const void* ap, const void* am, const double* mask, const Region& r,
+            const Geo& g) {
+  if (sizeof(T) != 4 || !al16(ap) || !al16(am) || !al16(mask)) return false;
+  if (r.nx % 4 || (r.i0 - g.lminx) % 4 || g.nit % 4 || g.nij % 4 || (r.i0 - 1) % 2 || g.ni % 2) return false;
+  for (int q = 0; q < ntr; q++) {
+    const adzc_bc_tracer& t = in[q];
+    if (!al16(t.p) || !al16(t.m) || !al16(t.lin) || !al16(t.min) || !al16(t.max) || !al16(t.fo) || !al16(t.fi) ||
+        !al16(t.pkps))
+      return false;
+  }
+  return true;
+}
 
 template <typename T>
 int run_bc(int ntr, const adzc_bc_tracer* in, const void* airm_p, const void* airm_m, const double* mask,
@@ -300,14 +436,20 @@ int run_bc(int ntr, const adzc_bc_tracer* in, const void* airm_p, const void* ai
   gm.mask = mask;
   // four passes over the fields: masses and weights; fluxes (boundary only);
   // correction with its mass; rescale with the final mass (clipped only)
-  k_reduce<T, kPMW><<<rg, kThreads, 0, s>>>(d_tr, core, gm, ap, am, d_part);
+  const bool vc = vec_ok<T>(ntr, in, ap, am, mask, core, gm);
+  const bool vb = vec_ok<T>(ntr, in, ap, am, mask, brange, gm);
+  if (vc) k_reduce<T, kPMW, true><<<rg, kThreads, 0, s>>>(d_tr, core, gm, ap, am, d_part);
+  else k_reduce<T, kPMW, false><<<rg, kThreads, 0, s>>>(d_tr, core, gm, ap, am, d_part);
   k_finish<kAfterPMW><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
-  k_reduce<T, kFlux><<<rg, kThreads, 0, s>>>(d_tr, brange, gm, ap, am, d_part);
+  if (vb) k_reduce<T, kFlux, true><<<rg, kThreads, 0, s>>>(d_tr, brange, gm, ap, am, d_part);
+  else k_reduce<T, kFlux, false><<<rg, kThreads, 0, s>>>(d_tr, brange, gm, ap, am, d_part);
   k_finish<kAfterFlux><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
-  k_correct<T><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, am, min_max, d_part);
+  if (vc) k_correct<T, true><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, am, min_max, d_part);
+  else k_correct<T, false><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, am, min_max, d_part);
   if (min_max) {
     k_finish<kAfterBcR><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
-    k_scale<T><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, am, d_part);
+    if (vc) k_scale<T, true><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, am, d_part);
+    else k_scale<T, false><<<rg, kThreads, 0, s>>>(d_tr, d_st, core, gm, am, d_part);
   }
   k_finish<kAfterBc><<<fb, 128, 0, s>>>(d_part, d_st, ntr, deficit, diag);
   return cudaGetLastError() == cudaSuccess ? ADZC_OK : ADZC_ERR_CUDA;

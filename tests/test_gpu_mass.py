@@ -17,13 +17,13 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-def _case(prec_name, ntr=3):
+def _case(prec_name, ntr=3, ni=56):
     from gem_b200 import adz as A, synth
     if not torch.cuda.is_available():
         pytest.fail("CUDA device required for -m gpu tests")
     prec = A.PREC_NAMES[prec_name]
     dt = A._field_dtype(prec)
-    cfg = synth.config_small(56, 48, 20)
+    cfg = synth.config_small(ni, 48, 20)
     cfg.ntracers, cfg.tracer_kind = ntr, "lognormal"
     inp = synth.make_inputs(cfg, device="cuda", dtype=dt)
     ad = A.Adz.from_config(cfg)
@@ -53,25 +53,48 @@ def _np(t):
     return t.cpu().numpy()
 
 
-def _close(a, b, before, ulps, dlam):
+def _close(a, b, before, ulps, dlam, dprop=0.0):
     """a, b agree to ulps units in the last place of the value, plus the
     correction m - before times the relative difference of the two lambdas
-    (a quotient of two FP64 sums, summed in different orders)."""
+    (a quotient of two FP64 sums, summed in different orders), plus the value
+    times the relative difference of the two proportional rescale factors
+    (another quotient of sums, applied to the whole field when min_max)."""
     a, b = np.asarray(a), np.asarray(b)
     eps = np.finfo(a.dtype).eps
-    tol = ulps * eps * np.maximum(np.abs(a), np.abs(b)) + (dlam + 4 * eps) * np.abs(b - before)
+    tol = ulps * eps * np.maximum(np.abs(a), np.abs(b)) + (dlam + 4 * eps) * np.abs(b - before) + dprop * np.abs(b)
     return np.all(np.abs(a - b) <= tol + np.finfo(a.dtype).tiny)
 
 
-@pytest.mark.parametrize("prec_name,weight,p_exp,min_max", [("mixed", 1, 1.0, True), ("ref32", 2, 2.0, True),
-                                                             ("fp64", 1, 1.0, False), ("mixed", 1, 1.0, False)])
-def test_bermejo_conde_vs_oracle(prec_name, weight, p_exp, min_max):
-    A, cfg, prec, ad, trs, m, post, airm_p, airm_m, mask = _case(prec_name)
+# FP32 fields take four cells at a time where every row start is 16-byte
+# aligned (ni = 56: extended rows of 64 cells); ni = 58 (rows of 66) takes the
+# cell-by-cell kernels
+# flux: LAM boundary fluxes fo, fi given (the flux pass), weight 3 with pkps
+@pytest.mark.parametrize("prec_name,weight,p_exp,min_max,ni,flux", [("mixed", 1, 1.0, True, 56, False),
+                                                                     ("ref32", 2, 2.0, True, 56, False),
+                                                                     ("fp64", 1, 1.0, False, 56, False),
+                                                                     ("mixed", 1, 1.0, False, 56, False),
+                                                                     ("mixed", 1, 1.0, True, 58, False),
+                                                                     ("ref32", 2, 2.0, True, 58, False),
+                                                                     ("mixed", 3, 1.0, True, 56, True),
+                                                                     ("ref32", 3, 1.5, True, 58, True),
+                                                                     ("fp64", 3, 1.0, True, 56, True)])
+def test_bermejo_conde_vs_oracle(prec_name, weight, p_exp, min_max, ni, flux):
+    A, cfg, prec, ad, trs, m, post, airm_p, airm_m, mask = _case(prec_name, ni=ni)
     lin, mn, mx = post
     ntr = len(trs)
     # tracer 0 made smooth in its last step: high and low order equal -> no correction (almost_zero)
     m[0].copy_(lin[0])
-    src = [dict(p=trs[q], m=m[q], lin=lin[q], min=mn[q], max=mx[q], weight=weight, p_exp=p_exp) for q in range(ntr)]
+    extra = [{} for _ in range(ntr)]
+    if flux or weight == 3:
+        g = torch.Generator(device="cuda").manual_seed(11)
+        rnd = lambda a: (a * torch.rand(ad.ext_shape, generator=g, device="cuda", dtype=torch.float64)).to(m[0].dtype)  # noqa: E731
+        for q in range(ntr):
+            if flux:
+                extra[q].update(fo=rnd(0.01), fi=rnd(0.01))
+            if weight == 3:
+                extra[q]["pkps"] = 0.5 + rnd(1.0)
+    src = [dict(p=trs[q], m=m[q], lin=lin[q], min=mn[q], max=mx[q], weight=weight, p_exp=p_exp, **extra[q])
+           for q in range(ntr)]
     before = [_np(t).copy() for t in m]
     deficit = torch.tensor([0.0, 1e-3, -2e-3][:ntr], dtype=torch.float64, device="cuda")
     d0 = _np(deficit).copy()
@@ -81,9 +104,10 @@ def test_bermejo_conde_vs_oracle(prec_name, weight, p_exp, min_max):
     st = O.Step(cfg, kind="oracle", prec="f32" if prec != A.FP64 else "f64")
     g_diag, g_def = _np(diag), _np(deficit)
     for q in range(ntr):
+        ex = {k: _np(v) for k, v in extra[q].items()}
         o_m, o_def, o_diag = st.bermejo_conde(_np(trs[q]), before[q], _np(lin[q]), _np(mn[q]), _np(mx[q]),
                                               _np(airm_p), _np(airm_m), _np(mask), deficit=d0[q], weight=weight,
-                                              p_exp=p_exp, min_max=min_max)
+                                              p_exp=p_exp, min_max=min_max, **ex)
         scale = max(abs(o_diag[0]), abs(o_diag[1]))
         masses = [0, 1, 2, 3, 4, 6, 7]
         assert np.all(np.abs(g_diag[q][masses] - o_diag[masses]) <= 1e-12 * scale), (q, g_diag[q], o_diag)
@@ -92,9 +116,15 @@ def test_bermejo_conde_vs_oracle(prec_name, weight, p_exp, min_max):
         gm = _np(m[q])
         bad = np.argmax(np.abs(gm - o_m))
         dlam = abs(g_diag[q][5] - o_diag[5]) / max(abs(o_diag[5]), 1e-300)
-        assert _close(gm, o_m, before[q], 2 if p_exp == 1.0 else 4, dlam), (
+        # rescale factor mass_bc / mass_bc_r of each side (min_max only)
+        dprop = 0.0
+        if min_max and o_diag[6] != 0 and g_diag[q][6] != 0 and o_diag[7] != 0:
+            dprop = 2 * abs((g_diag[q][7] / g_diag[q][6]) / (o_diag[7] / o_diag[6]) - 1.0)
+        assert _close(gm, o_m, before[q], 2 if p_exp == 1.0 else 4, dlam, dprop), (
             q, np.unravel_index(bad, gm.shape), gm.flat[bad], o_m.flat[bad], before[q].flat[bad],
             int(np.sum(gm != o_m)))
+    if flux:  # the mass balance then includes the boundary fluxes; the oracle comparison above covers it
+        return
     # tracer 0: nothing to fix, epsilon carried unchanged
     assert np.array_equal(_np(m[0]), before[0]) and g_def[0] == d0[0]
     # the fixed tracers hold the mass they had before advection (minus the old epsilon)
