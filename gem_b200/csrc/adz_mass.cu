@@ -120,6 +120,45 @@ __device__ __forceinline__ void block_rows(const Region& r, long long& r0, long 
   r1 = min(rows, r0 + chunk);
 }
 
+// cell t of a block's rows (row-major from row r0, x fastest) as (i, j, k),
+// advanced kThreads cells at a time without divisions
+struct Walk {
+  int i, j, k;
+};
+__device__ __forceinline__ Walk walk_start(const Region& r, int r0, int t) {
+  const int rr = t / r.nx, row = r0 + rr;
+  return Walk{r.i0 + (t - rr * r.nx), r.j0 + row % r.ny, r.k0 + row / r.ny};
+}
+__device__ __forceinline__ void walk_step(const Region& r, Walk& w) {
+  w.i += kThreads;
+  while (w.i >= r.i0 + r.nx) {
+    w.i -= r.nx;
+    if (++w.j == r.j0 + r.ny) {
+      w.j = r.j0;
+      ++w.k;
+    }
+  }
+}
+
+// every cell of the block's rows, each thread's cells in row order.  FP64
+// walks the flattened rows (no idle threads at the end of a row); FP32 takes
+// one row at a time, so that the four unrolled cells of a row load together
+template <typename T, typename F>
+__device__ __forceinline__ void for_cells(const Region& r, long long r0, long long r1, F&& f) {
+  if constexpr (sizeof(T) == 8) {
+    const int nt = (int)(r1 - r0) * r.nx;
+    Walk w = walk_start(r, (int)r0, threadIdx.x);
+#pragma unroll 4
+    for (int t = threadIdx.x; t < nt; t += kThreads, walk_step(r, w)) f(w.i, w.j, w.k);
+  } else {
+    for (long long row = r0; row < r1; row++) {
+      const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
+#pragma unroll 4
+      for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) f(i, j, k);
+    }
+  }
+}
+
 // masses before the correction and the weight sums of both deficit signs in
 // one read of the fields (kPMW), or the boundary fluxes (kFlux); blockIdx.y
 // = tracer.  A point's weight is non-zero for one sign only, and its value is
@@ -135,15 +174,15 @@ __global__ void __launch_bounds__(kThreads) k_reduce(const Tr<T>* __restrict__ t
   double v[kSums] = {0.0, 0.0, 0.0, 0.0};
   if constexpr (VEC && std::is_same<T, float>::value) {
     if (!(MODE == kFlux && (!tr.fo || !tr.fi)) && r.nx > 0) {
-      const int nx4 = r.nx >> 2;
-      for (long long row = r0; row < r1; row++) {
-        const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
-        const long long e0 = ext(g, r.i0, j, k);
-        const double* mrow = g.mask + (r.i0 - 1) + (long long)(j - 1) * g.ni;
-        for (int c = threadIdx.x; c < nx4; c += kThreads) {
-          const long long e = e0 + 4 * c;
-          double mk[4];
-          mask4(mrow + 4 * c, mk);
+      const int nx4 = r.nx >> 2, n4 = (int)(r1 - r0) * nx4;
+      for (int t = threadIdx.x; t < n4; t += kThreads) {  // the block's (row, 4-cell chunk) pairs
+        const int rr = t / nx4, c = t - rr * nx4;
+        const int row = (int)r0 + rr;
+        const int j = r.j0 + row % r.ny, k = r.k0 + row / r.ny;
+        const long long e = ext(g, r.i0, j, k) + 4 * c;
+        double mk[4];
+        mask4(g.mask + (r.i0 - 1) + (long long)(j - 1) * g.ni + 4 * c, mk);
+        {
           if (MODE == kPMW) {
             const float4 p4 = ld4(tr.p + e), ap4 = ld4(air_p + e), m4 = ld4(tr.m + e), am4 = ld4(air_m + e);
             const float4 l4 = ld4(tr.lin + e);
@@ -174,10 +213,7 @@ __global__ void __launch_bounds__(kThreads) k_reduce(const Tr<T>* __restrict__ t
       }
     }
   } else if (!(MODE == kFlux && (!tr.fo || !tr.fi)) && r.nx > 0) {
-    for (long long row = r0; row < r1; row++)
-#pragma unroll 4
-    for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) {
-      const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
+    for_cells<T>(r, r0, r1, [&](int i, int j, int k) {
       const long long e = ext(g, i, j, k);
       const double mk = __ldg(g.mask + (i - 1) + (long long)(j - 1) * g.ni);
       if (MODE == kPMW) {
@@ -195,7 +231,7 @@ __global__ void __launch_bounds__(kThreads) k_reduce(const Tr<T>* __restrict__ t
         v[0] += (double)a * mk;
         v[1] += (double)b * mk;
       }
-    }
+        });
   }
   block_sums(v, MODE == kPMW ? 4 : 2, q, part);
 }
@@ -268,15 +304,15 @@ __global__ void __launch_bounds__(kThreads) k_correct(const Tr<T>* __restrict__ 
   double v = 0.0;
   if constexpr (VEC && std::is_same<T, float>::value) {
     if (!skip && r.nx > 0) {
-      const int nx4 = r.nx >> 2;
-      for (long long row = r0; row < r1; row++) {
-        const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
-        const long long e0 = ext(g, r.i0, j, k);
-        const double* mrow = g.mask + (r.i0 - 1) + (long long)(j - 1) * g.ni;
-        for (int c = threadIdx.x; c < nx4; c += kThreads) {
-          const long long e = e0 + 4 * c;
-          double mk[4];
-          mask4(mrow + 4 * c, mk);
+      const int nx4 = r.nx >> 2, n4 = (int)(r1 - r0) * nx4;
+      for (int t = threadIdx.x; t < n4; t += kThreads) {  // the block's (row, 4-cell chunk) pairs
+        const int rr = t / nx4, c = t - rr * nx4;
+        const int row = (int)r0 + rr;
+        const int j = r.j0 + row % r.ny, k = r.k0 + row / r.ny;
+        const long long e = ext(g, r.i0, j, k) + 4 * c;
+        double mk[4];
+        mask4(g.mask + (r.i0 - 1) + (long long)(j - 1) * g.ni + 4 * c, mk);
+        {
           const float4 m4 = ld4(tr.m + e), l4 = ld4(tr.lin + e), am4 = ld4(air_m + e);
           const float4 k4 = tr.weight == 3 ? ld4(tr.pkps + e) : make_float4(0.f, 0.f, 0.f, 0.f);
           const float4 n4 = min_max ? ld4(tr.mn + e) : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -304,10 +340,7 @@ __global__ void __launch_bounds__(kThreads) k_correct(const Tr<T>* __restrict__ 
       }
     }
   } else if (!skip && r.nx > 0) {
-    for (long long row = r0; row < r1; row++)
-#pragma unroll 4
-    for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) {
-      const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
+    for_cells<T>(r, r0, r1, [&](int i, int j, int k) {
       const long long e = ext(g, i, j, k);
       const double corr = lambda * (double)bc_weight<T>(tr, e, sd);
       T nv;
@@ -322,7 +355,7 @@ __global__ void __launch_bounds__(kThreads) k_correct(const Tr<T>* __restrict__ 
       tr.m[e] = nv;
       const T a = nv * air_m[e];
       v += (double)a * __ldg(g.mask + (i - 1) + (long long)(j - 1) * g.ni);
-    }
+        });
   }
   block_sums(&v, 1, q, part);
 }
@@ -342,15 +375,15 @@ __global__ void __launch_bounds__(kThreads) k_scale(const Tr<T>* __restrict__ tr
   double v = 0.0;
   if constexpr (VEC && std::is_same<T, float>::value) {
     if (!skip && r.nx > 0) {
-      const int nx4 = r.nx >> 2;
-      for (long long row = r0; row < r1; row++) {
-        const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
-        const long long e0 = ext(g, r.i0, j, k);
-        const double* mrow = g.mask + (r.i0 - 1) + (long long)(j - 1) * g.ni;
-        for (int c = threadIdx.x; c < nx4; c += kThreads) {
-          const long long e = e0 + 4 * c;
-          double mk[4];
-          mask4(mrow + 4 * c, mk);
+      const int nx4 = r.nx >> 2, n4 = (int)(r1 - r0) * nx4;
+      for (int t = threadIdx.x; t < n4; t += kThreads) {  // the block's (row, 4-cell chunk) pairs
+        const int rr = t / nx4, c = t - rr * nx4;
+        const int row = (int)r0 + rr;
+        const int j = r.j0 + row % r.ny, k = r.k0 + row / r.ny;
+        const long long e = ext(g, r.i0, j, k) + 4 * c;
+        double mk[4];
+        mask4(g.mask + (r.i0 - 1) + (long long)(j - 1) * g.ni + 4 * c, mk);
+        {
           const float4 m4 = ld4(m + e), am4 = ld4(air_m + e);
           float out[4];
 #pragma unroll
@@ -365,16 +398,13 @@ __global__ void __launch_bounds__(kThreads) k_scale(const Tr<T>* __restrict__ tr
       }
     }
   } else if (!skip && r.nx > 0) {
-    for (long long row = r0; row < r1; row++)
-#pragma unroll 4
-    for (int i = r.i0 + threadIdx.x; i < r.i0 + r.nx; i += kThreads) {
-      const int j = r.j0 + (int)(row % r.ny), k = r.k0 + (int)(row / r.ny);
+    for_cells<T>(r, r0, r1, [&](int i, int j, int k) {
       const long long e = ext(g, i, j, k);
       const T nv = (T)(prop * (double)m[e]);
       m[e] = nv;
       const T a = nv * air_m[e];
       v += (double)a * __ldg(g.mask + (i - 1) + (long long)(j - 1) * g.ni);
-    }
+        });
   }
   block_sums(&v, 1, q, part);
 }
