@@ -82,9 +82,10 @@ __device__ __forceinline__ void prepare_cell(const DGrid& g, const typename Type
                                              typename Types<PREC>::F* __restrict__ uvw_d, long long e) {
   using F = typename Types<PREC>::F;
   const long long n = g.nij * g.nk;
-  const int k = (int)(e / g.nij) + 1;
+  // the extended volume is below 2^31 cells (adzc_setup refuses larger tiles)
+  const int k = (int)e / (int)g.nij + 1;
   const long long r = e - (long long)(k - 1) * g.nij;
-  const int jj = (int)(r / g.nit);
+  const int jj = (int)r / g.nit;
   const double cyj = __ldg(g.cy + jj);
   const double* vw = g.vw;
   const int nk = g.nk;
@@ -104,6 +105,63 @@ __device__ __forceinline__ void prepare_cell(const DGrid& g, const typename Type
         __ldg(vw + 2 * (nk + 1) + k) * (double)ww[e] + __ldg(vw + 3 * (nk + 1) + k) * (double)ww[e + g.nij];
   }
   uvw_d[cu + 2 * cs] = (F)w;
+}
+
+// MIXED, component planes: four consecutive cells of a row per thread with
+// 16-byte loads and stores (rows of a multiple of 4 cells, 16-byte aligned
+// arrays; the launcher checks), the arithmetic of prepare_cell
+template <int PREC>
+__global__ void __launch_bounds__(256) k_prepare4(DGrid g, const float* __restrict__ uu, const float* __restrict__ vv,
+                                                  const float* __restrict__ ww, float* __restrict__ uvw_d) {
+  const int nit4 = g.nit >> 2, nk = g.nk;
+  const int n4 = nit4 * g.njt * nk;
+  const int nij = (int)g.nij;
+  const long long n = g.nij * g.nk;
+  const double* vw = g.vw;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += gridDim.x * blockDim.x) {
+    const int row = t / nit4, c = t - row * nit4;
+    const int k = row / g.njt + 1, jj = row - (k - 1) * g.njt;
+    const int e = (k - 1) * nij + jj * g.nit + 4 * c;
+    const double cyj = __ldg(g.cy + jj);
+    const float4 u4 = *reinterpret_cast<const float4*>(uu + e);
+    const float4 v4 = *reinterpret_cast<const float4*>(vv + e);
+    const float u[4] = {u4.x, u4.y, u4.z, u4.w}, v[4] = {v4.x, v4.y, v4.z, v4.w};
+    float ou[4], ov[4], ow[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      ou[q] = (float)(g.inv_rayt * (double)u[q] * cyj);
+      ov[q] = (float)(g.inv_rayt * (double)v[q]);
+    }
+    if (k == 1) {
+      const float4 w4 = *reinterpret_cast<const float4*>(ww + e);
+      const float w[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+      for (int q = 0; q < 4; q++) ow[q] = (float)(g.vw5 * (double)w[q]);
+    } else if (k == nk) {
+      const float4 w4 = *reinterpret_cast<const float4*>(ww + e - nij);
+      const float w[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+      for (int q = 0; q < 4; q++) ow[q] = (float)(g.vw6 * (double)w[q]);
+    } else {
+      const int km2 = imax_(1, k - 2);
+      const double wx = (k >= 3) ? __ldg(vw + 0 * (nk + 1) + k) : 0.0;
+      const double w1 = __ldg(vw + 1 * (nk + 1) + k), w2 = __ldg(vw + 2 * (nk + 1) + k);
+      const double w3 = __ldg(vw + 3 * (nk + 1) + k);
+      const int r = e - (k - 1) * nij;
+      const float4 a4 = *reinterpret_cast<const float4*>(ww + r + (km2 - 1) * nij);
+      const float4 b4 = *reinterpret_cast<const float4*>(ww + e - nij);
+      const float4 c4 = *reinterpret_cast<const float4*>(ww + e);
+      const float4 d4 = *reinterpret_cast<const float4*>(ww + e + nij);
+      const float a[4] = {a4.x, a4.y, a4.z, a4.w}, b[4] = {b4.x, b4.y, b4.z, b4.w};
+      const float cc[4] = {c4.x, c4.y, c4.z, c4.w}, d[4] = {d4.x, d4.y, d4.z, d4.w};
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        ow[q] = (float)(wx * (double)a[q] + w1 * (double)b[q] + w2 * (double)cc[q] + w3 * (double)d[q]);
+    }
+    *reinterpret_cast<float4*>(uvw_d + e) = make_float4(ou[0], ou[1], ou[2], ou[3]);
+    *reinterpret_cast<float4*>(uvw_d + n + e) = make_float4(ov[0], ov[1], ov[2], ov[3]);
+    *reinterpret_cast<float4*>(uvw_d + 2 * n + e) = make_float4(ow[0], ow[1], ow[2], ow[3]);
+  }
 }
 
 template <int PREC>
@@ -900,6 +958,14 @@ cudaError_t launch_prepare(const DGrid& g, const void* uu, const void* vv, const
                            cudaStream_t s) {
   using F = typename Types<PREC>::F;
   const long long n = g.nij * g.nk;
+  if constexpr (WindLayout<PREC>::soa) {
+    auto a16 = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+    if (g.nit % 4 == 0 && a16(uu) && a16(vv) && a16(ww) && a16(uvw_d)) {
+      k_prepare4<PREC><<<grid_for(n / 4, 256), 256, 0, s>>>(g, (const float*)uu, (const float*)vv, (const float*)ww,
+                                                            (float*)uvw_d);
+      return cudaGetLastError();
+    }
+  }
   k_prepare<PREC><<<grid_for(n, 256), 256, 0, s>>>(g, (const F*)uu, (const F*)vv, (const F*)ww, (F*)uvw_d);
   return cudaGetLastError();
 }
