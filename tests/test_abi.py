@@ -64,3 +64,15 @@ def test_errors_without_device(L):
     lev = np.linspace(3000.0, 100.0, 3)
     out = C.c_void_p()
     assert L.adzc_ztab_create(lev.ctypes.data, 3, 10, 10, 0, 0, C.byref(out)) == 3  # nk < 4
+
+
+def test_no_library_no_fallback(monkeypatch, tmp_path):
+    """Without the built library every entry point raises: there is no CPU
+    fallback behind the binding."""
+    from gem_b200 import adz, synth
+    monkeypatch.setattr(adz, "LIB_PATH", str(tmp_path / "missing.so"))
+    monkeypatch.setattr(adz, "_LIB", None)
+    with pytest.raises(FileNotFoundError):
+        adz.lib()
+    with pytest.raises(FileNotFoundError):
+        adz.Adz.from_config(synth.config_small(16, 16, 8))
