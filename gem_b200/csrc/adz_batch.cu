@@ -429,7 +429,7 @@ extern "C" int adzc_batch_tune(adzc_batch* b, void* stream) {
 extern "C" int adzc_batch_query(const adzc_batch* b, int* rows, int* blocks_per_sm, long long* nitems) {
   if (!b) return adz_internal_fail(ADZC_ERR_ARG);
   if (rows) *rows = b->rows;
-  if (blocks_per_sm) *blocks_per_sm = b->phased ? b->pgrid[1] / b->sms : b->bps;
+  if (blocks_per_sm) *blocks_per_sm = b->phased == 2 ? 0 : b->phased ? b->pgrid[1] / b->sms : b->bps;
   if (nitems) *nitems = b->nitems;
   return ADZC_OK;
 }

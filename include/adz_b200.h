@@ -270,8 +270,9 @@ int adzc_batch_create(int prec, int ndom, const adzc_domain *doms, adzc_batch **
 int adzc_batch_tune(adzc_batch *b, void *stream);
 int adzc_batch_step(adzc_batch *b, void *stream);
 /* the plan in use; blocks_per_sm of the one-launch kernel (phased plan: of
- * its trajectory launch); phased: 1 for the phased plan, 2 for the
- * per-domain launches (may be NULL) */
+ * its trajectory launch; 0 for the per-domain launches, which have no
+ * persistent launch); phased: 1 for the phased plan, 2 for the per-domain
+ * launches (may be NULL) */
 int adzc_batch_query(const adzc_batch *b, int *rows_per_item, int *blocks_per_sm, long long *nitems);
 int adzc_batch_plan(const adzc_batch *b, int *phased);
 /* pin a plan instead of tuning: rows per work item, plan 0..2 = register
