@@ -164,7 +164,7 @@ __device__ __forceinline__ void for_cells(const Region& r, long long r0, long lo
 // = tracer.  A point's weight is non-zero for one sign only, and its value is
 // the one bc_weight gives for that sign.
 template <typename T, int MODE, bool VEC>
-__global__ void __launch_bounds__(kThreads) k_reduce(const Tr<T>* __restrict__ trs, Region r, Geo g,
+__global__ void __launch_bounds__(kThreads, VEC ? 3 : 0) k_reduce(const Tr<T>* __restrict__ trs, Region r, Geo g,
                                                      const T* __restrict__ air_p, const T* __restrict__ air_m,
                                                      double* __restrict__ part) {
   const int q = blockIdx.y;
@@ -292,7 +292,7 @@ __global__ void k_finish(const double* __restrict__ part, State* __restrict__ st
 // m - lambda w, clipped to the bound box when min_max (Bermejo_Conde.F90:163-199),
 // and the mass of the corrected field in the same pass
 template <typename T, bool VEC>
-__global__ void __launch_bounds__(kThreads) k_correct(const Tr<T>* __restrict__ trs, const State* __restrict__ st,
+__global__ void __launch_bounds__(kThreads, VEC ? 3 : 0) k_correct(const Tr<T>* __restrict__ trs, const State* __restrict__ st,
                                                       Region r, Geo g, const T* __restrict__ air_m, int min_max,
                                                       double* __restrict__ part) {
   const int q = blockIdx.y;
