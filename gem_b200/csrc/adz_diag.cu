@@ -52,7 +52,9 @@ __global__ void __launch_bounds__(kThreads) k_cfl_part(const double* __restrict_
   double bv[3] = {0.0, 0.0, 0.0};
   long long bt[3] = {-1, -1, -1};
   for (long long t = blockIdx.x * (long long)kThreads + threadIdx.x; t < n; t += (long long)gridDim.x * kThreads) {
-    const int i = i0 + (int)(t % nx), j = j0 + (int)((t / nx) % ny), k = k0 + (int)(t / ((long long)nx * ny));
+    // the tile's volume is below 2^31 cells (adzc_setup refuses larger tiles)
+    const int ti = (int)t, nxy = nx * ny;
+    const int i = i0 + ti % nx, j = j0 + (ti / nx) % ny, k = k0 + ti / nxy;
     const long long e = (long long)(i + 1) + (long long)(j + 1) * wnx + (long long)(k - 1) * plane;
     const double x = fabs(wp[e] - (double)l_i0 + 1.0 - (double)i);
     const double y = fabs(wp[e + comp] - (double)l_j0 + 1.0 - (double)j);
