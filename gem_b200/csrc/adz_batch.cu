@@ -362,6 +362,7 @@ extern "C" int adzc_batch_tune(adzc_batch* b, void* stream) {
   const cudaStream_t s = (cudaStream_t)stream;
   const int rows_c[] = {2, 8, 32};
   float best = 1e30f;
+  for (int q = 0; q < 3; q++) b->tuned_ms[q] = -1.f;  // this tune's timings only
   int br = b->rows, bb = b->bps, bv = b->variant, bp = b->phased;
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
