@@ -17,23 +17,23 @@
 
 // launch bounds of the gather kernels (minimum resident blocks of 128 threads
 // per SM; 0 lets ptxas choose).  A translation unit may set them before
-// including this header.
+// including this header; the _REF32 values apply to the REF32 instantiations
+// (they default to the others).  The bounds expressions name PREC, the
+// precision template parameter of every kernel that uses them.
 #ifndef ADZ_TRAJ_MINB
 #define ADZ_TRAJ_MINB 0
 #endif
 #ifndef ADZ_SET_MINB
 #define ADZ_SET_MINB 0
 #endif
-#if ADZ_TRAJ_MINB > 0
-#define ADZ_TRAJ_BOUNDS __launch_bounds__(128, ADZ_TRAJ_MINB)
-#else
-#define ADZ_TRAJ_BOUNDS __launch_bounds__(128)
+#ifndef ADZ_TRAJ_MINB_REF32
+#define ADZ_TRAJ_MINB_REF32 ADZ_TRAJ_MINB
 #endif
-#if ADZ_SET_MINB > 0
-#define ADZ_SET_BOUNDS __launch_bounds__(128, ADZ_SET_MINB)
-#else
-#define ADZ_SET_BOUNDS __launch_bounds__(128)
+#ifndef ADZ_SET_MINB_REF32
+#define ADZ_SET_MINB_REF32 ADZ_SET_MINB
 #endif
+#define ADZ_TRAJ_BOUNDS __launch_bounds__(128, PREC == kRef32 ? ADZ_TRAJ_MINB_REF32 : ADZ_TRAJ_MINB)
+#define ADZ_SET_BOUNDS __launch_bounds__(128, PREC == kRef32 ? ADZ_SET_MINB_REF32 : ADZ_SET_MINB)
 #ifndef ADZ_QV_MINB
 #define ADZ_QV_MINB 0
 #endif
