@@ -35,10 +35,10 @@ import torch  # noqa: E402
 
 HBM_FALLBACK_GBS = 6650.0
 TENSOR_FALLBACK_TFLOPS = 1590.0
-# DRAM bytes (read + write) per arrival point of each MIXED launch, from the
-# ncu capture of the 384x384x80 case with u, v, w + 4 tracers
-# (profiles/k_traject_k_tricub_parts_mixed_384x384x80.md); traffic grows in
-# proportion to the points, so it scales to the benched tile
+# DRAM bytes (read + write) per arrival point of each MIXED launch, measured
+# by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on a 384x384x80 tile
+# with u, v, w + 4 tracers; traffic grows in proportion to the points, so it
+# scales to the benched tile
 MEASURED_TRAFFIC_PER_POINT = {"traject": 74.25, "sets": 89.77}
 
 

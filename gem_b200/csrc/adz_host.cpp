@@ -1070,6 +1070,13 @@ void adz_internal_after_traject(adzc_handle* h) {
   h->cold = 0;
 }
 
+void adz_internal_forget_positions(adzc_handle* h) {
+  h->last_prec = -1;
+  h->wpxyz = nullptr;
+  h->pxyzm = nullptr;
+  h->zdt0 = nullptr;
+}
+
 adz::DtSplit adz_internal_dt_split(const adzc_grid& g, double dt) { return dt_split(g, dt); }
 
 void adz_internal_set_inputs(const adzc_handle* h, adz::SetArgs* a) {

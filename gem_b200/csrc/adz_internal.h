@@ -11,6 +11,9 @@
 int adz_internal_view(const adzc_handle* h, adz::DGrid* dg, adzc_info* info, adzc_grid* g, int* niter, int* cold);
 // the bookkeeping adzc_traject does after its launches (Adz_niter := Adz_itraj)
 void adz_internal_after_traject(adzc_handle* h);
+// drop the handle's record of its last trajectory: calls that read it
+// (adzc_tricub, adzc_bc_lam_flux) then refuse with ADZC_ERR_ARG
+void adz_internal_forget_positions(adzc_handle* h);
 // 1 when the handle has completed a trajectory and is past its cold start
 int adz_internal_warm(const adzc_handle* h);
 // dt split of adz_traject.F90:38-59

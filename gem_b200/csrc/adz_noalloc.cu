@@ -13,13 +13,18 @@
 //
 // The array's name is a host-side stand-in in host code, not a device
 // address.  Its device address is resolved here with cudaGetSymbolAddress,
-// once per device, with that device current, by the first call made on the
-// device; that first call should therefore come before any stream capture.
+// once per device context, with that device current, by the first call made
+// in the context; that first call should therefore come before any stream
+// capture.  A new primary context (after cudaDeviceReset) reloads the module
+// and moves the array, so the address is resolved again there.
 // All calls share the one array and it keeps the last call's contents, so
 // calls that overlap on the GPU (two streams, two threads, two handles) race.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
+#include <cmath>
 #include <mutex>
 
 #include "../../include/adz_b200.h"
@@ -33,16 +38,46 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[ADZC_NOALLOC_SC
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void* g_addr[kMaxDevices] = {};
+unsigned long long g_ctx_id[kMaxDevices] = {};
 
-// device address of the static array on the current device (set-up once per device)
+// unique id of the calling thread's current context (0: none yet, or not
+// available), through the runtime's entry-point lookup (no link to libcuda)
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = (GetCurrent)p;
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (GetId)p;
+  });
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// device address of the static array in the current device's context: looked
+// up once per context (the array moves when a reset gives the device a new
+// primary context); without a context id it is looked up on every call
 int scratch_address(void** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return ADZC_ERR_CUDA;
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_addr[dev]) {
+  const unsigned long long id = current_context_id();
+  if (!g_addr[dev] || id == 0 || id != g_ctx_id[dev]) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return ADZC_ERR_CUDA;
     g_addr[dev] = p;
+    g_ctx_id[dev] = current_context_id();  // the lookup created the context if there was none
   }
   *out = g_addr[dev];
   return ADZC_OK;
@@ -76,13 +111,15 @@ extern "C" int adzc_step_noalloc(adzc_handle* h, int prec, double dt, int niter,
                                  const void* const* srcs, void* const* dsts, const int* mono, void* stream) {
   AdzRange nvtx_range("ADZ_MAIN");
   if (!h || (prec != ADZC_REF32 && prec != ADZC_FP64 && prec != ADZC_MIXED) || !uu_ext || !vv_ext || !ww_ext ||
-      !ut0 || !vt0 || !zdt0 || !wpxyz || (prec == ADZC_REF32 && !pxyzm) || !nfields)
+      !ut0 || !vt0 || !zdt0 || !wpxyz || (prec == ADZC_REF32 && !pxyzm) || !nfields || !std::isfinite(dt))
     return adz_internal_fail(ADZC_ERR_ARG);
-  int ntot = 0;
+  long long total = 0;
   for (int s = 0; s < 4; s++) {
     if (nfields[s] < 0) return adz_internal_fail(ADZC_ERR_ARG);
-    ntot += nfields[s];
+    total += nfields[s];
   }
+  if (total > INT_MAX / 2) return adz_internal_fail(ADZC_ERR_ARG);
+  const int ntot = (int)total;
   if (ntot > 0 && (!srcs || !dsts)) return adz_internal_fail(ADZC_ERR_ARG);
   for (int f = 0; f < ntot; f++)
     if (!srcs[f] || !dsts[f]) return adz_internal_fail(ADZC_ERR_ARG);
@@ -122,6 +159,11 @@ extern "C" int adzc_step_noalloc(adzc_handle* h, int prec, double dt, int niter,
   a.cold = cold;
   a.k00 = (D.k0 > 1) ? 1 : D.k0m;
   a.dt = adz_internal_dt_split(G, dt);
+  // the positions and departure w of this step live in the caller's wpxyz
+  // and the shared array, not in the handle: follow-on calls that read the
+  // handle's last trajectory (adzc_tricub, adzc_bc_lam_flux) refuse until the
+  // next adzc_traject
+  adz_internal_forget_positions(h);
   if (traject(prec, D, a, s) != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
   adz_internal_after_traject(h);
 

@@ -472,10 +472,17 @@ int adzc_halo_unpack(const adzc_halo *x, int narrays, void *const *arrays, const
  * (3*nit*njt*nk + ni*nj*nk values of the field type, each part rounded up to
  * 256 bytes) are rejected with ADZC_ERR_SIZE before anything runs.
  *
- * Does what adzc_traject followed by adzc_tricub on sets Q, U, V, T does:
- * nfields[4] fields per set; srcs/dsts/mono hold all sets' entries in that
- * order (HOST arrays of DEVICE pointers; mono may be NULL).  The first call
- * on a device resolves the array's device address, so make it before any
+ * Computes what adzc_traject followed by adzc_tricub on sets Q, U, V, T
+ * computes: nfields[4] fields per set; srcs/dsts/mono hold all sets' entries
+ * in that order (HOST arrays of DEVICE pointers; mono may be NULL).  mono
+ * takes 0, 1 or 2 per field: BICUBH_QV fields (ADZC_QV) are not supported
+ * here (ADZC_ERR_ARG).  A non-finite dt is refused (ADZC_ERR_ARG).
+ * The step's positions stay in the caller's wpxyz and its departure vertical
+ * wind in the shared array, so the handle keeps no record of this trajectory:
+ * adzc_tricub and adzc_bc_lam_flux on the same handle return ADZC_ERR_ARG
+ * until the next adzc_traject.  The first call in a device's context resolves
+ * the array's device address (again after cudaDeviceReset, which gives the
+ * device a new context and the array a new address), so make it before any
  * stream capture.  All calls share the array and it keeps the last call's
  * contents: calls that overlap on the GPU race. */
 #define ADZC_NOALLOC_SCRATCH_BYTES (64u << 20)

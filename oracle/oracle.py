@@ -65,7 +65,9 @@ def build(ref: bool | None = None) -> None:
     """Compile the restatement (and the reference objects when the reference
     tree is present)."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    refsrc = "/root/reference/src/gemdyn/src/base/turbo_tricublin.c"
+    # the Makefile's REFDIR (overridable from the environment) names the reference source
+    refsrc = subprocess.run(["make", "-s", "-C", HERE, "refsrc"], check=True, capture_output=True,
+                            text=True).stdout.strip()
     if ref or (ref is None and os.path.exists(refsrc)):
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
 

@@ -91,3 +91,42 @@ def test_noalloc_rejects_tiles_above_capacity():
                                      wp.data_ptr(), nf, None, None, None, torch.cuda.current_stream().cuda_stream)
     assert st == 9  # ADZC_ERR_SIZE, checked before any launch
     assert adz.lib().adzc_error_string(9) == b"size above capacity"
+
+
+def test_noalloc_leaves_no_trajectory_on_the_handle():
+    """The step's positions stay in the caller's wpxyz and its departure
+    vertical wind in the shared array, so the calls that read the handle's
+    last trajectory (adzc_tricub, adzc_bc_lam_flux) refuse after it instead of
+    using an older step's positions; a non-finite dt is refused before any
+    launch, as adzc_traject refuses it."""
+    from gem_b200 import adz as A
+    prec = A.MIXED
+    adz, cfg, inp = _setup(prec)
+    ad = adz.Adz.from_config(cfg)
+    px, wp = ad.new_state(prec)
+    ad.adz_inittraj(prec, px, wp)
+    outs = {k: torch.zeros(ad.ext_shape, device="cuda") for k in ("u", "v", "w")}
+    tro = [torch.zeros(ad.ext_shape, device="cuda") for _ in inp["tracers"]]
+    # a regular trajectory first: without the reset the follow-on calls would use it
+    ad.adz_traject(prec, cfg.dt, inp, px, wp)
+    _noalloc_call(adz, ad, prec, cfg, inp, px, wp, outs, tro)
+    assert ad.status() == 0
+    with pytest.raises(A.AdzError) as e:
+        ad.adz_tricub_hlt(prec, 3, [inp["src_w"]], [outs["w"]])
+    assert e.value.status == 1  # ADZC_ERR_ARG
+    fo = [torch.zeros(ad.ext_shape, device="cuda")]
+    fi = [torch.zeros(ad.ext_shape, device="cuda")]
+    with pytest.raises(A.AdzError) as e:
+        ad.bc_lam_flux(prec, [inp["tracers"][0]], fo, fi)
+    assert e.value.status == 1
+    # the next regular trajectory restores them
+    ad.adz_traject(prec, cfg.dt, inp, px, wp)
+    ad.adz_tricub_hlt(prec, 3, [inp["src_w"]], [outs["w"]])
+    assert ad.status() == 0
+    nf = (C.c_int * 4)(0, 0, 0, 0)
+    for bad in (float("nan"), float("inf")):
+        st = adz.lib().adzc_step_noalloc(
+            ad.h, prec, C.c_double(bad), 0,
+            *(inp[k].data_ptr() for k in ("uu_ext", "vv_ext", "ww_ext", "ut0", "vt0", "zdt0")),
+            None, wp.data_ptr(), nf, None, None, None, torch.cuda.current_stream().cuda_stream)
+        assert st == 1
