@@ -137,7 +137,7 @@ def tile_seed(rank: int) -> int:
 
 
 # ---------------------------------------------------------------------------
-def cpu_reference(size, steps, warmup, threads=0, ntracers=4):
+def cpu_reference(size, steps, warmup, threads=0, ntracers=4, gen_device=None):
     """The reference's CPU path: its interpolator compiled unchanged plus the
     C restatement of the Fortran drivers (OpenMP over k-planes), FP32 fields,
     on a bounded sample of the workload.  Returns points/s and details."""
@@ -145,7 +145,7 @@ def cpu_reference(size, steps, warmup, threads=0, ntracers=4):
     from gem_b200 import synth
     kind = "ref" if O.have_ref() else "oracle"
     cfg = synth.config_large(*size, ntracers=ntracers)
-    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    dev = gen_device or ("cuda" if torch.cuda.is_available() else "cpu")
     inp = synth.make_inputs(cfg, device=dev, dtype=torch.float32)
     np_in = {k: (v.cpu().numpy() if torch.is_tensor(v) else [t.cpu().numpy() for t in v]) for k, v in inp.items()}
     del inp
@@ -364,9 +364,10 @@ def run_product(args):
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        cpu = cpu_reference(args.cpu_size, 2, 1, ntracers=args.ntr)
+        # the benchmarked tile, median of 5 steps after 1 warm-up, all host cores
+        cpu = cpu_reference(args.cpu_size, 5, 1, ntracers=args.ntr)
         # the same path on one core, on a smaller sample (256x256x80)
-        one = cpu_reference((256, 256, args.cpu_size[2]), 2, 1, threads=1, ntracers=args.ntr)
+        one = cpu_reference((256, 256, args.cpu_size[2]), 5, 1, threads=1, ntracers=args.ntr)
         cpu["single_core"] = {k: one[k] for k in ("value", "unit", "cores", "sample", "ms_per_step")}
     value = npts * ws / (ms32 * 1e-3)
     line = {
@@ -374,12 +375,7 @@ def run_product(args):
         "value": value, "unit": "grid-points/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 sums / f64 positions", "data": "synthetic (seeded analytic deformational flow + noise)",
-        "config": {"workload": f"adz step {ni}x{nj}x{nk} LAM tile, u,v,w+{args.ntr} cosine-bell tracers, "
-                               "2 trajectory iterations, dt=60 s, dx=2.5 km, 80 stretched levels",
-                   "points_per_step": npts, "l2": "inputs larger than L2 (no flush)", "parallelism":
-                   (f"{decomp.npx}x{decomp.npy} tiles of one {decomp.gni}x{decomp.gnj} domain, one per GPU; "
-                    "halo exchange (NCCL send/recv) of winds and sources, then of wpxyz, every step")
-                   if ws > 1 else "1 tile"},
+        "config": workload_config(args, ws, decomp),
         "fp64_value": npts * ws / (ms64 * 1e-3), "fp64_ms_per_step": ms64, "speedup_vs_fp64": ms64 / ms32,
         "ref32_value": npts * ws / (ms_ref32 * 1e-3), "ref32_ms_per_step": ms_ref32,
         "per_launch_ms": per,
@@ -397,6 +393,18 @@ def run_product(args):
         print(json.dumps(line))
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def workload_config(args, ws, decomp=None):
+    """The benched workload, shared by the product and the reference arm."""
+    ni, nj, nk = args.size
+    par = "1 tile"
+    if ws > 1 and decomp is not None:
+        par = (f"{decomp.npx}x{decomp.npy} tiles of one {decomp.gni}x{decomp.gnj} domain, one per GPU; "
+               "halo exchange (NCCL send/recv) of winds and sources, then of wpxyz, every step")
+    return {"workload": f"adz step {ni}x{nj}x{nk} LAM tile, u,v,w+{args.ntr} cosine-bell tracers, "
+                        "2 trajectory iterations, dt=60 s, dx=2.5 km, 80 stretched levels",
+            "points_per_step": ni * nj * nk, "l2": "inputs larger than L2 (no flush)", "parallelism": par}
 
 
 # kernels of one MIXED step: departure winds, trajectory, and one
@@ -592,24 +600,33 @@ def measure_batch(args, timed, ws, cfgs, label):
 
 
 def measure_tracers(args, timed, ws, rank):
-    """The multi-tracer workload: the 1024x1024x80 flow with u, v, w and 8
-    log-normal (sigma 1) tracers, mono clipping on; MIXED and the FP64
-    drop-in, one step each as in the headline."""
+    """The mixed-precision workload: the 1024x1024x80 flow with u, v, w and 8
+    log-normal (sigma 1) tracers, mono clipping on the tracers; MIXED and the
+    FP64 drop-in, one step each as in the headline, then the accuracy of the
+    MIXED interpolated fields against the FP64 path on the same FP32 source
+    values (interp_accuracy)."""
     from gem_b200 import adz, synth
     ni, nj, nk = args.size
     cfg = synth.config_mixed(ni, nj, nk, seed=tile_seed(rank), ntracers=8)
     out = {"workload": f"adz step {ni}x{nj}x{nk}, u,v,w + 8 log-normal tracers, mono clipping",
            "points_per_step": cfg.npoints}
+    inp = synth.make_inputs(cfg, device="cuda", dtype=torch.float64)
+    d32 = {k: (v.float() if torch.is_tensor(v) else [t.float() for t in v]) for k, v in inp.items()}
+    del inp
+    state = {}
     for name, prec in (("fp64", adz.FP64), ("mixed", adz.MIXED)):
         dt = adz._field_dtype(prec)
-        data = synth.make_inputs(cfg, device="cuda", dtype=dt)
+        # the FP64 path reads the same FP32 source values, promoted
+        data = d32 if prec == adz.MIXED else {k: (v.double() if torch.is_tensor(v) else [t.double() for t in v])
+                                               for k, v in d32.items()}
         ad = adz.Adz.from_config(cfg)
         px, wp = ad.new_state(prec)
         ad.adz_inittraj(prec, px, wp)
         outs = {k: torch.zeros(ad.ext_shape, dtype=dt, device="cuda") for k in ("u", "v", "w")}
         tro = [torch.zeros(ad.ext_shape, dtype=dt, device="cuda") for _ in data["tracers"]]
 
-        def step():
+        # bound now: the accuracy passes call each precision's step after the loop
+        def step(ad=ad, prec=prec, data=data, px=px, wp=wp, outs=outs, tro=tro):
             adz.step_fused(ad, prec, cfg.dt, data, data, data["tracers"], px, wp, outs, tro, cfg.mono)
         step()  # cold start, untimed
         ms, _ = timed(step, max(3, min(args.steps, 10)), args.warmup)
@@ -617,14 +634,107 @@ def measure_tracers(args, timed, ws, rank):
             raise RuntimeError("device status set during the multi-tracer steps")
         out[name + "_ms_per_step"] = ms
         out[name + "_value"] = cfg.npoints * ws / (ms * 1e-3)
-        del data, outs, tro, step, ad, px, wp
-        torch.cuda.empty_cache()
+        state[name] = (ad, prec, data, px, wp, outs, tro, step)
     out["speedup_vs_fp64"] = out["fp64_ms_per_step"] / out["mixed_ms_per_step"]
     hbm, _ = peaks()
     out["step_roofline"] = {"algorithmic_bytes_per_point": 160.0,
                             "achieved_gbs": 160.0 * cfg.npoints / (out["mixed_ms_per_step"] * 1e-3) / 1e9}
     out["step_roofline"]["frac"] = out["step_roofline"]["achieved_gbs"] / hbm
+    if not args.no_accuracy:
+        out["accuracy"] = interp_accuracy(cfg, state["fp64"], d32)
+        out["accuracy_full_step"] = step_accuracy(state["fp64"], state["mixed"])
+    del state, d32
+    torch.cuda.empty_cache()
     return out
+
+
+def _local_errors(x, r, mn, mx):
+    """Error metrics of one field (device tensors of arrival points, FP64):
+    local = max |x - r| / max(|r|, largest |source| of the point's monotone
+    bound box); norm = max |x - r| / max |r|; rms = RMS error / RMS value;
+    pointwise_floor_1e-3 = max |x - r| / max(|r|, 1e-3 max |r|)."""
+    d = (x - r).abs()
+    ra = r.abs()
+    b = torch.maximum(mn.abs(), mx.abs())
+    top = float(ra.max())
+    return {"local": float((d / torch.maximum(ra, b)).max()), "norm": float(d.max()) / top,
+            "rms": float(d.pow(2).mean().sqrt()) / float(r.pow(2).mean().sqrt()),
+            "pointwise_floor_1e-3": float((d / ra.clamp_min(1e-3 * top)).max())}
+
+
+def interp_accuracy(cfg, ref, d32):
+    """MIXED interpolated fields against the plain FP64 path (bit-exact with
+    the FP64 oracle) on the same FP32 source values at the same FP64
+    departure points: the position sets of one more FP64 step
+    (adzc_interp_traj), interpolated by the device interpolator with explicit
+    positions in both precisions.  That interpolator runs the same per-point
+    arithmetic as the step's set kernels.  Tracers are clipped to their bound
+    box as in the step.  The bar is local <= 1e-6 (see _local_errors)."""
+    from gem_b200 import adz
+    ad, prec, data, px, wp, outs, tro, step = ref
+    step()
+    I = ad.info
+    res = {"reference": "plain FP64 GPU path, same FP32 source values, same FP64 departure points "
+                        "(position sets of one FP64 step)",
+           "definition": "local: max |mixed - fp64| / max(|fp64|, largest |source| of the point's "
+                         "monotone bound box); bar 1e-6",
+           "fields": []}
+    names = ["u", "v", "w"] + [f"tracer{q + 1}" for q in range(len(d32["tracers"]))]
+    sets = [1, 2, 3] + [3] * len(d32["tracers"])
+    srcs32 = [d32["src_u"], d32["src_v"], d32["src_w"]] + list(d32["tracers"])
+    off = I.haloy * I.nit + I.halox
+    for s_id in (1, 2, 3):
+        pos = ad.adz_interp_traj(prec, s_id)
+        lev = (cfg.levels.zt if s_id == 3 else cfg.levels.zm)[1:cfg.nk + 1]
+        zt = adz.Ztab(lev, I.nit, I.njt, 1 - ad.grid.i0g, 1 - ad.grid.j0g)
+        for name, st, src in zip(names, sets, srcs32):
+            if st != s_id:
+                continue
+            f32 = src.reshape(-1)[off:]
+            f64 = src.double().reshape(-1)[off:]
+            r, _, rmn, rmx = (o[0] for o in adz.tricublin_mono_m_n(zt, adz.FP64, [f64], pos))
+            x, _, xmn, xmx = (o[0].double() for o in adz.tricublin_mono_m_n(zt, adz.MIXED, [f32], pos))
+            if name.startswith("tracer"):
+                r = torch.maximum(rmn, torch.minimum(rmx, r))
+                x = torch.maximum(xmn, torch.minimum(xmx, x))
+            e = _local_errors(x, r, rmn, rmx)
+            e["field"] = name
+            e["clipped"] = name.startswith("tracer")
+            res["fields"].append(e)
+            del f64, r, rmn, rmx, x, xmn, xmx
+        del pos, zt
+        torch.cuda.empty_cache()
+    res["max_local_all_fields"] = max(f["local"] for f in res["fields"])
+    res["max_norm_all_fields"] = max(f["norm"] for f in res["fields"])
+    return res
+
+
+def step_accuracy(ref, mix):
+    """Whole MIXED step (its own FP32-interpolated trajectory) against the
+    FP64 step, both from the same start positions.  The departure points
+    then differ by the trajectory's sensitivity to the winds' FP32
+    interpolation, so this measures the step, not the interpolation alone."""
+    ad64, p64, _, _, wp64, o64, t64, step64 = ref
+    ad32, p32, _, _, wp32, o32, t32, step32 = mix
+    start = wp64.clone()
+    step64()
+    wp32.copy_(start)
+    step32()
+    res = {"fields": []}
+    names = ["u", "v", "w"] + [f"tracer{q + 1}" for q in range(len(t64))]
+    sets = [1, 2, 3] + [3] * len(t64)
+    for name, st, a, b in zip(names, sets, [o32["u"], o32["v"], o32["w"]] + t32, [o64["u"], o64["v"], o64["w"]] + t64):
+        m = ad64.range_mask(st, device="cuda")
+        x, y = a[m].double(), b[m]
+        d = (x - y).abs()
+        res["fields"].append({"field": name, "norm": float(d.max()) / float(y.abs().max()),
+                              "rms": float(d.pow(2).mean().sqrt()) / float(y.pow(2).mean().sqrt())})
+        del m, x, y, d
+    w32, w64 = wp32[:, :, 2:-2, 2:-2], wp64[:, :, 2:-2, 2:-2]
+    res["cell_index_mismatches"] = int((w32.float().trunc() != w64.float().trunc()).sum())
+    res["positions"] = int(w32.numel())
+    res["max_position_diff_grid"] = float((w32 - w64).abs().max())
+    return res
 
 
 def measure_post(args, timed, ws, rank):
@@ -764,13 +874,14 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    r = cpu_reference(args.cpu_size, args.steps, args.warmup, ntracers=args.ntr)
+    # inputs made on the host: nothing of this package runs on the GPU in this arm
+    r = cpu_reference(args.cpu_size, args.steps, args.warmup, ntracers=args.ntr, gen_device="cpu")
     line = {"impl": "reference",
             "metric": "SL advection grid-points/s at 1024^2x80 (mixed-precision step; plain FP64 GPU drop-in alongside)",
             "value": r["value"], "unit": "grid-points/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 fields / f64 coefficients (reference precision)", "data": "synthetic",
-            "config": {"workload": f"adz step, bounded sample {r['sample']}"},
+            "config": workload_config(args, 1),
             "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": r["value"], "unit": "grid-points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -783,7 +894,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--size", type=lambda s: tuple(int(x) for x in s.split(",")), default=(1024, 1024, 80))
-    ap.add_argument("--cpu-size", type=lambda s: tuple(int(x) for x in s.split(",")), default=(512, 512, 80))
+    ap.add_argument("--cpu-size", type=lambda s: tuple(int(x) for x in s.split(",")), default=None,
+                    help="tile of the CPU reference (default: --size, the benchmarked tile)")
     ap.add_argument("--ntr", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -791,11 +903,14 @@ def main():
     ap.add_argument("--batch-domains", type=int, default=16)
     ap.add_argument("--no-guess", action="store_true", help="skip the learned-guess cold-start measurement")
     ap.add_argument("--no-tracers", action="store_true", help="skip the 8-tracer mono measurement")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the accuracy passes of the 8-tracer leg")
     ap.add_argument("--no-post", action="store_true", help="skip the QV / mass-fixer / ILMC / CFL measurement")
     ap.add_argument("--guess-weights", default=os.path.join(ROOT, "gem_b200", "data", "guess_mlp.npz"))
     ap.add_argument("--only", choices=["mixed"], default=None,
                     help="run the mixed-precision path alone (small profiling runs)")
     args = ap.parse_args()
+    if args.cpu_size is None:
+        args.cpu_size = args.size
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -98,6 +98,7 @@ def lib() -> C.CDLL:
         L.adzc_tricublin_mono_m_n.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, i, i, i, vp]
         L.adzc_tricublin_zyx3_n.argtypes = [vp, i, vp, vp, vp, i, vp]
         L.adzc_tricub_sets.argtypes = [vp, i, vp, vp, vp, vp, vp]
+        L.adzc_interp_traj.argtypes = [vp, i, i, vp, vp]
         L.adzc_step_noalloc.argtypes = [vp, i, d, i] + [vp] * 8 + [vp, vp, vp, vp, vp]
         L.adzc_batch_create.argtypes = [i, i, vp, C.POINTER(vp)]
         L.adzc_batch_tune.argtypes = [vp, vp]
@@ -329,6 +330,18 @@ class Adz:
         _check(lib().adzc_tricub(self.h, prec, set_id, n, C.cast(_ptr_array(srcs), C.c_void_p),
                                  C.cast(_ptr_array(dsts), C.c_void_p), mono_arr, lin, mn, mx, _stream(stream)),
                "adzc_tricub")
+
+    def adz_interp_traj(self, prec: int, set_id: int, stream=None):
+        """Positions of set set_id of the last trajectory as adz_interp_traj
+        stores them: an (n, 3) device tensor, float32 in REF32, float64
+        otherwise, arrival points in (k, j, i) order with i fastest."""
+        I = self.info
+        i0, i1, j0, j1, k0 = {0: (I.i0, I.in_, I.j0, I.jn, I.k0), 1: (I.i0u, I.inu, I.j0, I.jn, I.k0),
+                              2: (I.i0, I.in_, I.j0v, I.jnv, I.k0), 3: (I.i0, I.in_, I.j0, I.jn, I.k0t)}[set_id]
+        n = max(0, i1 - i0 + 1) * max(0, j1 - j0 + 1) * max(0, self.grid.nk - k0 + 1)
+        pos = torch.empty((n, 3), dtype=torch.float32 if prec == REF32 else torch.float64, device="cuda")
+        _check(lib().adzc_interp_traj(self.h, prec, set_id, pos.data_ptr(), _stream(stream)), "adzc_interp_traj")
+        return pos
 
     def adz_tricub_sets(self, prec: int, nfields, srcs, dsts, mono=None, stream=None):
         """All position sets in one call: nfields = [nQ, nU, nV, nT]."""

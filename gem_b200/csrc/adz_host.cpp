@@ -735,6 +735,24 @@ extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const
   return ADZC_OK;
 }
 
+extern "C" int adzc_interp_traj(adzc_handle* h, int prec, int set, void* pos, void* stream) {
+  AdzRange nvtx_range("adz_interp_traj");
+  if (!h || !check_prec(prec) || set < 0 || set > 3 || !pos) return fail(ADZC_ERR_ARG);
+  if (h->last_prec != prec || !h->wpxyz) return fail(ADZC_ERR_ARG);
+  int i0, nx, j0, ny, k0, nz;
+  set_box(h, set, i0, nx, j0, ny, k0, nz);
+  if (nx <= 0 || ny <= 0 || nz <= 0) return ADZC_OK;
+  const adz::SetArgs a = set_args(h);
+  const adz::DGrid& D = h->dg;
+  const cudaStream_t s = (cudaStream_t)stream;
+  switch (prec) {
+    case ADZC_REF32: ADZ_CK(adz::launch_positions<adz::kRef32>(D, set, i0, nx, j0, ny, k0, nz, a, pos, s)); break;
+    case ADZC_FP64: ADZ_CK(adz::launch_positions<adz::kFp64>(D, set, i0, nx, j0, ny, k0, nz, a, pos, s)); break;
+    default: ADZ_CK(adz::launch_positions<adz::kMixed>(D, set, i0, nx, j0, ny, k0, nz, a, pos, s)); break;
+  }
+  return ADZC_OK;
+}
+
 extern "C" int adzc_bc_lam_flux(adzc_handle* h, int prec, int ntr, const void* const* srcs, void* const* fo,
                                 void* const* fi, void* stream) {
   AdzRange nvtx_range("adz_BC_LAM_Aranami_hlt");

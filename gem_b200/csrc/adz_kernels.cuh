@@ -629,6 +629,34 @@ __device__ __forceinline__ void set_point(const DGrid& g, int set, const SetArgs
   }
 }
 
+// the positions of a set as adz_interp_traj stores them (Adz_pm, Adz_pmu,
+// Adz_pmv, Adz_pt: (3, nx, ny, nz), i fastest): FP32 (the reference's real
+// arrays, the FP64 value rounded to nearest) in REF32, FP64 otherwise
+template <int PREC>
+__global__ void __launch_bounds__(256) k_positions(DGrid g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
+                                                   SetArgs a, void* __restrict__ pos) {
+  const long long nplane = (long long)nx * ny;
+  const long long n = nplane * nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nx) + i0;
+    const int j = (int)((t / nx) % ny) + j0;
+    const int k = (int)(t / nplane) + k0;
+    double px, py, pz;
+    set_position<PREC, false>(g, a, set, i, j, k, px, py, pz);
+    if (PREC == kRef32) {
+      float* o = (float*)pos + 3 * t;
+      o[0] = (float)px;
+      o[1] = (float)py;
+      o[2] = (float)pz;
+    } else {
+      double* o = (double*)pos + 3 * t;
+      o[0] = px;
+      o[1] = py;
+      o[2] = pz;
+    }
+  }
+}
+
 template <int PREC, bool PERT>
 __global__ void ADZ_SET_BOUNDS k_tricub_set(DGrid g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
                                             SetArgs a, FieldPtrs fp) {
@@ -1003,6 +1031,15 @@ cudaError_t launch_tricub_set(const DGrid& g, int set, int i0, int nx, int j0, i
 }
 
 template <int PREC>
+cudaError_t launch_positions(const DGrid& g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
+                             const SetArgs& a, void* pos, cudaStream_t s) {
+  const long long n = (long long)nx * ny * nz;
+  if (n <= 0) return cudaSuccess;
+  k_positions<PREC><<<grid_for(n, 256, 1 << 30), 256, 0, s>>>(g, set, i0, nx, j0, ny, k0, nz, a, pos);
+  return cudaGetLastError();
+}
+
+template <int PREC>
 cudaError_t launch_tricub_parts(const DGrid& g, const SetArgs& a, const SetParts& sp, cudaStream_t s) {
   if (sp.n < 1 || sp.n > kMaxParts) return cudaErrorInvalidValue;
   long long most = 0;  // blocks of the largest part
@@ -1116,6 +1153,8 @@ int batch_resident_blocks(int variant) {
   template cudaError_t launch_tricub_set<P>(const DGrid&, int, int, int, int, int, int, int, const SetArgs&,       \
                                             const FieldPtrs&, cudaStream_t);                                       \
   template cudaError_t launch_interp_pos<P>(const DZtab&, int, int, const void*, const FieldPtrs&, cudaStream_t); \
+  template cudaError_t launch_positions<P>(const DGrid&, int, int, int, int, int, int, int, const SetArgs&, void*, \
+                                           cudaStream_t);                                                         \
   template cudaError_t launch_tricub_parts<P>(const DGrid&, const SetArgs&, const SetParts&, cudaStream_t);       \
   template cudaError_t launch_qv_set<P>(const DGrid&, int, int, int, int, int, int, const SetArgs&,               \
                                         const FieldPtrs&, cudaStream_t);                                          \

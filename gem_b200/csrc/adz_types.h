@@ -128,6 +128,9 @@ template <int PREC>
 cudaError_t launch_prepare(const DGrid& g, const void* uu, const void* vv, const void* ww, void* uvw_d,
                            cudaStream_t s);
 template <int PREC>
+cudaError_t launch_positions(const DGrid& g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
+                             const SetArgs& a, void* pos, cudaStream_t s);
+template <int PREC>
 cudaError_t launch_inittraj(const DGrid& g, float* pxyzm, double* wpxyz, cudaStream_t s);
 template <int PREC>
 cudaError_t launch_traject(const DGrid& g, const TrajArgs& a, cudaStream_t s);

@@ -194,6 +194,16 @@ int adzc_traject(adzc_handle *h, int prec, double dt, int niter, const void *uu_
 int adzc_tricub(adzc_handle *h, int prec, int set, int nfields, const void *const *srcs, void *const *dsts,
                 const int *mono, void *const *lin, void *const *mn, void *const *mx, void *stream);
 
+/* adz_interp_traj's position arrays (B/adz_interp_traj.F90:45-187): the
+ * departure points of one position set of the last trajectory, as Adz_pm,
+ * Adz_pmu, Adz_pmv or Adz_pt hold them: pos is a DEVICE array (3, nx, ny, nz)
+ * over the set's arrival range (i fastest, levels from the set's k0), FP32
+ * in REF32 (the reference's real arrays) and FP64 in ADZC_FP64 and
+ * ADZC_MIXED.  adzc_tricub derives the same positions in registers and never
+ * stores them; this call is for callers that read them (diagnostics, other
+ * interpolators, tests). */
+int adzc_interp_traj(adzc_handle *h, int prec, int set, void *pos, void *stream);
+
 /* Adz_uslt, Adz_vslt: DEVICE arrays (ni, nj) of the field type holding the
  * surface-layer winds.  When the grid sets slt_winds, the top-level points
  * of set T (k = nk) take their horizontal positions from them
