@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libadz_b200.so")
 
 REF32, FP64, MIXED = 0, 1, 2
-SET_Q, SET_U, SET_V, SET_T = 0, 1, 2, 3
+SET_Q, SET_U, SET_V, SET_T, SET_B = 0, 1, 2, 3, 4
 QV = 4  # mono flag bit: BICUBH_QV interpolation of that field (set T)
 PREC_NAMES = {"ref32": REF32, "fp64": FP64, "mixed": MIXED}
 
@@ -40,7 +40,8 @@ class AdzError(RuntimeError):
 class AdzcGrid(C.Structure):
     _fields_ = [(n, C.c_int) for n in (
         "ni", "nj", "nk", "maxcfl", "i0g", "j0g", "west", "east", "south", "north",
-        "pil_w", "pil_e", "pil_s", "pil_n", "lam_gbpil_t", "bc_lam_flux", "schm_advec", "itraj", "slt_winds")] + [
+        "pil_w", "pil_e", "pil_s", "pil_n", "lam_gbpil_t", "bc_lam_flux", "schm_advec", "itraj", "slt_winds",
+        "schm_autobar")] + [
         ("bA_m", C.c_double), ("bA", C.c_double), ("inv_rayt", C.c_double), ("inv_hx", C.c_double),
         ("inv_hy", C.c_double), ("cy", C.POINTER(C.c_double)), ("zm", C.POINTER(C.c_double)),
         ("zt", C.POINTER(C.c_double)), ("zx", C.POINTER(C.c_double)), ("zmin", C.c_double), ("zmax", C.c_double),
@@ -99,6 +100,7 @@ def lib() -> C.CDLL:
         L.adzc_tricublin_zyx3_n.argtypes = [vp, i, vp, vp, vp, i, vp]
         L.adzc_tricub_sets.argtypes = [vp, i, vp, vp, vp, vp, vp]
         L.adzc_interp_traj.argtypes = [vp, i, i, vp, vp]
+        L.adzc_bc_lam_zlf.argtypes = [vp, i, i, i, vp, vp, vp]
         L.adzc_step_noalloc.argtypes = [vp, i, d, i] + [vp] * 8 + [vp, vp, vp, vp, vp]
         L.adzc_batch_create.argtypes = [i, i, vp, C.POINTER(vp)]
         L.adzc_batch_tune.argtypes = [vp, vp]
@@ -229,12 +231,13 @@ class Adz:
 
     @classmethod
     def from_config(cls, cfg, lam=True, i0g=None, j0g=None, schm_advec=1, edges=None, slt_winds=False,
-                    lam_gbpil_t=0):
+                    lam_gbpil_t=0, bc_lam_flux=1, schm_autobar=False):
         """adz_set for a synthetic LAM tile (gem_b200.synth.Config).  The
         tile starts at global (i0g, j0g) (default: the config's tile origin)
         and touches the LAM edges flagged in ``edges`` = (west, east, south,
         north) (default: all of them when ``lam``); pilot zones lie on those
-        edges only."""
+        edges only.  bc_lam_flux: Adz_BC_LAM_flux (1 Aranami, 2 ZLF);
+        schm_autobar: Schm_autobar_L."""
         from . import synth
         ga = synth.grid_arrays(cfg)
         keep = {k: np.ascontiguousarray(ga[k], dtype=np.float64) for k in ("cy", "zm", "zt", "zx")}
@@ -246,8 +249,8 @@ class Adz:
         P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
         g = AdzcGrid(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk, maxcfl=cfg.maxcfl, i0g=i0g, j0g=j0g,
                      west=w, east=ea, south=so, north=no, pil_w=p * w, pil_e=p * ea, pil_s=p * so, pil_n=p * no,
-                     lam_gbpil_t=lam_gbpil_t, bc_lam_flux=1, schm_advec=schm_advec, itraj=cfg.niter,
-                     slt_winds=1 if slt_winds else 0,
+                     lam_gbpil_t=lam_gbpil_t, bc_lam_flux=bc_lam_flux, schm_advec=schm_advec, itraj=cfg.niter,
+                     slt_winds=1 if slt_winds else 0, schm_autobar=1 if schm_autobar else 0,
                      bA_m=0.6, bA=0.6, inv_rayt=ga["inv_rayt"], inv_hx=ga["inv_hx"], inv_hy=ga["inv_hy"],
                      cy=P(keep["cy"]), zm=P(keep["zm"]), zt=P(keep["zt"]), zx=P(keep["zx"]),
                      zmin=ga["zmin"], zmax=ga["zmax"], wmstar_nk=ga["wmstar_nk"], idz_t_nkm1=ga["idz_t_nkm1"])
@@ -273,7 +276,8 @@ class Adz:
     def set_range(self, s: int):
         I = self.info
         return {SET_Q: (I.i0, I.in_, I.j0, I.jn, I.k0), SET_U: (I.i0u, I.inu, I.j0, I.jn, I.k0),
-                SET_V: (I.i0, I.in_, I.j0v, I.jnv, I.k0), SET_T: (I.i0, I.in_, I.j0, I.jn, I.k0t)}[s]
+                SET_V: (I.i0, I.in_, I.j0v, I.jnv, I.k0), SET_T: (I.i0, I.in_, I.j0, I.jn, I.k0t),
+                SET_B: (I.i0b, I.inb, I.j0b, I.jnb, 1)}[s]
 
     def range_mask(self, s: int, device="cpu"):
         """Boolean mask (ext layout) of the arrival points of set s."""
@@ -310,6 +314,13 @@ class Adz:
                                       C.cast(_ptr_array(fo), C.c_void_p), C.cast(_ptr_array(fi), C.c_void_p),
                                       _stream(stream)), "adzc_bc_lam_flux")
 
+    def bc_lam_zlf(self, prec: int, setup: int, f1, f2=None, stream=None):
+        """adz_BC_LAM_zlf_hlt setup 1-4 (Zerroukat-Shipway LAM treatment) on
+        the ext tensors f1 (and f2 for setups 2 and 4), in place."""
+        _check(lib().adzc_bc_lam_zlf(self.h, prec, int(setup), len(f1), C.cast(_ptr_array(f1), C.c_void_p),
+                                     None if f2 is None else C.cast(_ptr_array(f2), C.c_void_p), _stream(stream)),
+               "adzc_bc_lam_zlf")
+
     def set_rhs_perturbation(self, mcrhsint=None):
         """mcrhsint (nj, ni) device tensor of the field type: every later
         interpolation writes value + mcrhsint * |value - lin|; None clears."""
@@ -335,9 +346,7 @@ class Adz:
         """Positions of set set_id of the last trajectory as adz_interp_traj
         stores them: an (n, 3) device tensor, float32 in REF32, float64
         otherwise, arrival points in (k, j, i) order with i fastest."""
-        I = self.info
-        i0, i1, j0, j1, k0 = {0: (I.i0, I.in_, I.j0, I.jn, I.k0), 1: (I.i0u, I.inu, I.j0, I.jn, I.k0),
-                              2: (I.i0, I.in_, I.j0v, I.jnv, I.k0), 3: (I.i0, I.in_, I.j0, I.jn, I.k0t)}[set_id]
+        i0, i1, j0, j1, k0 = self.set_range(set_id)
         n = max(0, i1 - i0 + 1) * max(0, j1 - j0 + 1) * max(0, self.grid.nk - k0 + 1)
         pos = torch.empty((n, 3), dtype=torch.float32 if prec == REF32 else torch.float64, device="cuda")
         _check(lib().adzc_interp_traj(self.h, prec, set_id, pos.data_ptr(), _stream(stream)), "adzc_interp_traj")

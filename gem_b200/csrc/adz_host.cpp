@@ -353,7 +353,8 @@ static double lag3(double zz, double z1, double z2, double z3, double z4) {  // 
 extern "C" int adzc_setup(const adzc_grid* gin, adzc_handle** out) {
   if (!gin || !out || !gin->zm || !gin->zt || !gin->zx || !gin->cy) return fail(ADZC_ERR_ARG);
   const adzc_grid& g = *gin;
-  if (g.ni < 1 || g.nj < 1) return fail(ADZC_ERR_ARG);
+  if (g.ni < 1 || g.nj < 1 || g.bc_lam_flux < 0 || g.bc_lam_flux > 2 || g.schm_autobar < 0 || g.schm_autobar > 1)
+    return fail(ADZC_ERR_ARG);
   if (g.nk < 4) return fail(ADZC_ERR_NK);
   {  // stencil offsets inside the extended array are 32-bit in the kernels
     const long long hx = std::max(1, g.maxcfl) + 1;
@@ -531,6 +532,7 @@ extern "C" int adzc_setup(const adzc_grid* gin, adzc_handle** out) {
   D.k0 = I.k0; D.k0t = I.k0t; D.k0m = I.k0m;
   D.pnz_m = I.pnz_m; D.pnz_t = I.pnz_t;
   D.slt_winds = g.slt_winds;
+  D.autobar = g.schm_autobar;
   D.imnx = I.iminposx; D.imxx = I.imaxposx; D.imny = I.iminposy; D.imxy = I.imaxposy;
   D.sig = h->sig; D.ovdzm = h->ovdzm; D.ovdzt = h->ovdzt;
   D.zmin = g.zmin; D.zmax = g.zmax;
@@ -636,7 +638,8 @@ extern "C" int adzc_traject(adzc_handle* h, int prec, double dt, int niter, cons
 
 namespace {
 
-// arrival points of a position set (B/adz_set.F90:94-114)
+// arrival points of a position set (B/adz_set.F90:94-114, 167-172); set B is
+// range b, all levels, at the t-set positions (Adz_pb)
 void set_box(const adzc_handle* h, int set, int& i0, int& nx, int& j0, int& ny, int& k0, int& nz) {
   const adzc_info& I = h->info;
   int i1, j1;
@@ -644,6 +647,7 @@ void set_box(const adzc_handle* h, int set, int& i0, int& nx, int& j0, int& ny, 
     case ADZC_SET_Q: i0 = I.i0; i1 = I.in; j0 = I.j0; j1 = I.jn; k0 = I.k0; break;
     case ADZC_SET_U: i0 = I.i0u; i1 = I.inu; j0 = I.j0; j1 = I.jn; k0 = I.k0; break;
     case ADZC_SET_V: i0 = I.i0; i1 = I.in; j0 = I.j0v; j1 = I.jnv; k0 = I.k0; break;
+    case ADZC_SET_B: i0 = I.i0b; i1 = I.inb; j0 = I.j0b; j1 = I.jnb; k0 = 1; break;
     default: i0 = I.i0; i1 = I.in; j0 = I.j0; j1 = I.jn; k0 = I.k0t; break;
   }
   nx = i1 - i0 + 1;
@@ -668,11 +672,14 @@ adz::SetArgs set_args(const adzc_handle* h) {
   return a;
 }
 
-// a mono flag of adzc_tricub: 0..2, | ADZC_QV on set T only
+// a mono flag of adzc_tricub: 0..2, | ADZC_QV on the thermo sets T and B only
 bool mono_ok(int mv, int set) {
   if ((mv & ~(3 | ADZC_QV)) != 0 || (mv & 3) == 3) return false;
-  return !((mv & ADZC_QV) && set != ADZC_SET_T);
+  return !((mv & ADZC_QV) && set != ADZC_SET_T && set != ADZC_SET_B);
 }
+
+// the position set a kernel derives: set B is range b of the t set
+int kernel_set(int set) { return set == ADZC_SET_B ? ADZC_SET_T : set; }
 
 }  // namespace
 
@@ -693,9 +700,10 @@ extern "C" int adzc_rhs_perturbation(adzc_handle* h, const void* mcrhsint, int l
 extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const void* const* srcs, void* const* dsts,
                            const int* mono, void* const* lin, void* const* mn, void* const* mx, void* stream) {
   AdzRange nvtx_range("adz_tricub_hlt");
-  if (!h || !check_prec(prec) || set < 0 || set > 3 || nfields < 0 || (nfields > 0 && (!srcs || !dsts)))
+  if (!h || !check_prec(prec) || set < 0 || set > ADZC_SET_B || nfields < 0 || (nfields > 0 && (!srcs || !dsts)))
     return fail(ADZC_ERR_ARG);
   if (h->last_prec != prec || !h->wpxyz) return fail(ADZC_ERR_ARG);
+  if (set == ADZC_SET_B && h->g.bc_lam_flux == 0) return fail(ADZC_ERR_ARG);  // range b needs k00 = 1
   const adz::DGrid& D = h->dg;
   int i0, nx, j0, ny, k0, nz;
   set_box(h, set, i0, nx, j0, ny, k0, nz);
@@ -726,7 +734,7 @@ extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const
         fp.mx[q] = mx ? mx[f] : nullptr;
       }
       if (kind == 0) {
-        ADZ_CK(dispatch_set(prec, D, set, i0, nx, j0, ny, k0, nz, a, fp, (cudaStream_t)stream));
+        ADZ_CK(dispatch_set(prec, D, kernel_set(set), i0, nx, j0, ny, k0, nz, a, fp, (cudaStream_t)stream));
       } else {
         ADZ_CK(dispatch_qv(prec, D, i0, nx, j0, ny, k0, nz, a, fp, (cudaStream_t)stream));
       }
@@ -737,18 +745,20 @@ extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const
 
 extern "C" int adzc_interp_traj(adzc_handle* h, int prec, int set, void* pos, void* stream) {
   AdzRange nvtx_range("adz_interp_traj");
-  if (!h || !check_prec(prec) || set < 0 || set > 3 || !pos) return fail(ADZC_ERR_ARG);
+  if (!h || !check_prec(prec) || set < 0 || set > ADZC_SET_B || !pos) return fail(ADZC_ERR_ARG);
   if (h->last_prec != prec || !h->wpxyz) return fail(ADZC_ERR_ARG);
+  if (set == ADZC_SET_B && h->g.bc_lam_flux == 0) return fail(ADZC_ERR_ARG);  // range b needs k00 = 1
   int i0, nx, j0, ny, k0, nz;
   set_box(h, set, i0, nx, j0, ny, k0, nz);
   if (nx <= 0 || ny <= 0 || nz <= 0) return ADZC_OK;
   const adz::SetArgs a = set_args(h);
   const adz::DGrid& D = h->dg;
   const cudaStream_t s = (cudaStream_t)stream;
+  const int ks = kernel_set(set);
   switch (prec) {
-    case ADZC_REF32: ADZ_CK(adz::launch_positions<adz::kRef32>(D, set, i0, nx, j0, ny, k0, nz, a, pos, s)); break;
-    case ADZC_FP64: ADZ_CK(adz::launch_positions<adz::kFp64>(D, set, i0, nx, j0, ny, k0, nz, a, pos, s)); break;
-    default: ADZ_CK(adz::launch_positions<adz::kMixed>(D, set, i0, nx, j0, ny, k0, nz, a, pos, s)); break;
+    case ADZC_REF32: ADZ_CK(adz::launch_positions<adz::kRef32>(D, ks, i0, nx, j0, ny, k0, nz, a, pos, s)); break;
+    case ADZC_FP64: ADZ_CK(adz::launch_positions<adz::kFp64>(D, ks, i0, nx, j0, ny, k0, nz, a, pos, s)); break;
+    default: ADZ_CK(adz::launch_positions<adz::kMixed>(D, ks, i0, nx, j0, ny, k0, nz, a, pos, s)); break;
   }
   return ADZC_OK;
 }
@@ -758,7 +768,7 @@ extern "C" int adzc_bc_lam_flux(adzc_handle* h, int prec, int ntr, const void* c
   AdzRange nvtx_range("adz_BC_LAM_Aranami_hlt");
   if (!h || !check_prec(prec) || ntr < 0 || (ntr > 0 && (!srcs || !fo || !fi))) return fail(ADZC_ERR_ARG);
   if (h->last_prec != prec || !h->wpxyz) return fail(ADZC_ERR_ARG);
-  if (h->g.bc_lam_flux == 0) return fail(ADZC_ERR_ARG);  // the range b positions need k00 = 1
+  if (h->g.bc_lam_flux != 1) return fail(ADZC_ERR_ARG);  // Aranami fluxes (adz_BC_LAM_flux 1) only
   if (!srcs) return fail(ADZC_ERR_ARG);
   for (int q = 0; q < ntr; q++)  // srcs[q] NULL: the masks alone (PSADJ)
     if (!fo[q] || !fi[q]) return fail(ADZC_ERR_ARG);
@@ -766,7 +776,7 @@ extern "C" int adzc_bc_lam_flux(adzc_handle* h, int prec, int ntr, const void* c
   const adzc_info& I = h->info;
   const adz::DGrid& D = h->dg;
   adz::BcMask m{D.lminx, D.lminy, D.nit, D.njt, D.nk, D.ni, D.nj, h->g.west, h->g.east, h->g.south, h->g.north,
-                h->g.pil_w, h->g.pil_e, h->g.pil_s, h->g.pil_n, I.k0t, I.i0b, I.inb, I.j0b, I.jnb};
+                h->g.pil_w, h->g.pil_e, h->g.pil_s, h->g.pil_n, I.k0t, I.i0b, I.inb, I.j0b, I.jnb, h->g.maxcfl + 1};
   const int nxb = I.inb - I.i0b + 1, nyb = I.jnb - I.j0b + 1;
   if (nxb <= 0 || nyb <= 0) return ADZC_OK;
   const size_t fb = prec == ADZC_FP64 ? sizeof(double) : sizeof(float);
@@ -796,6 +806,33 @@ extern "C" int adzc_bc_lam_flux(adzc_handle* h, int prec, int ntr, const void* c
     for (int q = 0; q < nf; q++)
       ADZ_CK(prec == ADZC_FP64 ? adz::launch_bc_zero<double>(m, fo[q0 + q], fi[q0 + q], s)
                                : adz::launch_bc_zero<float>(m, fo[q0 + q], fi[q0 + q], s));
+  }
+  return ADZC_OK;
+}
+
+extern "C" int adzc_bc_lam_zlf(adzc_handle* h, int prec, int setup, int ntr, void* const* f1, void* const* f2,
+                               void* stream) {
+  AdzRange nvtx_range("ZLF_0");
+  if (!h || !check_prec(prec) || setup < 1 || setup > 4 || ntr < 0 || (ntr > 0 && !f1)) return fail(ADZC_ERR_ARG);
+  if (h->g.bc_lam_flux != 2) return fail(ADZC_ERR_ARG);  // Adz_BC_LAM_flux 2: Zerroukat-Shipway
+  const bool two = setup == 2 || setup == 4;
+  if (ntr > 0 && two && !f2) return fail(ADZC_ERR_ARG);
+  for (int q = 0; q < ntr; q++)
+    if (!f1[q] || (two && !f2[q])) return fail(ADZC_ERR_ARG);
+  const adzc_info& I = h->info;
+  const adz::DGrid& D = h->dg;
+  const adz::BcMask m{D.lminx, D.lminy, D.nit, D.njt, D.nk, D.ni, D.nj, h->g.west, h->g.east, h->g.south,
+                      h->g.north, h->g.pil_w, h->g.pil_e, h->g.pil_s, h->g.pil_n, I.k0t, I.i0b, I.inb, I.j0b,
+                      I.jnb, h->g.maxcfl + 1};
+  const cudaStream_t s = (cudaStream_t)stream;
+  for (int q0 = 0; q0 < ntr; q0 += adz::kMaxFields) {
+    adz::ZlfPtrs fp{};
+    fp.n = std::min(adz::kMaxFields, ntr - q0);
+    for (int q = 0; q < fp.n; q++) {
+      fp.f1[q] = f1[q0 + q];
+      fp.f2[q] = two ? f2[q0 + q] : nullptr;
+    }
+    ADZ_CK(prec == ADZC_FP64 ? adz::launch_bc_zlf<double>(m, setup, fp, s) : adz::launch_bc_zlf<float>(m, setup, fp, s));
   }
   return ADZC_OK;
 }

@@ -498,10 +498,11 @@ extern "C" int adzc_bermejo_conde(adzc_handle* h, int prec, int ntr, const adzc_
   if (!h || (prec != ADZC_REF32 && prec != ADZC_MIXED && prec != ADZC_FP64) || ntr < 1 || !tracers || !airm_p ||
       !airm_m || !mask || !deficit || adz_internal_view(h, &D, &I, &G, &niter, &cold) != ADZC_OK)
     return adz_internal_fail(ADZC_ERR_ARG);
+  const bool zlf = G.bc_lam_flux == 2;
   for (int q = 0; q < ntr; q++) {
     const adzc_bc_tracer& t = tracers[q];
     if (!t.p || !t.m || !t.lin || (min_max && (!t.min || !t.max)) || t.weight < 1 || t.weight > 3 ||
-        (t.weight == 3 && !t.pkps) || (!t.fo) != (!t.fi) || !std::isfinite(t.p_exp))
+        (t.weight == 3 && !t.pkps) || (!t.fo) != (!t.fi) || (zlf && t.fo) || !std::isfinite(t.p_exp))
       return adz_internal_fail(ADZC_ERR_ARG);
   }
   // core region (B/adz_post_tr.F90:146-152) and the LAM flux range (b set, all levels)
@@ -510,6 +511,9 @@ extern "C" int adzc_bermejo_conde(adzc_handle* h, int prec, int ntr, const adzc_
   core.ny = D.nj - (G.north ? G.pil_n : 0) - core.j0 + 1;
   core.nz = D.nk - I.k0t + 1;
   Region br{I.i0b, I.inb - I.i0b + 1, I.j0b, I.jnb - I.j0b + 1, 1, D.nk};
+  // Zerroukat-Shipway fluxes (Adz_BC_LAM_flux 2): the fixer runs over range b,
+  // every level (B/adz_post_tr.F90:145-152), and reads no flux arrays
+  if (zlf) core = br;
   if (core.nx <= 0 || core.ny <= 0 || core.nz <= 0) return adz_internal_fail(ADZC_ERR_ARG);
   Geo g{D.lminx, D.lminy, D.nit, D.ni, D.nij, mask};
   const size_t ts = prec == ADZC_FP64 ? sizeof(Tr<double>) : sizeof(Tr<float>);

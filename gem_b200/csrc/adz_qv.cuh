@@ -1,5 +1,6 @@
 // BICUBH_QV: bicubic horizontal, quintic vertical interpolation on thermo
-// levels (cubic at levels 2 and nk-2, linear at the ends), with the trilinear
+// levels (cubic at levels 2 and nk-2, linear at the ends, linear everywhere
+// in an autobarotropic run), with the trilinear
 // value and min/max over the inner 2x2x2 box.
 //   coefficients   B/bicubHQV_lin_mono.F90:66-147
 //   sums, box      B/bicubHQV_lin_min_max_zyx.F90:20-83
@@ -44,8 +45,9 @@ __device__ __forceinline__ void qv_coef(const DGrid& g, double px, double py, do
   c.ly[0] = 1.0 - del;
   c.ly[1] = del;
   int kk1 = (int)(float)pz;
-  const bool quintic = (kk1 >= 3) && (kk1 <= nk - 3);
-  const bool cubic = (kk1 == 2) || (kk1 == nk - 2);
+  // an autobarotropic run (Schm_autobar_L) interpolates linearly in z at every level
+  const bool quintic = (kk1 >= 3) && (kk1 <= nk - 3) && !g.autobar;
+  const bool cubic = ((kk1 == 2) || (kk1 == nk - 2)) && !g.autobar;
   if (!quintic && !cubic) kk1 = kk1 < 1 ? 1 : (kk1 > nk - 1 ? nk - 1 : kk1);
   const double* posz = g.zt;
   const double zt = __ldg(posz + kk1) + (pz - (double)kk1) * __ldg(g.delz_t + kk1);

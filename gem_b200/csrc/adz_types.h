@@ -29,7 +29,7 @@ struct DGrid {
   long long nij;
   int i0g, j0g;
   int i0, in, j0, jn, i0u, inu, j0v, jnv, i0b, inb, j0b, jnb, k0, k0t, k0m;
-  int pnz_m, pnz_t, slt_winds;
+  int pnz_m, pnz_t, slt_winds, autobar;
   double imnx, imxx, imny, imxy, sig, ovdzm, ovdzt, zmin, zmax;
   double inv_rayt, inv_hx, inv_hy, vw5, vw6, ww, wp, wm;
   const int* search_m;
@@ -192,7 +192,17 @@ struct BcMask {
   int lminx, lminy, nit, njt, nk, ni, nj;
   int west, east, south, north, pil_w, pil_e, pil_s, pil_n, k0t;
   int i0b, inb, j0b, jnb;
+  int ext;  // Grd_maxcfl + 1: the ZLF extension of the core
 };
+// the Zerroukat-Shipway (ZLF) setups of adz_BC_LAM_zlf_hlt on up to
+// kMaxFields tracers at once: f1[q] (and f2[q] for setups 2 and 4)
+struct ZlfPtrs {
+  void* f1[kMaxFields];
+  void* f2[kMaxFields];
+  int n;
+};
+template <typename T>
+cudaError_t launch_bc_zlf(const BcMask& m, int setup, const ZlfPtrs& f, cudaStream_t s);
 template <typename T>
 cudaError_t launch_bc_mask(const BcMask& m, const void* src, void* mo, void* mi, cudaStream_t s);
 template <typename T>

@@ -59,6 +59,9 @@ extern "C" {
 #define ADZC_SET_U 1  /* Adz_pmu: momentum levels, u points                  */
 #define ADZC_SET_V 2  /* Adz_pmv: momentum levels, v points                  */
 #define ADZC_SET_T 3  /* Adz_pt : thermodynamic levels, mass points          */
+#define ADZC_SET_B 4  /* Adz_pb : the t-set positions over range b
+                       * (Adz_i0b:inb, Adz_j0b:jnb, 1:nk), B/adz_set.F90:167-172;
+                       * needs bc_lam_flux != 0 (the k00 = 1 positions)     */
 
 /* ------------------------------------------------------------------------ */
 /* Level A — reference interpolator ABI (host pointers)                      */
@@ -121,10 +124,11 @@ typedef struct {
   int west, east, south, north;   /* 1 when the tile touches that LAM edge         */
   int pil_w, pil_e, pil_s, pil_n; /* pilot zone widths (0 on interior edges)       */
   int lam_gbpil_t;                /* Lam_gbpil_t                                   */
-  int bc_lam_flux;                /* adz_BC_LAM_flux                               */
+  int bc_lam_flux;                /* Adz_BC_LAM_flux: 0 none, 1 Aranami, 2 ZLF      */
   int schm_advec;                 /* Schm_advec: 0 none, 1 traditional, 2, 3        */
   int itraj;                      /* Adz_itraj                                     */
   int slt_winds;                  /* Adz_slt_winds (surface-layer winds at k=nk)   */
+  int schm_autobar;               /* Schm_autobar_L: BICUBH_QV linear in z         */
   double bA_m, bA;                /* Cstv_bA_m_8, Cstv_bA_8                        */
   double inv_rayt;                /* Dcst_inv_rayt_8                               */
   double inv_hx, inv_hy;          /* geomh_inv_hx_8, geomh_inv_hy_8                */
@@ -222,6 +226,24 @@ int adzc_slt_winds(adzc_handle *h, const void *uslt, const void *vslt);
  * NULL clears it.  adzc_batch_create refuses a handle with a pattern set. */
 int adzc_rhs_perturbation(adzc_handle *h, const void *mcrhsint, int ld);
 
+/* Zerroukat-Shipway (ZLF) LAM boundary treatment for the Bermejo-Conde
+ * fixer, the grid's bc_lam_flux 2 (Adz_BC_LAM_flux 2):
+ * adz_BC_LAM_zlf_hlt (B/adz_BC_LAM_zlf_hlt.F90:18-319) on ntr tracers,
+ * DEVICE ext arrays, the tile's interior only:
+ *   setup 1  f1 = 0 outside the core widened by maxcfl+1 on the LAM edges the
+ *            tile touches, and below level nint(k0t/2) inside it;
+ *   setup 2  f2 = f1 outside the core and below level k0t inside it;
+ *   setup 3  f1 = 0 outside the BCS_BASE (4) extension on the LAM edges;
+ *   setup 4  f1 = f2 where setup 2 copies.
+ * f1, f2: HOST arrays of ntr DEVICE pointers (f2 for setups 2 and 4 only).
+ * The sequence of B/adz_tracers.F90:84-98, 155-174 for mass-fixed tracers:
+ * setup 1 on the sources and setup 2 from the destinations (still holding the
+ * piloting values) into a keep array; adzc_tricub on ADZC_SET_B with mono and
+ * post arrays; setup 3 on the destinations; the post-processing (ILMC,
+ * adzc_bermejo_conde, which then runs over range b at every level and takes
+ * no flux arrays); setup 4 from the keep array. */
+int adzc_bc_lam_zlf(adzc_handle *h, int prec, int setup, int ntr, void *const *f1, void *const *f2, void *stream);
+
 /* LAM boundary fluxes of Aranami et al. (2015), adz_BC_LAM_Aranami_hlt
  * (B/adz_BC_LAM_Aranami_hlt.F90:18-236 with the masks of
  * B/adz_BC_LAM_setup.F90:18-92), for the tracers Bermejo-Conde fixes
@@ -230,7 +252,7 @@ int adzc_rhs_perturbation(adzc_handle *h, const void *mcrhsint, int ld);
  * Adz_j0b:jnb, 1:nk, then zeroed as the reference does (FLUX_out on the
  * core, FLUX_in on the pilot zones and above k0t); the fo, fi fields of
  * adzc_bermejo_conde.  srcs[q] NULL interpolates the masks themselves, the
- * PSADJ branch (:84-101).  The grid must set bc_lam_flux. */
+ * PSADJ branch (:84-101).  The grid must set bc_lam_flux 1. */
 int adzc_bc_lam_flux(adzc_handle *h, int prec, int ntr, const void *const *srcs, void *const *fo, void *const *fi,
                      void *stream);
 
@@ -375,8 +397,10 @@ int adzc_mlp_read(adzc_mlp *t, int what, float *host_out, void *stream);
 /* After the interpolation of mass-conserving tracers (B/adz_post_tr.F90:140-236,
  * B/Bermejo_Conde.F90:16-251, B/mass_tr_PM.F90, B/mass_tr_X.F90): restores
  * each tracer's air-mass-weighted total over the core region (the tile minus
- * its pilot zones, levels k0t..nk) to its value before advection, plus the
- * LAM boundary flux when given, by adding lambda * w where the high-order
+ * its pilot zones, levels k0t..nk; with the grid's bc_lam_flux 2, ZLF, range
+ * b at every level, B/adz_post_tr.F90:145-152) to its value before advection,
+ * plus the Aranami LAM boundary flux when given (fo, fi: bc_lam_flux 1 only),
+ * by adding lambda * w where the high-order
  * value departs from the low-order one.  All arrays are DEVICE arrays in the
  * ext layout of the handle, of the precision's field type (double for
  * ADZC_FP64, float otherwise); mask is the (ni, nj) FP64 area mask

@@ -215,6 +215,7 @@ static void set_range(const orc_set *s, int set, int *r) {
     case 0: r[0] = s->i0; r[1] = s->in; r[2] = s->j0; r[3] = s->jn; r[4] = s->k0; break;
     case 1: r[0] = s->i0u; r[1] = s->inu; r[2] = s->j0; r[3] = s->jn; r[4] = s->k0; break;
     case 2: r[0] = s->i0; r[1] = s->in; r[2] = s->j0v; r[3] = s->jnv; r[4] = s->k0; break;
+    case 4: r[0] = s->i0b; r[1] = s->inb; r[2] = s->j0b; r[3] = s->jnb; r[4] = 1; break; /* Adz_pb */
     default: r[0] = s->i0; r[1] = s->in; r[2] = s->j0; r[3] = s->jn; r[4] = s->k0t; break;
   }
 }

@@ -359,16 +359,16 @@ void SFX(orc_tricub_p)(const orc_set *s, int set, const REAL *pos, int m, const 
       const int linmima = mono || pert;
 #if IS_F32
 #ifdef ORC_USE_REF
-      void *zt = (set == 3) ? ref_ztab_t_of(s) : ref_ztab_m_of(s);
+      void *zt = (set >= 3) ? ref_ztab_t_of(s) : ref_ztab_m_of(s);
       if (linmima) Tricublin_mono_zyx_m_n(wrk, wl, wmi, wma, fs, (pxpypz *)p, zt, (int)np, m);
       else Tricublin_zyx1_m_n(wrk, fs, (pxpypz *)p, zt, (int)np, m);
 #else
-      const orc_ztab *zt = (set == 3) ? s->ztab_t : s->ztab_m;
+      const orc_ztab *zt = (set >= 3) ? s->ztab_t : s->ztab_m;
       if (linmima) orc_mono_m_n_f32(wrk, wl, wmi, wma, (const float *const *)fs, p, zt, (int)np, m, 0);
       else orc_zyx1_m_n_f32(wrk, (const float *const *)fs, p, zt, (int)np, m);
 #endif
 #else
-      const orc_ztab *zt = (set == 3) ? s->ztab_t : s->ztab_m;
+      const orc_ztab *zt = (set >= 3) ? s->ztab_t : s->ztab_m;
       if (linmima) orc_mono_m_n_f64(wrk, wl, wmi, wma, (const double *const *)fs, p, zt, (int)np, m);
       else orc_zyx1_m_n_f64(wrk, (const double *const *)fs, p, zt, (int)np, m);
 #endif
@@ -433,8 +433,9 @@ static long SFX(qv_coef)(const orc_set *s, REAL px, REAL py, REAL pz, double cx[
   ly[0] = 1.0 - del;
   ly[1] = del;
   int kk1 = (int)(float)pz;
-  const int quintic = (kk1 >= 3) && (kk1 <= nk - 3);
-  const int cubic = (kk1 == 2) || (kk1 == nk - 2);
+  /* bicubHQV_lin_mono.F90:95-96: no quintic or cubic case with Schm_autobar_L */
+  const int quintic = (kk1 >= 3) && (kk1 <= nk - 3) && !s->g.schm_autobar;
+  const int cubic = ((kk1 == 2) || (kk1 == nk - 2)) && !s->g.schm_autobar;
   if (!quintic && !cubic) kk1 = kk1 < 1 ? 1 : (kk1 > nk - 1 ? nk - 1 : kk1);
   const double zt = posz[kk1] + ((double)pz - (double)kk1) * dz[kk1];
   lz[1] = (zt - posz[kk1]) * odz[kk1];
@@ -519,10 +520,11 @@ static void SFX(qv_point)(const REAL *src, long ni, const double cx[4], const do
 
 /* adz_tricub_hlt with F_QV_L (adz_interp_hlt.F90:113-116 and the scatter of
  * :119-158) on position set t, plus the clip of adz_post_tr.F90:81-94. */
-void SFX(orc_tricub_qv_p)(const orc_set *s, const REAL *pos, int m, const REAL *const *srcs, REAL *const *dsts,
-                          int clip, REAL *const *lin, REAL *const *mn, REAL *const *mx, const REAL *pert, int ld) {
+void SFX(orc_tricub_qv_set_p)(const orc_set *s, int set, const REAL *pos, int m, const REAL *const *srcs,
+                              REAL *const *dsts, int clip, REAL *const *lin, REAL *const *mn, REAL *const *mx,
+                              const REAL *pert, int ld) {
   int r[5];
-  set_range(s, 3, r);
+  set_range(s, set, r);
   const int nk = s->g.nk;
   const long nx = r[1] - r[0] + 1, ny = r[3] - r[2] + 1, np = nx * ny;
   if (np <= 0 || m <= 0) return;
@@ -552,9 +554,100 @@ void SFX(orc_tricub_qv_p)(const orc_set *s, const REAL *pos, int m, const REAL *
   }
 }
 
+void SFX(orc_tricub_qv_p)(const orc_set *s, const REAL *pos, int m, const REAL *const *srcs, REAL *const *dsts,
+                          int clip, REAL *const *lin, REAL *const *mn, REAL *const *mx, const REAL *pert, int ld) {
+  SFX(orc_tricub_qv_set_p)(s, 3, pos, m, srcs, dsts, clip, lin, mn, mx, pert, ld);
+}
+
 void SFX(orc_tricub_qv)(const orc_set *s, const REAL *pos, int m, const REAL *const *srcs, REAL *const *dsts,
                         int clip, REAL *const *lin, REAL *const *mn, REAL *const *mx) {
   SFX(orc_tricub_qv_p)(s, pos, m, srcs, dsts, clip, lin, mn, mx, NULL, 0);
+}
+
+/* adz_BC_LAM_zlf_hlt (adz_BC_LAM_zlf_hlt.F90:18-319): the four setups of the
+ * Zerroukat-Shipway LAM treatment, written as the reference's loops over the
+ * tile's interior (1..ni, 1..nj, 1..nk), with its pilot widths and edge flags.
+ *   1: F1 = 0 outside [i0_e:in_e]x[j0_e:jn_e] (the core widened by
+ *      ext = maxcfl + 1 on the LAM edges) and on levels 1..nint(k0/2)-1 inside;
+ *   2: F2 = F1 outside [i0_c:in_c]x[j0_c:jn_c] and on levels 1..k0-1 inside;
+ *   3: F1 = 0 outside the BCS_BASE extension [i0_b:in_b]x[j0_b:jn_b];
+ *   4: F1 = F2 where setup 2 copies.  k0 = Adz_k0t. */
+void SFX(orc_bc_lam_zlf)(const orc_set *s, int setup, REAL *F1, REAL *F2) {
+  const orc_grid *g = &s->g;
+  const int ni = g->ni, nj = g->nj, nk = g->nk, k0 = s->k0t;
+  const int k0d2 = (int)lround(k0 / 2.0); /* nint: halves away from zero */
+  const int west = g->west, east = g->east, south = g->south, north = g->north;
+#define F1_(i, j, k) F1[EXT(i, j, k)]
+#define F2_(i, j, k) F2[EXT(i, j, k)]
+  if (setup == 1) {
+    const int ext = g->maxcfl + 1;
+    const int i0_e = 1 + g->pil_w - ext * west, in_e = ni - g->pil_e + ext * east;
+    const int j0_e = 1 + g->pil_s - ext * south, jn_e = nj - g->pil_n + ext * north;
+    if (west)
+      for (int i = 1; i <= i0_e - 1; i++)
+        for (int j = 1; j <= nj; j++)
+          for (int k = 1; k <= nk; k++) F1_(i, j, k) = 0;
+    if (east)
+      for (int i = in_e + 1; i <= ni; i++)
+        for (int j = 1; j <= nj; j++)
+          for (int k = 1; k <= nk; k++) F1_(i, j, k) = 0;
+    if (south)
+      for (int i = 1; i <= ni; i++)
+        for (int j = 1; j <= j0_e - 1; j++)
+          for (int k = 1; k <= nk; k++) F1_(i, j, k) = 0;
+    if (north)
+      for (int i = 1; i <= ni; i++)
+        for (int j = jn_e + 1; j <= nj; j++)
+          for (int k = 1; k <= nk; k++) F1_(i, j, k) = 0;
+    for (int i = i0_e; i <= in_e; i++)
+      for (int j = j0_e; j <= jn_e; j++)
+        for (int k = 1; k <= k0d2 - 1; k++) F1_(i, j, k) = 0;
+  } else if (setup == 2 || setup == 4) {
+    const int i0_c = 1 + g->pil_w, in_c = ni - g->pil_e, j0_c = 1 + g->pil_s, jn_c = nj - g->pil_n;
+    REAL *dst = (setup == 2) ? F2 : F1;
+    const REAL *src = (setup == 2) ? F1 : F2;
+    if (west)
+      for (int i = 1; i <= i0_c - 1; i++)
+        for (int j = 1; j <= nj; j++)
+          for (int k = 1; k <= nk; k++) dst[EXT(i, j, k)] = src[EXT(i, j, k)];
+    if (east)
+      for (int i = in_c + 1; i <= ni; i++)
+        for (int j = 1; j <= nj; j++)
+          for (int k = 1; k <= nk; k++) dst[EXT(i, j, k)] = src[EXT(i, j, k)];
+    if (south)
+      for (int i = 1; i <= ni; i++)
+        for (int j = 1; j <= j0_c - 1; j++)
+          for (int k = 1; k <= nk; k++) dst[EXT(i, j, k)] = src[EXT(i, j, k)];
+    if (north)
+      for (int i = 1; i <= ni; i++)
+        for (int j = jn_c + 1; j <= nj; j++)
+          for (int k = 1; k <= nk; k++) dst[EXT(i, j, k)] = src[EXT(i, j, k)];
+    for (int i = i0_c; i <= in_c; i++)
+      for (int j = j0_c; j <= jn_c; j++)
+        for (int k = 1; k <= k0 - 1; k++) dst[EXT(i, j, k)] = src[EXT(i, j, k)];
+  } else if (setup == 3) {
+    const int BCS_BASE = 4;
+    const int i0_b = 1 + BCS_BASE * west, in_b = ni - BCS_BASE * east;
+    const int j0_b = 1 + BCS_BASE * south, jn_b = nj - BCS_BASE * north;
+    if (west)
+      for (int i = 1; i <= i0_b - 1; i++)
+        for (int j = 1; j <= nj; j++)
+          for (int k = 1; k <= nk; k++) F1_(i, j, k) = 0;
+    if (east)
+      for (int i = in_b + 1; i <= ni; i++)
+        for (int j = 1; j <= nj; j++)
+          for (int k = 1; k <= nk; k++) F1_(i, j, k) = 0;
+    if (south)
+      for (int i = 1; i <= ni; i++)
+        for (int j = 1; j <= j0_b - 1; j++)
+          for (int k = 1; k <= nk; k++) F1_(i, j, k) = 0;
+    if (north)
+      for (int i = 1; i <= ni; i++)
+        for (int j = jn_b + 1; j <= nj; j++)
+          for (int k = 1; k <= nk; k++) F1_(i, j, k) = 0;
+  }
+#undef F1_
+#undef F2_
 }
 
 /* LAM boundary fluxes of Aranami et al. (2015) (adz_BC_LAM_Aranami_hlt.F90:
@@ -675,10 +768,12 @@ void SFX(orc_bermejo_conde)(const orc_set *s, const REAL *p, REAL *m, const REAL
                             double *deficit, double *diag) {
   const orc_grid *g = &s->g;
   const int nk = g->nk;
-  /* adz_post_tr.F90:146-152: core limits */
-  const int i0 = 1 + (g->west ? g->pil_w : 0), in = g->ni - (g->east ? g->pil_e : 0);
-  const int j0 = 1 + (g->south ? g->pil_s : 0), jn = g->nj - (g->north ? g->pil_n : 0);
-  const int k0 = s->k0t;
+  /* adz_post_tr.F90:146-152: core limits, or range b at every level with
+   * the Zerroukat-Shipway fluxes (Adz_BC_LAM_flux 2) */
+  const int zlf = g->bc_lam_flux == 2;
+  const int i0 = zlf ? s->i0b : 1 + (g->west ? g->pil_w : 0), in = zlf ? s->inb : g->ni - (g->east ? g->pil_e : 0);
+  const int j0 = zlf ? s->j0b : 1 + (g->south ? g->pil_s : 0), jn = zlf ? s->jnb : g->nj - (g->north ? g->pil_n : 0);
+  const int k0 = zlf ? 1 : s->k0t;
   /* mass_tr_PM */
   double mass_p = SFX(bc_mass)(s, p, airm_p, mask, i0, in, j0, jn, k0, nk);
   const double mass_m = SFX(bc_mass)(s, m, airm_m, mask, i0, in, j0, jn, k0, nk);

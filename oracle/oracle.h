@@ -49,6 +49,7 @@ typedef struct {
   int schm_advec;              /* Schm_advec (0..3) */
   int itraj;                   /* Adz_itraj */
   int slt_winds;               /* Adz_slt_winds (needs uslt/vslt) */
+  int schm_autobar;            /* Schm_autobar_L */
   double bA_m, bA;             /* Cstv_bA_m_8, Cstv_bA_8 */
   double inv_rayt;             /* Dcst_inv_rayt_8 */
   double inv_hx, inv_hy;       /* geomh_inv_hx_8, geomh_inv_hy_8 */
@@ -177,6 +178,17 @@ void orc_tricub_qv_p_f64(const orc_set *s, const double *pos, int m, const doubl
  * adz_BC_pexp_list(n), adz_BC_min_max_L.  *deficit: in the previous step's
  * epsilon, out this step's.  diag[8] (may be NULL): mass_p, mass_m, mass_fo,
  * mass_fi, mass_wei, lambda, mass_bc_r, mass_bc. */
+/* adz_BC_LAM_zlf_hlt (adz_BC_LAM_zlf_hlt.F90:18-319), setups 1-4, on one
+ * ext-layout tracer (f2 for setups 2 and 4) */
+void orc_bc_lam_zlf_f32(const orc_set *s, int setup, float *f1, float *f2);
+void orc_bc_lam_zlf_f64(const orc_set *s, int setup, double *f1, double *f2);
+/* BICUBH_QV over any set's range (3: Adz_pt, 4: Adz_pb over range b) */
+void orc_tricub_qv_set_p_f32(const orc_set *s, int set, const float *pos, int m, const float *const *srcs,
+                             float *const *dsts, int clip, float *const *lin, float *const *mn, float *const *mx,
+                             const float *pert, int ld);
+void orc_tricub_qv_set_p_f64(const orc_set *s, int set, const double *pos, int m, const double *const *srcs,
+                             double *const *dsts, int clip, double *const *lin, double *const *mn,
+                             double *const *mx, const double *pert, int ld);
 void orc_bermejo_conde_f32(const orc_set *s, const float *p, float *m, const float *lin, const float *mn,
                            const float *mx, const float *fo, const float *fi, const float *pkps, int weight,
                            double p_exp, int min_max, const float *airm_p, const float *airm_m, const double *mask,

@@ -34,7 +34,7 @@ class OrcGrid(C.Structure):
                 ("west", C.c_int), ("east", C.c_int), ("south", C.c_int), ("north", C.c_int),
                 ("pil_w", C.c_int), ("pil_e", C.c_int), ("pil_s", C.c_int), ("pil_n", C.c_int),
                 ("lam_gbpil_t", C.c_int), ("bc_lam_flux", C.c_int), ("schm_advec", C.c_int),
-                ("itraj", C.c_int), ("slt_winds", C.c_int),
+                ("itraj", C.c_int), ("slt_winds", C.c_int), ("schm_autobar", C.c_int),
                 ("bA_m", C.c_double), ("bA", C.c_double), ("inv_rayt", C.c_double),
                 ("inv_hx", C.c_double), ("inv_hy", C.c_double),
                 ("cy", C.POINTER(C.c_double)), ("zm", C.POINTER(C.c_double)),
@@ -117,6 +117,10 @@ class _Lib:
             getattr(L, f"orc_tricub_qv_p_{sfx}").argtypes = [C.POINTER(OrcSet), vp, C.c_int, vp, vp, C.c_int,
                                                              vp, vp, vp, vp, C.c_int]
             getattr(L, f"orc_ilmc_{sfx}").argtypes = [C.POINTER(OrcSet), vp, vp, vp, vp, C.c_int, C.c_int]
+            getattr(L, f"orc_pb_{sfx}").argtypes = [C.POINTER(OrcSet), C.c_double, vp, vp, vp, vp, vp, vp]
+            getattr(L, f"orc_bc_lam_zlf_{sfx}").argtypes = [C.POINTER(OrcSet), C.c_int, vp, vp]
+            getattr(L, f"orc_tricub_qv_set_p_{sfx}").argtypes = [C.POINTER(OrcSet), C.c_int, vp, C.c_int, vp, vp,
+                                                                 C.c_int, vp, vp, vp, vp, C.c_int]
             getattr(L, f"orc_bermejo_conde_{sfx}").argtypes = [C.POINTER(OrcSet)] + [vp] * 8 + [
                 C.c_int, C.c_double, C.c_int, vp, vp, vp, vp, vp]
 
@@ -260,17 +264,21 @@ class RefKernels:
 # --------------------------------------------------------------------------
 # driver restatement: one advection step (adz_main + adz_tracers subset)
 # --------------------------------------------------------------------------
-def make_grid(cfg, i0g=1, j0g=1, lam=True, slt_winds=False, schm_advec=1, lam_gbpil_t=0):
-    """orc_grid for a synth.Config tile (LAM tile touching all four edges)."""
+def make_grid(cfg, i0g=1, j0g=1, lam=True, slt_winds=False, schm_advec=1, lam_gbpil_t=0, bc_lam_flux=1,
+              schm_autobar=False, edges=None):
+    """orc_grid for a synth.Config tile: a LAM tile touching the edges
+    flagged in edges = (west, east, south, north) (default: all four when
+    lam), with pilot zones on those edges only."""
     from gem_b200 import synth
     ga = synth.grid_arrays(cfg)
     keep = {k: np.ascontiguousarray(ga[k], dtype=np.float64) for k in ("cy", "zm", "zt", "zx")}
     e = 1 if lam else 0
+    w, ea, so, no = edges if edges is not None else (e, e, e, e)
     p = cfg.pil if lam else 0
     g = OrcGrid(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk, maxcfl=cfg.maxcfl, i0g=i0g, j0g=j0g,
-                west=e, east=e, south=e, north=e, pil_w=p, pil_e=p, pil_s=p, pil_n=p,
-                lam_gbpil_t=lam_gbpil_t, bc_lam_flux=1, schm_advec=schm_advec, itraj=cfg.niter,
-                slt_winds=1 if slt_winds else 0, bA_m=0.6, bA=0.6, inv_rayt=ga["inv_rayt"],
+                west=w, east=ea, south=so, north=no, pil_w=p * w, pil_e=p * ea, pil_s=p * so, pil_n=p * no,
+                lam_gbpil_t=lam_gbpil_t, bc_lam_flux=bc_lam_flux, schm_advec=schm_advec, itraj=cfg.niter,
+                slt_winds=1 if slt_winds else 0, schm_autobar=1 if schm_autobar else 0, bA_m=0.6, bA=0.6, inv_rayt=ga["inv_rayt"],
                 inv_hx=ga["inv_hx"], inv_hy=ga["inv_hy"],
                 cy=keep["cy"].ctypes.data_as(C.POINTER(C.c_double)),
                 zm=keep["zm"].ctypes.data_as(C.POINTER(C.c_double)),
@@ -367,6 +375,50 @@ class Step:
             *(None if x is None else x.ctypes.data for x in slt), len(srcs), C.cast(sp, C.c_void_p),
             C.cast(_ptrs(fo, ct), C.c_void_p), C.cast(_ptrs(fi, ct), C.c_void_p))
         return fo, fi
+
+    def pb(self):
+        """Adz_pb: the t-set positions over range b (i0b:inb, j0b:jnb, 1:nk)
+        of the last trajectory, (npoints, 3) with i fastest."""
+        s = self.s
+        n = (s.inb - s.i0b + 1) * (s.jnb - s.j0b + 1) * self.cfg.nk
+        pb = np.zeros((n, 3), self.dt)
+        slt = getattr(self, "_slt", [None, None])
+        getattr(self.L, f"orc_pb_{self.prec}")(
+            C.byref(s), self.cfg.dt, self.wpxyz.ctypes.data, self.uvw_dep.ctypes.data, self._zdt0.ctypes.data,
+            *(None if x is None else x.ctypes.data for x in slt), pb.ctypes.data)
+        return pb
+
+    def tricub_b(self, srcs, mono=False, clip=False, post=False, qv=False):
+        """adz_tricub_hlt at Adz_pb over range b, all levels (the ZLF call of
+        adz_tracers.F90:91-93, 130-133); tricubic, or BICUBH_QV when qv."""
+        m = len(srcs)
+        srcs = [np.ascontiguousarray(x, dtype=self.dt) for x in srcs]
+        dsts = [np.full(self.ext_shape, np.nan, self.dt) for _ in range(m)]
+        ct = C.c_float if self.prec == "f32" else C.c_double
+        extra = [[np.full(self.ext_shape, np.nan, self.dt) for _ in range(m)] for _ in range(3)]
+        ptr = [C.cast(_ptrs(z, ct), C.c_void_p) for z in extra]
+        pos = self.pb()
+        pert, ld = self._pert_args()
+        if qv:
+            getattr(self.L, f"orc_tricub_qv_set_p_{self.prec}")(
+                C.byref(self.s), 4, pos.ctypes.data, m, C.cast(_ptrs(srcs, ct), C.c_void_p),
+                C.cast(_ptrs(dsts, ct), C.c_void_p), int(clip), *ptr, pert, ld)
+        else:
+            getattr(self.L, f"orc_tricub_p_{self.prec}")(
+                C.byref(self.s), 4, pos.ctypes.data, m, C.cast(_ptrs(srcs, ct), C.c_void_p),
+                C.cast(_ptrs(dsts, ct), C.c_void_p), int(mono), int(clip), *(ptr if mono else (None,) * 3), pert, ld)
+        if post:
+            return dsts, tuple(extra)
+        return dsts
+
+    def bc_lam_zlf(self, setup, f1, f2=None):
+        """adz_BC_LAM_zlf_hlt setup 1-4 on ext arrays of the Step's precision,
+        in place (f2 for setups 2 and 4)."""
+        for a in (f1, f2):
+            if a is not None:
+                assert a.dtype == self.dt and a.flags.c_contiguous and a.shape == self.ext_shape
+        getattr(self.L, f"orc_bc_lam_zlf_{self.prec}")(C.byref(self.s), int(setup), f1.ctypes.data,
+                                                        None if f2 is None else f2.ctypes.data)
 
     def set_rhs_perturbation(self, mcrhsint=None):
         """mcrhsint (nj, ni) or None: the ensemble perturbation of every
