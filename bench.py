@@ -801,72 +801,158 @@ def measure_post(args, timed, ws, rank):
 
 
 def measure_guess(args, timed, ws, rank):
-    """Cold start of the 1024x1024x80 tile (no previous departure points):
-    the reference's 6 fixed updates from the arrival point, the plain update
-    run to the project tolerance from the arrival point, and the learned
-    guess (BF16 tensor-core inference) followed by the plain update to the
-    same tolerance.  Reports updates per point, fallbacks, the guess error
-    against the converged departure points (1e-6) and the time of each."""
+    """The learned starting guess against the starts the reference has.
+
+    Cold start of the 1024x1024x80 tile (no previous departure points): the
+    reference's 6 fixed updates from the arrival point, the plain update run
+    to the project tolerance from the arrival point, and the learned guess
+    (BF16 tensor-core inference on every point, or on every stride-th point in
+    i and j with bilinear interpolation between them) followed by the plain
+    update to the same tolerance.  Also at dt = 150 s (Courant numbers near
+    2.4), where the arrival point is a worse start.
+
+    Warm step: the next step of the same flow (time t + dt, fresh wind noise)
+    from the previous step's departure points, the reference's start after
+    its first step (adz_traject.F90:69-70), against the learned guess.
+
+    Reports updates per point, fallbacks, the guess error against the
+    converged departure points (1e-6) and the time of each."""
     from gem_b200 import adz, guess, synth
     prec = adz.MIXED
     ni, nj, nk = args.size
-    cfg = synth.config_cold(ni, nj, nk, seed=tile_seed(rank))
-    inp = synth.make_inputs(cfg, device="cuda", dtype=torch.float32, with_fields=False)
-    ad = adz.Adz.from_config(cfg)
-    n = guess.npoints(ad)
     net = guess.GuessNet(guess.load_weights(args.guess_weights))
-    _, wp_ref = ad.new_state(prec)
-    guess.traject_tol(ad, prec, cfg.dt, inp, wp_ref, tol=1e-6, maxit=60, start=0)
-    d_ref = guess.displacement(ad, wp_ref)
-    disp = torch.empty((n, 3), dtype=torch.float32, device="cuda")
-    net.apply(ad, cfg.dt, inp, disp=disp)
-    e = (disp.double() - d_ref).abs()
-    sub = e[torch.randint(0, n, (min(n, 1 << 22),), device="cuda")]
-    gerr = {"rms": [float(v) for v in e.pow(2).mean(0).sqrt()], "max": [float(v) for v in e.max(0).values],
-            "p99": [float(v) for v in torch.quantile(sub, 0.99, dim=0)], "unit": "grid indices (x, y, level)"}
-
-    wps = {k: ad.new_state(prec)[1] for k in ("fixed", "plain", "learned")}
-    stats = {k: torch.zeros(3, dtype=torch.int64, device="cuda") for k in ("plain", "learned")}
-
-    def fixed():
-        ad.adz_inittraj(prec, None, wps["fixed"])
-        ad.adz_traject(prec, cfg.dt, inp, None, wps["fixed"])
-
-    def plain():
-        stats["plain"].zero_()
-        guess.traject_tol(ad, prec, cfg.dt, inp, wps["plain"], start=0, stats=stats["plain"])
-
-    def learned():
-        stats["learned"].zero_()
-        net.apply(ad, cfg.dt, inp, wpxyz=wps["learned"])
-        guess.traject_tol(ad, prec, cfg.dt, inp, wps["learned"], start=1, stats=stats["learned"])
-
-    def infer():
-        net.apply(ad, cfg.dt, inp, disp=disp)
-
     K, W = max(3, min(args.steps, 10)), args.warmup
-    ms = {"fixed6": timed(fixed, K, W)[0], "plain_tol": timed(plain, K, W)[0], "learned_tol": timed(learned, K, W)[0],
-          "inference": timed(infer, K, W)[0]}
-    if ad.status() != 0:
-        raise RuntimeError("device status set during the cold-start measurement")
-    sp, sl = stats["plain"].cpu().tolist(), stats["learned"].cpu().tolist()
-    acc = {k: [float(v) for v in (guess.displacement(ad, wps[k]) - d_ref).abs().max(0).values] for k in wps}
+    strides = (1, 2, 4, 8, 16)
+
+    def starts(cfg, inp, ad, prev=None):
+        """Time and updates of every start on one workload; prev: the previous
+        step's departure points (warm step)."""
+        n = guess.npoints(ad)
+        _, wp_ref = ad.new_state(prec)
+        guess.traject_tol(ad, prec, cfg.dt, inp, wp_ref, tol=1e-6, maxit=60, start=0)
+        d_ref = guess.displacement(ad, wp_ref)
+        wps, fns = {}, {}
+        stats = {}
+
+        def tol_from(name, start, before=None):
+            wps[name] = ad.new_state(prec)[1]
+            stats[name] = torch.zeros(3, dtype=torch.int64, device="cuda")
+
+            def fn():
+                stats[name].zero_()
+                if before is not None:
+                    before(wps[name])
+                guess.traject_tol(ad, prec, cfg.dt, inp, wps[name], start=start, stats=stats[name])
+            fns[name] = fn
+
+        tol_from("plain", 0)
+        if prev is not None:
+            tol_from("warm", 1, lambda wp: wp.copy_(prev))
+        # every point: the start points stored, then the iteration from them
+        tol_from("learned_s1", 1, lambda wp: net.apply(ad, cfg.dt, inp, wpxyz=wp))
+        # coarse grids: one call, the displacements interpolated inside the iteration
+        for s_ in strides[1:]:
+            name = f"learned_s{s_}"
+            wps[name] = ad.new_state(prec)[1]
+            stats[name] = torch.zeros(3, dtype=torch.int64, device="cuda")
+
+            def fn(name=name, s_=s_):
+                stats[name].zero_()
+                guess.traject_guess(ad, net, cfg.dt, inp, wps[name], stride=s_, stats=stats[name])
+            fns[name] = fn
+        if prev is None:
+            def fixed():
+                wps.setdefault("fixed", ad.new_state(prec)[1])
+                ad.adz_inittraj(prec, None, wps["fixed"])
+                ad.adz_traject(prec, cfg.dt, inp, None, wps["fixed"])
+            fixed_name = "fixed6"
+        else:
+            def fixed():  # the reference's warm step: Adz_itraj = 2 updates from the previous departure points
+                wps.setdefault("fixed", ad.new_state(prec)[1])
+                wps["fixed"].copy_(prev)
+                ad.adz_traject(prec, cfg.dt, inp, None, wps["fixed"], niter=2)
+            fixed_name = "fixed2_from_previous"
+        ms = {fixed_name: timed(fixed, K, W)[0]}
+        for name, fn in fns.items():
+            ms[name] = timed(fn, K, W)[0]
+        for s_ in strides:  # the guess alone (inference + the departure-wind preparation)
+            wp = ad.new_state(prec)[1]
+            ms[f"inference_s{s_}"] = timed((lambda: net.apply(ad, cfg.dt, inp, wpxyz=wp)) if s_ == 1 else
+                                           (lambda s_=s_: net.apply_coarse(ad, cfg.dt, inp, wp, s_)), K, W)[0]
+        if ad.status() != 0:
+            raise RuntimeError("device status set during the guess measurement")
+        out = {"updates_per_point": {}, "fallback_rate": {}, "not_converged": {}, "guess_error_rms": {},
+               "max_error_vs_converged": {}, "ms": ms}
+        for name in fns:
+            st = stats[name].cpu().tolist()
+            out["updates_per_point"][name] = st[0] / n
+            out["fallback_rate"][name] = st[1] / n
+            out["not_converged"][name] = st[2]
+            out["max_error_vs_converged"][name] = [float(v) for v in
+                                                   (guess.displacement(ad, wps[name]) - d_ref).abs().max(0).values]
+        # error of each start itself against the converged departure points
+        for s_ in strides:
+            wp = ad.new_state(prec)[1]
+            if s_ == 1:
+                net.apply(ad, cfg.dt, inp, wpxyz=wp)
+            else:
+                net.apply_coarse(ad, cfg.dt, inp, wp, s_)
+            e = guess.displacement(ad, wp) - d_ref
+            out["guess_error_rms"][f"learned_s{s_}"] = [float(v) for v in e.pow(2).mean(0).sqrt()]
+        if prev is not None:
+            e = guess.displacement(ad, prev) - d_ref
+            out["guess_error_rms"]["warm"] = [float(v) for v in e.pow(2).mean(0).sqrt()]
+        base = "warm" if prev is not None else "plain"
+        best = min((k for k in ms if k.startswith("learned")), key=ms.get)
+        out["best_learned"] = best
+        out["speedup_best_learned_vs_" + base] = ms[base] / ms[best]
+        out["updates_saved_per_point_vs_" + base] = (out["updates_per_point"][base] -
+                                                     out["updates_per_point"][best])
+        out["wp_ref"] = wp_ref
+        return out
+
+    res = {"tolerance": guess.TOL, "max_updates": guess.MAXIT, "unit": "grid indices (x, y, level)",
+           "strides": list(strides)}
+    # cold starts
+    for label, dt in (("cold", None), ("cold_dt150", 150.0)):
+        cfg = synth.config_cold(ni, nj, nk, seed=tile_seed(rank))
+        if dt is not None:
+            cfg.dt = dt
+        inp = synth.make_inputs(cfg, device="cuda", dtype=torch.float32, with_fields=False)
+        ad = adz.Adz.from_config(cfg)
+        r = starts(cfg, inp, ad)
+        r.pop("wp_ref")
+        r["workload"] = (f"cold start of the {ni}x{nj}x{nk} tile, {guess.npoints(ad)} arrival points, MIXED, "
+                         f"dt={cfg.dt:g} s, vertical-wind noise 0.02 m/s")
+        res[label] = r
+        del inp, ad
+        torch.cuda.empty_cache()
+    # warm step: previous step at t, this step at t + dt with fresh wind noise
+    cfg = synth.config_cold(ni, nj, nk, seed=tile_seed(rank))
+    ad = adz.Adz.from_config(cfg)
+    inp0 = synth.make_inputs(cfg, device="cuda", dtype=torch.float32, with_fields=False)
+    _, prev = ad.new_state(prec)
+    guess.traject_tol(ad, prec, cfg.dt, inp0, prev, tol=1e-6, maxit=60, start=0)
+    del inp0
+    cfg.t_now, cfg.seed = cfg.dt, cfg.seed + 1
+    inp = synth.make_inputs(cfg, device="cuda", dtype=torch.float32, with_fields=False)
+    r = starts(cfg, inp, ad, prev=prev)
+    r.pop("wp_ref")
+    r["workload"] = (f"warm step of the {ni}x{nj}x{nk} tile: winds at t + dt with fresh noise, started from the "
+                     "previous step's departure points (converged to 1e-6)")
+    res["warm"] = r
+    # tensor-core roofline of the inference on every point (stride 1)
     _, hbm_kind = peaks()
     pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if hbm_kind == "measured" else {}
     peak_tf = float(pk.get("bf16_tflops", TENSOR_FALLBACK_TFLOPS))
+    n = guess.npoints(ad)
     flops = n * 2.0 * 128 * (96 + 128 + 16)  # padded MMA work per arrival point
-    tf = flops / (ms["inference"] * 1e-3) / 1e12
-    return {"workload": f"cold start of the {ni}x{nj}x{nk} tile, {n} arrival points, MIXED, "
-                        "vertical-wind noise 0.02 m/s",
-            "tolerance": guess.TOL, "max_updates": guess.MAXIT,
-            "updates_per_point": {"fixed_reference": 6, "plain": sp[0] / n, "learned": sl[0] / n},
-            "updates_saved_per_point": (sp[0] - sl[0]) / n,
-            "fallback_rate": sl[1] / n, "not_converged": {"plain": sp[2], "learned": sl[2]},
-            "guess_error": gerr, "max_error_vs_converged": acc, "ms": ms,
-            "speedup_learned_vs_plain": ms["plain_tol"] / ms["learned_tol"],
-            "inference_roofline": {"bound": "tensor", "achieved": tf, "peak": peak_tf, "unit": "TFLOP/s",
-                                   "frac": tf / peak_tf, "flops_per_point": flops / n,
-                                   "note": "includes the departure-wind preparation launch"}}
+    tf = flops / (res["cold"]["ms"]["inference_s1"] * 1e-3) / 1e12
+    res["inference_roofline"] = {"bound": "tensor", "achieved": tf, "peak": peak_tf, "unit": "TFLOP/s",
+                                 "frac": tf / peak_tf, "flops_per_point": flops / n,
+                                 "note": "stride 1; includes the departure-wind preparation launch"}
+    res["speedup_learned_vs_plain"] = res["cold"]["speedup_best_learned_vs_plain"]
+    return res
 
 
 def run_reference(args):

@@ -170,9 +170,12 @@ struct Args {
   float* feat;       // features out (training data), npts x 82
   const long long* idx;  // features of these points only (NULL: all)
   const unsigned char* net;
-  long long npts;
+  long long npts;    // points the network runs on (the coarse nodes when stride > 1)
   int k00;
   double dt;
+  // coarse evaluation: the network runs on the nodes i = min(1 + stride*m, ni),
+  // j likewise (nxc x nyc nodes per level, every level); stride 1 is every point
+  int stride, nxc, nyc;
 };
 
 __device__ __forceinline__ long long wp_at(const DGrid& g, int i, int j, int k, int c) {
@@ -186,6 +189,73 @@ __device__ __forceinline__ void point_of(const DGrid& g, int k00, long long t, i
   i = (int)(t % g.ni) + 1;
   j = (int)((t / g.ni) % g.nj) + 1;
   k = (int)(t / plane) + k00;
+}
+
+// node t of the network's grid (every point when stride is 1)
+__device__ __forceinline__ void node_of(const Args& a, long long t, int& i, int& j, int& k) {
+  const long long plane = (long long)a.nxc * a.nyc;
+  const int ic = (int)(t % a.nxc), jc = (int)((t / a.nxc) % a.nyc);
+  i = 1 + a.stride * ic;
+  j = 1 + a.stride * jc;
+  i = i > a.g.ni ? a.g.ni : i;
+  j = j > a.g.nj ? a.g.nj : j;
+  k = (int)(t / plane) + a.k00;
+}
+
+// start point from a displacement: X - dx, Y - dy, k - dz with the level
+// clipped to 1..nk
+__device__ __forceinline__ void put_start(const Args& a, int i, int j, int k, float dx, float dy, float dz) {
+  const DGrid& g = a.g;
+  const double X = (double)(i + g.i0g - 1), Y = (double)(j + g.j0g - 1);
+  double pz = (double)k - (double)dz;
+  pz = pz < 1.0 ? 1.0 : (pz > (double)g.nk ? (double)g.nk : pz);
+  a.wpxyz[wp_at(g, i, j, k, 1)] = X - (double)dx;
+  a.wpxyz[wp_at(g, i, j, k, 2)] = Y - (double)dy;
+  a.wpxyz[wp_at(g, i, j, k, 3)] = pz;
+}
+
+// bracketing nodes and weight of coordinate i along an axis of n points with
+// nodes at min(1 + s m, n), m = 0..nc-1
+__device__ __forceinline__ void bracket(int i, int s, int n, int nc, int& m0, float& w) {
+  if (nc < 2) {
+    m0 = 0;
+    w = 0.0f;
+    return;
+  }
+  m0 = (i - 1) / s;
+  m0 = m0 > nc - 2 ? nc - 2 : m0;
+  const int x0 = 1 + s * m0, x1r = 1 + s * (m0 + 1), x1 = x1r > n ? n : x1r;
+  w = (float)(i - x0) / (float)(x1 - x0);
+}
+
+// start points of every arrival point from the network's displacements on the
+// coarse nodes, bilinear in (i, j) on each level
+__global__ void __launch_bounds__(256) k_guess_interp(Args a, const float* __restrict__ cd) {
+  const DGrid& g = a.g;
+  const long long plane = (long long)g.ni * g.nj, n = plane * (g.nk - a.k00 + 1);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    point_of(g, a.k00, t, i, j, k);
+    int mx, my;
+    float wx, wy;
+    bracket(i, a.stride, g.ni, a.nxc, mx, wx);
+    bracket(j, a.stride, g.nj, a.nyc, my, wy);
+    const int mx1 = a.nxc > 1 ? mx + 1 : mx, my1 = a.nyc > 1 ? my + 1 : my;
+    const long long base = (long long)(k - a.k00) * a.nxc * a.nyc;
+    const float* c00 = cd + 3 * (base + (long long)my * a.nxc + mx);
+    const float* c10 = cd + 3 * (base + (long long)my * a.nxc + mx1);
+    const float* c01 = cd + 3 * (base + (long long)my1 * a.nxc + mx);
+    const float* c11 = cd + 3 * (base + (long long)my1 * a.nxc + mx1);
+    float d[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      // (1 - w) a + w b: exact at both nodes
+      const float lo = fmaf(wx, __ldg(c10 + q), (1.0f - wx) * __ldg(c00 + q));
+      const float hi = fmaf(wx, __ldg(c11 + q), (1.0f - wx) * __ldg(c01 + q));
+      d[q] = fmaf(wy, hi, (1.0f - wy) * lo);
+    }
+    put_start(a, i, j, k, d[0], d[1], d[2]);
+  }
 }
 
 // the 27 neighbourhood rows of an arrival point: row (dk, dj) starts at
@@ -350,7 +420,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_guess(Args a) {
     const long long t = tile * kRows + row;
     const bool valid = t < a.npts;
     int i = 1, j = 1, k = 1;
-    if (valid) point_of(g, a.k00, t, i, j, k);
+    if (valid) node_of(a, t, i, j, k);
     Nbr nb;
     neighbourhood(g, a.uvw, i, j, k, a.dt, nb);
     if (half == 0) {
@@ -416,14 +486,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_guess(Args a) {
         a.disp[3 * t + 1] = y[1];
         a.disp[3 * t + 2] = y[2];
       }
-      if (a.wpxyz) {
-        const double X = (double)(i + g.i0g - 1), Y = (double)(j + g.j0g - 1);
-        double pz = (double)k - (double)y[2];
-        pz = pz < 1.0 ? 1.0 : (pz > (double)g.nk ? (double)g.nk : pz);
-        a.wpxyz[wp_at(g, i, j, k, 1)] = X - (double)y[0];
-        a.wpxyz[wp_at(g, i, j, k, 2)] = Y - (double)y[1];
-        a.wpxyz[wp_at(g, i, j, k, 3)] = pz;
-      }
+      if (a.wpxyz) put_start(a, i, j, k, y[0], y[1], y[2]);
     }
   }
   if (failed) {
@@ -579,6 +642,9 @@ extern "C" int adzc_guess_apply(adzc_handle* h, const adzc_guess* net, double dt
   a.k00 = k00_of(D);
   a.npts = (long long)D.ni * D.nj * (D.nk - a.k00 + 1);
   a.dt = dt;
+  a.stride = 1;
+  a.nxc = D.ni;
+  a.nyc = D.nj;
   if (a.npts <= 0) return ADZC_OK;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -586,6 +652,114 @@ extern "C" int adzc_guess_apply(adzc_handle* h, const adzc_guess* net, double dt
   const int grid = (int)std::min<long long>(ntiles, 2LL * sms);
   k_guess<<<grid, kThreads, kSmem, s>>>(a);
   return cudaGetLastError() == cudaSuccess ? ADZC_OK : adz_internal_fail(ADZC_ERR_CUDA);
+}
+
+extern "C" int adzc_guess_apply_coarse(adzc_handle* h, const adzc_guess* net, double dt, const void* uu_ext,
+                                       const void* vv_ext, const void* ww_ext, int stride, double* wpxyz,
+                                       void* stream) {
+  AdzRange nvtx_range("adz guess coarse");
+  using namespace adz::guess;
+  adz::DGrid D;
+  adzc_info I;
+  adzc_grid G;
+  if (!h || !net || !uu_ext || !vv_ext || !ww_ext || !wpxyz || stride < 1 || stride > ADZC_GUESS_MAX_STRIDE ||
+      !std::isfinite(dt) || check_handle(h, &D, &I, &G) != ADZC_OK)
+    return adz_internal_fail(ADZC_ERR_ARG);
+  if (stride == 1) return adzc_guess_apply(h, net, dt, uu_ext, vv_ext, ww_ext, wpxyz, nullptr, stream);
+  const cudaStream_t s = (cudaStream_t)stream;
+  Args a{};
+  a.g = D;
+  a.net = net->d_net;
+  a.k00 = k00_of(D);
+  a.dt = dt;
+  a.stride = stride;
+  a.nxc = (D.ni - 1 + stride - 1) / stride + 1;
+  a.nyc = (D.nj - 1 + stride - 1) / stride + 1;
+  const long long nkp = D.nk - a.k00 + 1;
+  a.npts = (long long)a.nxc * a.nyc * nkp;
+  if (nkp <= 0) return ADZC_OK;
+  // the coarse displacements live in the handle's auxiliary buffer
+  void* cd = nullptr;
+  if (adz_internal_aux(h, (size_t)a.npts * 3 * sizeof(float), &cd) != ADZC_OK) return adz_internal_fail(ADZC_ERR_ALLOC);
+  void *uvw = nullptr, *wdep = nullptr;
+  int st = prepare_mixed(h, D, uu_ext, vv_ext, ww_ext, &uvw, &wdep, s);
+  if (st != ADZC_OK) return adz_internal_fail(st);
+  a.uvw = (const float*)uvw;
+  a.disp = (float*)cd;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (cudaFuncSetAttribute(k_guess, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem) != cudaSuccess)
+    return adz_internal_fail(ADZC_ERR_CUDA);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long ntiles = (a.npts + kRows - 1) / kRows;
+  k_guess<<<(int)std::min<long long>(ntiles, 2LL * sms), kThreads, kSmem, s>>>(a);
+  if (cudaGetLastError() != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
+  a.wpxyz = wpxyz;
+  const long long n = (long long)D.ni * D.nj * nkp;
+  const long long blocks = std::min<long long>((n + 255) / 256, (long long)sms * 16);
+  k_guess_interp<<<(int)blocks, 256, 0, s>>>(a, (const float*)cd);
+  return cudaGetLastError() == cudaSuccess ? ADZC_OK : adz_internal_fail(ADZC_ERR_CUDA);
+}
+
+extern "C" int adzc_traject_guess(adzc_handle* h, const adzc_guess* net, int stride, double dt, double tol,
+                                  int maxit, const void* uu_ext, const void* vv_ext, const void* ww_ext,
+                                  const void* ut0, const void* vt0, const void* zdt0, double* wpxyz,
+                                  unsigned char* iters, unsigned long long* stats, void* stream) {
+  AdzRange nvtx_range("adz_traject guess");
+  using namespace adz::guess;
+  adz::DGrid D;
+  adzc_info I;
+  adzc_grid G;
+  if (!h || !net || !uu_ext || !vv_ext || !ww_ext || !ut0 || !vt0 || !zdt0 || !wpxyz || stride < 1 ||
+      stride > ADZC_GUESS_MAX_STRIDE || maxit < 1 || maxit > 127 || !(tol >= 0.0) || !std::isfinite(dt) ||
+      check_handle(h, &D, &I, &G) != ADZC_OK)
+    return adz_internal_fail(ADZC_ERR_ARG);
+  const cudaStream_t s = (cudaStream_t)stream;
+  Args a{};
+  a.g = D;
+  a.net = net->d_net;
+  a.k00 = k00_of(D);
+  a.dt = dt;
+  a.stride = stride;
+  a.nxc = (D.ni - 1 + stride - 1) / stride + 1;
+  a.nyc = (D.nj - 1 + stride - 1) / stride + 1;
+  const long long nkp = D.nk - a.k00 + 1;
+  a.npts = (long long)a.nxc * a.nyc * nkp;
+  if (nkp <= 0) return ADZC_OK;
+  void* cd = nullptr;
+  if (adz_internal_aux(h, (size_t)a.npts * 3 * sizeof(float), &cd) != ADZC_OK) return adz_internal_fail(ADZC_ERR_ALLOC);
+  // the departure winds are prepared once, for the network and the iteration
+  void *uvw = nullptr, *wdep = nullptr;
+  int st = prepare_mixed(h, D, uu_ext, vv_ext, ww_ext, &uvw, &wdep, s);
+  if (st != ADZC_OK) return adz_internal_fail(st);
+  a.uvw = (const float*)uvw;
+  a.disp = (float*)cd;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (cudaFuncSetAttribute(k_guess, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem) != cudaSuccess)
+    return adz_internal_fail(ADZC_ERR_CUDA);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long ntiles = (a.npts + kRows - 1) / kRows;
+  k_guess<<<(int)std::min<long long>(ntiles, 2LL * sms), kThreads, kSmem, s>>>(a);
+  if (cudaGetLastError() != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
+  adz::TrajArgs t{};
+  t.uvw_d = uvw;
+  t.ut0 = ut0;
+  t.vt0 = vt0;
+  t.zdt0 = zdt0;
+  t.wpxyz = wpxyz;
+  t.wdep = wdep;
+  t.niter = maxit;
+  t.cold = 0;
+  t.k00 = a.k00;
+  t.dt = adz_internal_dt_split(G, dt);
+  const adz::GuessStart gs{(const float*)cd, stride, a.nxc, a.nyc};
+  if (adz::launch_traject_tol<adz::kMixed>(D, t, tol, maxit, iters, stats, s, gs) != cudaSuccess)
+    return adz_internal_fail(ADZC_ERR_CUDA);
+  adz_internal_record_positions(h, ADZC_MIXED, wpxyz, zdt0, t.dt);
+  return ADZC_OK;
 }
 
 extern "C" int adzc_traject_tol(adzc_handle* h, int prec, double dt, double tol, int maxit, int start,

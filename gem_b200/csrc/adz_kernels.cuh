@@ -338,6 +338,49 @@ __device__ __forceinline__ void warm_start(const DGrid& g, const TrajArgs& a, in
   }
 }
 
+// bracketing coarse nodes and weight of coordinate i on an axis of n points
+// with nodes at min(1 + s m, n), m = 0..nc-1
+__device__ __forceinline__ void coarse_bracket(int i, int s, int n, int nc, int& m0, int& m1, float& w) {
+  if (nc < 2) {
+    m0 = m1 = 0;
+    w = 0.0f;
+    return;
+  }
+  m0 = (i - 1) / s;
+  m0 = m0 > nc - 2 ? nc - 2 : m0;
+  m1 = m0 + 1;
+  const int x0 = 1 + s * m0, x1r = 1 + s * m1, x1 = x1r > n ? n : x1r;
+  w = (float)(i - x0) / (float)(x1 - x0);
+}
+
+// start point from the coarse guess of the tolerance iteration: the
+// displacement interpolated bilinearly, X - dx, Y - dy clipped as a warm
+// start is, k - dz clipped to the levels
+__device__ __forceinline__ void guess_start(const DGrid& g, const TrajArgs& a, const GuessStart& gs, int i, int j,
+                                            int k, double& px, double& py, double& pz) {
+  int mx0, mx1, my0, my1;
+  float wx, wy;
+  coarse_bracket(i, gs.stride, g.ni, gs.nxc, mx0, mx1, wx);
+  coarse_bracket(j, gs.stride, g.nj, gs.nyc, my0, my1, wy);
+  const long long base = (long long)(k - a.k00) * gs.nxc * gs.nyc;
+  const float* c00 = gs.d + 3 * (base + (long long)my0 * gs.nxc + mx0);
+  const float* c10 = gs.d + 3 * (base + (long long)my0 * gs.nxc + mx1);
+  const float* c01 = gs.d + 3 * (base + (long long)my1 * gs.nxc + mx0);
+  const float* c11 = gs.d + 3 * (base + (long long)my1 * gs.nxc + mx1);
+  float d[3];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    // (1 - w) a + w b: exact at both nodes
+    const float lo = fmaf(wx, __ldg(c10 + q), (1.0f - wx) * __ldg(c00 + q));
+    const float hi = fmaf(wx, __ldg(c11 + q), (1.0f - wx) * __ldg(c01 + q));
+    d[q] = fmaf(wy, hi, (1.0f - wy) * lo);
+  }
+  px = dmin_(dmax_((double)(i + g.i0g - 1) - (double)d[0], g.imnx), g.imxx);
+  py = dmin_(dmax_((double)(j + g.j0g - 1) - (double)d[1], g.imny), g.imxy);
+  const double z = (double)k - (double)d[2];
+  pz = z < 1.0 ? 1.0 : (z > (double)g.nk ? (double)g.nk : z);
+}
+
 // store the departure point of (i,j,k) (adz_traject.F90:112-118)
 template <int PREC>
 __device__ __forceinline__ void traj_store(const DGrid& g, const TrajArgs& a, int i, int j, int k, double xm, double ym,
@@ -392,8 +435,9 @@ __device__ __forceinline__ void traject_point(const DGrid& g, const TrajArgs& a,
 // +128 when the fallback ran), and block sums into stats[0] updates,
 // stats[1] fallbacks, stats[2] points not converged.
 template <int PREC>
-__device__ __forceinline__ void traject_point_tol(const DGrid& g, const TrajArgs& a, int i, int j, int k, double tol,
-                                                  int maxit, unsigned char* iters, unsigned long long* cnt) {
+__device__ __forceinline__ void traject_point_tol(const DGrid& g, const TrajArgs& a, const GuessStart& gs, int i,
+                                                  int j, int k, double tol, int maxit, unsigned char* iters,
+                                                  unsigned long long* cnt) {
   const long long e = ext_index(g, i, j, k);
   double ua, va, wa;
   arrival_winds<PREC>(g, a, j, k, e, ua, va, wa);
@@ -401,6 +445,8 @@ __device__ __forceinline__ void traject_point_tol(const DGrid& g, const TrajArgs
   double px, py, pz;
   if (a.cold) {
     px = X; py = Y; pz = Z;
+  } else if (gs.d) {
+    guess_start(g, a, gs, i, j, k, px, py, pz);
   } else {
     warm_start<PREC>(g, a, i, j, k, px, py, pz);
   }
@@ -449,7 +495,7 @@ __global__ void ADZ_TRAJ_BOUNDS k_traject(DGrid g, TrajArgs a) {
 
 template <int PREC>
 __global__ void ADZ_TRAJ_BOUNDS k_traject_tol(DGrid g, TrajArgs a, double tol, int maxit, unsigned char* iters,
-                                              unsigned long long* stats) {
+                                              unsigned long long* stats, GuessStart gs) {
   const long long nplane = (long long)g.ni * g.nj;
   const long long n = nplane * (g.nk - a.k00 + 1);
   unsigned long long cnt[3] = {0, 0, 0};
@@ -457,7 +503,7 @@ __global__ void ADZ_TRAJ_BOUNDS k_traject_tol(DGrid g, TrajArgs a, double tol, i
     const int i = (int)(t % g.ni) + 1;
     const int j = (int)((t / g.ni) % g.nj) + 1;
     const int k = (int)(t / nplane) + a.k00;
-    traject_point_tol<PREC>(g, a, i, j, k, tol, maxit, iters, cnt);
+    traject_point_tol<PREC>(g, a, gs, i, j, k, tol, maxit, iters, cnt);
   }
   if (stats) {
 #pragma unroll
@@ -1014,9 +1060,9 @@ cudaError_t launch_traject(const DGrid& g, const TrajArgs& a, cudaStream_t s) {
 
 template <int PREC>
 cudaError_t launch_traject_tol(const DGrid& g, const TrajArgs& a, double tol, int maxit, unsigned char* iters,
-                               unsigned long long* stats, cudaStream_t s) {
+                               unsigned long long* stats, cudaStream_t s, const GuessStart& gs) {
   const long long n = (long long)g.ni * g.nj * (g.nk - a.k00 + 1);
-  k_traject_tol<PREC><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, a, tol, maxit, iters, stats);
+  k_traject_tol<PREC><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, a, tol, maxit, iters, stats, gs);
   return cudaGetLastError();
 }
 
@@ -1149,7 +1195,7 @@ int batch_resident_blocks(int variant) {
   template cudaError_t launch_inittraj<P>(const DGrid&, float*, double*, cudaStream_t);                            \
   template cudaError_t launch_traject<P>(const DGrid&, const TrajArgs&, cudaStream_t);                             \
   template cudaError_t launch_traject_tol<P>(const DGrid&, const TrajArgs&, double, int, unsigned char*,           \
-                                             unsigned long long*, cudaStream_t);                                   \
+                                             unsigned long long*, cudaStream_t, const GuessStart&);                \
   template cudaError_t launch_tricub_set<P>(const DGrid&, int, int, int, int, int, int, int, const SetArgs&,       \
                                             const FieldPtrs&, cudaStream_t);                                       \
   template cudaError_t launch_interp_pos<P>(const DZtab&, int, int, const void*, const FieldPtrs&, cudaStream_t); \

@@ -104,6 +104,15 @@ struct TrajArgs {
   DtSplit dt;
 };
 
+// start of the tolerance iteration from displacements given on a coarse grid
+// (nodes i = min(1 + stride*m, ni), likewise j, every level from k00; 3
+// floats per node), interpolated bilinearly in (i, j); d NULL: from the
+// arrival point (cold) or from wpxyz
+struct GuessStart {
+  const float* d;
+  int stride, nxc, nyc;
+};
+
 struct SetArgs {
   const double* wpxyz;
   const float* pxyzm;  // REF32 only
@@ -136,7 +145,7 @@ template <int PREC>
 cudaError_t launch_traject(const DGrid& g, const TrajArgs& a, cudaStream_t s);
 template <int PREC>
 cudaError_t launch_traject_tol(const DGrid& g, const TrajArgs& a, double tol, int maxit, unsigned char* iters,
-                               unsigned long long* stats, cudaStream_t s);
+                               unsigned long long* stats, cudaStream_t s, const GuessStart& gs = GuessStart{});
 template <int PREC>
 cudaError_t launch_tricub_set(const DGrid& g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
                               const SetArgs& a, const FieldPtrs& fp, cudaStream_t s);

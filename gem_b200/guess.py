@@ -45,6 +45,8 @@ def _lib():
         L.adzc_guess_npoints.restype = C.c_longlong
         L.adzc_guess_apply.argtypes = [vp, vp, d, vp, vp, vp, vp, vp, vp]
         L.adzc_guess_features.argtypes = [vp, d, vp, vp, vp, vp, C.c_longlong, vp, vp]
+        L.adzc_guess_apply_coarse.argtypes = [vp, vp, d, vp, vp, vp, i, vp, vp]
+        L.adzc_traject_guess.argtypes = [vp, vp, i, d, d, i] + [vp] * 6 + [vp, vp, vp, vp]
         L.adzc_mlp_create.argtypes = [vp, i, C.POINTER(vp)]
         L.adzc_mlp_destroy.argtypes = [vp]
         L.adzc_mlp_forward.argtypes = [vp, vp, i, vp, vp]
@@ -115,6 +117,14 @@ class GuessNet:
                                          None if disp is None else disp.data_ptr(), A._stream(stream)),
                  "adzc_guess_apply")
 
+    def apply_coarse(self, ad: A.Adz, dt: float, winds: dict, wpxyz, stride: int, stream=None):
+        """The network on every stride-th point in i and j only, start points
+        of all points from the displacements interpolated bilinearly."""
+        A._check(_lib().adzc_guess_apply_coarse(ad.h, self.h, float(dt),
+                                                *(winds[k].data_ptr() for k in ("uu_ext", "vv_ext", "ww_ext")),
+                                                int(stride), wpxyz.data_ptr(), A._stream(stream)),
+                 "adzc_guess_apply_coarse")
+
     def __del__(self):
         try:
             _lib().adzc_guess_destroy(self.h)
@@ -140,6 +150,18 @@ def traject_tol(ad: A.Adz, prec: int, dt: float, winds: dict, wpxyz, tol=TOL, ma
                                      wpxyz.data_ptr(), None if iters is None else iters.data_ptr(),
                                      None if stats is None else stats.data_ptr(), A._stream(stream)),
              "adzc_traject_tol")
+
+
+def traject_guess(ad: A.Adz, net: GuessNet, dt: float, winds: dict, wpxyz, stride=8, tol=TOL, maxit=MAXIT,
+                  iters=None, stats=None, stream=None):
+    """adzc_traject_guess (MIXED): the network on every stride-th point in i
+    and j, then the tolerance iteration from the interpolated displacements."""
+    A._check(_lib().adzc_traject_guess(ad.h, net.h, int(stride), float(dt), float(tol), int(maxit),
+                                       *(winds[k].data_ptr() for k in ("uu_ext", "vv_ext", "ww_ext", "ut0", "vt0",
+                                                                       "zdt0")),
+                                       wpxyz.data_ptr(), None if iters is None else iters.data_ptr(),
+                                       None if stats is None else stats.data_ptr(), A._stream(stream)),
+             "adzc_traject_guess")
 
 
 def displacement(ad: A.Adz, wpxyz, i0g=1, j0g=1):

@@ -373,6 +373,25 @@ long long adzc_guess_npoints(adzc_handle *h);
  * and/or the raw displacement d into disp (npoints x 3) */
 int adzc_guess_apply(adzc_handle *h, const adzc_guess *net, double dt, const void *uu_ext, const void *vv_ext,
                      const void *ww_ext, double *wpxyz, float *disp, void *stream);
+/* The network on a coarse grid only: every stride-th point in i and j
+ * (nodes i = min(1 + stride*m, ni), likewise j) on every level, then the
+ * start point of each arrival point from its displacement interpolated
+ * bilinearly in (i, j) between the nodes around it; into wpxyz as
+ * adzc_guess_apply writes it.  stride 1..ADZC_GUESS_MAX_STRIDE (1 is
+ * adzc_guess_apply).  Uses the handle's auxiliary device buffer. */
+#define ADZC_GUESS_MAX_STRIDE 16
+int adzc_guess_apply_coarse(adzc_handle *h, const adzc_guess *net, double dt, const void *uu_ext,
+                            const void *vv_ext, const void *ww_ext, int stride, double *wpxyz, void *stream);
+/* The learned start and the iteration to a tolerance in one call (MIXED):
+ * the departure winds prepared once, the network on the coarse grid of
+ * stride (as adzc_guess_apply_coarse), then adzc_traject_tol from those
+ * displacements, interpolated per point inside the iteration (no start
+ * points stored), with the same fallback, counters and outputs as
+ * adzc_traject_tol with start 1.  Uses the handle's auxiliary buffer. */
+int adzc_traject_guess(adzc_handle *h, const adzc_guess *net, int stride, double dt, double tol, int maxit,
+                       const void *uu_ext, const void *vv_ext, const void *ww_ext, const void *ut0, const void *vt0,
+                       const void *zdt0, double *wpxyz, unsigned char *iters, unsigned long long *stats,
+                       void *stream);
 /* FP32 features (n x 82) of the points idx[0..n) (device; NULL: all points) */
 int adzc_guess_features(adzc_handle *h, double dt, const void *uu_ext, const void *vv_ext, const void *ww_ext,
                         const long long *idx, long long n, float *features, void *stream);

@@ -179,3 +179,117 @@ def test_features_and_bf16_inference_vs_oracle():
     print("bf16 inference: max err", err.max(), "mean err", err.mean(), "max |y|", np.abs(y_ref).max())
     assert np.all(err <= 0.02 + 0.01 * np.abs(y_ref))
     assert err.mean() <= 0.003
+
+
+def test_trained_network_saves_updates():
+    """The committed network (gem_b200/data/guess_mlp.npz, trained by the
+    project's kernels on the plain iteration's own trajectories) on a cold
+    start of the learned-guess flow: fewer updates per point than the plain
+    start from the arrival point, at most 1 % of points falling back, every
+    point converged to the tolerance; on every point and on a coarse grid of
+    every 4th point in i and j."""
+    _need_gpu()
+    from gem_b200 import adz as A, guess, synth
+    prec = A.MIXED
+    cfg = synth.config_cold(192, 160, 80, seed=77)
+    inp = synth.make_inputs(cfg, device="cuda", dtype=torch.float32, with_fields=False)
+    ad = A.Adz.from_config(cfg)
+    n = guess.npoints(ad)
+    net = guess.GuessNet(guess.load_weights())
+    _, wp_ref = ad.new_state(prec)
+    guess.traject_tol(ad, prec, cfg.dt, inp, wp_ref, tol=1e-6, maxit=60, start=0)
+    d_ref = guess.displacement(ad, wp_ref)
+    upd = {}
+    for name, stride in (("plain", 0), ("learned", 1), ("learned_coarse4", 4)):
+        _, wp = ad.new_state(prec)
+        if stride == 1:
+            net.apply(ad, cfg.dt, inp, wpxyz=wp)
+        elif stride > 1:
+            net.apply_coarse(ad, cfg.dt, inp, wp, stride)
+        if stride:
+            err = (guess.displacement(ad, wp) - d_ref).pow(2).mean(0).sqrt()
+            print(name, "guess RMS error (x, y, level)", err.tolist())
+            assert torch.all(err < 0.05)  # the arrival point is ~1 grid length and ~1.5 levels away
+        st = torch.zeros(3, dtype=torch.int64, device="cuda")
+        guess.traject_tol(ad, prec, cfg.dt, inp, wp, start=1 if stride else 0, stats=st)
+        torch.cuda.synchronize()
+        s = st.cpu().tolist()
+        assert ad.status() == 0 and s[2] == 0, (name, s)
+        assert s[1] <= 0.01 * n, (name, s)
+        upd[name] = s[0] / n
+        assert torch.max(torch.abs(guess.displacement(ad, wp) - d_ref)).item() <= 10 * guess.TOL
+    print("updates per point", upd)
+    assert upd["learned"] < upd["plain"] - 0.5
+    assert upd["learned_coarse4"] < upd["plain"] - 0.3
+
+
+def test_coarse_guess_interpolates_the_node_displacements():
+    """adzc_guess_apply_coarse: on the coarse nodes the start points equal
+    those of the network on every point; in between they are the bilinear
+    interpolation (in i, j) of the nodes' displacements."""
+    _need_gpu()
+    from gem_b200 import adz as A, guess, synth
+    prec = A.MIXED
+    cfg = synth.config_cold(45, 38, 16, seed=5)  # sizes not multiples of the stride
+    inp = synth.make_inputs(cfg, device="cuda", dtype=torch.float32, with_fields=False)
+    ad = A.Adz.from_config(cfg)
+    net = guess.GuessNet(guess.load_weights())
+    n = guess.npoints(ad)
+    disp = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    net.apply(ad, cfg.dt, inp, disp=disp)
+    k00, (nkp, nj, ni) = guess.arrival_index(ad)
+    d = disp.view(nkp, nj, ni, 3).double().cpu().numpy()
+    for stride in (3, 4):
+        _, wp = ad.new_state(prec)
+        net.apply_coarse(ad, cfg.dt, inp, wp, stride)
+        got = guess.displacement(ad, wp).view(nkp, nj, ni, 3).cpu().numpy()
+        xs = np.minimum(1 + stride * np.arange((ni - 2 + stride) // stride + 1), ni) - 1
+        ys = np.minimum(1 + stride * np.arange((nj - 2 + stride) // stride + 1), nj) - 1
+        want = np.empty_like(d)
+        for i in range(ni):
+            m = min(i // stride, len(xs) - 2)
+            wx = (i - xs[m]) / (xs[m + 1] - xs[m])
+            for j in range(nj):
+                q = min(j // stride, len(ys) - 2)
+                wy = (j - ys[q]) / (ys[q + 1] - ys[q])
+                c = lambda a, b: d[:, ys[b], xs[a]]  # noqa: E731
+                lo = c(m, q) + wx * (c(m + 1, q) - c(m, q))
+                hi = c(m, q + 1) + wx * (c(m + 1, q + 1) - c(m, q + 1))
+                want[:, j, i] = lo + wy * (hi - lo)
+        # the vertical start is clipped to the levels; compare where it is not
+        ok = np.abs(got[..., 2] - want[..., 2]) <= 1e-5
+        interior = (np.arange(nkp)[:, None, None] + k00 - want[..., 2] >= 1.0) & \
+                   (np.arange(nkp)[:, None, None] + k00 - want[..., 2] <= ad.nk)
+        assert np.all(ok | ~interior)
+        assert np.max(np.abs(got[..., :2] - want[..., :2])) <= 1e-5
+        # the nodes themselves: the network's own displacement
+        node = np.zeros((nj, ni), bool)
+        node[np.ix_(ys, xs)] = True
+        assert np.max(np.abs(got[:, node, :2] - d[:, node, :2])) <= 1e-6
+
+
+def test_fused_learned_trajectory_matches_the_two_calls():
+    """adzc_traject_guess (network on the coarse grid, displacements
+    interpolated inside the tolerance iteration) gives bit for bit the
+    positions and counters of adzc_guess_apply_coarse followed by
+    adzc_traject_tol from the stored start points."""
+    _need_gpu()
+    from gem_b200 import adz as A, guess, synth
+    prec = A.MIXED
+    cfg = synth.config_cold(70, 52, 24, seed=3)
+    inp = synth.make_inputs(cfg, device="cuda", dtype=torch.float32, with_fields=False)
+    ad = A.Adz.from_config(cfg)
+    net = guess.GuessNet(guess.load_weights())
+    for stride in (1, 4, 8):
+        _, wp_a = ad.new_state(prec)
+        st_a = torch.zeros(3, dtype=torch.int64, device="cuda")
+        net.apply_coarse(ad, cfg.dt, inp, wp_a, stride)
+        guess.traject_tol(ad, prec, cfg.dt, inp, wp_a, start=1, stats=st_a)
+        _, wp_b = ad.new_state(prec)
+        st_b = torch.zeros(3, dtype=torch.int64, device="cuda")
+        guess.traject_guess(ad, net, cfg.dt, inp, wp_b, stride=stride, stats=st_b)
+        torch.cuda.synchronize()
+        assert ad.status() == 0
+        assert torch.equal(st_a, st_b), stride
+        assert torch.equal(wp_a.view(torch.int64), wp_b.view(torch.int64)), stride
+        assert st_b[2].item() == 0
