@@ -40,6 +40,10 @@ TENSOR_FALLBACK_TFLOPS = 1590.0
 # with u, v, w + 4 tracers; traffic grows in proportion to the points, so it
 # scales to the benched tile
 MEASURED_TRAFFIC_PER_POINT = {"traject": 74.25, "sets": 89.77}
+# L1 data-pipe wavefronts (l1tex__data_pipe_lsu_wavefronts.sum) per grid point
+# of each MIXED launch, same capture (384x384x80, u, v, w + 4 tracers); the
+# pipe returns one wavefront per SM cycle, the bound both gather kernels reach
+MEASURED_L1_WAVEFRONTS_PER_POINT = {"traject": 29.74, "sets": 33.56}
 
 
 def peaks():
@@ -380,7 +384,8 @@ def run_product(args):
         "ref32_value": npts * ws / (ms_ref32 * 1e-3), "ref32_ms_per_step": ms_ref32,
         "per_launch_ms": per,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind},
+                     "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,
+                     "l1": l1_roofline(args, per, npts, clk)},
         "step_roofline": {"algorithmic_bytes_per_point": step_bytes / npts,
                           "achieved_gbs": step_bytes / (ms32 * 1e-3) / 1e9,
                           "frac": step_bytes / (ms32 * 1e-3) / 1e9 / hbm},
@@ -393,6 +398,28 @@ def run_product(args):
         print(json.dumps(line))
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def l1_roofline(args, per, npts, clk):
+    """The bound the gather kernels reach: the L1 data pipe, one wavefront per
+    SM cycle.  Wavefronts per grid point from the ncu capture of the small
+    case, times the points of the benched tile, over each launch's measured
+    time, against the SM count times the SM clock sampled during the timed
+    steps (the maximum clock when no sample)."""
+    if args.ntr != 4:
+        return None
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
+    peak = sms * mhz * 1e6
+    out = {"metric": "l1tex__data_pipe_lsu_wavefronts", "unit": "wavefronts/s", "peak": peak,
+           "peak_kind": f"1 wavefront per SM cycle, {sms} SMs at {mhz:g} MHz (sampled)", "kernels": {}}
+    for k, ms in per.items():
+        w = MEASURED_L1_WAVEFRONTS_PER_POINT[k] * npts
+        out["kernels"][k] = {"wavefronts_per_point": MEASURED_L1_WAVEFRONTS_PER_POINT[k],
+                             "achieved": w / (ms * 1e-3), "frac": w / (ms * 1e-3) / peak}
+    dom = max(per, key=per.get)
+    out["kernel"], out["achieved"], out["frac"] = dom, out["kernels"][dom]["achieved"], out["kernels"][dom]["frac"]
+    return out
 
 
 def workload_config(args, ws, decomp=None):
