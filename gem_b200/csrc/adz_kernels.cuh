@@ -20,6 +20,15 @@
 // including this header; the _REF32 values apply to the REF32 instantiations
 // (they default to the others).  The bounds expressions name PREC, the
 // precision template parameter of every kernel that uses them.
+// levels per block of the gather kernels: 1 walks the points in (i, k, j)
+// order, 128 consecutive i per block; 2 or 4 gives every block a tile of
+// 128/TK consecutive i by TK consecutive levels (one warp row per level)
+#ifndef ADZ_TRAJ_TILE_K
+#define ADZ_TRAJ_TILE_K 1
+#endif
+#ifndef ADZ_SET_TILE_K
+#define ADZ_SET_TILE_K 1
+#endif
 #ifndef ADZ_TRAJ_MINB
 #define ADZ_TRAJ_MINB 0
 #endif
@@ -483,26 +492,43 @@ __device__ __forceinline__ void traject_point_tol(const DGrid& g, const TrajArgs
 
 template <int PREC>
 __global__ void ADZ_TRAJ_BOUNDS k_traject(DGrid g, TrajArgs a) {
-  const long long nplane = (long long)g.ni * g.nj;
-  const long long n = nplane * (g.nk - a.k00 + 1);
+#if ADZ_TRAJ_TILE_K > 1
+  constexpr int TK = ADZ_TRAJ_TILE_K, TI = 128 / TK;
+  const int nkp = g.nk - a.k00 + 1;
+  const int nic = (g.ni + TI - 1) / TI, nkg = (nkp + TK - 1) / TK;
+  const long long b = blockIdx.x;
+  const int i = (int)(b % nic) * TI + (threadIdx.x % TI) + 1;
+  const int k = (int)((b / nic) % nkg) * TK + (threadIdx.x / TI) + a.k00;
+  const int j = (int)(b / ((long long)nic * nkg)) + 1;
+  if (i > g.ni || k > g.nk || j > g.nj) return;
+  traject_point<PREC>(g, a, i, j, k);
+#else
+  // points in (i, k, j) order: consecutive blocks walk the levels of one row,
+  // so each source row stays in L2 while every level that reads it runs
+  const int nkp = g.nk - a.k00 + 1;
+  const long long nrow = (long long)g.ni * nkp;
+  const long long n = nrow * g.nj;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t % g.ni) + 1;
-    const int j = (int)((t / g.ni) % g.nj) + 1;
-    const int k = (int)(t / nplane) + a.k00;
+    const int k = (int)((t / g.ni) % nkp) + a.k00;
+    const int j = (int)(t / nrow) + 1;
     traject_point<PREC>(g, a, i, j, k);
   }
+#endif
 }
 
 template <int PREC>
 __global__ void ADZ_TRAJ_BOUNDS k_traject_tol(DGrid g, TrajArgs a, double tol, int maxit, unsigned char* iters,
                                               unsigned long long* stats, GuessStart gs) {
-  const long long nplane = (long long)g.ni * g.nj;
-  const long long n = nplane * (g.nk - a.k00 + 1);
+  // points in (i, k, j) order, as in k_traject
+  const int nkp = g.nk - a.k00 + 1;
+  const long long nrow = (long long)g.ni * nkp;
+  const long long n = nrow * g.nj;
   unsigned long long cnt[3] = {0, 0, 0};
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t % g.ni) + 1;
-    const int j = (int)((t / g.ni) % g.nj) + 1;
-    const int k = (int)(t / nplane) + a.k00;
+    const int k = (int)((t / g.ni) % nkp) + a.k00;
+    const int j = (int)(t / nrow) + 1;
     traject_point_tol<PREC>(g, a, gs, i, j, k, tol, maxit, iters, cnt);
   }
   if (stats) {
@@ -706,12 +732,13 @@ __global__ void __launch_bounds__(256) k_positions(DGrid g, int set, int i0, int
 template <int PREC, bool PERT>
 __global__ void ADZ_SET_BOUNDS k_tricub_set(DGrid g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
                                             SetArgs a, FieldPtrs fp) {
-  const long long nplane = (long long)nx * ny;
-  const long long n = nplane * nz;
+  // points in (i, k, j) order, as in k_traject
+  const long long nrow = (long long)nx * nz;
+  const long long n = nrow * ny;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t % nx) + i0;
-    const int j = (int)((t / nx) % ny) + j0;
-    const int k = (int)(t / nplane) + k0;
+    const int k = (int)((t / nx) % nz) + k0;
+    const int j = (int)(t / nrow) + j0;
     set_point<PREC, false, PERT>(g, set, a, fp, i, j, k);
   }
 }
@@ -724,13 +751,25 @@ template <int PREC, bool PERT>
 __global__ void ADZ_SET_BOUNDS k_tricub_parts(DGrid g, SetArgs a, const __grid_constant__ SetParts sp) {
   const int q = (int)(blockIdx.x % (unsigned)sp.n);
   const SetPart& P = sp.p[q];
+#if ADZ_SET_TILE_K > 1
+  constexpr int TK = ADZ_SET_TILE_K, TI = 128 / TK;
+  const long long b = blockIdx.x / (unsigned)sp.n;
+  const int nic = (P.nx + TI - 1) / TI, nkg = (P.nz + TK - 1) / TK;
+  const int ii = (int)(b % nic) * TI + (threadIdx.x % TI);
+  const int kk = (int)((b / nic) % nkg) * TK + (threadIdx.x / TI);
+  const long long jj = b / ((long long)nic * nkg);
+  if (ii >= P.nx || kk >= P.nz || jj >= P.ny) return;
+  set_point<PREC, false, PERT>(g, P.set, a, P.fp, ii + P.i0, (int)jj + P.j0, kk + P.k0);
+#else
   const long long t = (long long)(blockIdx.x / (unsigned)sp.n) * blockDim.x + threadIdx.x;
-  const long long nplane = (long long)P.nx * P.ny;
-  if (t >= nplane * P.nz) return;
+  // points in (i, k, j) order, as in k_traject
+  const long long nrow = (long long)P.nx * P.nz;
+  if (t >= nrow * P.ny) return;
   const int i = (int)(t % P.nx) + P.i0;
-  const int j = (int)((t / P.nx) % P.ny) + P.j0;
-  const int k = (int)(t / nplane) + P.k0;
+  const int k = (int)((t / P.nx) % P.nz) + P.k0;
+  const int j = (int)(t / nrow) + P.j0;
   set_point<PREC, false, PERT>(g, P.set, a, P.fp, i, j, k);
+#endif
 }
 
 // BICUBH_QV fields at position set t (adz_interp_hlt.F90:113-116 with
@@ -784,12 +823,13 @@ __device__ __forceinline__ void qv_point(const DGrid& g, const SetArgs& a, const
 template <int PREC, bool PERT>
 __global__ void ADZ_QV_BOUNDS k_qv_set(DGrid g, int i0, int nx, int j0, int ny, int k0, int nz, SetArgs a,
                                                 FieldPtrs fp) {
-  const long long nplane = (long long)nx * ny;
-  const long long n = nplane * nz;
+  // points in (i, k, j) order, as in k_traject
+  const long long nrow = (long long)nx * nz;
+  const long long n = nrow * ny;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t % nx) + i0;
-    const int j = (int)((t / nx) % ny) + j0;
-    const int k = (int)(t / nplane) + k0;
+    const int k = (int)((t / nx) % nz) + k0;
+    const int j = (int)(t / nrow) + j0;
     qv_point<PREC, PERT>(g, a, fp, i, j, k);
   }
 }
@@ -1053,8 +1093,15 @@ cudaError_t launch_inittraj(const DGrid& g, float* pxyzm, double* wpxyz, cudaStr
 
 template <int PREC>
 cudaError_t launch_traject(const DGrid& g, const TrajArgs& a, cudaStream_t s) {
+#if ADZ_TRAJ_TILE_K > 1
+  constexpr int TK = ADZ_TRAJ_TILE_K, TI = 128 / TK;
+  const long long nb = (long long)((g.ni + TI - 1) / TI) * ((g.nk - a.k00 + 1 + TK - 1) / TK) * g.nj;
+  if (nb > 0x7fffffffLL) return cudaErrorInvalidValue;
+  k_traject<PREC><<<(unsigned)nb, 128, 0, s>>>(g, a);
+#else
   const long long n = (long long)g.ni * g.nj * (g.nk - a.k00 + 1);
   k_traject<PREC><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, a);
+#endif
   return cudaGetLastError();
 }
 
@@ -1090,7 +1137,12 @@ cudaError_t launch_tricub_parts(const DGrid& g, const SetArgs& a, const SetParts
   if (sp.n < 1 || sp.n > kMaxParts) return cudaErrorInvalidValue;
   long long most = 0;  // blocks of the largest part
   for (int q = 0; q < sp.n; q++) {
+#if ADZ_SET_TILE_K > 1
+    constexpr int TK = ADZ_SET_TILE_K, TI = 128 / TK;
+    const long long n = (long long)((sp.p[q].nx + TI - 1) / TI) * ((sp.p[q].nz + TK - 1) / TK) * sp.p[q].ny * 128;
+#else
     const long long n = (long long)sp.p[q].nx * sp.p[q].ny * sp.p[q].nz;
+#endif
     most = n > most ? n : most;
   }
   const long long blocks = (most + 127) / 128 * sp.n;
