@@ -966,18 +966,21 @@ __global__ void __launch_bounds__(128, MINB) k_batch(const __grid_constant__ Bat
         for (long long e = item.start + threadIdx.x; e < end; e += blockDim.x)
           prepare_cell<PREC>(C.g, (const F*)C.uu, (const F*)C.vv, (const F*)C.ww, (F*)C.ta.uvw_d, e);
       } else if (item.phase == 1) {
-        const long long plane = (long long)C.g.ni * C.g.nj;
+        // points in (i, k, j) order, as in k_traject
+        const int nkp = C.g.nk - C.ta.k00 + 1;
+        const long long nrow = (long long)C.g.ni * nkp;
         for (long long t = item.start + threadIdx.x; t < end; t += blockDim.x) {
-          const int i = (int)(t % C.g.ni) + 1, j = (int)((t / C.g.ni) % C.g.nj) + 1;
-          const int k = (int)(t / plane) + C.ta.k00;
+          const int i = (int)(t % C.g.ni) + 1, k = (int)((t / C.g.ni) % nkp) + C.ta.k00;
+          const int j = (int)(t / nrow) + 1;
           traject_point<PREC, true>(C.g, C.ta, i, j, k);
         }
       } else {
-        const int nx = srange[1], ny = srange[3];
-        const long long plane = (long long)nx * ny;
+        // points in (i, k, j) order, as in k_tricub_parts
+        const int nx = srange[1], nz = C.g.nk - srange[4] + 1;
+        const long long nrow = (long long)nx * nz;
         for (long long t = item.start + threadIdx.x; t < end; t += blockDim.x) {
-          const int i = (int)(t % nx) + srange[0], j = (int)((t / nx) % ny) + srange[2];
-          const int k = (int)(t / plane) + srange[4];
+          const int i = (int)(t % nx) + srange[0], k = (int)((t / nx) % nz) + srange[4];
+          const int j = (int)(t / nrow) + srange[2];
           set_point<PREC, true>(C.g, sset, C.sa, sfp, i, j, k);
         }
       }
@@ -1020,18 +1023,21 @@ __device__ __forceinline__ void batch_phase_body(const BatchParams& P, const BDo
       for (long long e = item.start + threadIdx.x; e < end; e += blockDim.x)
         prepare_cell<PREC>(C.g, (const F*)C.uu, (const F*)C.vv, (const F*)C.ww, (F*)C.ta.uvw_d, e);
     } else if (PH == 1) {
-      const long long plane = (long long)C.g.ni * C.g.nj;
+      // points in (i, k, j) order, as in k_traject
+      const int nkp = C.g.nk - C.ta.k00 + 1;
+      const long long nrow = (long long)C.g.ni * nkp;
       for (long long t = item.start + threadIdx.x; t < end; t += blockDim.x) {
-        const int i = (int)(t % C.g.ni) + 1, j = (int)((t / C.g.ni) % C.g.nj) + 1;
-        const int k = (int)(t / plane) + C.ta.k00;
+        const int i = (int)(t % C.g.ni) + 1, k = (int)((t / C.g.ni) % nkp) + C.ta.k00;
+        const int j = (int)(t / nrow) + 1;
         traject_point<PREC, false>(C.g, C.ta, i, j, k);
       }
     } else {
-      const int nx = srange[1], ny = srange[3];
-      const long long plane = (long long)nx * ny;
+      // points in (i, k, j) order, as in k_tricub_parts
+      const int nx = srange[1], nz = C.g.nk - srange[4] + 1;
+      const long long nrow = (long long)nx * nz;
       for (long long t = item.start + threadIdx.x; t < end; t += blockDim.x) {
-        const int i = (int)(t % nx) + srange[0], j = (int)((t / nx) % ny) + srange[2];
-        const int k = (int)(t / plane) + srange[4];
+        const int i = (int)(t % nx) + srange[0], k = (int)((t / nx) % nz) + srange[4];
+        const int j = (int)(t / nrow) + srange[2];
         set_point<PREC, false>(C.g, sset, C.sa, sfp, i, j, k);
       }
     }
