@@ -979,7 +979,53 @@ def measure_guess(args, timed, ws, rank):
                                  "frac": tf / peak_tf, "flops_per_point": flops / n,
                                  "note": "stride 1; includes the departure-wind preparation launch"}
     res["speedup_learned_vs_plain"] = res["cold"]["speedup_best_learned_vs_plain"]
+    del ad, inp, prev
+    torch.cuda.empty_cache()
+    res["composite_cold_step"] = measure_composite(args, timed, ws, rank, net)
     return res
+
+
+def measure_composite(args, timed, ws, rank, net):
+    """The whole first step of a run (no previous departure points), u, v, w
+    and 4 cosine-bell tracers on the learned-guess flow: the plain FP64
+    drop-in as the reference runs it (arrival-point start, max(6, itraj)
+    fixed updates, then every set) against the mixed-precision step with the
+    learned start on every 16th point and the iteration to the tolerance,
+    then every set."""
+    from gem_b200 import adz, guess, synth
+    ni, nj, nk = args.size
+    cfg = synth.config_cold(ni, nj, nk, seed=tile_seed(rank))
+    cfg.ntracers, cfg.tracer_kind = 4, "bells"
+    inp64 = synth.make_inputs(cfg, device="cuda", dtype=torch.float64)
+    K, W = max(3, min(args.steps, 10)), args.warmup
+    out = {"workload": f"first step of a run, {ni}x{nj}x{nk}, u,v,w + 4 cosine-bell tracers, dt={cfg.dt:g} s, "
+                       "vertical-wind noise 0.02 m/s"}
+    for name, prec in (("fp64_fixed6", adz.FP64), ("mixed_learned_s16", adz.MIXED)):
+        dt = adz._field_dtype(prec)
+        data = {k: (v.to(dt) if torch.is_tensor(v) else [t.to(dt) for t in v]) for k, v in inp64.items()}
+        ad = adz.Adz.from_config(cfg)
+        px, wp = ad.new_state(prec)
+        outs = [torch.zeros(ad.ext_shape, dtype=dt, device="cuda") for _ in range(3 + len(data["tracers"]))]
+        srcs = [data["src_u"], data["src_v"], data["src_w"]] + data["tracers"]
+        mono = [0, 0, 0] + [0] * len(data["tracers"])
+        nf = [0, 1, 1, 1 + len(data["tracers"])]
+
+        def step(ad=ad, prec=prec, data=data, px=px, wp=wp, srcs=srcs, outs=outs, name=name):
+            if name.startswith("fp64"):
+                ad.adz_inittraj(prec, px, wp)
+                ad.adz_traject(prec, cfg.dt, data, px, wp)
+            else:
+                guess.traject_guess(ad, net, cfg.dt, data, wp, stride=16)
+            ad.adz_tricub_sets(prec, nf, srcs, outs, mono)
+        ms, _ = timed(step, K, W)
+        if ad.status() != 0:
+            raise RuntimeError("device status set during the first-step measurement")
+        out[name + "_ms"] = ms
+        out[name + "_value"] = cfg.npoints * ws / (ms * 1e-3)
+        del data, ad, outs, srcs, step
+        torch.cuda.empty_cache()
+    out["speedup"] = out["fp64_fixed6_ms"] / out["mixed_learned_s16_ms"]
+    return out
 
 
 def run_reference(args):

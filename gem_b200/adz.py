@@ -101,6 +101,8 @@ def lib() -> C.CDLL:
         L.adzc_tricub_sets.argtypes = [vp, i, vp, vp, vp, vp, vp]
         L.adzc_interp_traj.argtypes = [vp, i, i, vp, vp]
         L.adzc_bc_lam_zlf.argtypes = [vp, i, i, i, vp, vp, vp]
+        L.adzc_traject_region.argtypes = [vp, i, d, i] + [vp] * 8 + [i, vp]
+        L.adzc_tricub_sets_region.argtypes = [vp, i, vp, vp, vp, vp, i, vp]
         L.adzc_step_noalloc.argtypes = [vp, i, d, i] + [vp] * 8 + [vp, vp, vp, vp, vp]
         L.adzc_batch_create.argtypes = [i, i, vp, C.POINTER(vp)]
         L.adzc_batch_tune.argtypes = [vp, vp]
@@ -299,6 +301,25 @@ class Adz:
                                   *(winds[k].data_ptr() for k in ("uu_ext", "vv_ext", "ww_ext", "ut0", "vt0", "zdt0")),
                                   None if pxyzm is None else pxyzm.data_ptr(), wpxyz.data_ptr(), _stream(stream)),
                "adzc_traject")
+
+    def adz_traject_region(self, prec: int, dt: float, winds: dict, pxyzm, wpxyz, region: int, niter: int = 0,
+                           stream=None):
+        """adzc_traject_region: 1 the interior of the tile, 2 the band around
+        it (after the winds' halos arrived); 0 the whole tile."""
+        self._zdt0 = winds["zdt0"]
+        _check(lib().adzc_traject_region(self.h, prec, float(dt), int(niter),
+                                         *(winds[k].data_ptr() for k in ("uu_ext", "vv_ext", "ww_ext", "ut0", "vt0",
+                                                                         "zdt0")),
+                                         None if pxyzm is None else pxyzm.data_ptr(), wpxyz.data_ptr(), int(region),
+                                         _stream(stream)), "adzc_traject_region")
+
+    def adz_tricub_sets_region(self, prec: int, nfields, srcs, dsts, mono, region: int, stream=None):
+        """adzc_tricub_sets_region: the position sets' interior (1) or band (2)."""
+        nf = (C.c_int * 4)(*nfields)
+        mono_arr = (C.c_int * len(srcs))(*mono) if mono is not None else None
+        _check(lib().adzc_tricub_sets_region(self.h, prec, nf, C.cast(_ptr_array(srcs), C.c_void_p),
+                                             C.cast(_ptr_array(dsts), C.c_void_p), mono_arr, int(region),
+                                             _stream(stream)), "adzc_tricub_sets_region")
 
     def set_slt_winds(self, uslt=None, vslt=None):
         """Adz_uslt, Adz_vslt (nj, ni) device tensors of the field type for

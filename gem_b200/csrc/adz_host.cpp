@@ -321,6 +321,11 @@ struct adzc_handle {
   // perturbation of every interpolation while set (adzc_rhs_perturbation)
   const void* pert = nullptr;
   int pert_ld = 0;
+  // a trajectory split into interior and band (adzc_traject_region): the
+  // iteration state its first part ran with, -1 when none is pending
+  int pending_prec = -1;
+  int pending_niter = 0;
+  int pending_cold = 0;
 };
 
 static int build_search(const std::vector<double>& z, int nk, double sig, const std::vector<double>& delz,
@@ -743,6 +748,124 @@ extern "C" int adzc_tricub(adzc_handle* h, int prec, int set, int nfields, const
   return ADZC_OK;
 }
 
+namespace {
+
+struct Box {
+  int i0, nx, j0, ny;
+};
+
+// the interior of a tile (points at least m from every side that has a
+// neighbour tile, i.e. is not a LAM edge) and the band around it, as boxes
+// in local point indices; a box is skipped when empty
+int region_boxes(const adzc_handle* h, int region, int m, Box* out) {
+  const adzc_grid& g = h->g;
+  const int ni = g.ni, nj = g.nj;
+  const int mw = g.west ? 0 : m, me = g.east ? 0 : m, ms = g.south ? 0 : m, mn = g.north ? 0 : m;
+  int n = 0;
+  auto add = [&](int i0, int i1, int j0, int j1) {
+    if (i1 >= i0 && j1 >= j0) out[n++] = Box{i0, i1 - i0 + 1, j0, j1 - j0 + 1};
+  };
+  if (region == 1) {
+    add(1 + mw, ni - me, 1 + ms, nj - mn);
+    return n;
+  }
+  // band: west and east strips over every row, south and north strips between them
+  const int xw1 = std::min(mw, ni), xe0 = std::max(mw + 1, ni - me + 1);
+  add(1, xw1, 1, nj);
+  add(xe0, ni, 1, nj);
+  const int ys1 = std::min(ms, nj), yn0 = std::max(ms + 1, nj - mn + 1);
+  add(xw1 + 1, xe0 - 1, 1, ys1);
+  add(xw1 + 1, xe0 - 1, yn0, nj);
+  return n;
+}
+
+// a box intersected with a horizontal range (i0..i1, j0..j1)
+bool clip_box(const Box& b, int i0, int i1, int j0, int j1, Box* out) {
+  const int a0 = std::max(b.i0, i0), a1 = std::min(b.i0 + b.nx - 1, i1);
+  const int c0 = std::max(b.j0, j0), c1 = std::min(b.j0 + b.ny - 1, j1);
+  if (a1 < a0 || c1 < c0) return false;
+  *out = Box{a0, a1 - a0 + 1, c0, c1 - c0 + 1};
+  return true;
+}
+
+cudaError_t dispatch_traject_box(int prec, const adz::DGrid& g, const adz::TrajArgs& a, const Box& b,
+                                 cudaStream_t s) {
+  switch (prec) {
+    case ADZC_REF32: return adz::launch_traject_box<adz::kRef32>(g, a, b.i0, b.nx, b.j0, b.ny, s);
+    case ADZC_FP64: return adz::launch_traject_box<adz::kFp64>(g, a, b.i0, b.nx, b.j0, b.ny, s);
+    default: return adz::launch_traject_box<adz::kMixed>(g, a, b.i0, b.nx, b.j0, b.ny, s);
+  }
+}
+cudaError_t dispatch_prepare_box(int prec, const adz::DGrid& g, const void* uu, const void* vv, const void* ww,
+                                 void* o, int ci0, int nci, int cj0, int ncj, cudaStream_t s) {
+  switch (prec) {
+    case ADZC_REF32: return adz::launch_prepare_box<adz::kRef32>(g, uu, vv, ww, o, ci0, nci, cj0, ncj, s);
+    case ADZC_FP64: return adz::launch_prepare_box<adz::kFp64>(g, uu, vv, ww, o, ci0, nci, cj0, ncj, s);
+    default: return adz::launch_prepare_box<adz::kMixed>(g, uu, vv, ww, o, ci0, nci, cj0, ncj, s);
+  }
+}
+
+}  // namespace
+
+extern "C" int adzc_traject_region(adzc_handle* h, int prec, double dt, int niter, const void* uu_ext,
+                                   const void* vv_ext, const void* ww_ext, const void* ut0, const void* vt0,
+                                   const void* zdt0, void* pxyzm, double* wpxyz, int region, void* stream) {
+  if (region == 0)
+    return adzc_traject(h, prec, dt, niter, uu_ext, vv_ext, ww_ext, ut0, vt0, zdt0, pxyzm, wpxyz, stream);
+  AdzRange nvtx_range(region == 1 ? "adz_traject interior" : "adz_traject band");
+  if (!h || !check_prec(prec) || !uu_ext || !vv_ext || !ww_ext || !ut0 || !vt0 || !zdt0 || !wpxyz ||
+      (prec == ADZC_REF32 && !pxyzm) || (region != 1 && region != 2) || !std::isfinite(dt))
+    return fail(ADZC_ERR_ARG);
+  if (region == 2 && h->pending_prec != prec) return fail(ADZC_ERR_ARG);  // the interior first
+  const cudaStream_t s = (cudaStream_t)stream;
+  const adz::DGrid& D = h->dg;
+  const size_t fb = field_bytes(prec);
+  if (ensure(&h->d_uvw, &h->uvw_bytes, adz::uvw_values(prec) * fb * (size_t)D.nij * D.nk) != ADZC_OK ||
+      ensure(&h->d_wdep, &h->wdep_bytes, fb * (size_t)D.ni * D.nj * D.nk) != ADZC_OK)
+    return fail(ADZC_ERR_ALLOC);
+  if (region == 1) {
+    // every cell; the halo cells are prepared again once their winds arrive
+    ADZ_CK(dispatch_prepare(prec, D, uu_ext, vv_ext, ww_ext, h->d_uvw, s));
+    h->pending_prec = prec;
+    h->pending_niter = niter > 0 ? niter : h->niter;
+    h->pending_cold = h->cold;
+  } else {
+    // the halo frame of the extended array: columns outside 1..ni, rows outside 1..nj
+    const int hx = h->info.halox, hy = h->info.haloy, nit = D.nit, njt = D.njt;
+    ADZ_CK(dispatch_prepare_box(prec, D, uu_ext, vv_ext, ww_ext, h->d_uvw, 0, nit, 0, hy, s));
+    ADZ_CK(dispatch_prepare_box(prec, D, uu_ext, vv_ext, ww_ext, h->d_uvw, 0, nit, njt - hy, hy, s));
+    ADZ_CK(dispatch_prepare_box(prec, D, uu_ext, vv_ext, ww_ext, h->d_uvw, 0, hx, hy, njt - 2 * hy, s));
+    ADZ_CK(dispatch_prepare_box(prec, D, uu_ext, vv_ext, ww_ext, h->d_uvw, nit - hx, hx, hy, njt - 2 * hy, s));
+  }
+  adz::TrajArgs a{};
+  a.uvw_d = h->d_uvw;
+  a.ut0 = ut0;
+  a.vt0 = vt0;
+  a.zdt0 = zdt0;
+  a.pxyzm = (float*)pxyzm;
+  a.wpxyz = wpxyz;
+  a.wdep = h->d_wdep;
+  a.niter = h->pending_niter;
+  a.cold = h->pending_cold;
+  a.k00 = (D.k0 > 1) ? 1 : D.k0m;  // B/adz_traject.F90:63-64
+  a.dt = dt_split(h->g, dt);
+  // a departure stencil reaches maxcfl + 1 cells, the arrival winds' averaging 2
+  Box boxes[4];
+  const int nb = region_boxes(h, region, std::max(1, h->g.maxcfl) + 3, boxes);
+  for (int q = 0; q < nb; q++) ADZ_CK(dispatch_traject_box(prec, D, a, boxes[q], s));
+  if (region == 2) {
+    h->pending_prec = -1;
+    h->niter = std::max(1, h->g.itraj);  // B/adz_traject.F90:120
+    h->cold = 0;
+    h->last_prec = prec;
+    h->wpxyz = wpxyz;
+    h->pxyzm = (const float*)pxyzm;
+    h->zdt0 = zdt0;
+    h->dt = a.dt;
+  }
+  return ADZC_OK;
+}
+
 extern "C" int adzc_interp_traj(adzc_handle* h, int prec, int set, void* pos, void* stream) {
   AdzRange nvtx_range("adz_interp_traj");
   if (!h || !check_prec(prec) || set < 0 || set > ADZC_SET_B || !pos) return fail(ADZC_ERR_ARG);
@@ -834,6 +957,86 @@ extern "C" int adzc_bc_lam_zlf(adzc_handle* h, int prec, int setup, int ntr, voi
     }
     ADZ_CK(prec == ADZC_FP64 ? adz::launch_bc_zlf<double>(m, setup, fp, s) : adz::launch_bc_zlf<float>(m, setup, fp, s));
   }
+  return ADZC_OK;
+}
+
+extern "C" int adzc_tricub_sets_region(adzc_handle* h, int prec, const int* nfields, const void* const* srcs,
+                                       void* const* dsts, const int* mono, int region, void* stream) {
+  if (region == 0) return adzc_tricub_sets(h, prec, nfields, srcs, dsts, mono, stream);
+  AdzRange nvtx_range(region == 1 ? "ADZ_MAIN sets interior" : "ADZ_MAIN sets band");
+  if (!h || !check_prec(prec) || !nfields || (region != 1 && region != 2)) return fail(ADZC_ERR_ARG);
+  if (h->last_prec != prec || !h->wpxyz) return fail(ADZC_ERR_ARG);
+  int ntot = 0;
+  for (int q = 0; q < 4; q++) {
+    if (nfields[q] < 0) return fail(ADZC_ERR_ARG);
+    ntot += nfields[q];
+  }
+  if (ntot == 0) return ADZC_OK;
+  if (!srcs || !dsts) return fail(ADZC_ERR_ARG);
+  for (int f = 0, set = 0, left = nfields[0]; f < ntot; f++, left--) {
+    while (left == 0) left = nfields[++set];
+    if (!srcs[f] || !dsts[f] || !mono_ok(mono ? mono[f] : 0, set)) return fail(ADZC_ERR_ARG);
+  }
+  // the position sets read Adz_wpxyz up to 2 points away (Adz_pmu, Adz_pmv)
+  Box rb[4];
+  const int nb = region_boxes(h, region, 2, rb);
+  const adz::SetArgs a = set_args(h);
+  const adz::DGrid& D = h->dg;
+  const cudaStream_t s = (cudaStream_t)stream;
+  adz::SetParts sp{};
+  int f0 = 0;
+  for (int set = 0; set < 4; set++) {
+    const int nf = nfields[set];
+    int i0, nx, j0, ny, k0, nz;
+    set_box(h, set, i0, nx, j0, ny, k0, nz);
+    for (int q = 0; q < nb && nf > 0 && nx > 0 && ny > 0 && nz > 0; q++) {
+      Box c;
+      if (!clip_box(rb[q], i0, i0 + nx - 1, j0, j0 + ny - 1, &c)) continue;
+      for (int qv = 0; qv < 2; qv++) {  // tricubic field groups, then BICUBH_QV ones
+        adz::FieldPtrs fp{};
+        for (int f = f0; f < f0 + nf; f++) {
+          const int mv = mono ? mono[f] : 0;
+          if (((mv & ADZC_QV) != 0) != (qv == 1)) continue;
+          const int k = fp.nf++;
+          fp.src[k] = srcs[f];
+          fp.dst[k] = dsts[f];
+          if ((mv & 3) != 0) fp.mono_mask |= 1u << k;
+          if ((mv & 3) == 1) fp.clip_mask |= 1u << k;
+          const bool last = f == f0 + nf - 1;
+          if (fp.nf < adz::kMaxFields && !last) continue;
+          if (qv) {
+            ADZ_CK(dispatch_qv(prec, D, c.i0, c.nx, c.j0, c.ny, k0, nz, a, fp, s));
+          } else {
+            if (sp.n == adz::kMaxParts) {
+              ADZ_CK(dispatch_parts(prec, D, a, sp, s));
+              sp = adz::SetParts{};
+            }
+            adz::SetPart& P = sp.p[sp.n++];
+            P.fp = fp;
+            P.set = set;
+            P.i0 = c.i0; P.nx = c.nx; P.j0 = c.j0; P.ny = c.ny; P.k0 = k0; P.nz = nz;
+          }
+          fp = adz::FieldPtrs{};
+        }
+        if (fp.nf > 0) {  // a group closed by a field of the other kind
+          if (qv) {
+            ADZ_CK(dispatch_qv(prec, D, c.i0, c.nx, c.j0, c.ny, k0, nz, a, fp, s));
+          } else {
+            if (sp.n == adz::kMaxParts) {
+              ADZ_CK(dispatch_parts(prec, D, a, sp, s));
+              sp = adz::SetParts{};
+            }
+            adz::SetPart& P = sp.p[sp.n++];
+            P.fp = fp;
+            P.set = set;
+            P.i0 = c.i0; P.nx = c.nx; P.j0 = c.j0; P.ny = c.ny; P.k0 = k0; P.nz = nz;
+          }
+        }
+      }
+    }
+    f0 += nf;
+  }
+  if (sp.n > 0) ADZ_CK(dispatch_parts(prec, D, a, sp, s));
   return ADZC_OK;
 }
 

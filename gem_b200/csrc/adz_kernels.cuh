@@ -183,6 +183,22 @@ __global__ void __launch_bounds__(256) k_prepare(DGrid g, const typename Types<P
     prepare_cell<PREC>(g, uu, vv, ww, uvw_d, e);
 }
 
+// departure winds of the extended cells in columns [ci0, ci0+nci) and rows
+// [cj0, cj0+ncj) of the extended array (0-based), every level: the strips of
+// the halo frame once its values have arrived
+template <int PREC>
+__global__ void __launch_bounds__(256) k_prepare_box(DGrid g, const typename Types<PREC>::F* __restrict__ uu,
+                                                     const typename Types<PREC>::F* __restrict__ vv,
+                                                     const typename Types<PREC>::F* __restrict__ ww,
+                                                     typename Types<PREC>::F* __restrict__ uvw_d, int ci0, int nci,
+                                                     int cj0, int ncj) {
+  const long long nbox = (long long)nci * ncj, n = nbox * g.nk;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int ci = ci0 + (int)(t % nci), cj = cj0 + (int)((t / nci) % ncj), k = (int)(t / nbox);
+    prepare_cell<PREC>(g, uu, vv, ww, uvw_d, (long long)k * g.nij + (long long)cj * g.nit + ci);
+  }
+}
+
 // ---------------------------------------------------------------------------
 template <int PREC>
 __global__ void __launch_bounds__(256) k_inittraj(DGrid g, float* __restrict__ pxyzm, double* __restrict__ wpxyz) {
@@ -515,6 +531,22 @@ __global__ void ADZ_TRAJ_BOUNDS k_traject(DGrid g, TrajArgs a) {
     traject_point<PREC>(g, a, i, j, k);
   }
 #endif
+}
+
+// the trajectory of the points of a box of the tile (i0..i0+nx-1,
+// j0..j0+ny-1, levels from k00), points in (i, k, j) order: the interior
+// and the band of a schedule that overlaps the halo exchange
+template <int PREC>
+__global__ void ADZ_TRAJ_BOUNDS k_traject_box(DGrid g, TrajArgs a, int i0, int nx, int j0, int ny) {
+  const int nkp = g.nk - a.k00 + 1;
+  const long long nrow = (long long)nx * nkp;
+  const long long n = nrow * ny;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nx) + i0;
+    const int k = (int)((t / nx) % nkp) + a.k00;
+    const int j = (int)(t / nrow) + j0;
+    traject_point<PREC>(g, a, i, j, k);
+  }
 }
 
 template <int PREC>
@@ -1112,6 +1144,25 @@ cudaError_t launch_traject(const DGrid& g, const TrajArgs& a, cudaStream_t s) {
 }
 
 template <int PREC>
+cudaError_t launch_traject_box(const DGrid& g, const TrajArgs& a, int i0, int nx, int j0, int ny, cudaStream_t s) {
+  const long long n = (long long)nx * ny * (g.nk - a.k00 + 1);
+  if (n <= 0) return cudaSuccess;
+  k_traject_box<PREC><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, a, i0, nx, j0, ny);
+  return cudaGetLastError();
+}
+
+template <int PREC>
+cudaError_t launch_prepare_box(const DGrid& g, const void* uu, const void* vv, const void* ww, void* uvw_d, int ci0,
+                               int nci, int cj0, int ncj, cudaStream_t s) {
+  using F = typename Types<PREC>::F;
+  const long long n = (long long)nci * ncj * g.nk;
+  if (n <= 0) return cudaSuccess;
+  k_prepare_box<PREC><<<grid_for(n, 256), 256, 0, s>>>(g, (const F*)uu, (const F*)vv, (const F*)ww, (F*)uvw_d, ci0,
+                                                       nci, cj0, ncj);
+  return cudaGetLastError();
+}
+
+template <int PREC>
 cudaError_t launch_traject_tol(const DGrid& g, const TrajArgs& a, double tol, int maxit, unsigned char* iters,
                                unsigned long long* stats, cudaStream_t s, const GuessStart& gs) {
   const long long n = (long long)g.ni * g.nj * (g.nk - a.k00 + 1);
@@ -1252,6 +1303,9 @@ int batch_resident_blocks(int variant) {
   template cudaError_t launch_prepare<P>(const DGrid&, const void*, const void*, const void*, void*, cudaStream_t); \
   template cudaError_t launch_inittraj<P>(const DGrid&, float*, double*, cudaStream_t);                            \
   template cudaError_t launch_traject<P>(const DGrid&, const TrajArgs&, cudaStream_t);                             \
+  template cudaError_t launch_traject_box<P>(const DGrid&, const TrajArgs&, int, int, int, int, cudaStream_t);      \
+  template cudaError_t launch_prepare_box<P>(const DGrid&, const void*, const void*, const void*, void*, int, int,  \
+                                             int, int, cudaStream_t);                                               \
   template cudaError_t launch_traject_tol<P>(const DGrid&, const TrajArgs&, double, int, unsigned char*,           \
                                              unsigned long long*, cudaStream_t, const GuessStart&);                \
   template cudaError_t launch_tricub_set<P>(const DGrid&, int, int, int, int, int, int, int, const SetArgs&,       \

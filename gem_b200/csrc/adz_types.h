@@ -137,6 +137,11 @@ template <int PREC>
 cudaError_t launch_prepare(const DGrid& g, const void* uu, const void* vv, const void* ww, void* uvw_d,
                            cudaStream_t s);
 template <int PREC>
+cudaError_t launch_traject_box(const DGrid& g, const TrajArgs& a, int i0, int nx, int j0, int ny, cudaStream_t s);
+template <int PREC>
+cudaError_t launch_prepare_box(const DGrid& g, const void* uu, const void* vv, const void* ww, void* uvw_d, int ci0,
+                               int nci, int cj0, int ncj, cudaStream_t s);
+template <int PREC>
 cudaError_t launch_positions(const DGrid& g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
                              const SetArgs& a, void* pos, cudaStream_t s);
 template <int PREC>

@@ -152,20 +152,32 @@ class HaloExchange:
         A._check(A.lib().adzc_halo_unpack(C.byref(self.desc), self.narrays, self._arrays(arrays),
                                           self.recv.data_ptr(), A._stream(stream)), "adzc_halo_unpack")
 
-    def transfer(self):
+    def start(self):
         """Send segment q to the neighbour in slot q and receive segment q
-        from it, for every neighbour, as one batch of point-to-point ops.
-        Two tiles of a non-periodic grid are neighbours in one direction
-        only, so every pair of ranks exchanges one message each way."""
+        from it, for every neighbour, as one batch of point-to-point ops,
+        without waiting: the requests to give to ``finish``.  Two tiles of a
+        non-periodic grid are neighbours in one direction only, so every pair
+        of ranks exchanges one message each way.  With NCCL the transfer runs
+        on NCCL's stream, ordered after the work already on the current
+        stream; work enqueued next on the current stream runs beside it."""
         ops = []
         for q, peer in enumerate(self.peers):
             if peer is None or self.offsets[q + 1] == self.offsets[q]:
                 continue
             ops.append(dist.P2POp(dist.isend, self.segment(self.send, q), peer, self.group))
             ops.append(dist.P2POp(dist.irecv, self.segment(self.recv, q), peer, self.group))
-        if ops:
-            for req in dist.batch_isend_irecv(ops):
-                req.wait()
+        return dist.batch_isend_irecv(ops) if ops else []
+
+    @staticmethod
+    def finish(reqs):
+        """Wait for a transfer started by ``start`` (with NCCL: the current
+        stream waits for it; with gloo: the host does)."""
+        for req in reqs:
+            req.wait()
+
+    def transfer(self):
+        """``start`` then ``finish``."""
+        self.finish(self.start())
 
     def exchange(self, arrays):
         """pack, transfer, unpack on the current stream (the one the
@@ -207,7 +219,14 @@ class TiledStep:
 
     Packing, unpacking and the step run on the current CUDA stream; the
     transfers are torch.distributed point-to-point batches in the
-    process group ``group``."""
+    process group ``group``.
+
+    With ``overlap`` (the default) each exchange runs beside the part of the
+    step that needs none of its values (adzc_traject_region,
+    adzc_tricub_sets_region): the winds' and sources' exchange beside the
+    trajectory of the tile's interior, the exchange of wpxyz beside the
+    interior's position sets; the band around the interior follows each
+    exchange.  The results are those of the plain schedule bit for bit."""
 
     def __init__(self, decomp: Decomposition, rank: int, ad: A.Adz, prec: int, ntracers: int, device="cuda",
                  group=None):
@@ -215,11 +234,27 @@ class TiledStep:
         self.ex = ext_exchange(decomp, rank, ad, A._field_dtype(prec), len(WIND_KEYS) + 3 + ntracers, device, group)
         self.exw = wpxyz_exchange(decomp, rank, ad, device, group)
 
-    def __call__(self, dt, winds, fields, tracers, pxyzm, wpxyz, outs, tr_outs, mono, niter=0):
+    def __call__(self, dt, winds, fields, tracers, pxyzm, wpxyz, outs, tr_outs, mono, niter=0, overlap=True):
         srcs = [fields["src_u"], fields["src_v"], fields["src_w"]] + list(tracers)
-        self.ex.exchange([winds[k] for k in WIND_KEYS] + srcs)
-        self.ad.adz_traject(self.prec, dt, winds, pxyzm, wpxyz, niter)
-        self.exw.exchange([wpxyz])
+        arrays = [winds[k] for k in WIND_KEYS] + srcs
         dsts = [outs["u"], outs["v"], outs["w"]] + list(tr_outs)
         monos = [0, 0, 0] + [1 if mono else 0] * len(tracers)
-        self.ad.adz_tricub_sets(self.prec, [0, 1, 1, 1 + len(tracers)], srcs, dsts, monos)
+        nf = [0, 1, 1, 1 + len(tracers)]
+        if not overlap:
+            self.ex.exchange(arrays)
+            self.ad.adz_traject(self.prec, dt, winds, pxyzm, wpxyz, niter)
+            self.exw.exchange([wpxyz])
+            self.ad.adz_tricub_sets(self.prec, nf, srcs, dsts, monos)
+            return
+        self.ex.pack(arrays)
+        reqs = self.ex.start()
+        self.ad.adz_traject_region(self.prec, dt, winds, pxyzm, wpxyz, 1, niter)
+        self.ex.finish(reqs)
+        self.ex.unpack(arrays)
+        self.ad.adz_traject_region(self.prec, dt, winds, pxyzm, wpxyz, 2, niter)
+        self.exw.pack([wpxyz])
+        reqs = self.exw.start()
+        self.ad.adz_tricub_sets_region(self.prec, nf, srcs, dsts, monos, 1)
+        self.exw.finish(reqs)
+        self.exw.unpack([wpxyz])
+        self.ad.adz_tricub_sets_region(self.prec, nf, srcs, dsts, monos, 2)

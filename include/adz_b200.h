@@ -263,6 +263,26 @@ int adzc_bc_lam_flux(adzc_handle *h, int prec, int ntr, const void *const *srcs,
 int adzc_tricub_sets(adzc_handle *h, int prec, const int *nfields, const void *const *srcs, void *const *dsts,
                      const int *mono, void *stream);
 
+/* The step in two parts, for a tile of a decomposed domain whose halo
+ * exchanges should overlap its own computation (B/dynstep.F90:52-53 and
+ * B/adz_traject.F90:121-122 exchange before the whole trajectory and before
+ * the whole interpolation).  region 0 is the whole tile (adzc_traject,
+ * adzc_tricub_sets); region 1 the interior: the points at least maxcfl+3
+ * (trajectory) or 2 (position sets) from every side that has a neighbour
+ * tile, which read no halo cell; region 2 the band around it.  A caller
+ * starts the exchange of the winds and sources, runs region 1 of the
+ * trajectory (it prepares the departure winds of every cell), completes the
+ * exchange, runs region 2 (it prepares the halo cells again from the winds
+ * that arrived); then starts the exchange of wpxyz, runs region 1 of the
+ * sets, completes it and runs region 2.  Together the two regions give the
+ * results of the whole-tile calls bit for bit.  adzc_traject_region 2 needs
+ * region 1 of the same precision just before (ADZC_ERR_ARG otherwise). */
+int adzc_traject_region(adzc_handle *h, int prec, double dt, int niter, const void *uu_ext, const void *vv_ext,
+                        const void *ww_ext, const void *ut0, const void *vt0, const void *zdt0, void *pxyzm,
+                        double *wpxyz, int region, void *stream);
+int adzc_tricub_sets_region(adzc_handle *h, int prec, const int *nfields, const void *const *srcs,
+                            void *const *dsts, const int *mono, int region, void *stream);
+
 /* Sticky device status of the handle's kernels (ADZC_ERR_HALO,
  * ADZC_ERR_NONFINITE ...); synchronises the stream; clears it when reset. */
 int adzc_status(adzc_handle *h, int reset, void *stream);

@@ -74,8 +74,13 @@ def _poison_ext(a, t, gni, gnj, H):
     a[:, inside_dom & ~interior] = float("nan")
 
 
-@pytest.mark.parametrize("prec_name,npx,npy", [("mixed", 2, 2), ("fp64", 3, 2), ("ref32", 2, 2)])
-def test_decomposed_step_equals_single_tile(prec_name, npx, npy):
+@pytest.mark.parametrize("prec_name,npx,npy,split", [("mixed", 2, 2, False), ("fp64", 3, 2, False),
+                                                      ("ref32", 2, 2, False), ("mixed", 2, 2, True),
+                                                      ("fp64", 3, 2, True), ("ref32", 2, 2, True)])
+def test_decomposed_step_equals_single_tile(prec_name, npx, npy, split):
+    """split: the schedule that overlaps the exchanges (adzc_traject_region,
+    adzc_tricub_sets_region): each tile's interior runs while its halo cells
+    are still NaN, the band after the exchange; bit-exact all the same."""
     _need_cuda()
     import copy
     from gem_b200 import adz as A, synth
@@ -117,23 +122,33 @@ def test_decomposed_step_equals_single_tile(prec_name, npx, npy):
                           ex=ext_exchange(D, r, adt, dt_, len(arrs)), exw=wpxyz_exchange(D, r, adt)))
     for T in tiles:
         T["ex"].pack(T["arrs"])
+        T["winds"] = dict(zip(names, T["arrs"][:6]))
+        T["ad"].adz_inittraj(prec, T["px"], T["wp"])
+        if split:  # the interior's trajectory before any halo has arrived
+            T["ad"].adz_traject_region(prec, cfg.dt, T["winds"], T["px"], T["wp"], 1)
     _route([T["ex"] for T in tiles], D)
     for T in tiles:
         T["ex"].unpack(T["arrs"])
         assert not any(torch.isnan(a).any() for a in T["arrs"])
-        winds = dict(zip(names, T["arrs"][:6]))
-        T["ad"].adz_inittraj(prec, T["px"], T["wp"])
-        T["ad"].adz_traject(prec, cfg.dt, winds, T["px"], T["wp"])
+        if split:
+            T["ad"].adz_traject_region(prec, cfg.dt, T["winds"], T["px"], T["wp"], 2)
+        else:
+            T["ad"].adz_traject(prec, cfg.dt, T["winds"], T["px"], T["wp"])
         T["wp"][:, :, :2, :] = float("nan")
         T["wp"][:, :, -2:, :] = float("nan")
         T["wp"][:, :, :, :2] = float("nan")
         T["wp"][:, :, :, -2:] = float("nan")
         T["exw"].pack([T["wp"]])
+        T["outs"] = [torch.zeros(T["ad"].ext_shape, dtype=dt_, device="cuda") for _ in fields]
+        if split:  # the interior's position sets before wpxyz's halo has arrived
+            T["ad"].adz_tricub_sets_region(prec, nf, T["arrs"][6:], T["outs"], mono, 1)
     _route([T["exw"] for T in tiles], D)
     for T in tiles:
         T["exw"].unpack([T["wp"]])
-        T["outs"] = [torch.zeros(T["ad"].ext_shape, dtype=dt_, device="cuda") for _ in fields]
-        T["ad"].adz_tricub_sets(prec, nf, T["arrs"][6:], T["outs"], mono)
+        if split:
+            T["ad"].adz_tricub_sets_region(prec, nf, T["arrs"][6:], T["outs"], mono, 2)
+        else:
+            T["ad"].adz_tricub_sets(prec, nf, T["arrs"][6:], T["outs"], mono)
         assert T["ad"].status() == 0
     torch.cuda.synchronize()
     for T in tiles:

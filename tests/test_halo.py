@@ -192,3 +192,100 @@ def test_bench_tiles_form_one_domain(ws):
     assert len(seen) == ws and len({c.seed for c, _, _ in tiles}) == ws
     if ws == 1:
         assert tiles[0][1].edges == (1, 1, 1, 1)
+
+
+def _band_boxes(t, m, region):
+    """Interior (region 1: at least m from every side with a neighbour) or
+    the band around it (region 2), as (i0, i1, j0, j1) boxes of local
+    indices, in the way adzc_traject_region cuts a tile."""
+    w, e, s, n = [0 if edge else m for edge in t.edges]
+    ni, nj = t.ni, t.nj
+    if region == 1:
+        return [(1 + w, ni - e, 1 + s, nj - n)] if ni - e >= 1 + w and nj - n >= 1 + s else []
+    xw1, xe0 = min(w, ni), max(w + 1, ni - e + 1)
+    ys1, yn0 = min(s, nj), max(s + 1, nj - n + 1)
+    boxes = [(1, xw1, 1, nj), (xe0, ni, 1, nj), (xw1 + 1, xe0 - 1, 1, ys1), (xw1 + 1, xe0 - 1, yn0, nj)]
+    return [b for b in boxes if b[1] >= b[0] and b[3] >= b[2]]
+
+
+def _stencil_sum(a, h, boxes, out, r=2):
+    """out(i, j) = sum of a over the (2r+1)^2 cells around (i, j), for the
+    points of the boxes (a, out: (planes, nj + 2h, ni + 2h))."""
+    for i0, i1, j0, j1 in boxes:
+        for j in range(j0, j1 + 1):
+            for i in range(i0, i1 + 1):
+                out[:, j + h - 1, i + h - 1] = a[:, j + h - 1 - r:j + h + r, i + h - 1 - r:i + h + r].sum(axis=(1, 2))
+
+
+def _overlap_worker(rank, ws, port, npx, npy, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(ws), RANK=str(rank))
+    import datetime
+    import torch.distributed as dist
+    from gem_b200 import halo
+    dist.init_process_group("gloo", rank=rank, world_size=ws, timeout=datetime.timedelta(seconds=60))
+    D = halo.Decomposition(21, 14, npx, npy)
+    h, nplanes = 4, 3
+    _, tiles = _tiles(D, h, nplanes, 1, seed=8)
+    t = D.tile(rank)
+    bounds = (1 - h, t.ni + h, 1 - h, t.nj + h)
+    nbr = [0 if p is None else 1 for p in D.neighbours(rank)]
+
+    class OracleExchange(halo.HaloExchange):
+        def pack(self, arrays, stream=None):
+            self.send.copy_(torch.from_numpy(HO.pack([a.numpy() for a in arrays], bounds, t.ni, t.nj, h, h, nbr)))
+
+        def unpack(self, arrays, stream=None):
+            HO.unpack([a.numpy() for a in arrays], self.recv.numpy(), bounds, t.ni, t.nj, h, h, nbr)
+
+    ex = OracleExchange(D, rank, bounds, nplanes, h, h, torch.float32, 1, device="cpu")
+    a = torch.from_numpy(tiles[rank][0])
+    out = np.full_like(tiles[rank][0], np.nan)
+    # the overlapped schedule: the interior while the halo is in flight (its
+    # halo cells still NaN), the band once it has arrived
+    ex.pack([a])
+    reqs = ex.start()
+    _stencil_sum(a.numpy(), h, _band_boxes(t, 2, 1), out)
+    ex.finish(reqs)
+    ex.unpack([a])
+    _stencil_sum(a.numpy(), h, _band_boxes(t, 2, 2), out)
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, out))
+
+
+@pytest.mark.skipif(not torch.distributed.is_gloo_available(), reason="gloo backend missing")
+@pytest.mark.parametrize("npx,npy", [(2, 2), (3, 1)])
+def test_gloo_ranks_overlap_interior_with_exchange(npx, npy):
+    """The schedule of TiledStep(overlap=True) on CPU ranks: the transfer is
+    started, the interior computed beside it, the transfer finished and
+    unpacked, the band computed.  Every point equals the plain schedule's
+    (exchange, then the whole tile), and the interior never read a halo cell
+    (they were NaN until the unpack)."""
+    from gem_b200.halo import Decomposition
+    ws = npx * npy
+    port = 31200 + (os.getpid() % 1500) + 7 * npx
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_overlap_worker, args=(r, ws, port, npx, npy, q)) for r in range(ws)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=180) for _ in range(ws))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    D = Decomposition(21, 14, npx, npy)
+    _, tiles = _tiles(D, 4, 3, 1, seed=8)
+    exp = _expected(D, tiles, 4, 0)
+    for r in range(ws):
+        t = D.tile(r)
+        want = np.full_like(exp[r], np.nan)
+        _stencil_sum(exp[r], 4, [(1, t.ni, 1, t.nj)], want)
+        inner = (slice(None), slice(4, 4 + t.nj), slice(4, 4 + t.ni))
+        assert not np.isnan(res[r][inner]).any()
+        np.testing.assert_array_equal(res[r][inner], want[inner])
+        # the band boxes and the interior cover the tile once
+        cover = np.zeros((t.nj, t.ni), int)
+        for reg in (1, 2):
+            for i0, i1, j0, j1 in _band_boxes(t, 2, reg):
+                cover[j0 - 1:j1, i0 - 1:i1] += 1
+        assert (cover == 1).all()
