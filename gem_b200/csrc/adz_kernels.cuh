@@ -42,6 +42,25 @@
 #define ADZ_SET_MINB_REF32 ADZ_SET_MINB
 #endif
 #define ADZ_TRAJ_BOUNDS __launch_bounds__(128, PREC == kRef32 ? ADZ_TRAJ_MINB_REF32 : ADZ_TRAJ_MINB)
+// the tiled trajectory kernel may take wider blocks: ADZ_TRAJ_TILE_I
+// consecutive i by ADZ_TRAJ_TILE_K levels, with its own resident-block budget
+// (in blocks of that size)
+#ifndef ADZ_TRAJ_TILE_I
+#define ADZ_TRAJ_TILE_I (128 / ADZ_TRAJ_TILE_K)
+#endif
+#if ADZ_TRAJ_TILE_K > 1
+#define ADZ_TRAJ_TILE_THREADS (ADZ_TRAJ_TILE_I * ADZ_TRAJ_TILE_K)
+#else
+#define ADZ_TRAJ_TILE_THREADS 128
+#endif
+#ifndef ADZ_TRAJ_TILE_MINB
+#define ADZ_TRAJ_TILE_MINB ADZ_TRAJ_MINB
+#endif
+#ifndef ADZ_TRAJ_TILE_MINB_REF32
+#define ADZ_TRAJ_TILE_MINB_REF32 ADZ_TRAJ_MINB_REF32
+#endif
+#define ADZ_TRAJ_TILE_BOUNDS \
+  __launch_bounds__(ADZ_TRAJ_TILE_THREADS, PREC == kRef32 ? ADZ_TRAJ_TILE_MINB_REF32 : ADZ_TRAJ_TILE_MINB)
 #define ADZ_SET_BOUNDS __launch_bounds__(128, PREC == kRef32 ? ADZ_SET_MINB_REF32 : ADZ_SET_MINB)
 #ifndef ADZ_QV_MINB
 #define ADZ_QV_MINB 0
@@ -507,9 +526,9 @@ __device__ __forceinline__ void traject_point_tol(const DGrid& g, const TrajArgs
 }
 
 template <int PREC>
-__global__ void ADZ_TRAJ_BOUNDS k_traject(DGrid g, TrajArgs a) {
+__global__ void ADZ_TRAJ_TILE_BOUNDS k_traject(DGrid g, TrajArgs a) {
 #if ADZ_TRAJ_TILE_K > 1
-  constexpr int TK = ADZ_TRAJ_TILE_K, TI = 128 / TK;
+  constexpr int TK = ADZ_TRAJ_TILE_K, TI = ADZ_TRAJ_TILE_I;
   const int nkp = g.nk - a.k00 + 1;
   const int nic = (g.ni + TI - 1) / TI, nkg = (nkp + TK - 1) / TK;
   const long long b = blockIdx.x;
@@ -1132,10 +1151,10 @@ cudaError_t launch_inittraj(const DGrid& g, float* pxyzm, double* wpxyz, cudaStr
 template <int PREC>
 cudaError_t launch_traject(const DGrid& g, const TrajArgs& a, cudaStream_t s) {
 #if ADZ_TRAJ_TILE_K > 1
-  constexpr int TK = ADZ_TRAJ_TILE_K, TI = 128 / TK;
+  constexpr int TK = ADZ_TRAJ_TILE_K, TI = ADZ_TRAJ_TILE_I;
   const long long nb = (long long)((g.ni + TI - 1) / TI) * ((g.nk - a.k00 + 1 + TK - 1) / TK) * g.nj;
   if (nb > 0x7fffffffLL) return cudaErrorInvalidValue;
-  k_traject<PREC><<<(unsigned)nb, 128, 0, s>>>(g, a);
+  k_traject<PREC><<<(unsigned)nb, TI * TK, 0, s>>>(g, a);
 #else
   const long long n = (long long)g.ni * g.nj * (g.nk - a.k00 + 1);
   k_traject<PREC><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, a);
