@@ -366,6 +366,11 @@ def run_product(args):
         torch.cuda.empty_cache()
         gsum = measure_guess(args, timed, ws, rank)
 
+    lvla = None
+    if rank == 0 and ws == 1 and not args.no_level_a:
+        torch.cuda.empty_cache()
+        lvla = measure_level_a(args, with_cpu=not args.no_cpu)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         # the benchmarked tile, median of 5 steps after 1 warm-up, all host cores
@@ -392,7 +397,7 @@ def run_product(args):
         "accuracy": acc,
         "e2e": e2e, "gpu_launches": (LAUNCHES_PER_STEP + (HALO_LAUNCHES_PER_STEP if ws > 1 else 0)) * args.steps,
         "clocks": clk, "cpu_baseline": cpu,
-        "tracers8": tsum, "post": psum, "batch": batch, "learned_guess": gsum,
+        "tracers8": tsum, "post": psum, "batch": batch, "learned_guess": gsum, "level_a": lvla,
     }
     if rank == 0:
         print(json.dumps(line))
@@ -423,6 +428,104 @@ def l1_roofline(args, per, npts, clk):
     dom = max(per, key=per.get)
     out["kernel"], out["achieved"], out["frac"] = dom, out["kernels"][dom]["achieved"], out["kernels"][dom]["frac"]
     return out
+
+
+def level_a_inputs(size, ntr, seed=11):
+    """Host arrays of the per-level Level A calls on the thermo set: w and the
+    tracers on the extended tile (halo 4), FP32, and departure positions of
+    every arrival point as fractional indices of the extended array, displaced
+    up to 1.5 grid lengths horizontally and about 0.3 levels vertically."""
+    ni, nj, nk = size
+    h = 4
+    nie, nje = ni + 2 * h, nj + 2 * h
+    rng = np.random.default_rng(seed)
+    fields = [rng.standard_normal(nie * nje * nk, dtype=np.float32) for _ in range(1 + ntr)]
+    th = np.geomspace(20.0, 1000.0, nk)
+    z = np.cumsum(th)[::-1].copy()
+    levels = np.ascontiguousarray(z * (25000.0 / z[0]))
+    ii, jj = np.meshgrid(np.arange(1, ni + 1, dtype=np.float32), np.arange(1, nj + 1, dtype=np.float32))
+    planes = []
+    for k in range(1, nk + 1):
+        pos = np.empty((ni * nj, 3), np.float32)
+        pos[:, 0] = np.clip(ii.ravel() + rng.uniform(-1.5, 1.5, ni * nj).astype(np.float32), 2.0 - h, nie - 2.0 - h - 1e-3)
+        pos[:, 1] = np.clip(jj.ravel() + rng.uniform(-1.5, 1.5, ni * nj).astype(np.float32), 2.0 - h, nje - 2.0 - h - 1e-3)
+        pos[:, 2] = np.clip(k + 0.3 * rng.standard_normal(ni * nj, dtype=np.float32), 1.0, float(nk))
+        planes.append(pos)
+    return {"fields": fields, "levels": levels, "planes": planes, "ext": (nie, nje, nk), "halo": h}
+
+
+def time_level_a(lib, setup, inp, threads, reps=3):
+    """Tricublin_mono_zyx_m_n once per level, as the reference's driver calls
+    it (one slice of ni*nj points per OpenMP thread), from ``threads`` host
+    threads; wall-clock seconds per pass over the tile (median), and the
+    outputs of the first and the middle level."""
+    import ctypes as C
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+    nie, nje, nk = inp["ext"]
+    h = inp["halo"]
+    lv = setup(inp["levels"], nk, nie, nje, h, h)
+    m = len(inp["fields"])
+    fs = (C.c_void_p * m)(*[f.ctypes.data for f in inp["fields"]])
+    n = inp["planes"][0].shape[0]
+    local = threading.local()
+    keep = {}
+    status = getattr(lib, "adzc_last_error", None)  # per-thread status of the product library
+
+    def call(k):
+        if not hasattr(local, "out"):
+            local.out = [np.empty((m, n), np.float32) for _ in range(4)]
+        out = local.out
+        lib.Tricublin_mono_zyx_m_n(*(o.ctypes.data for o in out), C.cast(fs, C.c_void_p),
+                                   inp["planes"][k].ctypes.data, lv, n, m)
+        if status is not None and status() != 0:
+            raise RuntimeError(f"Level A call of level {k} failed with status {status()}")
+        if k in (0, nk // 2):
+            keep[k] = [o.copy() for o in out]
+
+    times = []
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        for r in range(reps + 1):
+            t0 = time.perf_counter()
+            list(ex.map(call, range(nk)))
+            if r > 0:
+                times.append(time.perf_counter() - t0)
+    return statistics.median(times), keep
+
+
+def measure_level_a(args, with_cpu):
+    """The reference-named interpolator symbols with host arrays (Level A, the
+    link-level drop-in for the reference's interpolator) on the thermo set of
+    the benched tile, against the reference's own interpolator on the host
+    cores (the CPU leg, when the reference build is present)."""
+    import ctypes as C
+    from gem_b200 import adz
+    ni, nj, nk = args.size
+    inp = level_a_inputs(args.size, args.ntr)
+    threads = min(16, os.cpu_count() or 1)
+    L = adz.lib()
+    n, m = ni * nj, 1 + args.ntr
+    s_gpu, out_gpu = time_level_a(L, lambda lev, *a: L.Vsearch_setup_plus(lev.ctypes.data, *a), inp, threads)
+    npts = n * nk
+    res = {"workload": (f"thermo set of the {ni}x{nj}x{nk} tile: w + {args.ntr} tracers with bounds "
+                        f"(Tricublin_mono_zyx_m_n), one call per level of {n} points from {threads} host threads, "
+                        "host arrays in and out"),
+           "threads": threads,
+           "gpu": {"s_per_pass": s_gpu, "value": npts / s_gpu, "unit": "grid-points/s",
+                   "d2h_bytes_per_pass": 4 * m * npts * 4}}
+    if with_cpu:
+        from oracle import oracle as O
+        if O.have_ref():
+            R = O.RefKernels()
+            s_cpu, out_cpu = time_level_a(R.lib, lambda lev, *a: R.lib.Vsearch_setup_plus(lev, *a), inp, threads)
+            same = all(np.array_equal(a.view(np.int32), b.view(np.int32))
+                       for k in out_gpu for a, b in zip(out_gpu[k], out_cpu[k]))
+            res["cpu_reference"] = {"s_per_pass": s_cpu, "value": npts / s_cpu, "unit": "grid-points/s",
+                                    "cores": threads, "kind": "reference",
+                                    "sample": "the same calls into the reference's interpolator compiled unchanged"}
+            res["speedup_vs_cpu"] = s_cpu / s_gpu
+            res["bit_identical_levels"] = same
+    return res
 
 
 def workload_config(args, ws, decomp=None):
@@ -1067,6 +1170,8 @@ def main():
     ap.add_argument("--no-tracers", action="store_true", help="skip the 8-tracer mono measurement")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the accuracy passes of the 8-tracer leg")
     ap.add_argument("--no-post", action="store_true", help="skip the QV / mass-fixer / ILMC / CFL measurement")
+    ap.add_argument("--no-level-a", action="store_true",
+                    help="skip the reference-named interpolator calls on host arrays")
     ap.add_argument("--guess-weights", default=os.path.join(ROOT, "gem_b200", "data", "guess_mlp.npz"))
     ap.add_argument("--only", choices=["mixed"], default=None,
                     help="run the mixed-precision path alone (small profiling runs)")

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "../../include/adz_b200.h"
@@ -1122,15 +1123,88 @@ extern "C" int adzc_status(adzc_handle* h, int reset, void* stream) {
 // ---------------------------------------------------------------------------
 namespace {
 
+// The reference calls its interpolators from every OpenMP thread, one plane
+// each.  A Level A call takes one of kSlots staging slots (a stream, a device
+// buffer and a pinned buffer for the transposed layout), so calls from
+// different threads overlap their copies and kernels.  A thread whose slot is
+// busy takes the next free one, and waits for its own when all are busy.
+//
+// Host arrays are the caller's pageable memory.  Copies go through a ring of
+// pinned chunks per slot: the calling thread copies chunk c into pinned
+// memory while the DMA of chunk c-1 runs (and the other way round for the
+// results), which moves the bytes several times faster than pageable copies.
+constexpr int kSlots = 16;
+constexpr size_t kChunk = (size_t)8 << 20;
+constexpr int kRing = 4;
 struct Staging {
   std::mutex mu;
   cudaStream_t stream = nullptr;
   int device = -1;
   void* buf = nullptr;
   size_t cap = 0;
+  float* pinned = nullptr;
+  size_t pinned_cap = 0;
+  char* ring = nullptr;  // kRing chunks of pinned memory
+  cudaEvent_t ev[kRing] = {};
+  unsigned next = 0;
 };
-Staging& staging() {
-  static Staging s;
+
+// chunk r of the ring, once the copy that last used it has finished
+char* ring_chunk(Staging& S, unsigned r) {
+  return cudaEventSynchronize(S.ev[r]) == cudaSuccess ? S.ring + (size_t)r * kChunk : nullptr;
+}
+
+bool ring_h2d(Staging& S, void* dst, const void* src, size_t bytes) {
+  for (size_t off = 0; off < bytes; off += kChunk) {
+    const size_t len = std::min(kChunk, bytes - off);
+    const unsigned r = S.next++ % kRing;
+    char* c = ring_chunk(S, r);
+    if (!c) return false;
+    std::memcpy(c, (const char*)src + off, len);
+    if (cudaMemcpyAsync((char*)dst + off, c, len, cudaMemcpyHostToDevice, S.stream) != cudaSuccess ||
+        cudaEventRecord(S.ev[r], S.stream) != cudaSuccess)
+      return false;
+  }
+  return true;
+}
+
+// device -> caller's memory, up to kRing chunks in flight ahead of the
+// thread's copy out of the ring
+bool ring_d2h(Staging& S, void* dst, const void* src, size_t bytes) {
+  const size_t nch = (bytes + kChunk - 1) / kChunk;
+  const unsigned first = S.next;
+  size_t issued = 0;
+  for (size_t c = 0; c < nch; c++) {
+    for (; issued < nch && issued < c + kRing; issued++) {
+      const unsigned r = (first + (unsigned)issued) % kRing;
+      char* h = ring_chunk(S, r);
+      const size_t len = std::min(kChunk, bytes - issued * kChunk);
+      if (!h || cudaMemcpyAsync(h, (const char*)src + issued * kChunk, len, cudaMemcpyDeviceToHost, S.stream) !=
+                    cudaSuccess ||
+          cudaEventRecord(S.ev[r], S.stream) != cudaSuccess)
+        return false;
+    }
+    const unsigned r = (first + (unsigned)c) % kRing;
+    char* h = ring_chunk(S, r);
+    if (!h) return false;
+    std::memcpy((char*)dst + c * kChunk, h, std::min(kChunk, bytes - c * kChunk));
+  }
+  S.next = first + (unsigned)nch;
+  return true;
+}
+Staging& acquire_slot(std::unique_lock<std::mutex>* lock) {
+  static Staging slots[kSlots];
+  const size_t h = std::hash<std::thread::id>{}(std::this_thread::get_id());
+  for (int t = 0; t < kSlots; t++) {
+    Staging& s = slots[(h + t) % kSlots];
+    std::unique_lock<std::mutex> l(s.mu, std::try_to_lock);
+    if (l.owns_lock()) {
+      *lock = std::move(l);
+      return s;
+    }
+  }
+  Staging& s = slots[h % kSlots];
+  *lock = std::unique_lock<std::mutex>(s.mu);
   return s;
 }
 
@@ -1155,17 +1229,28 @@ void corner_f32(const adzc_ztab* lv, const pxpypz& p, long long* lo, long long* 
 // Stage the touched part of each source (elements [lo, hi] per field, in
 // units of ``comp`` floats) plus positions; returns device base pointers
 // already shifted so that base[off] addresses what f[off] addresses.
-int stage_inputs(const adzc_ztab* lv, int comp, const float* const* fs, int m, const pxpypz* pos, int n,
+int stage_inputs(Staging& S, const adzc_ztab* lv, int comp, const float* const* fs, int m, const pxpypz* pos, int n,
                  size_t out_floats, std::vector<const void*>* dbase, void** dpos, float** dout) {
-  Staging& S = staging();
   int dev = 0;
   ADZ_CK(cudaGetDevice(&dev));
   if (S.stream == nullptr || S.device != dev) {
     if (S.stream) cudaStreamDestroy(S.stream);
     cudaFree(S.buf);
+    cudaFreeHost(S.pinned);
+    cudaFreeHost(S.ring);
+    for (cudaEvent_t& e : S.ev) {
+      if (e) cudaEventDestroy(e);
+      e = nullptr;
+    }
     S.buf = nullptr;
     S.cap = 0;
+    S.pinned = nullptr;
+    S.pinned_cap = 0;
+    S.ring = nullptr;
+    S.device = -1;
     ADZ_CK(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
+    ADZ_CK(cudaMallocHost(&S.ring, kRing * kChunk));
+    for (cudaEvent_t& e : S.ev) ADZ_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     S.device = dev;
   }
   long long lo = (1LL << 62), hi = -(1LL << 62);
@@ -1192,11 +1277,11 @@ int stage_inputs(const adzc_ztab* lv, int comp, const float* const* fs, int m, c
   }
   char* p = (char*)S.buf;
   *dpos = p;
-  ADZ_CK(cudaMemcpyAsync(p, pos, sizeof(pxpypz) * n, cudaMemcpyHostToDevice, S.stream));
+  if (!ring_h2d(S, p, pos, sizeof(pxpypz) * n)) return fail(ADZC_ERR_CUDA);
   p += al(sizeof(pxpypz) * n);
   dbase->clear();
   for (int q = 0; q < m; q++) {
-    ADZ_CK(cudaMemcpyAsync(p, fs[q] + lo * comp, sizeof(float) * span, cudaMemcpyHostToDevice, S.stream));
+    if (!ring_h2d(S, p, fs[q] + lo * comp, sizeof(float) * span)) return fail(ADZC_ERR_CUDA);
     dbase->push_back((const float*)p - lo * comp);
     p += al(sizeof(float) * span);
   }
@@ -1210,15 +1295,16 @@ void level_a(int kind, float* d, float* l, float* mi, float* ma, float** dp, con
     if (n > 0) fail(ADZC_ERR_ARG);
     return;
   }
-  Staging& S = staging();
-  std::lock_guard<std::mutex> lock(S.mu);
+  std::unique_lock<std::mutex> lock;
+  Staging& S = acquire_slot(&lock);
   const int comp = (kind == 2) ? 3 : 1;
   const int nout = (kind == 1) ? 4 : 1;
   const size_t out_floats = (size_t)nout * m * n * comp;
   std::vector<const void*> base;
   void* dpos = nullptr;
   float* dout = nullptr;
-  if (stage_inputs(lv, comp, fs, (kind == 2) ? 1 : m, pxyz, n, out_floats, &base, &dpos, &dout) != ADZC_OK) return;
+  if (stage_inputs(S, lv, comp, fs, (kind == 2) ? 1 : m, pxyz, n, out_floats, &base, &dpos, &dout) != ADZC_OK)
+    return;
   const adz::DZtab t = lv->dev();
   int st;
   if (kind == 2) {
@@ -1236,31 +1322,40 @@ void level_a(int kind, float* d, float* l, float* mi, float* ma, float** dp, con
     fail(st);
     return;
   }
-  std::vector<float> host(out_floats);
-  if (cudaMemcpyAsync(host.data(), dout, sizeof(float) * out_floats, cudaMemcpyDeviceToHost, S.stream) !=
-          cudaSuccess ||
-      cudaStreamSynchronize(S.stream) != cudaSuccess) {
+  // results go straight into the caller's arrays where the layouts agree
+  float* outs[4] = {d, l, mi, ma};
+  bool ok = true;
+  if (kind == 2) {
+    ok = ring_d2h(S, d, dout, sizeof(float) * 3 * n);
+  } else if (layout == 0) {
+    for (int o = 0; o < nout && ok; o++) ok = ring_d2h(S, outs[o], dout + (size_t)o * m * n, sizeof(float) * m * n);
+  } else if (layout == 2) {
+    for (int q = 0; q < m && ok; q++) ok = ring_d2h(S, dp[q], dout + (size_t)q * n, sizeof(float) * n);
+  } else {  // n_m: through the slot's pinned buffer, transposed on the host
+    if (S.pinned_cap < out_floats) {
+      cudaFreeHost(S.pinned);
+      S.pinned = nullptr;
+      S.pinned_cap = 0;
+      if (cudaMallocHost(&S.pinned, sizeof(float) * out_floats) != cudaSuccess) {
+        fail(ADZC_ERR_ALLOC);
+        return;
+      }
+      S.pinned_cap = out_floats;
+    }
+    ok = cudaMemcpyAsync(S.pinned, dout, sizeof(float) * out_floats, cudaMemcpyDeviceToHost, S.stream) ==
+         cudaSuccess;
+  }
+  if (!ok || cudaStreamSynchronize(S.stream) != cudaSuccess) {
     fail(ADZC_ERR_CUDA);
     return;
   }
-  if (kind == 2) {
-    std::memcpy(d, host.data(), sizeof(float) * 3 * n);
-    return;
-  }
-  float* outs[4] = {d, l, mi, ma};
-  for (int o = 0; o < nout; o++) {
-    const float* src = host.data() + (size_t)o * m * n;
-    for (int q = 0; q < m; q++) {
-      const float* row = src + (size_t)q * n;
-      if (layout == 0) {
-        std::memcpy(outs[o] + (size_t)q * n, row, sizeof(float) * n);
-      } else if (layout == 1) {
+  if (kind != 2 && layout == 1) {
+    for (int o = 0; o < nout; o++)
+      for (int q = 0; q < m; q++) {
+        const float* row = S.pinned + ((size_t)o * m + q) * n;
         float* dst = outs[o];
         for (int j = 0; j < n; j++) dst[(size_t)j * m + q] = row[j];
-      } else {
-        std::memcpy(dp[q], row, sizeof(float) * n);
       }
-    }
   }
 }
 
