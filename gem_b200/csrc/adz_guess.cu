@@ -9,16 +9,17 @@
 // tolerance (k_traject_tol), falling back to the plain start where the guess
 // does not converge.
 //
-// Inference runs on the 5th-generation tensor cores: a persistent kernel keeps
-// the BF16 weights in shared memory, each CTA of 256 threads gathers the
-// features of 128 arrival points into a BF16 tile, and one elected thread
-// issues tcgen05.mma for each layer with the FP32 accumulator in tensor
-// memory; two threads per arrival point share the feature gathers and the
-// epilogue (tcgen05.ld, bias, GELU with the hardware tanh on BF16
-// pairs, BF16) writes the next layer's
-// input tile in place.  Operands use the K-major no-swizzle layout of 8x16-byte
-// core matrices (K chunks of a row group adjacent).  Every wait on the MMA barrier is bounded: on expiry the CTA
-// raises kErrTimeout in the handle's status, waits (bounded) for its MMA in
+// Inference runs on the 5th-generation tensor cores: a persistent kernel, one
+// CTA per SM, keeps the BF16 weights in shared memory and four 128-point
+// tiles in flight.  Gather warps write the features of a tile into a BF16
+// tile, one thread issues tcgen05.mma for each layer with the FP32
+// accumulator in tensor memory, and epilogue warps (tcgen05.ld, bias, GELU
+// with the hardware tanh on BF16 pairs, BF16) write the next layer's input
+// tile in place; mbarriers hand each tile from one role to the next, so the
+// gathers and epilogues of some tiles overlap the MMAs of others.  Operands
+// use the K-major no-swizzle layout of 8x16-byte core matrices (K chunks of a
+// row group adjacent).  Every wait is bounded: on expiry the CTA raises
+// kErrTimeout in the handle's status, waits (bounded) for its MMAs in
 // flight, frees its tensor memory and stops.
 //
 // Feature definition, network and training: oracle/guess_oracle.py restates
@@ -44,7 +45,6 @@ constexpr int kK1 = 96;                  // features padded to the MMA K step
 constexpr int kHid = ADZC_GUESS_HIDDEN;  // 128
 constexpr int kN3 = 16;                  // 3 outputs padded to the smallest N
 constexpr int kRows = 128;               // arrival points per tile (MMA M)
-constexpr int kThreads = 256;            // two threads per point: each half of the K chunks / columns
 
 // weight image: core-matrix layouts of W1 (128x96), W2 (128x128), W3 (16x128),
 // then FP32 biases b1 (128), b2 (128), b3 (16); copied verbatim to shared memory
@@ -55,13 +55,8 @@ constexpr int kB1 = kW3 + kN3 * kHid * 2;
 constexpr int kB2 = kB1 + kHid * 4;
 constexpr int kB3 = kB2 + kHid * 4;
 constexpr int kNetBytes = kB3 + kN3 * 4;  // 62528
-// shared memory of one CTA: weight image, activation tile, barrier, TMEM address
-constexpr int kA = (kNetBytes + 1023) / 1024 * 1024;
-constexpr int kBar = kA + kRows * kHid * 2;
-constexpr int kTaddr = kBar + 8;
-constexpr int kSmem = kTaddr + 8 + 1024;  // + alignment slack
-constexpr int kTmemCols = 128;
 constexpr unsigned kWaitPolls = 1u << 20;
+constexpr unsigned kIdleSweeps = 1u << 24;  // bound of a polling role's sweeps without progress
 static_assert(kNetBytes % 16 == 0, "weight image copied in 16-byte words");
 
 // byte offset of element (r, k) of a K-major BF16 operand with row length
@@ -308,24 +303,6 @@ __device__ __forceinline__ void features8(const Nbr& nb, float* f) {
   f[7] = feature<Q0 + 7>(nb);
 }
 
-// features of a chunk of 8 into the tile (row r, K chunk KC)
-template <int KC>
-__device__ __forceinline__ void put_chunk(unsigned char* A, int r, bool valid, const Nbr& nb) {
-  float f[8];
-  if (valid) {
-    features8<KC * 8>(nb, f);
-  } else {
-#pragma unroll
-    for (int q = 0; q < 8; q++) f[q] = 0.0f;
-  }
-  uint4 w;
-  w.x = pack_bf16(f[0], f[1]);
-  w.y = pack_bf16(f[2], f[3]);
-  w.z = pack_bf16(f[4], f[5]);
-  w.w = pack_bf16(f[6], f[7]);
-  *reinterpret_cast<uint4*>(A + core_off(r, KC * 8, kHid)) = w;
-}
-
 // training features: FP32, all 82 per point
 __global__ void __launch_bounds__(128) k_features(Args a, long long n) {
   const DGrid& g = a.g;
@@ -348,13 +325,14 @@ __global__ void __launch_bounds__(128) k_features(Args a, long long n) {
   }
 }
 
-// epilogue of a hidden layer: this thread's half (64) of the accumulator
+// epilogue of a hidden layer: this thread's part (NCOLS columns) of the accumulator
 // columns of its row,
 // + bias, GELU, BF16, written as the next layer's K-major input row
+template <int NCOLS>
 __device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, const float* bias, unsigned char* A, int r,
-                                                int half) {
+                                                int part) {
 #pragma unroll
-  for (int c0 = half * (kHid / 2); c0 < (half + 1) * (kHid / 2); c0 += 32) {
+  for (int c0 = part * NCOLS; c0 < (part + 1) * NCOLS; c0 += 32) {
     float v[32];
     tmem_ld32(tmem_row + c0, v);
 #pragma unroll
@@ -376,127 +354,373 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, const float* 
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 2) k_guess(Args a) {
+// ---------------------------------------------------------------------------
+// The inference kernel: one CTA per SM, warp-specialised, kStages tiles in
+// flight.  Each stage is one 128-row activation tile in shared memory and
+// one 128-column FP32 accumulator in tensor memory.
+//   gather warps (8)    features of the stage's 128 arrival points -> tile
+//                       (two threads per point, as the K chunks split);
+//   MMA thread (1)      whichever layer of whichever stage is ready: 6, 8 and
+//                       8 K steps, committed to the stage's done barrier;
+//   epilogue warps (8)  whichever stage's accumulator is complete: bias,
+//                       GELU, BF16 into the same tile (the next layer's
+//                       input), or the 3 outputs + bias of the last layer.
+// So one stage's gather and epilogue overlap the other stages' MMAs.  Per
+// stage barriers: full (gather -> MMA), hid (epilogue -> MMA, twice per
+// tile), done (MMA commit -> epilogue, three times per tile) and empty
+// (last epilogue -> gather).  Every wait is bounded: on expiry a role sets
+// the CTA's abort flag and raises kErrTimeout; the others see the flag and
+// stop, and the MMA thread waits (bounded) for its last commits before the
+// tensor memory is freed.
+constexpr int kStages = 4;
+#ifndef ADZ_GUESS_GATHER_GROUPS
+#define ADZ_GUESS_GATHER_GROUPS 1
+#endif
+// gather groups of 8 warps; group q gathers the tiles n = q mod groups
+constexpr int kGatherGroups = ADZ_GUESS_GATHER_GROUPS;
+#ifndef ADZ_GUESS_EPI_WARPS
+#define ADZ_GUESS_EPI_WARPS 8
+#endif
+#ifndef ADZ_GUESS_EPI_GROUPS
+#define ADZ_GUESS_EPI_GROUPS 2
+#endif
+// epilogue groups: group e serves the stages st = e mod groups, so that the
+// groups' epilogues of different tiles run side by side.  A group's warps
+// are 4 row quarters (the TMEM lanes a warp may read) times kEpiWarps / 4
+// column parts of kEpiCols columns
+constexpr int kEpiGroups = ADZ_GUESS_EPI_GROUPS;
+constexpr int kEpiGroupWarps = ADZ_GUESS_EPI_WARPS, kEpiWarps = kEpiGroupWarps * kEpiGroups;
+constexpr int kEpiCols = kHid / (kEpiGroupWarps / 4);
+constexpr int kGroupWarps = 8, kGatherWarps = kGroupWarps * kGatherGroups;
+static_assert(kEpiGroupWarps % 4 == 0 && kEpiCols % 32 == 0, "epilogue column parts of 32-column loads");
+static_assert(kStages % kEpiGroups == 0 && kStages % kGatherGroups == 0, "stages split evenly between groups");
+constexpr int kPipeThreads = (kEpiWarps + kGatherWarps + 1) * 32;
+constexpr int kStageBytes = kRows * kHid * 2;
+constexpr int kPA = (kNetBytes + 1023) / 1024 * 1024;
+constexpr int kPBar = kPA + kStages * kStageBytes;  // full[S], hid[S], done[S], empty[S]
+constexpr int kPTaddr = kPBar + 4 * kStages * 8;
+constexpr int kPAbort = kPTaddr + 4;
+constexpr int kPSmem = kPAbort + 4 + 1024;  // + alignment slack
+constexpr int kPTmemCols = kStages * kHid;  // 512: the whole of an SM's tensor memory
+static_assert(kPSmem <= 227 * 1024, "pipelined inference shared memory");
+
+// non-blocking test of a phase (try_wait may suspend the thread for a while,
+// which a role that polls several stages in turn must not do)
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__global__ void __launch_bounds__(kPipeThreads, 1) k_guess(Args a) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  // thread tid: row (arrival point) tid % 128 of the tile, half tid / 128;
-  // warp w reads TMEM lanes 32 (w % 4) .. +31, the lanes of its rows
-  const int tid = threadIdx.x, warp = tid >> 5, row = tid & (kRows - 1), half = tid / kRows;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const DGrid& g = a.g;
-  // weight image -> shared memory
   {
     const uint4* src = reinterpret_cast<const uint4*>(a.net);
     uint4* dst = reinterpret_cast<uint4*>(sm);
     for (int q = tid; q < kNetBytes / 16; q += blockDim.x) dst[q] = src[q];
   }
+  fence_async_smem();  // the weights are read by the MMAs (async proxy)
   const uint32_t s_base = smem_u32(sm);
-  const uint32_t bar = s_base + kBar;
+  const uint32_t bar0 = s_base + kPBar;
+  auto full_bar = [&](int st) { return bar0 + 8u * st; };
+  auto hid_bar = [&](int st) { return bar0 + 8u * (kStages + st); };
+  auto done_bar = [&](int st) { return bar0 + 8u * (2 * kStages + st); };
+  auto empty_bar = [&](int st) { return bar0 + 8u * (3 * kStages + st); };
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + kPAbort);
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    for (int st = 0; st < kStages; st++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(full_bar(st)), "r"(kGroupWarps) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(hid_bar(st)), "r"(kEpiGroupWarps) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(done_bar(st)) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(empty_bar(st)), "r"(kEpiGroupWarps) : "memory");
+    }
+    *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s_base + kTaddr),
-                 "r"(kTmemCols)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s_base + kPTaddr),
+                 "r"(kPTmemCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   fence_before();
   __syncthreads();
   fence_after();
-  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kTaddr);
-  const uint32_t tmem_row = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-  unsigned char* A = sm + kA;
-  const float* b1 = reinterpret_cast<const float*>(sm + kB1);
-  const float* b2 = reinterpret_cast<const float*>(sm + kB2);
-  const float* b3 = reinterpret_cast<const float*>(sm + kB3);
-  const uint32_t a_addr = s_base + kA, w1 = s_base + kW1, w2 = s_base + kW2, w3 = s_base + kW3;
-  const uint32_t id_hid = instr_desc(kRows, kHid), id_out = instr_desc(kRows, kN3);
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kPTaddr);
   const long long ntiles = (a.npts + kRows - 1) / kRows;
-  uint32_t parity = 0;
-  bool failed = false, pending = false;
+  // tiles of this CTA: blockIdx.x + n * gridDim.x, n = 0 .. nt-1, stage n % kStages
+  const long long nt = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  auto stage_tiles = [&](int st) { return nt > st ? (nt - 1 - st) / kStages + 1 : 0LL; };
+  auto give_up = [&]() {
+    *abort_flag = 1;
+    atomicOr(g.status, kErrTimeout);
+  };
 
-  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long long t = tile * kRows + row;
-    const bool valid = t < a.npts;
-    int i = 1, j = 1, k = 1;
-    if (valid) node_of(a, t, i, j, k);
-    Nbr nb;
-    neighbourhood(g, a.uvw, i, j, k, a.dt, nb);
-    if (half == 0) {
-      put_chunk<0>(A, row, valid, nb);
-      put_chunk<1>(A, row, valid, nb);
-      put_chunk<2>(A, row, valid, nb);
-      put_chunk<3>(A, row, valid, nb);
-      put_chunk<4>(A, row, valid, nb);
-      put_chunk<5>(A, row, valid, nb);
-    } else {
-      put_chunk<6>(A, row, valid, nb);
-      put_chunk<7>(A, row, valid, nb);
-      put_chunk<8>(A, row, valid, nb);
-      put_chunk<9>(A, row, valid, nb);
-      put_chunk<10>(A, row, valid, nb);
-      put_chunk<11>(A, row, valid, nb);
-    }
-
-    // three layers: tile [128 x K] . W^T -> TMEM, epilogue back into the tile
-    float y[3] = {0.f, 0.f, 0.f};
-#pragma unroll 1
-    for (int layer = 0; layer < 3; layer++) {
+  if (warp >= kEpiWarps && warp < kEpiWarps + kGatherWarps) {
+    // ---- gather: tile n into stage n % kStages once its previous tile left
+    const int gq = (warp - kEpiWarps) / kGroupWarps;
+    const int gt = tid - (kEpiWarps + gq * kGroupWarps) * 32, row = gt & (kRows - 1), half = gt / kRows;
+    for (long long n = gq; n < nt; n += kGatherGroups) {
+      const int st = (int)(n % kStages);
+      const long long use = n / kStages;
+      if (use > 0) {
+        // lane 0 polls, then every lane acquires the completed phase
+        const uint32_t par = (uint32_t)((use - 1) & 1);
+        int ok = 0;
+        if (lane == 0)
+          for (unsigned q = 0; q < kWaitPolls && !ok; q++) {
+            ok = mbar_try_wait(empty_bar(st), par);
+            if (!ok && *abort_flag) break;
+          }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (ok) ok = __all_sync(0xffffffffu, mbar_wait_bounded(empty_bar(st), par));
+        if (!ok) {
+          if (lane == 0 && !*abort_flag) give_up();
+          break;
+        }
+      }
+      const long long t = (blockIdx.x + n * gridDim.x) * kRows + row;
+      const bool valid = t < a.npts;
+      int i = 1, j = 1, k = 1;
+      if (valid) node_of(a, t, i, j, k);
+      Nbr nb;
+      neighbourhood(g, a.uvw, i, j, k, a.dt, nb);
+      unsigned char* A = sm + kPA + st * kStageBytes;
+      // every load of the thread's 6 K chunks first, so that they are all in
+      // flight at once, then the BF16 stores
+      float f[48];
+      if (half == 0) {
+        features8<0>(nb, f);
+        features8<8>(nb, f + 8);
+        features8<16>(nb, f + 16);
+        features8<24>(nb, f + 24);
+        features8<32>(nb, f + 32);
+        features8<40>(nb, f + 40);
+      } else {
+        features8<48>(nb, f);
+        features8<56>(nb, f + 8);
+        features8<64>(nb, f + 16);
+        features8<72>(nb, f + 24);
+        features8<80>(nb, f + 32);
+        features8<88>(nb, f + 40);
+      }
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        uint4 w = make_uint4(0u, 0u, 0u, 0u);
+        if (valid) {
+          w.x = pack_bf16(f[8 * c + 0], f[8 * c + 1]);
+          w.y = pack_bf16(f[8 * c + 2], f[8 * c + 3]);
+          w.z = pack_bf16(f[8 * c + 4], f[8 * c + 5]);
+          w.w = pack_bf16(f[8 * c + 6], f[8 * c + 7]);
+        }
+        *reinterpret_cast<uint4*>(A + core_off(row, (half * 6 + c) * 8, kHid)) = w;
+      }
       fence_async_smem();
-      fence_before();
-      __syncthreads();
-      fence_after();
-      if (tid == 0) {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(full_bar(st));
+    }
+  } else if (warp == kEpiWarps + kGatherWarps) {
+    // ---- MMA issue: one thread, whichever stage has a layer ready.  The
+    // per-stage state is indexed by unrolled loops only (registers); the
+    // issue code runs once per pick.
+    if (lane == 0) {
+      const uint32_t a0 = s_base + kPA, w1 = s_base + kW1, w2 = s_base + kW2, w3 = s_base + kW3;
+      const uint32_t id_hid = instr_desc(kRows, kHid), id_out = instr_desc(kRows, kN3);
+      int job[kStages];   // next layer of the stage's tile; 3: no tile left
+      int left[kStages];  // tiles of the stage not yet begun
+      unsigned fpar[kStages], commits[kStages];
+#pragma unroll
+      for (int st = 0; st < kStages; st++) {
+        left[st] = (int)stage_tiles(st);
+        job[st] = left[st] > 0 ? 0 : 3;
+        fpar[st] = 0;
+        commits[st] = 0;
+      }
+      unsigned idle = 0;
+      for (;;) {
+        int pick = -1, any = 0;
+#pragma unroll
+        for (int st = 0; st < kStages; st++) {
+          if (job[st] == 3) continue;
+          any = 1;
+          if (pick >= 0) continue;
+          const bool ready = job[st] == 0 ? mbar_test(full_bar(st), fpar[st]) : mbar_test(hid_bar(st), (uint32_t)(job[st] - 1));
+          if (ready) pick = st;
+        }
+        if (!any) break;
+        if (pick < 0) {
+          if (*abort_flag || ++idle > kIdleSweeps) {
+            if (!*abort_flag) give_up();
+            break;
+          }
+          continue;
+        }
+        idle = 0;
+        int layer = 0;
+#pragma unroll
+        for (int st = 0; st < kStages; st++)
+          if (st == pick) layer = job[st];
+        fence_after();
         const int ksteps = layer == 0 ? kK1 / 16 : kHid / 16;
         const uint32_t wb = layer == 0 ? w1 : layer == 1 ? w2 : w3;
-        const uint32_t wsbo = (layer == 0 ? kK1 : kHid) * 16;  // row-group stride of the weights
+        const uint32_t wsbo = (layer == 0 ? kK1 : kHid) * 16;
         const uint32_t idesc = layer == 2 ? id_out : id_hid;
-        for (int s = 0; s < ksteps; s++) {  // K step of 16 = two 16-byte chunks
-          const unsigned long long da = smem_desc(a_addr + s * 256, 128, kHid * 16);
-          const unsigned long long db = smem_desc(wb + s * 256, 128, wsbo);
-          mma_bf16(tmem, da, db, idesc, s > 0 ? 1u : 0u);
+        const uint32_t at = a0 + pick * kStageBytes, acc = tmem + pick * kHid;
+        for (int q = 0; q < ksteps; q++) {
+          const unsigned long long da = smem_desc(at + q * 256, 128, kHid * 16);
+          const unsigned long long db = smem_desc(wb + q * 256, 128, wsbo);
+          mma_bf16(acc, da, db, idesc, q > 0 ? 1u : 0u);
         }
-        mma_commit(bar);
+        mma_commit(done_bar(pick));
+#pragma unroll
+        for (int st = 0; st < kStages; st++)
+          if (st == pick) {
+            commits[st]++;
+            if (layer == 0) {
+              fpar[st] ^= 1u;
+              left[st]--;
+            }
+            job[st] = layer < 2 ? layer + 1 : (left[st] > 0 ? 0 : 3);
+          }
       }
-      pending = true;
-      // one thread waits for the MMA; the block barrier releases the others
-      const bool ok = tid == 0 ? mbar_wait_bounded(bar, parity) : true;
-      if (__syncthreads_or(!ok)) {
-        failed = true;
+      if (*abort_flag) {  // let the MMAs in flight finish before the memory is freed
+#pragma unroll
+        for (int st = 0; st < kStages; st++)
+          if (commits[st] > 0) mbar_wait_bounded(done_bar(st), (commits[st] - 1) & 1u);
+      }
+    }
+  } else {
+    // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (its rows),
+    // column part w / 4 of each hidden layer, for the stages of its group.
+    // As in the MMA thread, the per-stage state is indexed by unrolled loops
+    // only and the epilogue code runs once per pick.
+    constexpr int kMine = kStages / kEpiGroups;  // stages of a group: egrp + m * kEpiGroups
+    const int egrp = warp / kEpiGroupWarps, ew = warp % kEpiGroupWarps;
+    const int quarter = ew & 3, part = ew >> 2, row = quarter * 32 + lane;
+    const float* b1 = reinterpret_cast<const float*>(sm + kB1);
+    const float* b2 = reinterpret_cast<const float*>(sm + kB2);
+    const float* b3 = reinterpret_cast<const float*>(sm + kB3);
+    int layer[kMine], used[kMine], total[kMine];
+    unsigned seen[kMine];  // commits of the stage consumed
+#pragma unroll
+    for (int m = 0; m < kMine; m++) {
+      layer[m] = 0;
+      used[m] = 0;
+      seen[m] = 0;
+      total[m] = (int)stage_tiles(egrp + m * kEpiGroups);
+    }
+    unsigned idle = 0;
+    for (;;) {
+      int pick = -1, any = 0;
+#pragma unroll
+      for (int m = 0; m < kMine; m++) {
+        if (used[m] >= total[m]) continue;
+        any = 1;
+        if (pick >= 0) continue;
+        const int ready =
+            __shfl_sync(0xffffffffu, lane == 0 ? (int)mbar_test(done_bar(egrp + m * kEpiGroups), seen[m] & 1u) : 0, 0);
+        if (ready) pick = m;
+      }
+      if (!any) break;
+      if (pick < 0) {
+        if (*abort_flag || ++idle > kIdleSweeps) {
+          if (lane == 0 && !*abort_flag) give_up();
+          break;
+        }
+        __nanosleep(32);  // leave the issue slots to the warps with work
+        continue;
+      }
+      idle = 0;
+      int ly = 0, u = 0;
+      unsigned par = 0;
+#pragma unroll
+      for (int m = 0; m < kMine; m++)
+        if (m == pick) {
+          ly = layer[m];
+          u = used[m];
+          par = seen[m] & 1u;
+        }
+      const int st = egrp + pick * kEpiGroups;
+      if (!__all_sync(0xffffffffu, mbar_wait_bounded(done_bar(st), par))) {  // completed for lane 0: every lane acquires
+        if (lane == 0) give_up();
         break;
       }
-      pending = false;
-      parity ^= 1u;
       fence_after();
-      if (layer < 2) {
-        hidden_epilogue(tmem_row, layer == 0 ? b1 : b2, A, row, half);
-      } else if (half == 0) {
-        float v[32];
-        tmem_ld32(tmem_row, v);  // columns 0..31; the first 3 are the outputs
-        y[0] = v[0] + b3[0];
-        y[1] = v[1] + b3[1];
-        y[2] = v[2] + b3[2];
+      const uint32_t taddr = tmem + st * kHid + ((uint32_t)(quarter * 32) << 16);
+      unsigned char* A = sm + kPA + st * kStageBytes;
+      if (ly < 2) {
+        hidden_epilogue<kEpiCols>(taddr, ly == 0 ? b1 : b2, A, row, part);
+        fence_async_smem();
+        fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(hid_bar(st));
+      } else {
+        if (part == 0) {
+          float v[32];
+          tmem_ld32(taddr, v);  // columns 0..31; the first 3 are the outputs
+          const long long n = st + (long long)kStages * u;
+          const long long t = (blockIdx.x + n * gridDim.x) * kRows + row;
+          if (t < a.npts) {
+            const float y0 = v[0] + b3[0], y1 = v[1] + b3[1], y2 = v[2] + b3[2];
+            if (a.disp) {
+              a.disp[3 * t + 0] = y0;
+              a.disp[3 * t + 1] = y1;
+              a.disp[3 * t + 2] = y2;
+            }
+            if (a.wpxyz) {
+              int i, j, k;
+              node_of(a, t, i, j, k);
+              put_start(a, i, j, k, y0, y1, y2);
+            }
+          }
+        }
+        fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty_bar(st));
       }
+#pragma unroll
+      for (int m = 0; m < kMine; m++)
+        if (m == pick) {
+          seen[m]++;
+          if (ly < 2) {
+            layer[m] = ly + 1;
+          } else {
+            layer[m] = 0;
+            used[m]++;
+          }
+        }
     }
-    if (failed) break;
-    if (valid && half == 0) {
-      if (a.disp) {
-        a.disp[3 * t + 0] = y[0];
-        a.disp[3 * t + 1] = y[1];
-        a.disp[3 * t + 2] = y[2];
-      }
-      if (a.wpxyz) put_start(a, i, j, k, y[0], y[1], y[2]);
-    }
-  }
-  if (failed) {
-    if (tid == 0) atomicOr(g.status, kErrTimeout);
-    if (pending && tid == 0) mbar_wait_bounded(bar, parity);  // let the MMA in flight finish before freeing its memory
   }
   fence_before();
   __syncthreads();
   fence_after();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kPTmemCols) : "memory");
+}
+
+// launch of the inference kernel: one CTA per SM
+inline cudaError_t launch_guess(const Args& a, cudaStream_t s) {
+  if (a.npts <= 0) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(k_guess, cudaFuncAttributeMaxDynamicSharedMemorySize, kPSmem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long ntiles = (a.npts + kRows - 1) / kRows;
+  k_guess<<<(int)std::min<long long>(ntiles, sms), kPipeThreads, kPSmem, s>>>(a);
+  return cudaGetLastError();
 }
 
 // BF16 round to nearest even on the host
@@ -629,10 +853,6 @@ extern "C" int adzc_guess_apply(adzc_handle* h, const adzc_guess* net, double dt
   void *uvw = nullptr, *wdep = nullptr;
   int st = prepare_mixed(h, D, uu_ext, vv_ext, ww_ext, &uvw, &wdep, s);
   if (st != ADZC_OK) return adz_internal_fail(st);
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (cudaFuncSetAttribute(k_guess, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem) != cudaSuccess)
-    return adz_internal_fail(ADZC_ERR_CUDA);
   Args a{};
   a.g = D;
   a.uvw = (const float*)uvw;
@@ -645,13 +865,7 @@ extern "C" int adzc_guess_apply(adzc_handle* h, const adzc_guess* net, double dt
   a.stride = 1;
   a.nxc = D.ni;
   a.nyc = D.nj;
-  if (a.npts <= 0) return ADZC_OK;
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long ntiles = (a.npts + kRows - 1) / kRows;
-  const int grid = (int)std::min<long long>(ntiles, 2LL * sms);
-  k_guess<<<grid, kThreads, kSmem, s>>>(a);
-  return cudaGetLastError() == cudaSuccess ? ADZC_OK : adz_internal_fail(ADZC_ERR_CUDA);
+  return launch_guess(a, s) == cudaSuccess ? ADZC_OK : adz_internal_fail(ADZC_ERR_CUDA);
 }
 
 extern "C" int adzc_guess_apply_coarse(adzc_handle* h, const adzc_guess* net, double dt, const void* uu_ext,
@@ -686,15 +900,10 @@ extern "C" int adzc_guess_apply_coarse(adzc_handle* h, const adzc_guess* net, do
   if (st != ADZC_OK) return adz_internal_fail(st);
   a.uvw = (const float*)uvw;
   a.disp = (float*)cd;
-  int dev = 0;
+  int dev = 0, sms = 148;
   cudaGetDevice(&dev);
-  if (cudaFuncSetAttribute(k_guess, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem) != cudaSuccess)
-    return adz_internal_fail(ADZC_ERR_CUDA);
-  int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long ntiles = (a.npts + kRows - 1) / kRows;
-  k_guess<<<(int)std::min<long long>(ntiles, 2LL * sms), kThreads, kSmem, s>>>(a);
-  if (cudaGetLastError() != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
+  if (launch_guess(a, s) != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
   a.wpxyz = wpxyz;
   const long long n = (long long)D.ni * D.nj * nkp;
   const long long blocks = std::min<long long>((n + 255) / 256, (long long)sms * 16);
@@ -735,15 +944,7 @@ extern "C" int adzc_traject_guess(adzc_handle* h, const adzc_guess* net, int str
   if (st != ADZC_OK) return adz_internal_fail(st);
   a.uvw = (const float*)uvw;
   a.disp = (float*)cd;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (cudaFuncSetAttribute(k_guess, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem) != cudaSuccess)
-    return adz_internal_fail(ADZC_ERR_CUDA);
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long ntiles = (a.npts + kRows - 1) / kRows;
-  k_guess<<<(int)std::min<long long>(ntiles, 2LL * sms), kThreads, kSmem, s>>>(a);
-  if (cudaGetLastError() != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
+  if (launch_guess(a, s) != cudaSuccess) return adz_internal_fail(ADZC_ERR_CUDA);
   adz::TrajArgs t{};
   t.uvw_d = uvw;
   t.ut0 = ut0;
