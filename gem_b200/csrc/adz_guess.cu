@@ -56,7 +56,6 @@ constexpr int kB2 = kB1 + kHid * 4;
 constexpr int kB3 = kB2 + kHid * 4;
 constexpr int kNetBytes = kB3 + kN3 * 4;  // 62528
 constexpr unsigned kWaitPolls = 1u << 20;
-constexpr unsigned kIdleSweeps = 1u << 24;  // bound of a polling role's sweeps without progress
 static_assert(kNetBytes % 16 == 0, "weight image copied in 16-byte words");
 
 // byte offset of element (r, k) of a K-major BF16 operand with row length
@@ -356,22 +355,27 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, const float* 
 
 // ---------------------------------------------------------------------------
 // The inference kernel: one CTA per SM, warp-specialised, kStages tiles in
-// flight.  Each stage is one 128-row activation tile in shared memory and
-// one 128-column FP32 accumulator in tensor memory.
-//   gather warps (8)    features of the stage's 128 arrival points -> tile
-//                       (two threads per point, as the K chunks split);
-//   MMA thread (1)      whichever layer of whichever stage is ready: 6, 8 and
-//                       8 K steps, committed to the stage's done barrier;
-//   epilogue warps (8)  whichever stage's accumulator is complete: bias,
-//                       GELU, BF16 into the same tile (the next layer's
-//                       input), or the 3 outputs + bias of the last layer.
-// So one stage's gather and epilogue overlap the other stages' MMAs.  Per
-// stage barriers: full (gather -> MMA), hid (epilogue -> MMA, twice per
-// tile), done (MMA commit -> epilogue, three times per tile) and empty
-// (last epilogue -> gather).  Every wait is bounded: on expiry a role sets
-// the CTA's abort flag and raises kErrTimeout; the others see the flag and
-// stop, and the MMA thread waits (bounded) for its last commits before the
-// tensor memory is freed.
+// flight.  Tile n (of this CTA) lives in stage n mod kStages: one 128-row
+// activation tile in shared memory and one 128-column FP32 accumulator in
+// tensor memory.
+//   gather warps (8)     features of tile n's 128 arrival points -> tile
+//                        (two threads per point, as the K chunks split);
+//   MMA thread (1)       a fixed schedule: step n issues layer 2 of tile
+//                        n-1, layer 3 of tile n-2 and layer 1 of tile n
+//                        (8, 8 and 6 K steps), each committed to its stage's
+//                        done barrier;
+//   epilogue groups (2 x 8 warps)  group e takes the tiles n = e mod 2 in
+//                        the same order: the 3 outputs + bias of tile n-2,
+//                        then bias, GELU and BF16 of the two hidden layers of
+//                        tile n, written into the same tile as the next
+//                        layer's input.
+// So the gathers and epilogues of some tiles overlap the MMAs of others, and
+// the MMA thread never polls.  Per stage barriers: full (gather -> MMA), hid
+// (epilogue -> MMA, twice per tile), done (MMA commit -> epilogue, three
+// times per tile) and empty (last epilogue -> gather).  Every wait is
+// bounded: on expiry a role sets the CTA's abort flag and raises
+// kErrTimeout; the others see the flag and stop, and the MMA thread waits
+// (bounded) for its last commits before the tensor memory is freed.
 constexpr int kStages = 4;
 #ifndef ADZ_GUESS_GATHER_GROUPS
 #define ADZ_GUESS_GATHER_GROUPS 1
@@ -393,7 +397,6 @@ constexpr int kEpiGroupWarps = ADZ_GUESS_EPI_WARPS, kEpiWarps = kEpiGroupWarps *
 constexpr int kEpiCols = kHid / (kEpiGroupWarps / 4);
 constexpr int kGroupWarps = 8, kGatherWarps = kGroupWarps * kGatherGroups;
 static_assert(kEpiGroupWarps % 4 == 0 && kEpiCols % 32 == 0, "epilogue column parts of 32-column loads");
-static_assert(kStages % kEpiGroups == 0 && kStages % kGatherGroups == 0, "stages split evenly between groups");
 constexpr int kPipeThreads = (kEpiWarps + kGatherWarps + 1) * 32;
 constexpr int kStageBytes = kRows * kHid * 2;
 constexpr int kPA = (kNetBytes + 1023) / 1024 * 1024;
@@ -403,20 +406,6 @@ constexpr int kPAbort = kPTaddr + 4;
 constexpr int kPSmem = kPAbort + 4 + 1024;  // + alignment slack
 constexpr int kPTmemCols = kStages * kHid;  // 512: the whole of an SM's tensor memory
 static_assert(kPSmem <= 227 * 1024, "pipelined inference shared memory");
-
-// non-blocking test of a phase (try_wait may suspend the thread for a while,
-// which a role that polls several stages in turn must not do)
-__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
@@ -463,7 +452,13 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_guess(Args a) {
   const long long ntiles = (a.npts + kRows - 1) / kRows;
   // tiles of this CTA: blockIdx.x + n * gridDim.x, n = 0 .. nt-1, stage n % kStages
   const long long nt = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  auto stage_tiles = [&](int st) { return nt > st ? (nt - 1 - st) / kStages + 1 : 0LL; };
+  auto wait_or_abort = [&](uint32_t bar, uint32_t parity) {
+    for (unsigned q = 0; q < kWaitPolls; q++) {
+      if (mbar_try_wait(bar, parity)) return true;
+      if (*abort_flag) return false;
+    }
+    return false;
+  };
   auto give_up = [&]() {
     *abort_flag = 1;
     atomicOr(g.status, kErrTimeout);
@@ -533,176 +528,111 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_guess(Args a) {
       if (lane == 0) mbar_arrive(full_bar(st));
     }
   } else if (warp == kEpiWarps + kGatherWarps) {
-    // ---- MMA issue: one thread, whichever stage has a layer ready.  The
-    // per-stage state is indexed by unrolled loops only (registers); the
-    // issue code runs once per pick.
+    // ---- MMA issue, one thread, on a fixed schedule: step n issues layer
+    // 2 of tile n-1, layer 3 of tile n-2, then layer 1 of tile n, each once
+    // its input is ready (one bounded wait each)
     if (lane == 0) {
-      const uint32_t a0 = s_base + kPA, w1 = s_base + kW1, w2 = s_base + kW2, w3 = s_base + kW3;
       const uint32_t id_hid = instr_desc(kRows, kHid), id_out = instr_desc(kRows, kN3);
-      int job[kStages];   // next layer of the stage's tile; 3: no tile left
-      int left[kStages];  // tiles of the stage not yet begun
-      unsigned fpar[kStages], commits[kStages];
-#pragma unroll
-      for (int st = 0; st < kStages; st++) {
-        left[st] = (int)stage_tiles(st);
-        job[st] = left[st] > 0 ? 0 : 3;
-        fpar[st] = 0;
-        commits[st] = 0;
-      }
-      unsigned idle = 0;
-      for (;;) {
-        int pick = -1, any = 0;
-#pragma unroll
-        for (int st = 0; st < kStages; st++) {
-          if (job[st] == 3) continue;
-          any = 1;
-          if (pick >= 0) continue;
-          const bool ready = job[st] == 0 ? mbar_test(full_bar(st), fpar[st]) : mbar_test(hid_bar(st), (uint32_t)(job[st] - 1));
-          if (ready) pick = st;
-        }
-        if (!any) break;
-        if (pick < 0) {
-          if (*abort_flag || ++idle > kIdleSweeps) {
-            if (!*abort_flag) give_up();
-            break;
-          }
-          continue;
-        }
-        idle = 0;
-        int layer = 0;
-#pragma unroll
-        for (int st = 0; st < kStages; st++)
-          if (st == pick) layer = job[st];
+      // descriptors of K step 0; a K step of 16 is 256 bytes further (16 in
+      // the descriptor's address field)
+      const unsigned long long dw1 = smem_desc(s_base + kW1, 128, kK1 * 16);
+      const unsigned long long dw2 = smem_desc(s_base + kW2, 128, kHid * 16);
+      const unsigned long long dw3 = smem_desc(s_base + kW3, 128, kHid * 16);
+      const unsigned long long da0 = smem_desc(s_base + kPA, 128, kHid * 16);
+      unsigned commits[kStages] = {};
+      bool ok = true;
+      auto issue = [&](long long n, int layer) {
+        const int st = (int)(n % kStages);
+        const long long u = n / kStages;  // earlier tiles of this stage
+        const bool ready = layer == 0 ? wait_or_abort(full_bar(st), (uint32_t)(u & 1))
+                                      : wait_or_abort(hid_bar(st), (uint32_t)(layer - 1));
+        if (!ready) return false;
         fence_after();
+        const unsigned long long da = da0 + (unsigned long long)((st * kStageBytes) >> 4);
+        const unsigned long long db = layer == 0 ? dw1 : layer == 1 ? dw2 : dw3;
+        const uint32_t idesc = layer == 2 ? id_out : id_hid, acc = tmem + st * kHid;
         const int ksteps = layer == 0 ? kK1 / 16 : kHid / 16;
-        const uint32_t wb = layer == 0 ? w1 : layer == 1 ? w2 : w3;
-        const uint32_t wsbo = (layer == 0 ? kK1 : kHid) * 16;
-        const uint32_t idesc = layer == 2 ? id_out : id_hid;
-        const uint32_t at = a0 + pick * kStageBytes, acc = tmem + pick * kHid;
-        for (int q = 0; q < ksteps; q++) {
-          const unsigned long long da = smem_desc(at + q * 256, 128, kHid * 16);
-          const unsigned long long db = smem_desc(wb + q * 256, 128, wsbo);
-          mma_bf16(acc, da, db, idesc, q > 0 ? 1u : 0u);
-        }
-        mma_commit(done_bar(pick));
-#pragma unroll
-        for (int st = 0; st < kStages; st++)
-          if (st == pick) {
-            commits[st]++;
-            if (layer == 0) {
-              fpar[st] ^= 1u;
-              left[st]--;
-            }
-            job[st] = layer < 2 ? layer + 1 : (left[st] > 0 ? 0 : 3);
-          }
+        for (int q = 0; q < ksteps; q++) mma_bf16(acc, da + 16ull * q, db + 16ull * q, idesc, q > 0 ? 1u : 0u);
+        mma_commit(done_bar(st));
+        commits[st]++;
+        return true;
+      };
+      for (long long n = 0; n < nt + 2 && ok; n++) {
+        if (n >= 1 && n - 1 < nt) ok = issue(n - 1, 1);
+        if (ok && n >= 2) ok = issue(n - 2, 2);
+        if (ok && n < nt) ok = issue(n, 0);
       }
-      if (*abort_flag) {  // let the MMAs in flight finish before the memory is freed
-#pragma unroll
+      if (!ok) {
+        if (!*abort_flag) give_up();
+        // let the MMAs in flight finish before the memory is freed
         for (int st = 0; st < kStages; st++)
           if (commits[st] > 0) mbar_wait_bounded(done_bar(st), (commits[st] - 1) & 1u);
       }
     }
   } else {
     // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (its rows),
-    // column part w / 4 of each hidden layer, for the stages of its group.
-    // As in the MMA thread, the per-stage state is indexed by unrolled loops
-    // only and the epilogue code runs once per pick.
-    constexpr int kMine = kStages / kEpiGroups;  // stages of a group: egrp + m * kEpiGroups
+    // column part w / 4 of each hidden layer.  Group e takes the tiles
+    // n = e mod kEpiGroups in the MMA thread's order: the outputs of tile
+    // n-2, then the first and the second hidden layer of tile n.
     const int egrp = warp / kEpiGroupWarps, ew = warp % kEpiGroupWarps;
     const int quarter = ew & 3, part = ew >> 2, row = quarter * 32 + lane;
     const float* b1 = reinterpret_cast<const float*>(sm + kB1);
     const float* b2 = reinterpret_cast<const float*>(sm + kB2);
     const float* b3 = reinterpret_cast<const float*>(sm + kB3);
-    int layer[kMine], used[kMine], total[kMine];
-    unsigned seen[kMine];  // commits of the stage consumed
-#pragma unroll
-    for (int m = 0; m < kMine; m++) {
-      layer[m] = 0;
-      used[m] = 0;
-      seen[m] = 0;
-      total[m] = (int)stage_tiles(egrp + m * kEpiGroups);
-    }
-    unsigned idle = 0;
-    for (;;) {
-      int pick = -1, any = 0;
-#pragma unroll
-      for (int m = 0; m < kMine; m++) {
-        if (used[m] >= total[m]) continue;
-        any = 1;
-        if (pick >= 0) continue;
-        const int ready =
-            __shfl_sync(0xffffffffu, lane == 0 ? (int)mbar_test(done_bar(egrp + m * kEpiGroups), seen[m] & 1u) : 0, 0);
-        if (ready) pick = m;
-      }
-      if (!any) break;
-      if (pick < 0) {
-        if (*abort_flag || ++idle > kIdleSweeps) {
-          if (lane == 0 && !*abort_flag) give_up();
-          break;
-        }
-        __nanosleep(32);  // leave the issue slots to the warps with work
-        continue;
-      }
-      idle = 0;
-      int ly = 0, u = 0;
-      unsigned par = 0;
-#pragma unroll
-      for (int m = 0; m < kMine; m++)
-        if (m == pick) {
-          ly = layer[m];
-          u = used[m];
-          par = seen[m] & 1u;
-        }
-      const int st = egrp + pick * kEpiGroups;
-      if (!__all_sync(0xffffffffu, mbar_wait_bounded(done_bar(st), par))) {  // completed for lane 0: every lane acquires
-        if (lane == 0) give_up();
-        break;
-      }
-      fence_after();
+    // wait for commit c (0, 1, 2: layer) of tile n's stage; every lane acquires
+    auto await = [&](long long n, int c) {
+      const uint32_t par = (uint32_t)((3 * (n / kStages) + c) & 1);
+      const bool ok = __all_sync(0xffffffffu, wait_or_abort(done_bar((int)(n % kStages)), par));
+      if (ok) fence_after();
+      return ok;
+    };
+    auto hidden = [&](long long n, int layer) {
+      const int st = (int)(n % kStages);
       const uint32_t taddr = tmem + st * kHid + ((uint32_t)(quarter * 32) << 16);
-      unsigned char* A = sm + kPA + st * kStageBytes;
-      if (ly < 2) {
-        hidden_epilogue<kEpiCols>(taddr, ly == 0 ? b1 : b2, A, row, part);
-        fence_async_smem();
-        fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(hid_bar(st));
-      } else {
-        if (part == 0) {
-          float v[32];
-          tmem_ld32(taddr, v);  // columns 0..31; the first 3 are the outputs
-          const long long n = st + (long long)kStages * u;
-          const long long t = (blockIdx.x + n * gridDim.x) * kRows + row;
-          if (t < a.npts) {
-            const float y0 = v[0] + b3[0], y1 = v[1] + b3[1], y2 = v[2] + b3[2];
-            if (a.disp) {
-              a.disp[3 * t + 0] = y0;
-              a.disp[3 * t + 1] = y1;
-              a.disp[3 * t + 2] = y2;
-            }
-            if (a.wpxyz) {
-              int i, j, k;
-              node_of(a, t, i, j, k);
-              put_start(a, i, j, k, y0, y1, y2);
-            }
+      hidden_epilogue<kEpiCols>(taddr, layer == 0 ? b1 : b2, sm + kPA + st * kStageBytes, row, part);
+      fence_async_smem();
+      fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(hid_bar(st));
+    };
+    auto outputs = [&](long long n) {
+      const int st = (int)(n % kStages);
+      if (part == 0) {
+        float v[32];
+        tmem_ld32(tmem + st * kHid + ((uint32_t)(quarter * 32) << 16), v);  // the first 3 columns are the outputs
+        const long long t = (blockIdx.x + n * gridDim.x) * kRows + row;
+        if (t < a.npts) {
+          const float y0 = v[0] + b3[0], y1 = v[1] + b3[1], y2 = v[2] + b3[2];
+          if (a.disp) {
+            a.disp[3 * t + 0] = y0;
+            a.disp[3 * t + 1] = y1;
+            a.disp[3 * t + 2] = y2;
+          }
+          if (a.wpxyz) {
+            int i, j, k;
+            node_of(a, t, i, j, k);
+            put_start(a, i, j, k, y0, y1, y2);
           }
         }
-        fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(empty_bar(st));
       }
-#pragma unroll
-      for (int m = 0; m < kMine; m++)
-        if (m == pick) {
-          seen[m]++;
-          if (ly < 2) {
-            layer[m] = ly + 1;
-          } else {
-            layer[m] = 0;
-            used[m]++;
-          }
-        }
+      fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(empty_bar(st));
+    };
+    bool ok = true;
+    for (long long n = egrp; n - 2 < nt && ok; n += kEpiGroups) {
+      if (n >= 2) {
+        if (!(ok = await(n - 2, 2))) break;
+        outputs(n - 2);
+      }
+      if (n < nt) {
+        if (!(ok = await(n, 0))) break;
+        hidden(n, 0);
+        if (!(ok = await(n, 1))) break;
+        hidden(n, 1);
+      }
     }
+    if (!ok && lane == 0 && !*abort_flag) give_up();
   }
   fence_before();
   __syncthreads();
