@@ -360,10 +360,11 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, const float* 
 // tensor memory.
 //   gather warps (8)     features of tile n's 128 arrival points -> tile
 //                        (two threads per point, as the K chunks split);
-//   MMA thread (1)       a fixed schedule: step n issues layer 2 of tile
-//                        n-1, layer 3 of tile n-2 and layer 1 of tile n
+//   MMA thread (1)       a fixed schedule: step n issues layer 3 of tile
+//                        n-2, layer 2 of tile n-1 and layer 1 of tile n
 //                        (8, 8 and 6 K steps), each committed to its stage's
-//                        done barrier;
+//                        done barrier (of the six orders, the one a model of
+//                        the roles' measured durations puts first);
 //   epilogue groups (2 x 8 warps)  group e takes the tiles n = e mod 2 in
 //                        the same order: the 3 outputs + bias of tile n-2,
 //                        then bias, GELU and BF16 of the two hidden layers of
@@ -529,7 +530,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_guess(Args a) {
     }
   } else if (warp == kEpiWarps + kGatherWarps) {
     // ---- MMA issue, one thread, on a fixed schedule: step n issues layer
-    // 2 of tile n-1, layer 3 of tile n-2, then layer 1 of tile n, each once
+    // 3 of tile n-2, layer 2 of tile n-1, then layer 1 of tile n, each once
     // its input is ready (one bounded wait each)
     if (lane == 0) {
       const uint32_t id_hid = instr_desc(kRows, kHid), id_out = instr_desc(kRows, kN3);
@@ -558,8 +559,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_guess(Args a) {
         return true;
       };
       for (long long n = 0; n < nt + 2 && ok; n++) {
-        if (n >= 1 && n - 1 < nt) ok = issue(n - 1, 1);
-        if (ok && n >= 2) ok = issue(n - 2, 2);
+        if (n >= 2) ok = issue(n - 2, 2);
+        if (ok && n >= 1 && n - 1 < nt) ok = issue(n - 1, 1);
         if (ok && n < nt) ok = issue(n, 0);
       }
       if (!ok) {
