@@ -13,7 +13,9 @@
 // around L1.
 //
 // The tile of an item is ``rows`` consecutive rows of one level band
-// (rows * row length points); adzc_batch_tune times candidate row counts and
+// (rows * row length points; a trajectory item is the tiles of 32 i by 4
+// levels that cover rows / 4 such rows, as the per-domain trajectory kernel
+// walks its points); adzc_batch_tune times candidate row counts and
 // resident block counts and keeps the fastest.  The tuned launch is captured
 // in a CUDA graph (counter reset + persistent kernel) and replayed per step.
 //
@@ -86,7 +88,11 @@ int build_items(adzc_batch* b, int rows) {
         }
       };
       if (phase == 0) push(0, D.g.nij * D.g.nk, (long long)rows * D.g.nit);
-      if (phase == 1) push(0, (long long)D.g.ni * D.g.nj * (D.g.nk - D.ta.k00 + 1), (long long)rows * D.g.ni);
+      if (phase == 1) {  // in tiles of kBatchTileI i by kBatchTileK levels; rows / kBatchTileK tile rows an item
+        const long long nic = (D.g.ni + adz::kBatchTileI - 1) / adz::kBatchTileI;
+        const long long nkg = (D.g.nk - D.ta.k00 + 1 + adz::kBatchTileK - 1) / adz::kBatchTileK;
+        push(0, nic * nkg * D.g.nj, std::max(1, rows / adz::kBatchTileK) * nic);
+      }
       if (phase == 2)
         for (int q = 0; q < D.ngroups; q++) {
           const int* r = D.grange[q];

@@ -964,6 +964,22 @@ __device__ __forceinline__ void block_copy(T* dst, const T* src) {
   for (int q = threadIdx.x; q < (int)(sizeof(T) / 8); q += blockDim.x) d[q] = s[q];
 }
 
+// trajectory tiles [t0, t1) of a domain (one block of 128 threads per tile):
+// tile T covers i = 32 ic + 1 .., levels 4 kg + k00 .., row j, with T in
+// (ic, kg, j) order
+template <int PREC, bool DYN>
+__device__ __forceinline__ void batch_traject_tiles(const BDomC& C, long long t0, long long t1) {
+  const int nkp = C.g.nk - C.ta.k00 + 1;
+  const int nic = (C.g.ni + kBatchTileI - 1) / kBatchTileI, nkg = (nkp + kBatchTileK - 1) / kBatchTileK;
+  const int di = threadIdx.x % kBatchTileI, dk = threadIdx.x / kBatchTileI;
+  for (long long T = t0; T < t1; T++) {
+    const int i = (int)(T % nic) * kBatchTileI + di + 1;
+    const int k = (int)((T / nic) % nkg) * kBatchTileK + dk + C.ta.k00;
+    const int j = (int)(T / ((long long)nic * nkg)) + 1;
+    if (i <= C.g.ni && k <= C.g.nk) traject_point<PREC, DYN>(C.g, C.ta, i, j, k);
+  }
+}
+
 // MINB: minimum resident blocks per SM handed to ptxas (register budget);
 // the autotuner picks the variant
 template <int PREC, int MINB>
@@ -1017,14 +1033,8 @@ __global__ void __launch_bounds__(128, MINB) k_batch(const __grid_constant__ Bat
         for (long long e = item.start + threadIdx.x; e < end; e += blockDim.x)
           prepare_cell<PREC>(C.g, (const F*)C.uu, (const F*)C.vv, (const F*)C.ww, (F*)C.ta.uvw_d, e);
       } else if (item.phase == 1) {
-        // points in (i, k, j) order, as in k_traject
-        const int nkp = C.g.nk - C.ta.k00 + 1;
-        const long long nrow = (long long)C.g.ni * nkp;
-        for (long long t = item.start + threadIdx.x; t < end; t += blockDim.x) {
-          const int i = (int)(t % C.g.ni) + 1, k = (int)((t / C.g.ni) % nkp) + C.ta.k00;
-          const int j = (int)(t / nrow) + 1;
-          traject_point<PREC, true>(C.g, C.ta, i, j, k);
-        }
+        // tiles of 32 i by 4 levels in (i, k, j) tile order, as in k_traject
+        batch_traject_tiles<PREC, true>(C, item.start, end);
       } else {
         // points in (i, k, j) order, as in k_tricub_parts
         const int nx = srange[1], nz = C.g.nk - srange[4] + 1;
@@ -1074,14 +1084,7 @@ __device__ __forceinline__ void batch_phase_body(const BatchParams& P, const BDo
       for (long long e = item.start + threadIdx.x; e < end; e += blockDim.x)
         prepare_cell<PREC>(C.g, (const F*)C.uu, (const F*)C.vv, (const F*)C.ww, (F*)C.ta.uvw_d, e);
     } else if (PH == 1) {
-      // points in (i, k, j) order, as in k_traject
-      const int nkp = C.g.nk - C.ta.k00 + 1;
-      const long long nrow = (long long)C.g.ni * nkp;
-      for (long long t = item.start + threadIdx.x; t < end; t += blockDim.x) {
-        const int i = (int)(t % C.g.ni) + 1, k = (int)((t / C.g.ni) % nkp) + C.ta.k00;
-        const int j = (int)(t / nrow) + 1;
-        traject_point<PREC, false>(C.g, C.ta, i, j, k);
-      }
+      batch_traject_tiles<PREC, false>(C, item.start, end);
     } else {
       // points in (i, k, j) order, as in k_tricub_parts
       const int nx = srange[1], nz = C.g.nk - srange[4] + 1;

@@ -199,6 +199,11 @@ struct BItem {
 };
 
 constexpr int kBatchVariants = 3;  // register budgets of the batch kernel
+// trajectory items of the batch are runs of tiles of kBatchTileI consecutive
+// i by kBatchTileK consecutive levels (one warp row per level, a block of 128
+// threads per tile), as the per-domain trajectory kernel walks its points
+constexpr int kBatchTileI = 32, kBatchTileK = 4;
+static_assert(kBatchTileI * kBatchTileK == 128, "a batch trajectory tile is one block of 128 threads");
 template <int PREC>
 cudaError_t launch_tricub_parts(const DGrid& g, const SetArgs& a, const SetParts& sp, cudaStream_t s);
 // the tile geometry of the LAM boundary-flux masks (adz_bcflux.cu)
