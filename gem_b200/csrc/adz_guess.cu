@@ -55,6 +55,7 @@ constexpr int kB1 = kW3 + kN3 * kHid * 2;
 constexpr int kB2 = kB1 + kHid * 4;
 constexpr int kB3 = kB2 + kHid * 4;
 constexpr int kNetBytes = kB3 + kN3 * 4;  // 62528
+static_assert(kB1 % 16 == 0 && kB2 % 16 == 0, "biases read as 16-byte vectors");
 constexpr unsigned kWaitPolls = 1u << 20;
 static_assert(kNetBytes % 16 == 0, "weight image copied in 16-byte words");
 
@@ -338,12 +339,12 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, const float* 
     for (int q = 0; q < 4; q++) {
       uint4 w;
       const int c = c0 + 8 * q;
-      const float2 b01 = *reinterpret_cast<const float2*>(bias + c), b23 = *reinterpret_cast<const float2*>(bias + c + 2);
-      const float2 b45 = *reinterpret_cast<const float2*>(bias + c + 4), b67 = *reinterpret_cast<const float2*>(bias + c + 6);
-      const float2 h01 = __fadd2_rn(make_float2(v[8 * q + 0], v[8 * q + 1]), b01);
-      const float2 h23 = __fadd2_rn(make_float2(v[8 * q + 2], v[8 * q + 3]), b23);
-      const float2 h45 = __fadd2_rn(make_float2(v[8 * q + 4], v[8 * q + 5]), b45);
-      const float2 h67 = __fadd2_rn(make_float2(v[8 * q + 6], v[8 * q + 7]), b67);
+      // the biases are 16-byte aligned in shared memory (c is a multiple of 8)
+      const float4 b0 = *reinterpret_cast<const float4*>(bias + c), b1 = *reinterpret_cast<const float4*>(bias + c + 4);
+      const float2 h01 = __fadd2_rn(make_float2(v[8 * q + 0], v[8 * q + 1]), make_float2(b0.x, b0.y));
+      const float2 h23 = __fadd2_rn(make_float2(v[8 * q + 2], v[8 * q + 3]), make_float2(b0.z, b0.w));
+      const float2 h45 = __fadd2_rn(make_float2(v[8 * q + 4], v[8 * q + 5]), make_float2(b1.x, b1.y));
+      const float2 h67 = __fadd2_rn(make_float2(v[8 * q + 6], v[8 * q + 7]), make_float2(b1.z, b1.w));
       w.x = gelu_bf16x2(h01);
       w.y = gelu_bf16x2(h23);
       w.z = gelu_bf16x2(h45);

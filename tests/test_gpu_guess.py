@@ -146,12 +146,15 @@ def _odelz_m(levels):
     return np.array([1.0 / (zm[k + 1] - zm[k]) for k in range(nk + 1)])
 
 
-def test_features_and_bf16_inference_vs_oracle():
+# 40x36x16: 180 full tiles, one or two per CTA (no stage reused); 67x53x29:
+# about 800 tiles with a partial last one, so every CTA reuses its four stages
+@pytest.mark.parametrize("size", [(40, 36, 16), (67, 53, 29)])
+def test_features_and_bf16_inference_vs_oracle(size):
     _need_gpu()
     from gem_b200 import adz as A, guess, synth
     from oracle import oracle as O
     prec = A.MIXED
-    adz, cfg, inp, ad = _case(prec, (40, 36, 16))
+    adz, cfg, inp, ad = _case(prec, size)
     # oracle departure winds from the same FP32 inputs, in FP64
     st = O.Step(cfg, kind="oracle", prec="f64")
     st.inittraj()
