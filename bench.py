@@ -107,6 +107,8 @@ def dist_init():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)  # before the process group, so NCCL binds this rank's GPU
     if ws > 1 and not torch.distributed.is_initialized():
         import datetime
         backend = "nccl" if torch.cuda.is_available() else "gloo"
