@@ -171,6 +171,10 @@ struct Args {
   // coarse evaluation: the network runs on the nodes i = min(1 + stride*m, ni),
   // j likewise (nxc x nyc nodes per level, every level); stride 1 is every point
   int stride, nxc, nyc;
+  // failure-path tests (adzc_guess_inject): bound of a pipeline wait in polls
+  // (0: kWaitPolls), and whether each CTA's first gather withholds its signal
+  unsigned polls;
+  int withhold;
 };
 
 __device__ __forceinline__ long long wp_at(const DGrid& g, int i, int j, int k, int c) {
@@ -454,8 +458,9 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_guess(Args a) {
   const long long ntiles = (a.npts + kRows - 1) / kRows;
   // tiles of this CTA: blockIdx.x + n * gridDim.x, n = 0 .. nt-1, stage n % kStages
   const long long nt = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const unsigned polls = a.polls ? a.polls : kWaitPolls;
   auto wait_or_abort = [&](uint32_t bar, uint32_t parity) {
-    for (unsigned q = 0; q < kWaitPolls; q++) {
+    for (unsigned q = 0; q < polls; q++) {
       if (mbar_try_wait(bar, parity)) return true;
       if (*abort_flag) return false;
     }
@@ -478,7 +483,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_guess(Args a) {
         const uint32_t par = (uint32_t)((use - 1) & 1);
         int ok = 0;
         if (lane == 0)
-          for (unsigned q = 0; q < kWaitPolls && !ok; q++) {
+          for (unsigned q = 0; q < polls && !ok; q++) {
             ok = mbar_try_wait(empty_bar(st), par);
             if (!ok && *abort_flag) break;
           }
@@ -527,7 +532,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_guess(Args a) {
       }
       fence_async_smem();
       __syncwarp();
-      if (lane == 0) mbar_arrive(full_bar(st));
+      if (lane == 0 && !(a.withhold && n == 0)) mbar_arrive(full_bar(st));
     }
   } else if (warp == kEpiWarps + kGatherWarps) {
     // ---- MMA issue, one thread, on a fixed schedule: step n issues layer
@@ -670,6 +675,8 @@ inline uint16_t bf16_bits(float f) {
 struct adzc_guess {
   unsigned char* d_net = nullptr;
   int device = 0;
+  unsigned polls = 0;  // adzc_guess_inject
+  int withhold = 0;
 };
 
 namespace {
@@ -725,6 +732,18 @@ extern "C" int adzc_guess_create(const float* const* params, adzc_guess** out) {
     return adz_internal_fail(ADZC_ERR_CUDA);
   }
   *out = net;
+  return ADZC_OK;
+}
+
+extern "C" int adzc_guess_inject(adzc_guess* net, int what, long long value) {
+  if (!net || value < 0) return adz_internal_fail(ADZC_ERR_ARG);
+  if (what == ADZC_INJECT_SPINS && value <= 0x7fffffffLL) {
+    net->polls = (unsigned)value;
+  } else if (what == ADZC_INJECT_WITHHOLD && value <= 1) {
+    net->withhold = (int)value;
+  } else {
+    return adz_internal_fail(ADZC_ERR_ARG);
+  }
   return ADZC_OK;
 }
 
@@ -791,6 +810,8 @@ extern "C" int adzc_guess_apply(adzc_handle* h, const adzc_guess* net, double dt
   a.wpxyz = wpxyz;
   a.disp = disp;
   a.net = net->d_net;
+  a.polls = net->polls;
+  a.withhold = net->withhold;
   a.k00 = k00_of(D);
   a.npts = (long long)D.ni * D.nj * (D.nk - a.k00 + 1);
   a.dt = dt;
@@ -816,6 +837,8 @@ extern "C" int adzc_guess_apply_coarse(adzc_handle* h, const adzc_guess* net, do
   Args a{};
   a.g = D;
   a.net = net->d_net;
+  a.polls = net->polls;
+  a.withhold = net->withhold;
   a.k00 = k00_of(D);
   a.dt = dt;
   a.stride = stride;
@@ -860,6 +883,8 @@ extern "C" int adzc_traject_guess(adzc_handle* h, const adzc_guess* net, int str
   Args a{};
   a.g = D;
   a.net = net->d_net;
+  a.polls = net->polls;
+  a.withhold = net->withhold;
   a.k00 = k00_of(D);
   a.dt = dt;
   a.stride = stride;

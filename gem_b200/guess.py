@@ -41,6 +41,7 @@ def _lib():
         L.adzc_traject_tol.argtypes = [vp, i, d, d, i, i] + [vp] * 6 + [vp, vp, vp, vp]
         L.adzc_guess_create.argtypes = [vp, C.POINTER(vp)]
         L.adzc_guess_destroy.argtypes = [vp]
+        L.adzc_guess_inject.argtypes = [vp, i, C.c_longlong]
         L.adzc_guess_npoints.argtypes = [vp]
         L.adzc_guess_npoints.restype = C.c_longlong
         L.adzc_guess_apply.argtypes = [vp, vp, d, vp, vp, vp, vp, vp, vp]
@@ -108,6 +109,14 @@ class GuessNet:
         ptrs = (C.c_void_p * 6)(*(a.ctypes.data for a in self._arrs))
         self.h = C.c_void_p()
         A._check(_lib().adzc_guess_create(C.cast(ptrs, C.c_void_p), C.byref(self.h)), "adzc_guess_create")
+
+    INJECT_SPINS, INJECT_WITHHOLD = 1, 3  # inject(): fault injection for failure-path tests
+
+    def inject(self, what: int, value: int):
+        """adzc_guess_inject: INJECT_SPINS sets the bound of the kernel's
+        waits in polls (0: default); INJECT_WITHHOLD 1 makes each CTA's first
+        tile never signal its MMA, so the wait runs out (0 clears)."""
+        A._check(_lib().adzc_guess_inject(self.h, int(what), int(value)), "adzc_guess_inject")
 
     def apply(self, ad: A.Adz, dt: float, winds: dict, wpxyz=None, disp=None, stream=None):
         """Start points into wpxyz and/or the displacement into disp (npoints x 3)."""

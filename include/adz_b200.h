@@ -387,6 +387,15 @@ int adzc_traject_tol(adzc_handle *h, int prec, double dt, double tol, int maxit,
 typedef struct adzc_guess adzc_guess;
 int adzc_guess_create(const float *const *params, adzc_guess **out);
 int adzc_guess_destroy(adzc_guess *net);
+/* Fault injection for tests of the inference kernel's failure path, on the
+ * host (no GPU fault); no counterpart in the reference.  ADZC_INJECT_SPINS:
+ * bound of a wait between the kernel's roles, in polls (0: the default,
+ * about 1 s).  ADZC_INJECT_WITHHOLD (value 1): the features of each CTA's
+ * first tile never signal the MMA thread, so its wait runs out; the kernel
+ * raises ADZC_ERR_TIMEOUT in the handle's status (adzc_status), frees its
+ * tensor memory and returns (0 clears).  Applies to the calls that follow. */
+#define ADZC_INJECT_WITHHOLD 3
+int adzc_guess_inject(adzc_guess *net, int what, long long value);
 /* arrival points of the trajectory (ni*nj*(nk-k00+1)), -1 on a bad handle */
 long long adzc_guess_npoints(adzc_handle *h);
 /* start points X - d, Y - d, k - d (vertical clipped to 1..nk) into wpxyz,

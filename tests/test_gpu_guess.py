@@ -296,3 +296,39 @@ def test_fused_learned_trajectory_matches_the_two_calls():
         assert torch.equal(st_a, st_b), stride
         assert torch.equal(wp_a.view(torch.int64), wp_b.view(torch.int64)), stride
         assert st_b[2].item() == 0
+
+
+def test_inference_wait_times_out_and_recovers():
+    """Failure detection without a GPU fault: each CTA's first tile is made to
+    withhold its signal to the MMA thread (host-side injection) under a short
+    wait bound.  The wait runs out, every role of the kernel stops, the host
+    reads ADZC_ERR_TIMEOUT, and the next call (injection cleared) gives the
+    same displacements as a network that never saw the fault: the context
+    stays usable."""
+    import time
+    _need_gpu()
+    from gem_b200 import adz as A, guess
+    _, cfg, inp, ad = _case(A.MIXED, (67, 53, 29))
+    n = guess.npoints(ad)
+    ref = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    guess.GuessNet(_params(13)).apply(ad, cfg.dt, inp, disp=ref)
+    torch.cuda.synchronize()
+    assert ad.status() == 0
+    net = guess.GuessNet(_params(13))
+    net.inject(net.INJECT_SPINS, 1 << 14)
+    net.inject(net.INJECT_WITHHOLD, 1)
+    out = torch.zeros_like(ref)
+    t0 = time.time()
+    net.apply(ad, cfg.dt, inp, disp=out)
+    torch.cuda.synchronize()
+    assert time.time() - t0 < 60
+    assert ad.status() == 6  # ADZC_ERR_TIMEOUT, read and reset
+    assert ad.status() == 0
+    net.inject(net.INJECT_WITHHOLD, 0)
+    net.inject(net.INJECT_SPINS, 0)
+    net.apply(ad, cfg.dt, inp, disp=out)
+    torch.cuda.synchronize()
+    assert ad.status() == 0
+    assert torch.equal(out, ref)
+    with pytest.raises(A.AdzError):
+        net.inject(9, 1)
