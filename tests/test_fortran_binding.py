@@ -209,3 +209,40 @@ def test_nullable_host_arrays_are_optional():
                      ("adzc_step_noalloc", ("mono",)), ("adzc_ilmc", ("rounds",))):
         for a in args:
             assert "optional" in f[fn]["decl"][a][1], f"{fn}({a})"
+
+
+def _header_constants():
+    """#define ADZC_* of the header with their values (integer or real)."""
+    out = {}
+    for m in re.finditer(r"^#define\s+(ADZC_\w+)\s+(.+?)\s*(?:/\*.*)?$", open(HDR).read(), re.M):
+        expr = m.group(2).strip()
+        shift = re.fullmatch(r"\((\d+)u?\s*<<\s*(\d+)\)", expr)
+        if shift:
+            out[m.group(1)] = int(shift.group(1)) << int(shift.group(2))
+        elif re.fullmatch(r"-?\d+", expr):
+            out[m.group(1)] = int(expr)
+        elif re.fullmatch(r"-?\d+\.\d*", expr):
+            out[m.group(1)] = float(expr)
+    return out
+
+
+def _include_parameters():
+    """parameter :: NAME = value of the include, continuation lines joined."""
+    text = re.sub(r"&\s*\n\s*&?", " ", open(INC).read())
+    out = {}
+    for m in re.finditer(r"^\s*(integer|real)\((C_\w+)\),\s*parameter\s*::\s*(.+)$", text, re.M | re.I):
+        for item in m.group(3).split(","):
+            name, value = (x.strip() for x in item.split("=", 1))
+            value = re.sub(r"_C_\w+$", "", value)
+            out[name] = float(value.replace("d", "e")) if m.group(1).lower() == "real" else int(value)
+    return out
+
+
+def test_constants_match_header():
+    """Every ADZC_ constant of the header is a parameter of the include, with
+    the same value (status codes, precisions, sets, limits)."""
+    h, f = _header_constants(), _include_parameters()
+    assert len(h) > 30
+    missing = sorted(set(h) - set(f))
+    assert not missing, missing
+    assert {k: f[k] for k in h} == h
