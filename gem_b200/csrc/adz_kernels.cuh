@@ -803,14 +803,17 @@ __global__ void ADZ_SET_BOUNDS k_tricub_parts(DGrid g, SetArgs a, const __grid_c
   const int q = (int)(blockIdx.x % (unsigned)sp.n);
   const SetPart& P = sp.p[q];
 #if ADZ_SET_TILE_K > 1
+  // 32-bit tile arithmetic (the grid stays below 2^31 blocks): 64-bit
+  // indices here cost registers the point code needs at 9 resident blocks
   constexpr int TK = ADZ_SET_TILE_K, TI = 128 / TK;
-  const long long b = blockIdx.x / (unsigned)sp.n;
-  const int nic = (P.nx + TI - 1) / TI, nkg = (P.nz + TK - 1) / TK;
-  const int ii = (int)(b % nic) * TI + (threadIdx.x % TI);
-  const int kk = (int)((b / nic) % nkg) * TK + (threadIdx.x / TI);
-  const long long jj = b / ((long long)nic * nkg);
+  const unsigned b = blockIdx.x / (unsigned)sp.n;
+  const unsigned nic = (unsigned)(P.nx + TI - 1) / TI, nkg = (unsigned)(P.nz + TK - 1) / TK;
+  const unsigned bj = b / nic, bk = bj % nkg;
+  const int ii = (int)(b - bj * nic) * TI + (int)(threadIdx.x % TI);
+  const int kk = (int)bk * TK + (int)(threadIdx.x / TI);
+  const int jj = (int)(bj / nkg);
   if (ii >= P.nx || kk >= P.nz || jj >= P.ny) return;
-  set_point<PREC, false, PERT>(g, P.set, a, P.fp, ii + P.i0, (int)jj + P.j0, kk + P.k0);
+  set_point<PREC, false, PERT>(g, P.set, a, P.fp, ii + P.i0, jj + P.j0, kk + P.k0);
 #else
   const long long t = (long long)(blockIdx.x / (unsigned)sp.n) * blockDim.x + threadIdx.x;
   // points in (i, k, j) order, as in k_traject
