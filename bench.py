@@ -39,11 +39,11 @@ TENSOR_FALLBACK_TFLOPS = 1590.0
 # by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on a 384x384x80 tile
 # with u, v, w + 4 tracers; traffic grows in proportion to the points, so it
 # scales to the benched tile
-MEASURED_TRAFFIC_PER_POINT = {"traject": 73.65, "sets": 84.71}
+MEASURED_TRAFFIC_PER_POINT = {"traject": 73.59, "sets": 84.65}
 # L1 data-pipe wavefronts (l1tex__data_pipe_lsu_wavefronts.sum) per grid point
 # of each MIXED launch, same capture (384x384x80, u, v, w + 4 tracers); the
 # pipe returns one wavefront per SM cycle, the bound both gather kernels reach
-MEASURED_L1_WAVEFRONTS_PER_POINT = {"traject": 25.61, "sets": 33.76}
+MEASURED_L1_WAVEFRONTS_PER_POINT = {"traject": 25.66, "sets": 30.24}
 
 
 def peaks():

@@ -13,9 +13,10 @@
 // around L1.
 //
 // The tile of an item is ``rows`` consecutive rows of one level band
-// (rows * row length points; a trajectory item is the tiles of 32 i by 4
-// levels that cover rows / 4 such rows, as the per-domain trajectory kernel
-// walks its points); adzc_batch_tune times candidate row counts and
+// (rows * row length points; trajectory and interpolation items of regions
+// that tiles of 32 i by 4 levels cover with few idle lanes are the tiles that
+// cover rows / 4 such rows, as the per-domain kernels walk their points);
+// adzc_batch_tune times candidate row counts and
 // resident block counts and keeps the fastest.  The tuned launch is captured
 // in a CUDA graph (counter reset + persistent kernel) and replayed per step.
 //
@@ -75,12 +76,13 @@ int build_items(adzc_batch* b, int rows) {
     b->pstart[phase] = (long long)items.size();
     for (int d = 0; d < b->ndom; d++) {
       const adz::BDom& D = b->doms[d];
-      auto push = [&](int group, long long n, long long chunk) {
+      auto push = [&](int group, long long n, long long chunk, int tiles = 0) {
         for (long long s = 0; s < n; s += chunk) {
           adz::BItem it{};
           it.dom = d;
           it.phase = phase;
           it.group = group;
+          it.tiles = tiles;
           it.start = s;
           it.count = std::min(chunk, n - s);
           items.push_back(it);
@@ -88,15 +90,23 @@ int build_items(adzc_batch* b, int rows) {
         }
       };
       if (phase == 0) push(0, D.g.nij * D.g.nk, (long long)rows * D.g.nit);
-      if (phase == 1) {  // in tiles of kBatchTileI i by kBatchTileK levels; rows / kBatchTileK tile rows an item
-        const long long nic = (D.g.ni + adz::kBatchTileI - 1) / adz::kBatchTileI;
-        const long long nkg = (D.g.nk - D.ta.k00 + 1 + adz::kBatchTileK - 1) / adz::kBatchTileK;
-        push(0, nic * nkg * D.g.nj, std::max(1, rows / adz::kBatchTileK) * nic);
-      }
+      // a region of nx i by nz levels by ny rows: tiles of kBatchTileI i by
+      // kBatchTileK levels (rows / kBatchTileK tile rows an item) where they
+      // leave few lanes idle, else points in (i, k, j) order (rows rows)
+      auto region = [&](int group, long long nx, long long nz, long long ny) {
+        if (adz::batch_use_tiles(nx, nz)) {
+          const long long nic = (nx + adz::kBatchTileI - 1) / adz::kBatchTileI;
+          const long long nkg = (nz + adz::kBatchTileK - 1) / adz::kBatchTileK;
+          push(group, nic * nkg * ny, std::max(1, rows / adz::kBatchTileK) * nic, 1);
+        } else {
+          push(group, nx * nz * ny, (long long)rows * nx, 0);
+        }
+      };
+      if (phase == 1) region(0, D.g.ni, D.g.nk - D.ta.k00 + 1, D.g.nj);
       if (phase == 2)
         for (int q = 0; q < D.ngroups; q++) {
           const int* r = D.grange[q];
-          push(q, (long long)r[1] * r[3] * (D.g.nk - r[4] + 1), (long long)rows * r[1]);
+          region(q, r[1], D.g.nk - r[4] + 1, r[3]);
         }
     }
   }

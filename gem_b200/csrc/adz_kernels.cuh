@@ -967,20 +967,36 @@ __device__ __forceinline__ void block_copy(T* dst, const T* src) {
   for (int q = threadIdx.x; q < (int)(sizeof(T) / 8); q += blockDim.x) d[q] = s[q];
 }
 
-// trajectory tiles [t0, t1) of a domain (one block of 128 threads per tile):
-// tile T covers i = 32 ic + 1 .., levels 4 kg + k00 .., row j, with T in
-// (ic, kg, j) order
-template <int PREC, bool DYN>
-__device__ __forceinline__ void batch_traject_tiles(const BDomC& C, long long t0, long long t1) {
-  const int nkp = C.g.nk - C.ta.k00 + 1;
-  const int nic = (C.g.ni + kBatchTileI - 1) / kBatchTileI, nkg = (nkp + kBatchTileK - 1) / kBatchTileK;
-  const int di = threadIdx.x % kBatchTileI, dk = threadIdx.x / kBatchTileI;
-  for (long long T = t0; T < t1; T++) {
-    const int i = (int)(T % nic) * kBatchTileI + di + 1;
-    const int k = (int)((T / nic) % nkg) * kBatchTileK + dk + C.ta.k00;
-    const int j = (int)(T / ((long long)nic * nkg)) + 1;
-    if (i <= C.g.ni && k <= C.g.nk) traject_point<PREC, DYN>(C.g, C.ta, i, j, k);
+// The points of a batch item, one per thread per unit.  A tiled item counts
+// tiles of kBatchTileI i by kBatchTileK levels of a region (nx i by nz levels
+// by ny rows from i0, k0, j0) in (i, k, j) tile order, one unit per tile; a
+// row item counts points in (i, k, j) order, 128 per unit.  32-bit tile
+// arithmetic; the point code is inlined once per phase.
+struct BatchRegion {
+  int i0, nx, j0, k0, nz;
+};
+__device__ __forceinline__ long long batch_units(const BItem& item) {
+  return item.tiles ? item.count : (item.count + 127) / 128;
+}
+__device__ __forceinline__ bool batch_point(const BItem& item, const BatchRegion& R, long long u, int& i, int& j,
+                                            int& k) {
+  if (item.tiles) {
+    const unsigned nic = ((unsigned)R.nx + kBatchTileI - 1) / kBatchTileI;
+    const unsigned nkg = ((unsigned)R.nz + kBatchTileK - 1) / kBatchTileK;
+    const unsigned T = (unsigned)(item.start + u), bj = T / nic;
+    const unsigned ii = (T - bj * nic) * kBatchTileI + threadIdx.x % kBatchTileI;
+    const unsigned kk = (bj % nkg) * kBatchTileK + threadIdx.x / kBatchTileI;
+    i = (int)ii + R.i0;
+    k = (int)kk + R.k0;
+    j = (int)(bj / nkg) + R.j0;
+    return ii < (unsigned)R.nx && kk < (unsigned)R.nz;
   }
+  const long long t = item.start + u * 128 + threadIdx.x;
+  const long long nrow = (long long)R.nx * R.nz;
+  i = (int)(t % R.nx) + R.i0;
+  k = (int)((t / R.nx) % R.nz) + R.k0;
+  j = (int)(t / nrow) + R.j0;
+  return t < item.start + item.count;
 }
 
 // MINB: minimum resident blocks per SM handed to ptxas (register budget);
@@ -1037,15 +1053,16 @@ __global__ void __launch_bounds__(128, MINB) k_batch(const __grid_constant__ Bat
           prepare_cell<PREC>(C.g, (const F*)C.uu, (const F*)C.vv, (const F*)C.ww, (F*)C.ta.uvw_d, e);
       } else if (item.phase == 1) {
         // tiles of 32 i by 4 levels in (i, k, j) tile order, as in k_traject
-        batch_traject_tiles<PREC, true>(C, item.start, end);
+        const BatchRegion R{1, C.g.ni, 1, C.ta.k00, C.g.nk - C.ta.k00 + 1};
+        for (long long u = 0; u < batch_units(item); u++) {
+          int i, j, k;
+          if (batch_point(item, R, u, i, j, k)) traject_point<PREC, true>(C.g, C.ta, i, j, k);
+        }
       } else {
-        // points in (i, k, j) order, as in k_tricub_parts
-        const int nx = srange[1], nz = C.g.nk - srange[4] + 1;
-        const long long nrow = (long long)nx * nz;
-        for (long long t = item.start + threadIdx.x; t < end; t += blockDim.x) {
-          const int i = (int)(t % nx) + srange[0], k = (int)((t / nx) % nz) + srange[4];
-          const int j = (int)(t / nrow) + srange[2];
-          set_point<PREC, true>(C.g, sset, C.sa, sfp, i, j, k);
+        const BatchRegion R{srange[0], srange[1], srange[2], srange[4], C.g.nk - srange[4] + 1};
+        for (long long u = 0; u < batch_units(item); u++) {
+          int i, j, k;
+          if (batch_point(item, R, u, i, j, k)) set_point<PREC, true>(C.g, sset, C.sa, sfp, i, j, k);
         }
       }
     }
@@ -1087,15 +1104,16 @@ __device__ __forceinline__ void batch_phase_body(const BatchParams& P, const BDo
       for (long long e = item.start + threadIdx.x; e < end; e += blockDim.x)
         prepare_cell<PREC>(C.g, (const F*)C.uu, (const F*)C.vv, (const F*)C.ww, (F*)C.ta.uvw_d, e);
     } else if (PH == 1) {
-      batch_traject_tiles<PREC, false>(C, item.start, end);
+      const BatchRegion R{1, C.g.ni, 1, C.ta.k00, C.g.nk - C.ta.k00 + 1};
+      for (long long u = 0; u < batch_units(item); u++) {
+        int i, j, k;
+        if (batch_point(item, R, u, i, j, k)) traject_point<PREC, false>(C.g, C.ta, i, j, k);
+      }
     } else {
-      // points in (i, k, j) order, as in k_tricub_parts
-      const int nx = srange[1], nz = C.g.nk - srange[4] + 1;
-      const long long nrow = (long long)nx * nz;
-      for (long long t = item.start + threadIdx.x; t < end; t += blockDim.x) {
-        const int i = (int)(t % nx) + srange[0], k = (int)((t / nx) % nz) + srange[4];
-        const int j = (int)(t / nrow) + srange[2];
-        set_point<PREC, false>(C.g, sset, C.sa, sfp, i, j, k);
+      const BatchRegion R{srange[0], srange[1], srange[2], srange[4], C.g.nk - srange[4] + 1};
+      for (long long u = 0; u < batch_units(item); u++) {
+        int i, j, k;
+        if (batch_point(item, R, u, i, j, k)) set_point<PREC, false>(C.g, sset, C.sa, sfp, i, j, k);
       }
     }
     __syncthreads();  // every thread is done with cur and sfp

@@ -194,7 +194,8 @@ struct BatchParams {
 static_assert(sizeof(BatchParams) <= 32000, "kernel parameter limit");
 
 struct BItem {
-  int dom, phase, group, pad;
+  int dom, phase, group;
+  int tiles;  // phases 1 and 2: 1 when start/count count tiles of kBatchTileI x kBatchTileK, 0 points
   long long start, count;
 };
 
@@ -203,6 +204,12 @@ constexpr int kBatchVariants = 3;  // register budgets of the batch kernel
 // i by kBatchTileK consecutive levels (one warp row per level, a block of 128
 // threads per tile), as the per-domain trajectory kernel walks its points
 constexpr int kBatchTileI = 32, kBatchTileK = 4;
+// a region walks tiles when they leave at most 10 % of their lanes idle,
+// else rows of consecutive i (narrow and shallow domains)
+inline bool batch_use_tiles(long long nx, long long nz) {
+  const long long nic = (nx + kBatchTileI - 1) / kBatchTileI, nkg = (nz + kBatchTileK - 1) / kBatchTileK;
+  return nx > 0 && nz > 0 && nic * kBatchTileI * nkg * kBatchTileK * 10 <= nx * nz * 11;
+}
 static_assert(kBatchTileI * kBatchTileK == 128, "a batch trajectory tile is one block of 128 threads");
 template <int PREC>
 cudaError_t launch_tricub_parts(const DGrid& g, const SetArgs& a, const SetParts& sp, cudaStream_t s);
