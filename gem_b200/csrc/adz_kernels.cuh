@@ -59,6 +59,18 @@
 #ifndef ADZ_TRAJ_TILE_MINB_REF32
 #define ADZ_TRAJ_TILE_MINB_REF32 ADZ_TRAJ_MINB_REF32
 #endif
+// the iteration to a tolerance (k_traject_tol) has its own resident-block
+// budget and walks the trajectory's tiles of 32 i by 4 levels (ADZ_TOL_TILES
+// 0: points in (i, k, j) order).  MIXED, 1024x1024x80 cold start to 1e-4:
+// tiles at 7 blocks 13.26 ms against 14.82 ms in (i, k, j) order (204 bytes
+// of spills there against 40); 6 and 5 blocks were slower either way
+#ifndef ADZ_TOL_MINB
+#define ADZ_TOL_MINB ADZ_TRAJ_MINB
+#endif
+#ifndef ADZ_TOL_TILES
+#define ADZ_TOL_TILES 1
+#endif
+#define ADZ_TOL_BOUNDS __launch_bounds__(128, PREC == kRef32 ? ADZ_TRAJ_MINB_REF32 : ADZ_TOL_MINB)
 #define ADZ_TRAJ_TILE_BOUNDS \
   __launch_bounds__(ADZ_TRAJ_TILE_THREADS, PREC == kRef32 ? ADZ_TRAJ_TILE_MINB_REF32 : ADZ_TRAJ_TILE_MINB)
 #define ADZ_SET_BOUNDS __launch_bounds__(128, PREC == kRef32 ? ADZ_SET_MINB_REF32 : ADZ_SET_MINB)
@@ -569,19 +581,33 @@ __global__ void ADZ_TRAJ_BOUNDS k_traject_box(DGrid g, TrajArgs a, int i0, int n
 }
 
 template <int PREC>
-__global__ void ADZ_TRAJ_BOUNDS k_traject_tol(DGrid g, TrajArgs a, double tol, int maxit, unsigned char* iters,
-                                              unsigned long long* stats, GuessStart gs) {
+__global__ void ADZ_TOL_BOUNDS k_traject_tol(DGrid g, TrajArgs a, double tol, int maxit, unsigned char* iters,
+                                             unsigned long long* stats, GuessStart gs) {
+  unsigned long long cnt[3] = {0, 0, 0};
+#if ADZ_TOL_TILES
+  // one tile of 32 i by 4 levels per block, as in k_traject; lanes outside
+  // the grid still take part in the reduction below
+  {
+    const int nkp = g.nk - a.k00 + 1;
+    const int nic = (g.ni + 31) / 32, nkg = (nkp + 3) / 4;
+    const long long b = blockIdx.x;
+    const int i = (int)(b % nic) * 32 + (threadIdx.x % 32) + 1;
+    const int k = (int)((b / nic) % nkg) * 4 + (threadIdx.x / 32) + a.k00;
+    const int j = (int)(b / ((long long)nic * nkg)) + 1;
+    if (i <= g.ni && k <= g.nk && j <= g.nj) traject_point_tol<PREC>(g, a, gs, i, j, k, tol, maxit, iters, cnt);
+  }
+#else
   // points in (i, k, j) order, as in k_traject
   const int nkp = g.nk - a.k00 + 1;
   const long long nrow = (long long)g.ni * nkp;
   const long long n = nrow * g.nj;
-  unsigned long long cnt[3] = {0, 0, 0};
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t % g.ni) + 1;
     const int k = (int)((t / g.ni) % nkp) + a.k00;
     const int j = (int)(t / nrow) + 1;
     traject_point_tol<PREC>(g, a, gs, i, j, k, tol, maxit, iters, cnt);
   }
+#endif
   if (stats) {
 #pragma unroll
     for (int q = 0; q < 3; q++) {
@@ -1208,8 +1234,14 @@ cudaError_t launch_prepare_box(const DGrid& g, const void* uu, const void* vv, c
 template <int PREC>
 cudaError_t launch_traject_tol(const DGrid& g, const TrajArgs& a, double tol, int maxit, unsigned char* iters,
                                unsigned long long* stats, cudaStream_t s, const GuessStart& gs) {
+#if ADZ_TOL_TILES
+  const long long nb = (long long)((g.ni + 31) / 32) * ((g.nk - a.k00 + 1 + 3) / 4) * g.nj;
+  if (nb > 0x7fffffffLL) return cudaErrorInvalidValue;
+  k_traject_tol<PREC><<<(unsigned)nb, 128, 0, s>>>(g, a, tol, maxit, iters, stats, gs);
+#else
   const long long n = (long long)g.ni * g.nj * (g.nk - a.k00 + 1);
   k_traject_tol<PREC><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, a, tol, maxit, iters, stats, gs);
+#endif
   return cudaGetLastError();
 }
 
