@@ -809,6 +809,18 @@ __global__ void __launch_bounds__(256) k_positions(DGrid g, int set, int i0, int
 template <int PREC, bool PERT>
 __global__ void ADZ_SET_BOUNDS k_tricub_set(DGrid g, int set, int i0, int nx, int j0, int ny, int k0, int nz,
                                             SetArgs a, FieldPtrs fp) {
+#if ADZ_SET_TILE_K > 1
+  // one tile of 128/TK i by TK levels per block, as in k_tricub_parts
+  constexpr int TK = ADZ_SET_TILE_K, TI = 128 / TK;
+  const unsigned b = blockIdx.x;
+  const unsigned nic = (unsigned)(nx + TI - 1) / TI, nkg = (unsigned)(nz + TK - 1) / TK;
+  const unsigned bj = b / nic;
+  const int ii = (int)(b - bj * nic) * TI + (int)(threadIdx.x % TI);
+  const int kk = (int)(bj % nkg) * TK + (int)(threadIdx.x / TI);
+  const int jj = (int)(bj / nkg);
+  if (ii >= nx || kk >= nz || jj >= ny) return;
+  set_point<PREC, false, PERT>(g, set, a, fp, ii + i0, jj + j0, kk + k0);
+#else
   // points in (i, k, j) order, as in k_traject
   const long long nrow = (long long)nx * nz;
   const long long n = nrow * ny;
@@ -818,6 +830,7 @@ __global__ void ADZ_SET_BOUNDS k_tricub_set(DGrid g, int set, int i0, int nx, in
     const int j = (int)(t / nrow) + j0;
     set_point<PREC, false, PERT>(g, set, a, fp, i, j, k);
   }
+#endif
 }
 
 // the tricubic groups of several sets in one launch.  Consecutive blocks
@@ -1250,8 +1263,16 @@ cudaError_t launch_tricub_set(const DGrid& g, int set, int i0, int nx, int j0, i
                               const SetArgs& a, const FieldPtrs& fp, cudaStream_t s) {
   const long long n = (long long)nx * ny * nz;
   if (n <= 0) return cudaSuccess;
-  if (a.pert) k_tricub_set<PREC, true><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, set, i0, nx, j0, ny, k0, nz, a, fp);
-  else k_tricub_set<PREC, false><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, set, i0, nx, j0, ny, k0, nz, a, fp);
+#if ADZ_SET_TILE_K > 1
+  constexpr int TK = ADZ_SET_TILE_K, TI = 128 / TK;
+  const long long nb = (long long)((nx + TI - 1) / TI) * ((nz + TK - 1) / TK) * ny;
+  if (nb > 0x7fffffffLL) return cudaErrorInvalidValue;
+  const unsigned grid = (unsigned)nb;
+#else
+  const int grid = grid_for(n, 128, 1 << 30);
+#endif
+  if (a.pert) k_tricub_set<PREC, true><<<grid, 128, 0, s>>>(g, set, i0, nx, j0, ny, k0, nz, a, fp);
+  else k_tricub_set<PREC, false><<<grid, 128, 0, s>>>(g, set, i0, nx, j0, ny, k0, nz, a, fp);
   return cudaGetLastError();
 }
 
