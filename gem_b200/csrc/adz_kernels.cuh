@@ -77,6 +77,12 @@
 #ifndef ADZ_QV_MINB
 #define ADZ_QV_MINB 0
 #endif
+// BICUBH_QV on tiles of 32 i by 4 levels (0: points in (i, k, j) order).
+// MIXED, 8 tracers at 1024x1024x80, 5 blocks: 17.48 ms against 18.70 ms in
+// (i, k, j) order (6 blocks on tiles: 17.64)
+#ifndef ADZ_QV_TILES
+#define ADZ_QV_TILES 1
+#endif
 #if ADZ_QV_MINB > 0
 #define ADZ_QV_BOUNDS __launch_bounds__(128, ADZ_QV_MINB)
 #else
@@ -916,6 +922,17 @@ __device__ __forceinline__ void qv_point(const DGrid& g, const SetArgs& a, const
 template <int PREC, bool PERT>
 __global__ void ADZ_QV_BOUNDS k_qv_set(DGrid g, int i0, int nx, int j0, int ny, int k0, int nz, SetArgs a,
                                                 FieldPtrs fp) {
+#if ADZ_QV_TILES
+  // one tile of 32 i by 4 levels per block, 32-bit tile arithmetic
+  const unsigned b = blockIdx.x;
+  const unsigned nic = (unsigned)(nx + 31) / 32, nkg = (unsigned)(nz + 3) / 4;
+  const unsigned bj = b / nic;
+  const int ii = (int)(b - bj * nic) * 32 + (int)(threadIdx.x % 32);
+  const int kk = (int)(bj % nkg) * 4 + (int)(threadIdx.x / 32);
+  const int jj = (int)(bj / nkg);
+  if (ii >= nx || kk >= nz || jj >= ny) return;
+  qv_point<PREC, PERT>(g, a, fp, ii + i0, jj + j0, kk + k0);
+#else
   // points in (i, k, j) order, as in k_traject
   const long long nrow = (long long)nx * nz;
   const long long n = nrow * ny;
@@ -925,6 +942,7 @@ __global__ void ADZ_QV_BOUNDS k_qv_set(DGrid g, int i0, int nx, int j0, int ny, 
     const int j = (int)(t / nrow) + j0;
     qv_point<PREC, PERT>(g, a, fp, i, j, k);
   }
+#endif
 }
 
 // ---------------------------------------------------------------------------
@@ -1311,8 +1329,15 @@ cudaError_t launch_qv_set(const DGrid& g, int i0, int nx, int j0, int ny, int k0
                           const FieldPtrs& fp, cudaStream_t s) {
   const long long n = (long long)nx * ny * nz;
   if (n <= 0) return cudaSuccess;
-  if (a.pert) k_qv_set<PREC, true><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, i0, nx, j0, ny, k0, nz, a, fp);
-  else k_qv_set<PREC, false><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, i0, nx, j0, ny, k0, nz, a, fp);
+#if ADZ_QV_TILES
+  const long long nb = (long long)((nx + 31) / 32) * ((nz + 3) / 4) * ny;
+  if (nb > 0x7fffffffLL) return cudaErrorInvalidValue;
+  const unsigned grid = (unsigned)nb;
+#else
+  const int grid = grid_for(n, 128, 1 << 30);
+#endif
+  if (a.pert) k_qv_set<PREC, true><<<grid, 128, 0, s>>>(g, i0, nx, j0, ny, k0, nz, a, fp);
+  else k_qv_set<PREC, false><<<grid, 128, 0, s>>>(g, i0, nx, j0, ny, k0, nz, a, fp);
   return cudaGetLastError();
 }
 
