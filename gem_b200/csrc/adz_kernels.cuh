@@ -573,9 +573,21 @@ __global__ void ADZ_TRAJ_TILE_BOUNDS k_traject(DGrid g, TrajArgs a) {
 // the trajectory of the points of a box of the tile (i0..i0+nx-1,
 // j0..j0+ny-1, levels from k00), points in (i, k, j) order: the interior
 // and the band of a schedule that overlaps the halo exchange
-template <int PREC>
+// TILED: one tile of 32 i by 4 levels per block (boxes that tiles cover with
+// few idle lanes, as the interior), else points in (i, k, j) order (bands)
+template <int PREC, bool TILED>
 __global__ void ADZ_TRAJ_BOUNDS k_traject_box(DGrid g, TrajArgs a, int i0, int nx, int j0, int ny) {
   const int nkp = g.nk - a.k00 + 1;
+  if (TILED) {
+    const unsigned b = blockIdx.x;
+    const unsigned nic = (unsigned)(nx + 31) / 32, nkg = (unsigned)(nkp + 3) / 4;
+    const unsigned bj = b / nic;
+    const int ii = (int)(b - bj * nic) * 32 + (int)(threadIdx.x % 32);
+    const int kk = (int)(bj % nkg) * 4 + (int)(threadIdx.x / 32);
+    const int jj = (int)(bj / nkg);
+    if (ii < nx && kk < nkp && jj < ny) traject_point<PREC>(g, a, ii + i0, jj + j0, kk + a.k00);
+    return;
+  }
   const long long nrow = (long long)nx * nkp;
   const long long n = nrow * ny;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
@@ -1245,9 +1257,15 @@ cudaError_t launch_traject(const DGrid& g, const TrajArgs& a, cudaStream_t s) {
 
 template <int PREC>
 cudaError_t launch_traject_box(const DGrid& g, const TrajArgs& a, int i0, int nx, int j0, int ny, cudaStream_t s) {
-  const long long n = (long long)nx * ny * (g.nk - a.k00 + 1);
+  const long long nkp = g.nk - a.k00 + 1, n = (long long)nx * ny * nkp;
   if (n <= 0) return cudaSuccess;
-  k_traject_box<PREC><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, a, i0, nx, j0, ny);
+  if (batch_use_tiles(nx, nkp)) {
+    const long long nb = (long long)((nx + 31) / 32) * ((nkp + 3) / 4) * ny;
+    if (nb > 0x7fffffffLL) return cudaErrorInvalidValue;
+    k_traject_box<PREC, true><<<(unsigned)nb, 128, 0, s>>>(g, a, i0, nx, j0, ny);
+  } else {
+    k_traject_box<PREC, false><<<grid_for(n, 128, 1 << 30), 128, 0, s>>>(g, a, i0, nx, j0, ny);
+  }
   return cudaGetLastError();
 }
 
