@@ -318,7 +318,9 @@ int adzc_batch_create(int prec, int ndom, const adzc_domain *doms, adzc_batch **
 /* autotuner: times candidate tile heights (rows per work item), register
  * budgets (resident blocks per SM) of the one-launch kernel and the phased
  * plan on these domains, keeps the fastest and re-captures the graph.  The
- * timed launches are real steps: they advance the domains' positions. */
+ * timed launches are real steps: they advance the domains' positions.  A
+ * work item of a region that tiles of 32 i by 4 levels cover with at most
+ * 10 % idle lanes holds the tiles of rows/4 such rows (at least one). */
 int adzc_batch_tune(adzc_batch *b, void *stream);
 int adzc_batch_step(adzc_batch *b, void *stream);
 /* the plan in use; blocks_per_sm of the one-launch kernel (phased plan: of
