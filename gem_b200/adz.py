@@ -459,6 +459,7 @@ class Batch:
 
     PHASED = 3  # plan of select(): one persistent launch per phase
     DOMAINS = 4  # plan of select(): every domain's own launches in turn
+    DOMAINS_CONCURRENT = 5  # plan of select(): the same launches on 4 concurrent graph branches
     INJECT_SPINS, INJECT_NEED = 1, 2  # inject(): fault injection for failure-path tests
 
     def inject(self, what: int, value: int):
@@ -475,7 +476,7 @@ class Batch:
 
     def select(self, rows: int, plan: int):
         """Pin a plan: rows per work item and 0..2 (register budget of the
-        one-launch kernel), Batch.PHASED or Batch.DOMAINS."""
+        one-launch kernel), Batch.PHASED, Batch.DOMAINS or Batch.DOMAINS_CONCURRENT."""
         _check(lib().adzc_batch_select(self.h, int(rows), int(plan)), "adzc_batch_select")
 
     def query(self):
@@ -484,7 +485,8 @@ class Batch:
         _check(lib().adzc_batch_plan(self.h, C.byref(p)), "adzc_batch_plan")
         return {"rows_per_item": r.value, "blocks_per_sm": b.value, "items": n.value,
                 "plan": {0: "one launch", 1: "phased (one launch per phase)",
-                         2: "per-domain launches (3 per domain)"}[p.value]}
+                         2: "per-domain launches (3 per domain)",
+                         3: "per-domain launches (3 per domain) on 4 concurrent branches"}[p.value]}
 
     def status(self, reset=True, stream=None) -> int:
         return lib().adzc_batch_status(self.h, 1 if reset else 0, _stream(stream))

@@ -63,6 +63,11 @@ struct adzc_batch {
   int pgrid[3] = {};        // persistent grid of each phased launch
   float tuned_ms[3] = {-1.f, -1.f, -1.f};  // tuner: best ms per step of each plan family (one launch, phased, per-domain)
   cudaStream_t cap = nullptr;
+  // the per-domain plan on concurrent branches: lanes streams (lane 0 is the
+  // caller's), a fork event and one join event per lane
+  int lanes = 1;
+  cudaStream_t lane_s[adz::kBatchLanes] = {};
+  cudaEvent_t fork = nullptr, join[adz::kBatchLanes] = {};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -126,33 +131,74 @@ int build_items(adzc_batch* b, int rows) {
   return ADZC_OK;
 }
 
-// every domain's own launches in turn (the per-domain plan)
+// one domain's own launches: departure winds, trajectory and all field
+// groups in one k_tricub_parts launch
+template <int PREC>
+cudaError_t enqueue_domain(const adz::BDom& D, cudaStream_t s) {
+  cudaError_t e = adz::launch_prepare<PREC>(D.g, D.uu, D.vv, D.ww, const_cast<void*>(D.ta.uvw_d), s);
+  if (e == cudaSuccess) e = adz::launch_traject<PREC>(D.g, D.ta, s);
+  adz::SetParts sp{};
+  for (int q = 0; q < D.ngroups && e == cudaSuccess; q++) {
+    adz::SetPart& P = sp.p[sp.n++];
+    P.fp = D.gfp[q];
+    P.set = D.gset[q];
+    P.i0 = D.grange[q][0];
+    P.nx = D.grange[q][1];
+    P.j0 = D.grange[q][2];
+    P.ny = D.grange[q][3];
+    P.k0 = D.grange[q][4];
+    P.nz = D.g.nk - P.k0 + 1;
+    if (P.nx <= 0 || P.ny <= 0 || P.nz <= 0) sp.n--;
+    if (sp.n == adz::kMaxParts || (q == D.ngroups - 1 && sp.n > 0)) {
+      e = adz::launch_tricub_parts<PREC>(D.g, D.sa, sp, s);
+      sp = adz::SetParts{};
+    }
+  }
+  return e;
+}
+
+// the per-domain plan: every domain's own launches in turn, or spread over
+// b->lanes concurrent branches (a fork and a join event; domains assigned
+// largest first to the least loaded branch), so that one domain's launch
+// tails and its memory-bound departure winds overlap another's gathers
 template <int PREC>
 cudaError_t enqueue_domains(const adzc_batch* b, cudaStream_t s) {
+  if (b->lanes <= 1) {
+    for (int d = 0; d < b->ndom; d++) {
+      const cudaError_t e = enqueue_domain<PREC>(b->doms[d], s);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  std::vector<std::pair<double, int>> cost(b->ndom);
   for (int d = 0; d < b->ndom; d++) {
     const adz::BDom& D = b->doms[d];
-    cudaError_t e = adz::launch_prepare<PREC>(D.g, D.uu, D.vv, D.ww, const_cast<void*>(D.ta.uvw_d), s);
-    if (e == cudaSuccess) e = adz::launch_traject<PREC>(D.g, D.ta, s);
-    adz::SetParts sp{};
-    for (int q = 0; q < D.ngroups && e == cudaSuccess; q++) {
-      adz::SetPart& P = sp.p[sp.n++];
-      P.fp = D.gfp[q];
-      P.set = D.gset[q];
-      P.i0 = D.grange[q][0];
-      P.nx = D.grange[q][1];
-      P.j0 = D.grange[q][2];
-      P.ny = D.grange[q][3];
-      P.k0 = D.grange[q][4];
-      P.nz = D.g.nk - P.k0 + 1;
-      if (P.nx <= 0 || P.ny <= 0 || P.nz <= 0) sp.n--;
-      if (sp.n == adz::kMaxParts || (q == D.ngroups - 1 && sp.n > 0)) {
-        e = adz::launch_tricub_parts<PREC>(D.g, D.sa, sp, s);
-        sp = adz::SetParts{};
-      }
-    }
-    if (e != cudaSuccess) return e;
+    double c = (double)D.g.nij * D.g.nk;  // winds and trajectory
+    for (int q = 0; q < D.ngroups; q++)
+      c += (double)D.grange[q][1] * D.grange[q][3] * (D.g.nk - D.grange[q][4] + 1) * (0.5 + 0.5 * D.gfp[q].nf);
+    cost[d] = {c, d};
   }
-  return cudaSuccess;
+  std::sort(cost.begin(), cost.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+  std::vector<double> load(b->lanes, 0.0);
+  std::vector<std::vector<int>> lane_doms(b->lanes);
+  for (const auto& c : cost) {
+    const int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    load[l] += c.first;
+    lane_doms[l].push_back(c.second);
+  }
+  cudaError_t e = cudaEventRecord(b->fork, s);
+  for (int l = 1; l < b->lanes && e == cudaSuccess; l++) e = cudaStreamWaitEvent(b->lane_s[l], b->fork, 0);
+  for (int l = 0; l < b->lanes && e == cudaSuccess; l++)
+    for (int d : lane_doms[l]) {
+      e = enqueue_domain<PREC>(b->doms[d], l == 0 ? s : b->lane_s[l]);
+      if (e != cudaSuccess) break;
+    }
+  for (int l = 1; l < b->lanes; l++) {  // join every branch even after an error
+    const cudaError_t r = cudaEventRecord(b->join[l], b->lane_s[l]);
+    const cudaError_t w = cudaStreamWaitEvent(s, b->join[l], 0);
+    if (e == cudaSuccess) e = r != cudaSuccess ? r : w;
+  }
+  return e;
 }
 
 cudaError_t enqueue(adzc_batch* b, cudaStream_t s) {
@@ -214,6 +260,11 @@ extern "C" int adzc_batch_destroy(adzc_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->cap) cudaStreamDestroy(b->cap);
+  for (int l = 0; l < adz::kBatchLanes; l++) {
+    if (b->lane_s[l]) cudaStreamDestroy(b->lane_s[l]);
+    if (b->join[l]) cudaEventDestroy(b->join[l]);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
   delete b->params;
   cudaFree(b->d_doms);
   cudaFree(b->d_items);
@@ -350,9 +401,17 @@ extern "C" int adzc_batch_create(int prec, int ndom, const adzc_domain* doms, ad
       cudaMalloc(&b->d_status, sizeof(int)) != cudaSuccess ||
       cudaMemcpy(b->d_doms, b->doms.data(), ndom * sizeof(adz::BDom), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemset(b->d_status, 0, sizeof(int)) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) {
     adzc_batch_destroy(b);
     return adz_internal_fail(ADZC_ERR_CUDA);
+  }
+  for (int l = 1; l < adz::kBatchLanes; l++) {
+    if (cudaStreamCreateWithFlags(&b->lane_s[l], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->join[l], cudaEventDisableTiming) != cudaSuccess) {
+      adzc_batch_destroy(b);
+      return adz_internal_fail(ADZC_ERR_CUDA);
+    }
   }
   int st = build_items(b, b->rows);
   if (st == ADZC_OK) st = capture(b);
@@ -421,17 +480,21 @@ extern "C" int adzc_batch_tune(adzc_batch* b, void* stream) {
       }
     }
   }
-  if (st == ADZC_OK) {  // the per-domain launches (rows unused)
+  int blanes = b->lanes;
+  for (int lanes : {1, adz::kBatchLanes}) {  // the per-domain launches (rows unused), in turn or concurrent
+    if (st != ADZC_OK) break;
     b->phased = 2;
+    b->lanes = lanes;
     float ms = 0.f;
     if (enqueue(b, s) != cudaSuccess || cudaEventRecord(e0, s) != cudaSuccess || enqueue(b, s) != cudaSuccess ||
         enqueue(b, s) != cudaSuccess || cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess)
       st = ADZC_ERR_CUDA;
     else if (cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) {
-      b->tuned_ms[2] = ms / 2;
-      if (ms < best) best = ms, bp = 2;
+      if (b->tuned_ms[2] < 0.f || ms / 2 < b->tuned_ms[2]) b->tuned_ms[2] = ms / 2;
+      if (ms < best) best = ms, bp = 2, blanes = lanes;
     }
   }
+  b->lanes = bp == 2 ? blanes : 1;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   b->bps = bb;
@@ -452,7 +515,7 @@ extern "C" int adzc_batch_query(const adzc_batch* b, int* rows, int* blocks_per_
 }
 
 extern "C" int adzc_batch_select(adzc_batch* b, int rows, int plan) {
-  if (!b || rows < 1 || plan < 0 || plan > ADZC_BATCH_DOMAINS) return adz_internal_fail(ADZC_ERR_ARG);
+  if (!b || rows < 1 || plan < 0 || plan > ADZC_BATCH_DOMAINS_CONCURRENT) return adz_internal_fail(ADZC_ERR_ARG);
   if (plan < adz::kBatchVariants) {
     const int res = resident(b, plan);
     if (res < 1) return adz_internal_fail(ADZC_ERR_ARG);
@@ -460,8 +523,9 @@ extern "C" int adzc_batch_select(adzc_batch* b, int rows, int plan) {
     b->bps = res;
     b->phased = 0;
   } else {
-    b->phased = plan == ADZC_BATCH_DOMAINS ? 2 : 1;
+    b->phased = plan == ADZC_BATCH_PHASED ? 1 : 2;
   }
+  b->lanes = plan == ADZC_BATCH_DOMAINS_CONCURRENT ? adz::kBatchLanes : 1;
   int st = build_items(b, rows);
   if (st == ADZC_OK) st = capture(b);
   return st == ADZC_OK ? ADZC_OK : adz_internal_fail(st);
@@ -490,7 +554,7 @@ extern "C" int adzc_batch_tuned(const adzc_batch* b, float* ms) {
 
 extern "C" int adzc_batch_plan(const adzc_batch* b, int* phased) {
   if (!b || !phased) return adz_internal_fail(ADZC_ERR_ARG);
-  *phased = b->phased;
+  *phased = b->phased == 2 && b->lanes > 1 ? 3 : b->phased;
   return ADZC_OK;
 }
 

@@ -200,6 +200,7 @@ struct BItem {
 };
 
 constexpr int kBatchVariants = 3;  // register budgets of the batch kernel
+constexpr int kBatchLanes = 4;     // concurrent graph branches of the per-domain plan
 // trajectory items of the batch are runs of tiles of kBatchTileI consecutive
 // i by kBatchTileK consecutive levels (one warp row per level, a block of 128
 // threads per tile), as the per-domain trajectory kernel walks its points

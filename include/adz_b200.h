@@ -332,12 +332,16 @@ int adzc_batch_plan(const adzc_batch *b, int *phased);
 /* pin a plan instead of tuning: rows per work item, plan 0..2 = register
  * budget of the one-launch kernel, 3 = phased, 4 = every domain's own
  * launches (departure winds, trajectory, all field groups) in turn inside the
- * graph, rows unused; re-captures the graph */
+ * graph, 5 = the same launches spread over 4 concurrent branches of the graph
+ * (rows unused by 4 and 5); re-captures the graph.  adzc_batch_plan reports
+ * 0 (one launch), 1 (phased), 2 (per-domain in turn) or 3 (per-domain on
+ * concurrent branches). */
 #define ADZC_BATCH_PHASED 3
 #define ADZC_BATCH_DOMAINS 4
+#define ADZC_BATCH_DOMAINS_CONCURRENT 5
 /* after adzc_batch_tune: the best time per step the tuner measured for each
  * plan family, ms[0] the one-launch kernel, ms[1] the phased plan, ms[2] the
- * per-domain launches (-1: not timed) */
+ * per-domain launches, in turn or concurrent (-1: not timed) */
 int adzc_batch_tuned(const adzc_batch *b, float ms[3]);
 int adzc_batch_select(adzc_batch *b, int rows_per_item, int plan);
 /* Fault injection for tests of the failure path, on the host (no GPU fault).

@@ -70,11 +70,13 @@ def _compare(a, b, what):
 
 
 @pytest.mark.parametrize("precname,plan", [("mixed", None), ("fp64", None), ("mixed", (8, 2)), ("mixed", (2, 3)),
-                                           ("fp64", (32, 3)), ("mixed", (8, 4)), ("fp64", (8, 4))])
+                                           ("fp64", (32, 3)), ("mixed", (8, 4)), ("fp64", (8, 4)),
+                                           ("mixed", (8, 5))])
 def test_batch_matches_per_domain_steps(precname, plan):
     """plan None: the default one-launch plan; (rows, 0..2): that register
     budget of the one-launch kernel; (rows, 3): the phased plan; (rows, 4):
-    every domain's own launches in the graph."""
+    every domain's own launches in the graph; (rows, 5): the same on
+    concurrent graph branches."""
     from gem_b200 import adz as A
     prec = A.PREC_NAMES[precname]
     adz, doms = _domains(prec)
@@ -85,10 +87,11 @@ def test_batch_matches_per_domain_steps(precname, plan):
     if plan is not None:
         batch.select(*plan)
     q = batch.query()
-    per_domain = plan is not None and plan[1] == adz.Batch.DOMAINS
+    per_domain = plan is not None and plan[1] in (adz.Batch.DOMAINS, adz.Batch.DOMAINS_CONCURRENT)
     assert q["items"] > 0 and (q["blocks_per_sm"] == 0 if per_domain else q["blocks_per_sm"] >= 1)
     assert q["plan"].startswith("phased") == (plan is not None and plan[1] == adz.Batch.PHASED)
-    assert q["plan"].startswith("per-domain") == (plan is not None and plan[1] == adz.Batch.DOMAINS)
+    assert q["plan"].startswith("per-domain") == per_domain
+    assert q["plan"].endswith("concurrent branches") == (plan is not None and plan[1] == adz.Batch.DOMAINS_CONCURRENT)
     if plan is not None:
         assert q["rows_per_item"] == plan[0]
     for step in range(2):
@@ -148,7 +151,7 @@ def test_batch_rejects_bad_domains():
     with pytest.raises(adz.AdzError):
         adz.Batch(A.REF32, [])  # no domains / REF32 not batched
     ok = _batch(adz, A.MIXED, doms, wps, outs)
-    for rows, plan in ((0, 0), (8, -1), (8, 5)):
+    for rows, plan in ((0, 0), (8, -1), (8, 6)):
         with pytest.raises(adz.AdzError):
             ok.select(rows, plan)
     # a handle still in its cold start is refused
