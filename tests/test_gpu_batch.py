@@ -71,7 +71,7 @@ def _compare(a, b, what):
 
 @pytest.mark.parametrize("precname,plan", [("mixed", None), ("fp64", None), ("mixed", (8, 2)), ("mixed", (2, 3)),
                                            ("fp64", (32, 3)), ("mixed", (8, 4)), ("fp64", (8, 4)),
-                                           ("mixed", (8, 5))])
+                                           ("mixed", (8, 5)), ("fp64", (8, 5))])
 def test_batch_matches_per_domain_steps(precname, plan):
     """plan None: the default one-launch plan; (rows, 0..2): that register
     budget of the one-launch kernel; (rows, 3): the phased plan; (rows, 4):
