@@ -74,6 +74,19 @@
 #define ADZ_TRAJ_TILE_BOUNDS \
   __launch_bounds__(ADZ_TRAJ_TILE_THREADS, PREC == kRef32 ? ADZ_TRAJ_TILE_MINB_REF32 : ADZ_TRAJ_TILE_MINB)
 #define ADZ_SET_BOUNDS __launch_bounds__(128, PREC == kRef32 ? ADZ_SET_MINB_REF32 : ADZ_SET_MINB)
+// rows per block of the interleaved sets launch on tiles (blocks of
+// 128 * ADZ_SET_TILE_J threads), with its own budget in such blocks
+#ifndef ADZ_SET_TILE_J
+#define ADZ_SET_TILE_J 1
+#endif
+#ifndef ADZ_PARTS_MINB
+#define ADZ_PARTS_MINB ADZ_SET_MINB
+#endif
+#ifndef ADZ_PARTS_MINB_REF32
+#define ADZ_PARTS_MINB_REF32 ADZ_SET_MINB_REF32
+#endif
+#define ADZ_PARTS_BOUNDS \
+  __launch_bounds__(128 * ADZ_SET_TILE_J, PREC == kRef32 ? ADZ_PARTS_MINB_REF32 : ADZ_PARTS_MINB)
 #ifndef ADZ_QV_MINB
 #define ADZ_QV_MINB 0
 #endif
@@ -856,19 +869,19 @@ __global__ void ADZ_SET_BOUNDS k_tricub_set(DGrid g, int set, int i0, int nx, in
 // issue-bound one-field sets and the load-bound multi-field set at once;
 // each thread interpolates one arrival point of its part as k_tricub_set does
 template <int PREC, bool PERT>
-__global__ void ADZ_SET_BOUNDS k_tricub_parts(DGrid g, SetArgs a, const __grid_constant__ SetParts sp) {
+__global__ void ADZ_PARTS_BOUNDS k_tricub_parts(DGrid g, SetArgs a, const __grid_constant__ SetParts sp) {
   const int q = (int)(blockIdx.x % (unsigned)sp.n);
   const SetPart& P = sp.p[q];
 #if ADZ_SET_TILE_K > 1
   // 32-bit tile arithmetic (the grid stays below 2^31 blocks): 64-bit
   // indices here cost registers the point code needs at 9 resident blocks
-  constexpr int TK = ADZ_SET_TILE_K, TI = 128 / TK;
+  constexpr int TK = ADZ_SET_TILE_K, TI = 128 / TK, TJ = ADZ_SET_TILE_J;
   const unsigned b = blockIdx.x / (unsigned)sp.n;
   const unsigned nic = (unsigned)(P.nx + TI - 1) / TI, nkg = (unsigned)(P.nz + TK - 1) / TK;
   const unsigned bj = b / nic, bk = bj % nkg;
   const int ii = (int)(b - bj * nic) * TI + (int)(threadIdx.x % TI);
-  const int kk = (int)bk * TK + (int)(threadIdx.x / TI);
-  const int jj = (int)(bj / nkg);
+  const int kk = (int)bk * TK + (int)((threadIdx.x / TI) % TK);
+  const int jj = (int)(bj / nkg) * TJ + (int)(threadIdx.x / 128);
   if (ii >= P.nx || kk >= P.nz || jj >= P.ny) return;
   set_point<PREC, false, PERT>(g, P.set, a, P.fp, ii + P.i0, jj + P.j0, kk + P.k0);
 #else
@@ -1350,8 +1363,9 @@ cudaError_t launch_tricub_parts(const DGrid& g, const SetArgs& a, const SetParts
   long long most = 0;  // blocks of the largest part
   for (int q = 0; q < sp.n; q++) {
 #if ADZ_SET_TILE_K > 1
-    constexpr int TK = ADZ_SET_TILE_K, TI = 128 / TK;
-    const long long n = (long long)((sp.p[q].nx + TI - 1) / TI) * ((sp.p[q].nz + TK - 1) / TK) * sp.p[q].ny * 128;
+    constexpr int TK = ADZ_SET_TILE_K, TI = 128 / TK, TJ = ADZ_SET_TILE_J;
+    const long long n = (long long)((sp.p[q].nx + TI - 1) / TI) * ((sp.p[q].nz + TK - 1) / TK) *
+                        ((sp.p[q].ny + TJ - 1) / TJ) * 128;
 #else
     const long long n = (long long)sp.p[q].nx * sp.p[q].ny * sp.p[q].nz;
 #endif
@@ -1360,8 +1374,13 @@ cudaError_t launch_tricub_parts(const DGrid& g, const SetArgs& a, const SetParts
   const long long blocks = (most + 127) / 128 * sp.n;
   if (blocks < 1) return cudaSuccess;
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
-  if (a.pert) k_tricub_parts<PREC, true><<<(unsigned)blocks, 128, 0, s>>>(g, a, sp);
-  else k_tricub_parts<PREC, false><<<(unsigned)blocks, 128, 0, s>>>(g, a, sp);
+#if ADZ_SET_TILE_K > 1
+  constexpr int threads = 128 * ADZ_SET_TILE_J;
+#else
+  constexpr int threads = 128;
+#endif
+  if (a.pert) k_tricub_parts<PREC, true><<<(unsigned)blocks, threads, 0, s>>>(g, a, sp);
+  else k_tricub_parts<PREC, false><<<(unsigned)blocks, threads, 0, s>>>(g, a, sp);
   return cudaGetLastError();
 }
 

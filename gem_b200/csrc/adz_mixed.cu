@@ -11,7 +11,8 @@
 //               for 128 i of one level in (i, k, j) order in the same runs
 //               (8 blocks on tiles: 11.27).  The tile index is 32-bit
 //               arithmetic: with 64-bit indices the kernel spilled 144 bytes
-//               at the 56 registers of 9 blocks and took 12.51 ms;
+//               at the 56 registers of 9 blocks and took 12.51 ms; blocks of
+//               2 rows of such tiles (256 threads) at 4, 5 blocks: 11.75, 12.56;
 #define ADZ_SET_TILE_K 4
 //   BICUBH_QV   5 blocks (96 registers, no spills; 27.4 ms for 8 tracers at
 //               the unbounded 128 registers, 21.4 ms at 5 or 6 blocks, 24.8
